@@ -1,0 +1,531 @@
+#!/usr/bin/env python
+"""Benchmark: RELION-style project + backproject throughput at 256^3.
+
+Workload (single-particle scale): a 256^3 FP32 volume of 2,000 Gaussian
+blobs, padding 2 (decentred complex64 half volume 257 x 512 x 512), and a
+pool of 256 x 256 particles with orientations from a 3-lobe von Mises-Fisher
+mixture (kappa 5-40) plus 30 % uniform, a CTF each (300 kV, Cs 2.7 mm,
+1 A/px, defocus 0.5-3 um, astigmatism <= 0.1 um) and white noise at SNR
+0.05.  All data are synthetic (seeded) and generated on the GPU before the
+timed region.
+
+One step = one batch of B particles through the hot path: d_rlnProject of
+the B reference slices (h_angles/matrix overload, rmax 128) and
+d_rlnBackproject of the B CTF-weighted particles and their CTF^2 weights
+into the centred 257 x 513 x 513 accumulators.  `value` is slices per second
+(one slice = one projection + one insertion) over the whole job.  After the
+timed steps the 10-iteration gridding reconstruction of the accumulated
+volume (P = 512) is timed once and reported under "gridding".
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B]
+    python bench.py --impl reference ...   # the reference's CPU path (port)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+BOX = 256
+PAD = 2
+SEED = 1002
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=10000, help="particles per step")
+    ap.add_argument("--pool", type=int, default=40000, help="distinct particles resident on the GPU")
+    ap.add_argument("--e2e-batch", type=int, default=2000)
+    ap.add_argument("--no-gridding", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip gridding, e2e, CPU baseline and L2 probes (profiling runs)")
+    ap.add_argument("--cpu-sample", type=int, default=256, help="slices timed on the host cores")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers --
+def counts(n: int, rmax: int):
+    """Per-slice element count, samples inside rmax for the projector (<=)
+    and for the backprojector (<, x = 0 & y < 0 skipped)."""
+    x = np.arange(n // 2 + 1)
+    y = np.arange(n)
+    y = np.where(y <= n // 2, y, y - n)
+    r2 = x[None, :] ** 2 + y[:, None] ** 2
+    e = (n // 2 + 1) * n
+    sp = int((r2 <= rmax * rmax).sum())
+    sb = int(((r2 < rmax * rmax) & ~((x[None, :] == 0) & (y[:, None] < 0))).sum())
+    return e, sp, sb
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, index: int, period: float = 0.2):
+        self.index, self.period = index, period
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            names = {
+                "hw_slowdown": getattr(pynvml, "nvmlClocksEventReasonHwSlowdown", 0x8),
+                "hw_thermal_slowdown": getattr(pynvml, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+                "sw_thermal_slowdown": getattr(pynvml, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+                "sw_power_cap": getattr(pynvml, "nvmlClocksEventReasonSwPowerCap", 0x4),
+                "hw_power_brake": getattr(pynvml, "nvmlClocksEventReasonHwPowerBrakeSlowdown", 0x80),
+            }
+
+            def run():
+                while not self._stop.is_set():
+                    try:
+                        self.samples.append(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                        r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        for k, bit in names.items():
+                            if r & bit:
+                                self.reasons.add(k)
+                    except Exception:
+                        pass
+                    self._stop.wait(self.period)
+
+            self._t = threading.Thread(target=run, daemon=True)
+            self._t.start()
+        except Exception:
+            self._t = None
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=2)
+
+    def summary(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples)}
+
+
+# ----------------------------------------------------------------- workload --
+def make_workload(args, device, seed):
+    import torch
+    import gtom_b200 as G
+    from gtom_b200 import synth
+
+    n, P = BOX, BOX * PAD
+    D = P + 1
+    rmax = n // 2
+    e, sp, sb = counts(n, rmax)
+    rng = np.random.default_rng(seed)
+    vol = synth.blob_volume(n, 2000, seed, device)
+    volft = synth.padded_half_ft(vol, PAD).reshape(-1)
+    del vol
+    N = args.pool
+    ang = synth.vmf_mixture_angles(rng, N)
+    mats = torch.from_numpy(G.matrices_from_angles(ang, float(PAD))).to(device)
+    data = torch.empty((N, e), dtype=torch.complex64, device=device)
+    wts = torch.empty((N, e), dtype=torch.float32, device=device)
+    disk = synth.in_disk_mask(n, rmax, device).reshape(-1)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    chunk = 2000
+    proj = torch.empty((chunk, e), dtype=torch.complex64, device=device)
+    for c0 in range(0, N, chunk):
+        c = min(chunk, N - c0)
+        G.d_rlnProject(volft, (P, P, P), proj, (n, n, 1), rmax, mats[c0:c0 + c].reshape(-1), c)
+        df = torch.from_numpy(rng.uniform(0.5, 3.0, c).astype(np.float32)).to(device)
+        da = torch.from_numpy(rng.uniform(0.0, 0.1, c).astype(np.float32)).to(device)
+        aa = torch.from_numpy(rng.uniform(0.0, np.pi, c).astype(np.float32)).to(device)
+        ctf = synth.ctf_half(n, df, da, aa).reshape(c, e)
+        sig = proj[:c] * ctf
+        pw = (sig.abs() ** 2 * disk).sum(1, keepdim=True) / disk.sum()
+        sd = torch.sqrt(pw / 0.05 / 2)
+        noise = torch.complex(torch.randn((c, e), device=device, generator=gen),
+                              torch.randn((c, e), device=device, generator=gen)) * sd
+        data[c0:c0 + c] = (sig + noise) * ctf
+        wts[c0:c0 + c] = ctf * ctf
+    del proj
+    torch.cuda.synchronize()
+    return dict(n=n, P=P, D=D, rmax=rmax, e=e, sp=sp, sb=sb, volft=volft, angles=ang, mats=mats,
+                data=data, wts=wts, N=N)
+
+
+# --------------------------------------------------------------------- ours --
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import gtom_b200 as G
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    B = args.batch
+    if args.pool % B:
+        args.pool = (args.pool // B + 1) * B
+    ws = make_workload(args, dev, SEED + 17 * rank)
+    n, P, D, rmax, e = ws["n"], ws["P"], ws["D"], ws["rmax"], ws["e"]
+    nvol = (D // 2 + 1) * D * D
+    acc_ft = torch.zeros(nvol, dtype=torch.complex64, device=dev)
+    acc_w = torch.zeros(nvol, dtype=torch.float32, device=dev)
+    proj = torch.empty(B * e, dtype=torch.complex64, device=dev)
+    stream = torch.cuda.current_stream()
+    ev = []
+
+    def step(i, timed):
+        s = (i * B) % ws["N"]
+        m = ws["mats"][s:s + B].reshape(-1)
+        if timed:
+            a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            a.record(stream)
+        G.d_rlnProject(ws["volft"], (P, P, P), proj, (n, n, 1), rmax, m, B)
+        if timed:
+            b.record(stream)
+        G.d_rlnBackproject(acc_ft, acc_w, (D, D, D), ws["data"][s:s + B].reshape(-1),
+                           ws["wts"][s:s + B].reshape(-1), (n, n, 1), rmax, m, None, (1, 0, 0, 1), 0.0,
+                           False, False, B)
+        if timed:
+            c.record(stream)
+            ev.append((a, b, c))
+
+    for i in range(args.warmup):
+        step(i, False)
+    acc_ft.zero_()
+    acc_w.zero_()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        start.record(stream)
+        for k in range(args.steps):
+            step(args.warmup + k, True)
+        if world > 1:  # the one exchange: sum the partial volumes of all ranks
+            dist.all_reduce(torch.view_as_real(acc_ft))
+            dist.all_reduce(acc_w)
+        end.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = start.elapsed_time(end)
+    t_proj = sum(a.elapsed_time(b) for a, b, _ in ev)
+    t_bp = sum(b.elapsed_time(c) for _, b, c in ev)
+    if world > 1:
+        t = torch.tensor([ms, t_proj, t_bp], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, t_proj, t_bp = t.tolist()
+    slices = world * args.steps * B
+    value = slices / (ms / 1e3)
+
+    # roofline of the two kernels
+    hbm_peak, peak_kind = measured_peaks()
+    probe = {} if args.no_extras else l2_probe()
+    proj_bytes = B * (ws["sp"] * 72 + (e - ws["sp"]) * 8)
+    proj_ms = t_proj / args.steps
+    proj_gbs = proj_bytes / (proj_ms * 1e-3) / 1e9
+    bp_reds = B * ws["sb"] * 24
+    bp_ms = t_bp / args.steps
+    bp_rate = bp_reds / (bp_ms * 1e-3) / 1e9
+    traffic = ncu_traffic()
+    roof_proj = {"kernel": "project", "bound": "hbm", "achieved": round(proj_gbs, 1), "peak": hbm_peak,
+                 "unit": "GB/s", "frac": round(proj_gbs / hbm_peak, 4),
+                 "traffic": None if traffic.get("project_per_slice") is None
+                 else int(traffic["project_per_slice"] * B),
+                 "algorithmic_bytes": proj_bytes, "ms_per_launch": round(proj_ms, 4),
+                 "peak_of": peak_kind,
+                 "l2_gather_peak_gbs": probe.get("l2_gather_gbs"),
+                 "frac_of_l2_gather": None if not probe.get("l2_gather_gbs")
+                 else round(proj_gbs / probe["l2_gather_gbs"], 4)}
+    red_peak = probe.get("l2_red_v2_gadds") or probe.get("l2_red_gadds")
+    roof_bp = {"kernel": "backproject", "bound": "l2_atomic", "achieved": round(bp_rate, 2),
+               "peak": red_peak, "unit": "G FP32 reductions/s",
+               "frac": None if not red_peak else round(bp_rate / red_peak, 4),
+               "traffic": None if traffic.get("backproject_per_slice") is None
+               else int(traffic["backproject_per_slice"] * B),
+               "algorithmic_reductions": bp_reds, "ms_per_launch": round(bp_ms, 4),
+               "peak_of": "measured (l2_probe, same run)"}
+    dominant = roof_proj if t_proj >= t_bp else roof_bp
+
+    out = {"metric": "project+backproject slices/s @256^3", "value": round(value, 1),
+           "unit": "slices/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded blob volume, vMF+uniform "
+           "orientations, CTF, SNR 0.05 noise)",
+           "config": {"workload": "single-particle 256^3, padding 2: project + CTF-weighted backproject",
+                      "box": n, "padding": PAD, "batch_per_step": B, "pool": ws["N"],
+                      "volume": f"{P // 2 + 1}x{P}x{P} c64 decentred", "accumulators": f"{D // 2 + 1}x{D}x{D} "
+                      "c64 + f32 centred", "l2_flush": "inputs larger than L2 (per-step data 3.96 GB)",
+                      "parallelism": f"dp{world}"},
+           "gpu_launches": 2 * args.steps,
+           "roofline": dominant, "rooflines": [roof_proj, roof_bp],
+           "kernel_ms_per_step": {"project": round(proj_ms, 4), "backproject": round(bp_ms, 4)},
+           "peaks": probe, "clocks": clocks.summary()}
+
+    if not (args.no_gridding or args.no_extras) and rank == 0:
+        out["gridding"] = time_gridding(G, torch, acc_ft, acc_w, n, D, dev)
+    if rank == 0 and not args.no_extras:
+        out["e2e"] = run_e2e(args, G, torch, ws, dev)
+        out["cpu_baseline"] = cpu_baseline(args, ws)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def time_gridding(G, torch, acc_ft, acc_w, n, D, dev):
+    out = torch.empty(n ** 3, dtype=torch.float32, device=dev)
+    G.d_ReconstructGridding(acc_ft, acc_w, out, (n,) * 3, (D,) * 3, PAD, 0, 0, 1)  # plans, pool
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    G.d_ReconstructGridding(acc_ft, acc_w, out, (n,) * 3, (D,) * 3, PAD, 0, 0, 10)
+    b.record()
+    torch.cuda.synchronize()
+    ms10 = a.elapsed_time(b)
+    t0 = time.perf_counter()
+    it, ch = G.reconstruct_gridding_tol(acc_ft, acc_w, out, (n,) * 3, (D,) * 3, PAD, max_iterations=200,
+                                        tolerance=1e-4)
+    torch.cuda.synchronize()
+    ms_tol = (time.perf_counter() - t0) * 1e3
+    P = n * PAD
+    nc, nr = (P // 2 + 1) * P * P, P ** 3
+    compulsory = 12 * nc + 8 * nr
+    return {"ms_10_iterations": round(ms10, 3), "P": P,
+            "compulsory_bytes_per_iteration": compulsory,
+            "plain_to_1e-4": {"iterations": it, "final_change": ch, "ms": round(ms_tol, 3)}}
+
+
+def run_e2e(args, G, torch, ws, dev):
+    """The same metric through the public API with host buffers: per step the
+    particle data and weights are copied from pinned host memory, the h_angles
+    overloads build and upload the matrices, and the projections are read
+    back to pinned host memory."""
+    Be = min(args.e2e_batch, ws["N"])
+    n, P, D, rmax, e = ws["n"], ws["P"], ws["D"], ws["rmax"], ws["e"]
+    h_data = ws["data"][:Be].cpu().pin_memory()
+    h_wts = ws["wts"][:Be].cpu().pin_memory()
+    h_proj = torch.empty((Be, e), dtype=torch.complex64).pin_memory()
+    ang = ws["angles"][:Be].copy()
+    d_data = torch.empty((Be, e), dtype=torch.complex64, device=dev)
+    d_wts = torch.empty((Be, e), dtype=torch.float32, device=dev)
+    d_proj = torch.empty((Be, e), dtype=torch.complex64, device=dev)
+    nvol = (D // 2 + 1) * D * D
+    acc_ft = torch.zeros(nvol, dtype=torch.complex64, device=dev)
+    acc_w = torch.zeros(nvol, dtype=torch.float32, device=dev)
+
+    def step():
+        d_data.copy_(h_data, non_blocking=True)
+        d_wts.copy_(h_wts, non_blocking=True)
+        G.d_rlnProject(ws["volft"], (P, P, P), d_proj.reshape(-1), (n, n, 1), ang, float(PAD), Be)
+        G.d_rlnBackproject(acc_ft, acc_w, (D, D, D), d_data.reshape(-1), d_wts.reshape(-1), (n, n, 1), rmax,
+                           ang, None, (1, 0, 0, 1), 0.0, float(PAD), False, False, Be)
+        h_proj.copy_(d_proj, non_blocking=True)
+
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        step()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    return {"value": round(args.steps * Be / (ms / 1e3), 1), "unit": "slices/s",
+            "h2d_bytes_per_step": Be * e * 12, "d2h_bytes_per_step": Be * e * 8,
+            "batch_per_step": Be, "ms_per_step": round(ms / args.steps, 3)}
+
+
+# ------------------------------------------------------------- CPU baseline --
+def cpu_sample_inputs(ws, count):
+    """Host copies of the volume and the first `count` particles."""
+    vol = ws["volft"].cpu().numpy()
+    data = ws["data"][:count].cpu().numpy()
+    wts = ws["wts"][:count].cpu().numpy()
+    mats = ws["mats"][:count].cpu().numpy()
+    return vol, data, wts, mats
+
+
+def time_cpu_port(vol, data, wts, mats, n, P, D, rmax, threads=None):
+    from oracle import oracle as O
+    if threads:
+        O.set_threads(threads)
+    count = mats.shape[0]
+    t0 = time.perf_counter()
+    O.project(vol, P, n, rmax, mats, fp32=True)
+    t1 = time.perf_counter()
+    nv = (D // 2 + 1) * D * D
+    vf, vw = np.zeros(nv, np.complex64), np.zeros(nv, np.float32)
+    O.backproject(vf, vw, D, data, wts, n, rmax, mats, decentered=False, fp32=True)
+    t2 = time.perf_counter()
+    return count / (t2 - t0), t1 - t0, t2 - t1
+
+
+def cpu_baseline(args, ws):
+    from oracle import oracle as O
+    count = min(args.cpu_sample, ws["N"])
+    vol, data, wts, mats = cpu_sample_inputs(ws, count)
+    rate, tp, tb = time_cpu_port(vol, data, wts, mats, ws["n"], ws["P"], ws["D"], ws["rmax"])
+    return {"value": round(rate, 2), "unit": "slices/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"{count} slices of the 256^3 workload (project {tp:.2f} s + backproject {tb:.2f} s), "
+                      "OpenMP FP32 restatement of the reference kernels"}
+
+
+# ---------------------------------------------------------------- reference --
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import torch
+    from oracle import oracle as O
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    a2 = argparse.Namespace(**vars(args))
+    a2.pool = max(args.cpu_sample, args.batch)
+    ws = make_workload(a2, dev, SEED)
+    count = args.cpu_sample
+    vol, data, wts, mats = cpu_sample_inputs(ws, count)
+    n, P, D, rmax = ws["n"], ws["P"], ws["D"], ws["rmax"]
+    for _ in range(min(args.warmup, 1)):
+        time_cpu_port(vol, data[:16], wts[:16], mats[:16], n, P, D, rmax)
+    t0 = time.perf_counter()
+    per = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        time_cpu_port(vol, data, wts, mats, n, P, D, rmax)
+        per.append(time.perf_counter() - t)
+    el = time.perf_counter() - t0
+    value = args.steps * count / el
+    out = {"impl": "reference", "metric": "project+backproject slices/s @256^3", "value": round(value, 2),
+           "unit": "slices/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(el / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "single-particle 256^3, padding 2: project + CTF-weighted backproject",
+                      "box": n, "padding": PAD, "batch_per_step": count, "parallelism": "host cores"},
+           "cpu_baseline": {"value": round(value, 2), "unit": "slices/s", "cores": O.num_threads(),
+                            "kind": "port",
+                            "sample": f"{count} slices per step; the reference ships no CPU path for this "
+                                      "(liblion is not vendored), so the OpenMP FP32 restatement of its "
+                                      "kernels runs"},
+           "e2e": {"value": round(value, 2), "unit": "slices/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    rc = reference_cuda(args, ws, dev)
+    if rc is not None:
+        out["reference_cuda"] = rc
+    print(json.dumps(out), flush=True)
+
+
+def reference_cuda(args, ws, dev):
+    """Times the reference's own CUDA kernels (rebuilt from its sources for
+    sm_100a into oracle/_ref/) on the same workload, for the GPU-to-GPU ratio."""
+    import ctypes as C
+    import torch
+    from oracle import oracle as O
+    if not O.REF_PATH.exists():
+        return None
+    ref = C.CDLL(str(O.REF_PATH))
+    p, i, f = C.c_void_p, C.c_int, C.c_float
+    ref.ref_project.argtypes = [p, i, p, i, i, i, p, i]
+    ref.ref_backproject.argtypes = [p, p, i, p, p, i, i, i, p, p, f, f, f, f, f, i, i, i]
+    n, P, D, rmax, e = ws["n"], ws["P"], ws["D"], ws["rmax"], ws["e"]
+    B = min(args.batch, ws["N"])
+    vol = torch.zeros(ws["volft"].numel() + 64, dtype=torch.complex64, device=dev)
+    vol[: ws["volft"].numel()] = ws["volft"]
+    proj = torch.empty(B * e, dtype=torch.complex64, device=dev)
+    nvol = (D // 2 + 1) * D * D
+    acc_ft = torch.zeros(nvol, dtype=torch.complex64, device=dev)
+    acc_w = torch.zeros(nvol, dtype=torch.float32, device=dev)
+    m = ws["mats"][:B].contiguous()
+    t = []
+    for rep in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc1 = ref.ref_project(vol.data_ptr(), P, proj.data_ptr(), n, 2, rmax, m.data_ptr(), B)
+        t1 = time.perf_counter()
+        rc2 = ref.ref_backproject(acc_ft.data_ptr(), acc_w.data_ptr(), D, ws["data"].data_ptr(),
+                                  ws["wts"].data_ptr(), n, 2, rmax, m.data_ptr(), None, 1, 0, 0, 1, 0.0, 0, 0, B)
+        t2 = time.perf_counter()
+        if rc1 or rc2:
+            return {"error": f"reference CUDA returned {rc1}, {rc2}"}
+        t.append((t1 - t0, t2 - t1))
+    tp = min(x[0] for x in t)
+    tb = min(x[1] for x in t)
+    return {"value": round(B / (tp + tb), 1), "unit": "slices/s", "batch": B,
+            "project_ms": round(tp * 1e3, 3), "backproject_ms": round(tb * 1e3, 3),
+            "how": "reference d_rlnProject / d_rlnBackproject (matrix overloads) rebuilt from source for "
+                   "sm_100a with its own flags; each call synchronises (as the reference does)"}
+
+
+def l2_probe():
+    import ctypes as C
+    path = ROOT / "gtom_b200" / "lib" / "libgtomrln_probe.so"
+    if not path.exists():
+        return {}
+    L = C.CDLL(str(path))
+    L.gtomrln_probe_l2_red.restype = C.c_double
+    L.gtomrln_probe_l2_red.argtypes = [C.c_int] * 5
+    L.gtomrln_probe_l2_gather.restype = C.c_double
+    L.gtomrln_probe_l2_gather.argtypes = [C.c_int] * 4
+    out = {}
+    for vec, key in ((1, "l2_red_gadds"), (2, "l2_red_v2_gadds"), (4, "l2_red_v4_gadds")):
+        v = L.gtomrln_probe_l2_red(vec, 26, 148 * 8, 256, 256)
+        out[key] = round(v / 1e9, 2) if v > 0 else None
+    g = L.gtomrln_probe_l2_gather(26, 148 * 8, 256, 256)
+    out["l2_gather_gbs"] = round(g / 1e9, 1) if g > 0 else None
+    out["how"] = "random addresses in a 64 MiB L2-resident buffer, 148*8 blocks x 256 threads"
+    return out
+
+
+def ncu_traffic():
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            return {}
+    return {}
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,14 @@
+"""B200-native RELION-style Fourier projector, backprojector and gridding
+reconstructor: a drop-in for gtom's d_rlnProject / d_rlnBackproject /
+d_ReconstructGridding.  The compute lives in libgtomrln.so (CUDA, sm_100a);
+this package binds its C ABI."""
+from ._lib import GtomError, GtomLibraryMissing  # noqa: F401
+from .relion import (  # noqa: F401
+    d_ReconstructGridding,
+    d_rlnBackproject,
+    d_rlnProject,
+    elements_fft,
+    kaiser_bessel_table,
+    matrices_from_angles,
+    reconstruct_gridding_tol,
+)

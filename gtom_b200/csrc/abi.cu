@@ -1,0 +1,126 @@
+// Library-wide pieces of the C ABI: error state, version, the device memory
+// pool for per-call scratch, and the host matrix builder.
+#include <cmath>
+#include <cstdarg>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+
+namespace gtomrln {
+
+static thread_local std::string g_last_error;
+
+int set_error(int status, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return status;
+}
+
+void clear_error() { g_last_error.clear(); }
+
+// Single-precision ZYZ Euler matrix in the order src/Helpers/Euler.cu:39-68
+// evaluates it, transposed and scaled (Project.cu:16).  For s = 1 or a power
+// of two the scale is exact.
+void matrices_from_angles(const float* angles, float s, unsigned batch, float* out) {
+  for (unsigned b = 0; b < batch; b++) {
+    float alpha = angles[3 * b], beta = angles[3 * b + 1], gamma = angles[3 * b + 2];
+    float ca = std::cos(alpha), cb = std::cos(beta), cg = std::cos(gamma);
+    float sa = std::sin(alpha), sb = std::sin(beta), sg = std::sin(gamma);
+    float cc = cb * ca, cs = cb * sa, sc = sb * ca, ss = sb * sa;
+    // E as a math matrix, row-major E[r][c] (glm column c = (E[0][c], E[1][c], E[2][c])).
+    float E[3][3];
+    E[0][0] = cg * cc - sg * sa;  E[1][0] = -sg * cc - cg * sa;  E[2][0] = sc;
+    E[0][1] = cg * cs + sg * ca;  E[1][1] = -sg * cs + cg * ca;  E[2][1] = ss;
+    E[0][2] = -cg * sb;           E[1][2] = sg * sb;             E[2][2] = cb;
+    // M = E^T * s; column-major M[c*3 + r] = M(r, c) = E(c, r) * s.
+    float* o = out + 9 * (size_t)b;
+    for (int c = 0; c < 3; c++)
+      for (int r = 0; r < 3; r++) o[c * 3 + r] = E[c][r] * s;
+  }
+}
+
+// One pool per device; its release threshold keeps up to 4 GiB of freed
+// scratch mapped so that repeated calls do not remap it.
+static std::mutex g_pool_mutex;
+static std::vector<cudaMemPool_t> g_pools;
+
+static int get_pool(cudaMemPool_t* out) {
+  int dev = 0;
+  GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  if ((int)g_pools.size() <= dev) g_pools.resize(dev + 1, nullptr);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool;
+    GTOMRLN_CUDA_TRY(cudaMemPoolCreate(&pool, &props));
+    uint64_t threshold = 4ull << 30;
+    GTOMRLN_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    g_pools[dev] = pool;
+  }
+  *out = g_pools[dev];
+  return GTOMRLN_OK;
+}
+
+int pool_alloc(void** ptr, size_t bytes, cudaStream_t stream) {
+  cudaMemPool_t pool;
+  int st = get_pool(&pool);
+  if (st) return st;
+  if (bytes == 0) bytes = 256;
+  cudaError_t e = cudaMallocFromPoolAsync(ptr, bytes, pool, stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(GTOMRLN_ERR_ALLOC, "device allocation of %zu bytes failed: %s", bytes,
+                     cudaGetErrorString(e));
+  }
+  return GTOMRLN_OK;
+}
+
+int pool_free(void* ptr, cudaStream_t stream) {
+  if (!ptr) return GTOMRLN_OK;
+  GTOMRLN_CUDA_TRY(cudaFreeAsync(ptr, stream));
+  return GTOMRLN_OK;
+}
+
+int release_gridding_plans();  // gridding.cu
+
+}  // namespace gtomrln
+
+using namespace gtomrln;
+
+extern "C" {
+
+int gtomrln_version(void) { return 100; }
+
+const char* gtomrln_last_error(void) { return g_last_error.c_str(); }
+
+int gtomrln_release_caches(void) {
+  int st = release_gridding_plans();
+  if (st) return st;
+  int dev = 0;
+  GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  if ((int)g_pools.size() > dev && g_pools[dev]) {
+    GTOMRLN_CUDA_TRY(cudaDeviceSynchronize());
+    GTOMRLN_CUDA_TRY(cudaMemPoolTrimTo(g_pools[dev], 0));
+  }
+  return GTOMRLN_OK;
+}
+
+int gtomrln_matrices_from_angles(const float* h_angles, float supersample, unsigned batch,
+                                 float* h_matrices) {
+  clear_error();
+  if (batch && (!h_angles || !h_matrices))
+    return set_error(GTOMRLN_ERR_INVALID, "matrices_from_angles: NULL array");
+  matrices_from_angles(h_angles, supersample, batch, h_matrices);
+  return GTOMRLN_OK;
+}
+
+}  // extern "C"

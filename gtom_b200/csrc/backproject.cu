@@ -1,0 +1,232 @@
+// Backprojector: trilinear scatter-insert of half-complex slices and their
+// weights into a half-complex volume, the B200 replacement of
+// Backproject3DtoNDKernel (src/Relion/Backproject.cu:126-322).
+//
+// Direct kernel: one thread per slice element, all slices of a batch in one
+// flattened launch.  Per sample and neighbour the (re, im) pair goes to L2 as
+// one vector reduction (red.global.add.v2.f32) instead of two scalar
+// atomics; the weight as one scalar reduction.  Geometry, binary16 rounding
+// of the trilinear weights, Friedel mirroring, the second insertion on the
+// x = 0 plane and the clamps are the reference's, step for step.
+#include "common.cuh"
+
+namespace gtomrln {
+
+constexpr int kBpThreads = 256;
+constexpr int kBpPerThread = 2;
+constexpr int kBpTile = kBpThreads * kBpPerThread;
+
+struct BpArgs {
+  int n, dimft;
+  int64_t area, elements;
+  int tiles;
+  int rmax2;
+  int P, rowlen;
+  int64_t nvox;
+  float4 mag;            // columns of the 2x2 magnification
+  float ewalddiaminv;    // 1 / (2 R), R = ewald radius * supersample; 0 = flat
+};
+
+// Stored location of neighbour (x, y, z) (Backproject.cu:261-274).  The
+// clamps compare as unsigned like the reference's tmin(uint, short), so a
+// negative coordinate clamps to the upper bound.
+template <bool DECENTERED>
+__device__ __forceinline__ int64_t place(int x, int y, int z, int P, int rowlen) {
+  if (DECENTERED) {
+    y = y < 0 ? y + P : y;
+    z = z < 0 ? z + P : z;
+  } else {
+    y += P / 2;
+    z += P / 2;
+  }
+  unsigned half = (unsigned)(P / 2), last = (unsigned)(P - 1);
+  x = (unsigned)x > half ? (int)half : x;
+  y = (unsigned)y > last ? (int)last : y;
+  z = (unsigned)z > last ? (int)last : z;
+  return ((int64_t)z * P + y) * rowlen + x;
+}
+
+template <int NDIMS, bool DECENTERED, bool SQUARE>
+__global__ void __launch_bounds__(kBpThreads)
+backproject_direct_kernel(float2* __restrict__ volft, float* __restrict__ volw,
+                          const float2* __restrict__ projft, const float* __restrict__ projw,
+                          const float* __restrict__ mats, const int* __restrict__ ivolume,
+                          BpArgs a) {
+  const int slice = blockIdx.x / a.tiles;
+  const int tile = blockIdx.x - slice * a.tiles;
+  float m[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) m[i] = __ldg(mats + 9 * (int64_t)slice + i);
+  if (ivolume) {
+    int64_t off = (int64_t)__ldg(ivolume + slice) * a.nvox;
+    if (volft) volft += off;
+    if (volw) volw += off;
+  }
+  const int half = a.n / 2;
+
+  for (int k = 0; k < kBpPerThread; k++) {
+    int64_t id = (int64_t)tile * kBpTile + k * kBpThreads + threadIdx.x;
+    if (id >= a.elements) break;
+    int idx = (int)(id % a.dimft);
+    int idy = (int)((NDIMS == 3 ? id % a.area : id) / a.dimft);
+    int idz = NDIMS == 3 ? (int)(id / a.area) : 0;
+    int x = idx;
+    int y = idy <= half ? idy : idy - a.n;
+    int z = NDIMS == 3 ? (idz <= half ? idz : idz - a.n) : 0;
+    if (NDIMS == 3) {
+      if (x == 0 && y < 0 && z < 0) continue;
+    } else {
+      if (x == 0 && y < 0) continue;
+    }
+    float qx = (float)x, qy = (float)y, qz = (float)z;
+    if (NDIMS == 2) {  // glm mat2 * vec2, contracted like mat_apply
+      qx = fmaf(a.mag.x, (float)x, a.mag.z * (float)y);
+      qy = fmaf(a.mag.y, (float)x, a.mag.w * (float)y);
+      qz = a.ewalddiaminv * (float)(x * x + y * y);
+    }
+    int r2 = NDIMS == 3 ? (z * z + y * y + x * x) : (int)fmaf(qz, qz, fmaf(qx, qx, qy * qy));
+    if (r2 >= a.rmax2) continue;
+
+    float3 pos = mat_apply(m, qx, qy, qz);
+    int x0 = (short)floorf(pos.x + 1e-5f);
+    int y0 = (short)floorf(pos.y);
+    int z0 = (short)floorf(pos.z);
+    float fx = pos.x - (float)x0, fy = pos.y - (float)y0, fz = pos.z - (float)z0;
+
+    // Trilinear weights rounded through binary16 (Backproject.cu:221-238).
+    float c0 = 1.f - fz, c1 = fz;
+    float c00 = half_round((1.f - fy) * c0), c10 = half_round(fy * c0);
+    float c01 = half_round((1.f - fy) * c1), c11 = half_round(fy * c1);
+    float w[8];
+    w[0] = half_round((1.f - fx) * c00); w[1] = half_round(fx * c00);
+    w[2] = half_round((1.f - fx) * c10); w[3] = half_round(fx * c10);
+    w[4] = half_round((1.f - fx) * c01); w[5] = half_round(fx * c01);
+    w[6] = half_round((1.f - fx) * c11); w[7] = half_round(fx * c11);
+
+    float2 v = projft ? __ldg(projft + a.elements * slice + id) : make_float2(1.f, 0.f);
+    float pw = projw ? __ldg(projw + a.elements * slice + id) : 1.f;
+
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      int nx = x0 + (i & 1), ny = y0 + ((i >> 1) & 1), nz = z0 + ((i >> 2) & 1);
+      float iw = w[i];
+      if (SQUARE) iw *= iw;
+      float sre = v.x, sim = v.y;
+      int tx = nx, ty = ny, tz = nz;
+      if (tx < 0) {
+        tx = -tx; ty = -ty; tz = -tz;
+        sim = -sim;
+      }
+      int64_t o = place<DECENTERED>(tx, ty, tz, a.P, a.rowlen);
+      if (volft) red_add2((float*)(volft + o), iw * sre, iw * sim);
+      if (volw) red_add(volw + o, iw * pw);
+      if (nx == 0 && (ny != 0 || nz != 0)) {  // x = 0 plane (Backproject.cu:289-319)
+        o = place<DECENTERED>(0, -ny, -nz, a.P, a.rowlen);
+        if (volft) red_add2((float*)(volft + o), iw * sre, iw * -sim);
+        if (volw) red_add(volw + o, iw * pw);
+      }
+    }
+  }
+}
+
+static int backproject_launch(float* d_volumeft, float* d_volumeweights, int vx, int vy, int vz,
+                              const float* d_projft, const float* d_projweights, int px, int py,
+                              int pz, unsigned rmax, const float* d_matrices, const int* d_ivolume,
+                              float4 mag, float ewaldradiussuper, int decentered, int square,
+                              unsigned batch, cudaStream_t stream) {
+  int ndv = dimension_count(vx, vy, vz), ndp = dimension_count(px, py, pz);
+  if (ndv < ndp)
+    return set_error(GTOMRLN_ERR_INVALID,
+                     "backproject: volume has %d dimensions, projections %d (reference throws)",
+                     ndv, ndp);
+  if (vx <= 0 || px <= 0) return set_error(GTOMRLN_ERR_INVALID, "backproject: non-positive dimension");
+  // A 2D volume is a silent no-op in the reference (Backproject.cu:105-123).
+  if (ndv != 3 || batch == 0) return GTOMRLN_OK;
+  if (ndp != 2 && ndp != 3)
+    return set_error(GTOMRLN_ERR_INVALID, "backproject: projections must be 2D or 3D");
+  if (!d_matrices) return set_error(GTOMRLN_ERR_INVALID, "backproject: d_matrices is NULL");
+  if (rmax > (unsigned)(px / 2)) rmax = px / 2;
+
+  BpArgs a;
+  a.n = px;
+  a.dimft = px / 2 + 1;
+  a.area = (int64_t)a.dimft * px;
+  a.elements = ndp == 3 ? a.area * px : a.area;
+  a.tiles = (int)((a.elements + kBpTile - 1) / kBpTile);
+  a.rmax2 = (int)(rmax * rmax);
+  a.P = vx;
+  a.rowlen = vx / 2 + 1;
+  a.nvox = (int64_t)a.rowlen * vx * vx;
+  a.mag = mag;
+  a.ewalddiaminv = ewaldradiussuper == 0 ? 0.f : 1.0f / (2.0f * ewaldradiussuper);
+  if ((int64_t)a.tiles * batch > 0x7fffffffLL)
+    return set_error(GTOMRLN_ERR_INVALID, "backproject: batch too large for one launch");
+
+  dim3 grid((unsigned)(a.tiles * (int64_t)batch));
+  float2* vf = (float2*)d_volumeft;
+  const float2* pf = (const float2*)d_projft;
+#define GTOMRLN_BP(ND, DEC, SQ)                                                           \
+  backproject_direct_kernel<ND, DEC, SQ><<<grid, kBpThreads, 0, stream>>>(vf, d_volumeweights, \
+                                                                         pf, d_projweights,  \
+                                                                         d_matrices, d_ivolume, a)
+  if (ndp == 2) {
+    if (decentered) { if (square) GTOMRLN_BP(2, true, true); else GTOMRLN_BP(2, true, false); }
+    else            { if (square) GTOMRLN_BP(2, false, true); else GTOMRLN_BP(2, false, false); }
+  } else {
+    if (decentered) { if (square) GTOMRLN_BP(3, true, true); else GTOMRLN_BP(3, true, false); }
+    else            { if (square) GTOMRLN_BP(3, false, true); else GTOMRLN_BP(3, false, false); }
+  }
+#undef GTOMRLN_BP
+  GTOMRLN_LAUNCH_CHECK("backproject_direct_kernel");
+  return GTOMRLN_OK;
+}
+
+}  // namespace gtomrln
+
+using namespace gtomrln;
+
+extern "C" {
+
+int gtomrln_backproject(float* d_volumeft, float* d_volumeweights, int vx, int vy, int vz,
+                        const float* d_projft, const float* d_projweights, int px, int py, int pz,
+                        unsigned rmax, const float* d_matrices, const int* d_ivolume, float mag_x,
+                        float mag_y, float mag_z, float mag_w, float ewaldradiussuper,
+                        int outputdecentered, int squareinterpweights, unsigned batch,
+                        void* stream) {
+  clear_error();
+  return backproject_launch(d_volumeft, d_volumeweights, vx, vy, vz, d_projft, d_projweights, px,
+                            py, pz, rmax, d_matrices, d_ivolume,
+                            make_float4(mag_x, mag_y, mag_z, mag_w), ewaldradiussuper,
+                            outputdecentered, squareinterpweights, batch, (cudaStream_t)stream);
+}
+
+int gtomrln_backproject_angles(float* d_volumeft, float* d_volumeweights, int vx, int vy, int vz,
+                               const float* d_projft, const float* d_projweights, int px, int py,
+                               int pz, unsigned rmax, const float* h_angles, const int* h_ivolume,
+                               float mag_x, float mag_y, float mag_z, float mag_w,
+                               float ewaldradius, float supersample, int outputdecentered,
+                               int squareinterpweights, unsigned batch, void* stream) {
+  clear_error();
+  cudaStream_t s = (cudaStream_t)stream;
+  return with_device_matrices(h_angles, supersample, batch, s, [&](const float* d_m) -> int {
+    int* d_iv = nullptr;
+    if (h_ivolume && batch) {
+      int st = pool_alloc((void**)&d_iv, sizeof(int) * (size_t)batch, s);
+      if (st) return st;
+      cudaError_t e =
+          cudaMemcpyAsync(d_iv, h_ivolume, sizeof(int) * (size_t)batch, cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) {
+        pool_free(d_iv, s);
+        return set_error(GTOMRLN_ERR_CUDA, "ivolume upload failed: %s", cudaGetErrorString(e));
+      }
+    }
+    int st = backproject_launch(d_volumeft, d_volumeweights, vx, vy, vz, d_projft, d_projweights,
+                                px, py, pz, rmax, d_m, d_iv, make_float4(mag_x, mag_y, mag_z, mag_w),
+                                ewaldradius * supersample, outputdecentered, squareinterpweights,
+                                batch, s);
+    int st2 = pool_free(d_iv, s);
+    return st ? st : st2;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,121 @@
+// Shared helpers of the gtomrln library: status handling, the slice
+// geometry, binary16 weight rounding and vector reductions.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/gtomrln.h"
+
+namespace gtomrln {
+
+// ---------------------------------------------------------------- errors --
+// Records msg as the calling thread's last error and returns status.
+int set_error(int status, const char* fmt, ...);
+void clear_error();
+
+#define GTOMRLN_CUDA_TRY(expr)                                                    \
+  do {                                                                            \
+    cudaError_t _e = (expr);                                                      \
+    if (_e != cudaSuccess)                                                        \
+      return ::gtomrln::set_error(GTOMRLN_ERR_CUDA, "%s failed: %s (%s:%d)", #expr, \
+                                  cudaGetErrorString(_e), __FILE__, __LINE__);    \
+  } while (0)
+
+#define GTOMRLN_LAUNCH_CHECK(what)                                                 \
+  do {                                                                             \
+    cudaError_t _e = cudaGetLastError();                                           \
+    if (_e != cudaSuccess)                                                         \
+      return ::gtomrln::set_error(GTOMRLN_ERR_CUDA, "launch of %s failed: %s", what, \
+                                  cudaGetErrorString(_e));                         \
+  } while (0)
+
+// Number of dimensions the reference assigns to an int3
+// (include/Prerequisites.cuh:219, DimensionCount).
+inline int dimension_count(int x, int y, int z) {
+  auto mx = [](int a, int b) { return a > b ? a : b; };
+  return 3 - mx(2 - mx(z, 1), 0) - mx(2 - mx(y, 1), 0) - mx(2 - mx(x, 1), 0);
+}
+
+// Host matrices exactly as Project.cu:14-16 builds them (single precision).
+void matrices_from_angles(const float* angles, float supersample, unsigned batch, float* out);
+
+// Stream-ordered device scratch from the library's memory pool.
+int pool_alloc(void** ptr, size_t bytes, cudaStream_t stream);
+int pool_free(void* ptr, cudaStream_t stream);
+
+// ---------------------------------------------------------------- device --
+struct Mat3 {
+  float m[9];  // column-major, as glm::mat3
+};
+
+// glm's mat3 * vec3 (m[0][0]*v.x + m[1][0]*v.y + m[2][0]*v.z per row),
+// contracted the way the compiler contracts that sum in the reference: the
+// left product is fused with the rounded middle one, then the right product
+// is fused onto that.  Keeping the same roundings matters because the
+// backprojector rounds its weights to binary16, which turns a one-ulp
+// difference in a position into a 2^-11 difference in a weight.
+__device__ __forceinline__ float3 mat_apply(const float* m, float x, float y, float z) {
+  float3 r;
+  r.x = fmaf(m[6], z, fmaf(m[0], x, m[3] * y));
+  r.y = fmaf(m[7], z, fmaf(m[1], x, m[4] * y));
+  r.z = fmaf(m[8], z, fmaf(m[2], x, m[5] * y));
+  return r;
+}
+
+// lerp of cutil_math_bugfixes.cuh:212: fma(b - a, t, a).
+__device__ __forceinline__ float lerpf(float a, float b, float t) { return fmaf(b - a, t, a); }
+
+__device__ __forceinline__ float half_round(float v) { return __half2float(__float2half_rn(v)); }
+
+// Fire-and-forget FP32 reductions in L2 (no return value).
+__device__ __forceinline__ void red_add(float* p, float a) {
+  asm volatile("red.relaxed.gpu.global.add.f32 [%0], %1;" ::"l"(p), "f"(a) : "memory");
+}
+__device__ __forceinline__ void red_add2(float* p, float a, float b) {
+  asm volatile("red.relaxed.gpu.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b)
+               : "memory");
+}
+__device__ __forceinline__ void red_add4(float* p, float a, float b, float c, float d) {
+  asm volatile("red.relaxed.gpu.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a),
+               "f"(b), "f"(c), "f"(d)
+               : "memory");
+}
+
+// Slice element id -> signed Fourier coordinates (Project.cu:103-109).
+struct SliceGeom {
+  int n;         // dimsproj.x
+  int dimft;     // n/2 + 1
+  int64_t area;  // dimft * n
+  int64_t elements;
+};
+
+// Copies host-built matrices to stream-ordered scratch, runs fn, frees.
+template <class Fn>
+inline int with_device_matrices(const float* h_angles, float supersample, unsigned batch,
+                                cudaStream_t stream, Fn fn) {
+  if (batch == 0) return fn((const float*)nullptr);
+  if (!h_angles) return set_error(GTOMRLN_ERR_INVALID, "h_angles is NULL");
+  std::vector<float> h(9 * (size_t)batch);
+  matrices_from_angles(h_angles, supersample, batch, h.data());
+  void* d = nullptr;
+  int st = pool_alloc(&d, h.size() * sizeof(float), stream);
+  if (st) return st;
+  cudaError_t e = cudaMemcpyAsync(d, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) {
+    pool_free(d, stream);
+    return set_error(GTOMRLN_ERR_CUDA, "matrix upload failed: %s", cudaGetErrorString(e));
+  }
+  st = fn((const float*)d);
+  int st2 = pool_free(d, stream);
+  if (!st) st = st2;
+  // The pageable source buffer h dies here; cudaMemcpyAsync from pageable
+  // memory has already staged it before returning.
+  return st;
+}
+
+}  // namespace gtomrln

@@ -1,0 +1,490 @@
+// Gridding reconstructor: RELION-style iterative gridding-weight correction
+// followed by the inverse FFT, crop and sinc^2 correction — the B200
+// replacement of gtom::d_ReconstructGridding
+// (src/Reconstruction/RecFourier.cu:98-332).
+//
+// The reference makes 5 + 4 * iterations element-wise passes over the P-grid
+// around its FFTs (decentre, sphere mask, fill, Iteration1, renormalise,
+// blob multiply, Iteration2, ...).  Here they are fused into
+//   init   : decentre + mask of the weights, Fnewweight = sphere mask, and
+//            the first iteration's conv spectrum, in one pass;
+//   blob   : 1/P^3 renormalisation and the real-space blob multiply, with
+//            the blob computed on the fly from its radial table (no P^3
+//            blob volume);
+//   update : Iteration2 fused with the next iteration's Iteration1, plus the
+//            optional relative-change reduction;
+//   final  : decentre of the data, the weight product (or the division of
+//            the iterations == 0 branch) and the centring shift as a sign;
+//   crop   : centred crop, sinc^2 correction and the 1/(pad^3 ori) scale.
+// The P^3 R2C / C2R transforms are cuFFT library calls; plans are cached
+// per (device, P).
+#include <cufft.h>
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "common.cuh"
+
+namespace gtomrln {
+
+double kaiser_fourier_value(double w, double a, double alpha, int m);  // below
+
+constexpr int kBlobSamples = 10000;
+
+// ---------------------------------------------------------------- kernels --
+struct GridGeom {
+  int P;         // padded working grid
+  int rowlen;    // P/2 + 1
+  int64_t nc;    // rowlen * P * P complex elements
+  int64_t nr;    // P^3 real elements
+};
+
+// RecFourier.cu:264-285 (DecenterKernel) for the weights + SphereMask.cu:167-189
+// (Fnewweight = 1 inside r^2 < (r_max*pad)^2) + Iteration1Kernel
+// (RecFourier.cu:287-291).  old* are the centred input dims.
+__global__ void grid_init_kernel(const float* __restrict__ weight, int oldx, int oldy, int oldz,
+                                 float* __restrict__ Fw, float* __restrict__ Fnw,
+                                 float2* __restrict__ convft, GridGeom g, int maskr2,
+                                 int write_conv) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.nc) return;
+  int x = (int)(i % g.rowlen);
+  int64_t t = i / g.rowlen;
+  int y = (int)(t % g.P);
+  int z = (int)(t / g.P);
+  int zp = z < g.P / 2 + 1 ? z : z - g.P;
+  int yp = y < g.P / 2 + 1 ? y : y - g.P;
+  float r = (float)(zp * zp) + (float)(yp * yp);
+  float rr = r + (float)(x * x);
+  float mask = rr < (float)(g.P * g.P / 4) ? 1.f : 0.f;
+  int zi = zp + oldz / 2, yi = yp + oldy / 2;
+  float w = 0.f;
+  if (zi >= 0 && zi < oldz && yi >= 0 && yi < oldy && x < oldx / 2 + 1)
+    w = __ldg(weight + ((int64_t)zi * oldy + yi) * (oldx / 2 + 1) + x) * mask;
+  Fw[i] = w;
+  // SphereMaskFTKernel uses y < dims.y/2+1 ? y : y - dims.x, the same split.
+  int r2 = x * x + yp * yp + zp * zp;
+  float nw = r2 < maskr2 ? 1.f : 0.f;
+  Fnw[i] = nw;
+  if (write_conv) convft[i] = make_float2(w * nw, 0.f);
+}
+
+// conv <- (conv * 1/P^3) * blob(r): d_IFFTC2R's renormalisation
+// (IFFT.cu:36-46) and d_MultiplyByVector with PrecomputeBlobKernel's table
+// lookup (RecFourier.cu:243-262), the radius evaluated as the reference does.
+__global__ void grid_blob_kernel(float* __restrict__ conv, const float* __restrict__ table,
+                                 GridGeom g, float inv_n, float funcsampling) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.nr) return;
+  int x = (int)(i % g.P);
+  int64_t t = i / g.P;
+  int y = (int)(t % g.P);
+  int z = (int)(t / g.P);
+  int zp = z < g.P / 2 ? z : z - g.P;
+  int yp = y < g.P / 2 ? y : y - g.P;
+  float xp = (float)(x < g.P / 2 ? x : x - g.P);
+  float r = sqrtf(xp * xp + (float)(yp * yp) + (float)(zp * zp)) / (float)g.P / funcsampling;
+  int ti = (int)r;
+  ti = ti < kBlobSamples - 1 ? ti : kBlobSamples - 1;
+  float v = conv[i] * inv_n;
+  conv[i] = v * __ldg(table + ti);
+}
+
+// Iteration2Kernel (RecFourier.cu:293-308) fused with the next iteration's
+// Iteration1Kernel.  Optionally accumulates the convergence measure
+// sum((Fw*(new-old))^2) and sum((Fw*old)^2): the change of the corrected
+// weight Fw*Fnw.  Unweighted, voxels with Fw = 0 would dominate: there
+// Fnw grows by 1e4 per iteration until the 1e20 clamp and never matters.
+__global__ void grid_update_kernel(float2* __restrict__ convft, const float* __restrict__ Fw,
+                                   float* __restrict__ Fnw, GridGeom g, int write_conv,
+                                   double* __restrict__ change) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double d2 = 0, o2 = 0;
+  if (i < g.nc) {
+    float c = convft[i].x;
+    float w = fmaxf(1e-4f, c);
+    float old = Fnw[i];
+    float nw = fminf(1e20f, old / w);
+    float fw = Fw[i];
+    Fnw[i] = nw;
+    if (write_conv) convft[i] = make_float2(fw * nw, 0.f);
+    if (change) {
+      double d = (double)fw * ((double)nw - (double)old);
+      double o = (double)fw * (double)old;
+      d2 = d * d;
+      o2 = o * o;
+    }
+  }
+  if (change) {
+    for (int off = 16; off > 0; off >>= 1) {
+      d2 += __shfl_down_sync(0xffffffffu, d2, off);
+      o2 += __shfl_down_sync(0xffffffffu, o2, off);
+    }
+    __shared__ double s[2][32];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { s[0][warp] = d2; s[1][warp] = o2; }
+    __syncthreads();
+    if (warp == 0) {
+      int nw = blockDim.x >> 5;
+      d2 = lane < nw ? s[0][lane] : 0;
+      o2 = lane < nw ? s[1][lane] : 0;
+      for (int off = 16; off > 0; off >>= 1) {
+        d2 += __shfl_down_sync(0xffffffffu, d2, off);
+        o2 += __shfl_down_sync(0xffffffffu, o2, off);
+      }
+      if (lane == 0) {
+        atomicAdd(change, d2);
+        atomicAdd(change + 1, o2);
+      }
+    }
+  }
+}
+
+// DecenterKernel<tcomplex> for the data (RecFourier.cu:175-179), then
+// x Fnewweight (RecFourier.cu:206) or / max(|Fweight|, 1e-4) when no
+// iteration ran (RecFourier.cu:200-202), then d_Shift by P/2 in every axis
+// (RecFourier.cu:213-214), which is the factor (-1)^(x+y+z).
+__global__ void grid_final_kernel(const float2* __restrict__ data, int oldx, int oldy, int oldz,
+                                  const float* __restrict__ Fw, const float* __restrict__ Fnw,
+                                  float2* __restrict__ convft, GridGeom g, int divide) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.nc) return;
+  int x = (int)(i % g.rowlen);
+  int64_t t = i / g.rowlen;
+  int y = (int)(t % g.P);
+  int z = (int)(t / g.P);
+  int zp = z < g.P / 2 + 1 ? z : z - g.P;
+  int yp = y < g.P / 2 + 1 ? y : y - g.P;
+  float r = (float)(zp * zp) + (float)(yp * yp);
+  float rr = r + (float)(x * x);
+  float mask = rr < (float)(g.P * g.P / 4) ? 1.f : 0.f;
+  int zi = zp + oldz / 2, yi = yp + oldy / 2;
+  float2 v = make_float2(0.f, 0.f);
+  if (zi >= 0 && zi < oldz && yi >= 0 && yi < oldy && x < oldx / 2 + 1) {
+    v = __ldg(data + ((int64_t)zi * oldy + yi) * (oldx / 2 + 1) + x);
+    v.x *= mask;
+    v.y *= mask;
+  }
+  if (divide) {
+    float inv = 1.0f / fmaxf(fabsf(Fw[i]), 1e-4f);  // Arithmetics.cu:310-311
+    v.x *= inv;
+    v.y *= inv;
+  } else {
+    float f = Fnw[i];
+    v.x *= f;
+    v.y *= f;
+  }
+  if ((x + y + z) & 1) {
+    v.x = -v.x;
+    v.y = -v.y;
+  }
+  convft[i] = v;
+}
+
+// d_Pad T_PAD_VALUE centred crop P^3 -> ori^3 (Padding.cu:97-135),
+// CorrectGriddingKernel (RecFourier.cu:310-332) and the final scale
+// (RecFourier.cu:237).
+__global__ void grid_crop_kernel(const float* __restrict__ conv, float* __restrict__ out, int P,
+                                 int ori, int off, float scale) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t total = (int64_t)ori * ori * ori;
+  if (i >= total) return;
+  int x = (int)(i % ori);
+  int64_t t = i / ori;
+  int y = (int)(t % ori);
+  int z = (int)(t / ori);
+  float v = conv[((int64_t)(z + off) * P + (y + off)) * P + (x + off)];
+  int yy = (y - ori / 2) * (y - ori / 2);
+  int zz = (z - ori / 2) * (z - ori / 2);
+  float xx = (float)(x - ori / 2);
+  float r = sqrtf(xx * xx + (float)yy + (float)zz) / (float)P;
+  if (r > 0) {
+    float s = fabsf(r) <= 1e-4f ? 1.f : sinpif(r) / (r * 3.14159265358979f);
+    v /= s * s;
+  }
+  out[i] = v * scale;
+}
+
+// ----------------------------------------------------------------- plans --
+struct PlanPair {
+  cufftHandle r2c = 0, c2r = 0;
+};
+static std::mutex g_plan_mutex;
+static std::map<std::pair<int, int>, PlanPair> g_plans;  // (device, P)
+
+static int get_plans(int P, PlanPair* out) {
+  int dev = 0;
+  GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_plan_mutex);
+  auto it = g_plans.find({dev, P});
+  if (it != g_plans.end()) {
+    *out = it->second;
+    return GTOMRLN_OK;
+  }
+  PlanPair pp;
+  cufftResult r = cufftPlan3d(&pp.r2c, P, P, P, CUFFT_R2C);
+  if (r != CUFFT_SUCCESS) return set_error(GTOMRLN_ERR_CUFFT, "cufftPlan3d R2C %d^3 failed (%d)", P, (int)r);
+  r = cufftPlan3d(&pp.c2r, P, P, P, CUFFT_C2R);
+  if (r != CUFFT_SUCCESS) {
+    cufftDestroy(pp.r2c);
+    return set_error(GTOMRLN_ERR_CUFFT, "cufftPlan3d C2R %d^3 failed (%d)", P, (int)r);
+  }
+  g_plans[{dev, P}] = pp;
+  *out = pp;
+  return GTOMRLN_OK;
+}
+
+int release_gridding_plans() {
+  std::lock_guard<std::mutex> lock(g_plan_mutex);
+  for (auto& kv : g_plans) {
+    cufftDestroy(kv.second.r2c);
+    cufftDestroy(kv.second.c2r);
+  }
+  g_plans.clear();
+  return GTOMRLN_OK;
+}
+
+// Blob tables are cached per (device, radius, alpha, order).
+static std::mutex g_table_mutex;
+static std::map<std::tuple<int, double, double, int>, float*> g_tables;
+
+int build_blob_table(double radius, double alpha, int order, int nsamples, float* out) {
+  if (order != 0 && order != 2)
+    return set_error(GTOMRLN_ERR_INVALID, "blob order %d not supported (0 or 2)", order);
+  double sampling = 0.5 / nsamples;
+  // The reference stores the raw values as float and normalises in float
+  // (RecFourier.cu:110-115).
+  for (int i = 0; i < nsamples; i++) out[i] = (float)kaiser_fourier_value(i * sampling, radius, alpha, order);
+  float norm = out[0];
+  for (int i = 0; i < nsamples; i++) out[i] /= norm;
+  return GTOMRLN_OK;
+}
+
+static int get_table(double radius, double alpha, int order, const float** out) {
+  int dev = 0;
+  GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_table_mutex);
+  auto key = std::make_tuple(dev, radius, alpha, order);
+  auto it = g_tables.find(key);
+  if (it != g_tables.end()) {
+    *out = it->second;
+    return GTOMRLN_OK;
+  }
+  std::vector<float> h(kBlobSamples);
+  int st = build_blob_table(radius, alpha, order, kBlobSamples, h.data());
+  if (st) return st;
+  float* d = nullptr;
+  GTOMRLN_CUDA_TRY(cudaMalloc(&d, kBlobSamples * sizeof(float)));
+  GTOMRLN_CUDA_TRY(cudaMemcpy(d, h.data(), kBlobSamples * sizeof(float), cudaMemcpyHostToDevice));
+  g_tables[key] = d;
+  *out = d;
+  return GTOMRLN_OK;
+}
+
+// ------------------------------------------------------------- pipeline --
+#define GTOMRLN_CUFFT_TRY(expr)                                                         \
+  do {                                                                                  \
+    cufftResult _r = (expr);                                                            \
+    if (_r != CUFFT_SUCCESS) {                                                          \
+      st = set_error(GTOMRLN_ERR_CUFFT, "%s failed (%d)", #expr, (int)_r);              \
+      goto done;                                                                        \
+    }                                                                                   \
+  } while (0)
+
+#define GTOMRLN_STEP(expr) \
+  do {                     \
+    st = (expr);           \
+    if (st) goto done;     \
+  } while (0)
+
+static int launch_check(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_error(GTOMRLN_ERR_CUDA, "launch of %s failed: %s", what, cudaGetErrorString(e));
+  return GTOMRLN_OK;
+}
+
+static int reconstruct(const float* d_dataft, const float* d_weight, float* d_out, int ori,
+                       int oldx, int oldy, int oldz, int pad, cufftHandle planf, cufftHandle planb,
+                       int iterations, double tolerance, double radius, int order, double alpha,
+                       int* iterations_done, double* final_change, cudaStream_t stream) {
+  if (ori <= 0 || pad <= 0) return set_error(GTOMRLN_ERR_INVALID, "gridding: non-positive size");
+  if (iterations < 0) return set_error(GTOMRLN_ERR_INVALID, "gridding: negative iteration count");
+  if (!d_dataft || !d_weight || !d_out) return set_error(GTOMRLN_ERR_INVALID, "gridding: NULL pointer");
+  const int P = ori * pad;
+  GridGeom g;
+  g.P = P;
+  g.rowlen = P / 2 + 1;
+  g.nc = (int64_t)g.rowlen * P * P;
+  g.nr = (int64_t)P * P * P;
+  int r_max = ori / 2;
+  int maskr2 = (r_max * pad) * (r_max * pad);
+
+  const float* table = nullptr;
+  int st = get_table(radius * pad, alpha, order, &table);
+  if (st) return st;
+  PlanPair plans;
+  if (!planf || !planb) {
+    st = get_plans(P, &plans);
+    if (st) return st;
+  }
+  if (planf) plans.r2c = planf;
+  if (planb) plans.c2r = planb;
+
+  float2* convft = nullptr;
+  float* conv = nullptr;
+  float *Fw = nullptr, *Fnw = nullptr;
+  double* change = nullptr;
+  double h_change[2] = {0, 0};
+  int done_iters = 0;
+  double last_change = 0;
+  const int T = 256;
+  unsigned bc = (unsigned)((g.nc + T - 1) / T), br = (unsigned)((g.nr + T - 1) / T);
+
+  GTOMRLN_STEP(pool_alloc((void**)&convft, g.nc * sizeof(float2), stream));
+  GTOMRLN_STEP(pool_alloc((void**)&conv, g.nr * sizeof(float), stream));
+  GTOMRLN_STEP(pool_alloc((void**)&Fw, g.nc * sizeof(float), stream));
+  GTOMRLN_STEP(pool_alloc((void**)&Fnw, g.nc * sizeof(float), stream));
+  if (tolerance > 0) GTOMRLN_STEP(pool_alloc((void**)&change, 2 * sizeof(double), stream));
+
+  GTOMRLN_CUFFT_TRY(cufftSetStream(plans.r2c, stream));
+  GTOMRLN_CUFFT_TRY(cufftSetStream(plans.c2r, stream));
+
+  grid_init_kernel<<<bc, T, 0, stream>>>(d_weight, oldx, oldy, oldz, Fw, Fnw, convft, g, maskr2,
+                                         iterations > 0);
+  GTOMRLN_STEP(launch_check("grid_init_kernel"));
+
+  for (int it = 0; it < iterations; it++) {
+    GTOMRLN_CUFFT_TRY(cufftExecC2R(plans.c2r, (cufftComplex*)convft, conv));
+    grid_blob_kernel<<<br, T, 0, stream>>>(conv, table, g, 1.0f / (float)g.nr,
+                                           (float)(0.5 / kBlobSamples));
+    GTOMRLN_STEP(launch_check("grid_blob_kernel"));
+    GTOMRLN_CUFFT_TRY(cufftExecR2C(plans.r2c, conv, (cufftComplex*)convft));
+    if (change) GTOMRLN_CUDA_TRY(cudaMemsetAsync(change, 0, 2 * sizeof(double), stream));
+    grid_update_kernel<<<bc, T, 0, stream>>>(convft, Fw, Fnw, g, it + 1 < iterations, change);
+    GTOMRLN_STEP(launch_check("grid_update_kernel"));
+    done_iters = it + 1;
+    if (change) {
+      GTOMRLN_CUDA_TRY(cudaMemcpyAsync(h_change, change, sizeof(h_change), cudaMemcpyDeviceToHost, stream));
+      GTOMRLN_CUDA_TRY(cudaStreamSynchronize(stream));
+      last_change = h_change[1] > 0 ? std::sqrt(h_change[0] / h_change[1]) : 0.0;
+      if (last_change <= tolerance) break;
+      if (it + 1 == iterations) break;
+    }
+  }
+
+  grid_final_kernel<<<bc, T, 0, stream>>>((const float2*)d_dataft, oldx, oldy, oldz, Fw, Fnw,
+                                          convft, g, iterations == 0);
+  GTOMRLN_STEP(launch_check("grid_final_kernel"));
+  GTOMRLN_CUFFT_TRY(cufftExecC2R(plans.c2r, (cufftComplex*)convft, conv));
+  {
+    int64_t total = (int64_t)ori * ori * ori;
+    grid_crop_kernel<<<(unsigned)((total + T - 1) / T), T, 0, stream>>>(
+        conv, d_out, P, ori, P / 2 - ori / 2, 1.0f / (float)(pad * pad * pad * ori));
+    GTOMRLN_STEP(launch_check("grid_crop_kernel"));
+  }
+  if (iterations_done) *iterations_done = done_iters;
+  if (final_change) *final_change = last_change;
+
+done:
+  pool_free(convft, stream);
+  pool_free(conv, stream);
+  pool_free(Fw, stream);
+  pool_free(Fnw, stream);
+  pool_free(change, stream);
+  return st;
+}
+
+// ------------------------------------------------------- Kaiser-Bessel --
+// Fourier transform of the generalised Kaiser-Bessel blob of radius a,
+// taper alpha and order m (the function of src/Helpers/KaiserBessel.cpp:
+// 357-376), from the closed forms of the Bessel functions of half-integer
+// order:
+//   I_{1/2}(x) = sqrt(2/(pi x)) sinh x,  I_{3/2}(x) = sqrt(2/(pi x))(cosh x - sinh x / x)
+//   J_{1/2}(x) = sqrt(2/(pi x)) sin x,   J_{3/2}(x) = sqrt(2/(pi x))(sin x / x - cos x)
+// with the recurrences I_{v+1} = I_{v-1} - (2v/x) I_v and
+// J_{v+1} = (2v/x) J_v - J_{v-1}; I_0 by its power series.
+static const double kPiD = 3.14159265358979323846;
+
+static double bessel_i0(double x) {
+  double t = x * x / 4, term = 1, sum = 1;
+  for (int k = 1; k < 500; k++) {
+    term *= t / ((double)k * k);
+    sum += term;
+    if (term < sum * 1e-18) break;
+  }
+  return sum;
+}
+
+static double bessel_half(double x, int twice_order, bool modified) {
+  if (x == 0) return 0;
+  double f = std::sqrt(2 / (kPiD * x));
+  double lo, hi;  // orders 1/2 and 3/2
+  if (modified) {
+    lo = f * std::sinh(x);
+    hi = f * (std::cosh(x) - std::sinh(x) / x);
+  } else {
+    lo = f * std::sin(x);
+    hi = f * (std::sin(x) / x - std::cos(x));
+  }
+  if (twice_order == 1) return lo;
+  for (int v2 = 3; v2 < twice_order; v2 += 2) {
+    double next = modified ? lo - ((double)v2 / x) * hi : ((double)v2 / x) * hi - lo;
+    lo = hi;
+    hi = next;
+  }
+  return hi;
+}
+
+double kaiser_fourier_value(double w, double a, double alpha, int m) {
+  double t = 2 * kPiD * a * w;
+  double sigma = std::sqrt(std::fabs(alpha * alpha - t * t));
+  int twice = m == 0 ? 3 : 7;
+  double p = m == 0 ? 1.5 : 3.5;
+  double bes = bessel_half(sigma, twice, !(t > alpha));
+  double lead = std::pow(2 * kPiD, 1.5) * a * a * a * (m == 2 ? alpha * alpha : 1.0);
+  return lead * bes / (bessel_i0(alpha) * std::pow(sigma, p));
+}
+
+}  // namespace gtomrln
+
+using namespace gtomrln;
+
+extern "C" {
+
+int gtomrln_reconstruct_gridding(const float* d_dataft, const float* d_weight,
+                                 float* d_reconstructed, int ox, int oy, int oz, int padx, int pady,
+                                 int padz, int paddingfactor, int pre_planforw, int pre_planback,
+                                 int iterations, double blobradius, int bloborder,
+                                 double blobalpha, void* stream) {
+  clear_error();
+  (void)oy;
+  (void)oz;
+  return reconstruct(d_dataft, d_weight, d_reconstructed, ox, padx, pady, padz, paddingfactor,
+                     (cufftHandle)pre_planforw, (cufftHandle)pre_planback, iterations, 0.0,
+                     blobradius, bloborder, blobalpha, nullptr, nullptr, (cudaStream_t)stream);
+}
+
+int gtomrln_reconstruct_gridding_tol(const float* d_dataft, const float* d_weight,
+                                     float* d_reconstructed, int ox, int oy, int oz, int padx,
+                                     int pady, int padz, int paddingfactor, int max_iterations,
+                                     double tolerance, double blobradius, int bloborder,
+                                     double blobalpha, int* iterations_done, double* final_change,
+                                     void* stream) {
+  clear_error();
+  (void)oy;
+  (void)oz;
+  return reconstruct(d_dataft, d_weight, d_reconstructed, ox, padx, pady, padz, paddingfactor, 0,
+                     0, max_iterations, tolerance, blobradius, bloborder, blobalpha,
+                     iterations_done, final_change, (cudaStream_t)stream);
+}
+
+int gtomrln_kaiser_bessel_table(double radius, double alpha, int order, int nsamples,
+                                float* h_out) {
+  clear_error();
+  if (nsamples <= 0 || !h_out) return set_error(GTOMRLN_ERR_INVALID, "kaiser_bessel_table: bad arguments");
+  return build_blob_table(radius, alpha, order, nsamples, h_out);
+}
+
+}  // extern "C"

@@ -1,0 +1,128 @@
+// Roofline denominators that the driver's peak file does not hold, measured
+// on the device the benchmark runs on:
+//   * L2 FP32 reduction rate: fire-and-forget red.global.add to random
+//     addresses of an L2-resident buffer (scalar, .v2 and .v4 forms),
+//   * L2 -> SM gather bandwidth: random 8-byte loads from an L2-resident
+//     buffer, the access pattern of the projector's corner fetches.
+// Built into a separate library (gtom_b200/lib/libgtomrln_probe.so); the
+// product library does not contain it.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace {
+
+__device__ __forceinline__ uint32_t hash32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352dU;
+  x ^= x >> 15;
+  x *= 0x846ca68bU;
+  x ^= x >> 16;
+  return x;
+}
+
+template <int VEC>
+__global__ void red_probe_kernel(float* __restrict__ buf, uint32_t mask_vec, int iters) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t h = hash32(t * 2654435761U + 12345U);
+  for (int i = 0; i < iters; i++) {
+    h = hash32(h + (uint32_t)i);
+    float* p = buf + (size_t)(h & mask_vec) * VEC;
+    if (VEC == 1)
+      asm volatile("red.relaxed.gpu.global.add.f32 [%0], %1;" ::"l"(p), "f"(1.0f) : "memory");
+    else if (VEC == 2)
+      asm volatile("red.relaxed.gpu.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(1.0f), "f"(1.0f)
+                   : "memory");
+    else
+      asm volatile("red.relaxed.gpu.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(1.0f),
+                   "f"(1.0f), "f"(1.0f), "f"(1.0f)
+                   : "memory");
+  }
+}
+
+__global__ void gather_probe_kernel(const float2* __restrict__ buf, uint32_t mask, int iters,
+                                    float* __restrict__ sink) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t h = hash32(t * 2654435761U + 777U);
+  float acc = 0.f;
+  for (int i = 0; i < iters; i += 8) {
+    float2 v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      h = hash32(h + (uint32_t)(i + k));
+      v[k] = __ldg(buf + (h & mask));
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc += v[k].x + v[k].y;
+  }
+  if (acc == 123.456f) sink[t] = acc;  // keeps the loads alive
+}
+
+}  // namespace
+
+extern "C" {
+
+__attribute__((visibility("default")))
+// Returns FP32 additions per second (vec * reductions), or a negative CUDA error.
+double gtomrln_probe_l2_red(int vec, int log2_bytes, int blocks, int threads, int iters) {
+  size_t bytes = (size_t)1 << log2_bytes;
+  float* buf = nullptr;
+  if (cudaMalloc(&buf, bytes) != cudaSuccess) return -1;
+  cudaMemset(buf, 0, bytes);
+  uint32_t nvec = (uint32_t)(bytes / (4 * vec));
+  uint32_t mask = nvec - 1;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  auto launch = [&]() {
+    if (vec == 1) red_probe_kernel<1><<<blocks, threads>>>(buf, mask, iters);
+    else if (vec == 2) red_probe_kernel<2><<<blocks, threads>>>(buf, mask, iters);
+    else red_probe_kernel<4><<<blocks, threads>>>(buf, mask, iters);
+  };
+  launch();  // warm-up
+  cudaEventRecord(a);
+  launch();
+  cudaEventRecord(b);
+  cudaEventSynchronize(b);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaError_t e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(buf);
+  if (e != cudaSuccess) return -(double)e;
+  return (double)blocks * threads * iters * vec / (ms * 1e-3);
+}
+
+__attribute__((visibility("default")))
+// Returns bytes per second of random 8-byte gathers from a buffer of 2^log2_bytes.
+double gtomrln_probe_l2_gather(int log2_bytes, int blocks, int threads, int iters) {
+  size_t bytes = (size_t)1 << log2_bytes;
+  float2* buf = nullptr;
+  float* sink = nullptr;
+  if (cudaMalloc(&buf, bytes) != cudaSuccess) return -1;
+  if (cudaMalloc(&sink, (size_t)blocks * threads * sizeof(float)) != cudaSuccess) {
+    cudaFree(buf);
+    return -1;
+  }
+  cudaMemset(buf, 0, bytes);
+  uint32_t mask = (uint32_t)(bytes / 8) - 1;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  gather_probe_kernel<<<blocks, threads>>>(buf, mask, iters, sink);
+  cudaEventRecord(a);
+  gather_probe_kernel<<<blocks, threads>>>(buf, mask, iters, sink);
+  cudaEventRecord(b);
+  cudaEventSynchronize(b);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaError_t e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(buf);
+  cudaFree(sink);
+  if (e != cudaSuccess) return -(double)e;
+  return (double)blocks * threads * iters * 8.0 / (ms * 1e-3);
+}
+
+}  // extern "C"

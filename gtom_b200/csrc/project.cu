@@ -1,0 +1,213 @@
+// Projector: trilinear central-slice gather from a decentred half-complex
+// Fourier volume (RELION convention), the B200 replacement of
+// Project3DArraytoNDKernel / Project3DtoNDKernel (src/Relion/Project.cu:89-272).
+//
+// Direct kernel: one thread per output element.  The block's slice matrix is
+// read once into registers; the eight corner voxels are fetched through the
+// read-only path so that consecutive slices of similar orientation hit L2.
+// The per-sample arithmetic is the reference's, operation for operation, so
+// the result is the same for the same inputs.
+#include "common.cuh"
+
+namespace gtomrln {
+
+constexpr int kProjThreads = 256;
+constexpr int kProjPerThread = 4;
+constexpr int kProjTile = kProjThreads * kProjPerThread;
+
+struct ProjArgs {
+  int n;          // dimsproj.x
+  int dimft;      // n/2 + 1
+  int64_t area;   // dimft * n
+  int64_t elements;
+  int tiles;      // tiles per slice
+  int rmax2;
+  int P;          // dimsvolume.x
+  int64_t nvox;   // (P/2+1) * P * P
+};
+
+struct ArrayFetch {
+  const float2* __restrict__ vol;
+  int P, rowlen;
+  int64_t last;
+  __device__ __forceinline__ float2 operator()(int x, int y, int z) const {
+    // Flat index as in Project.cu:154-161; x == P/2+1 continues into the
+    // next row like the reference, the one read past the end is clamped.
+    int64_t i = ((int64_t)z * P + y) * rowlen + x;
+    i = i < 0 ? 0 : (i > last ? last : i);
+    return __ldg(vol + i);
+  }
+};
+
+struct TexFetch {
+  cudaTextureObject_t re, im;
+  __device__ __forceinline__ float2 operator()(int x, int y, int z) const {
+    // Project.cu:249-256: integer coordinates passed as floats.
+    return make_float2(tex3D<float>(re, (float)x, (float)y, (float)z),
+                       tex3D<float>(im, (float)x, (float)y, (float)z));
+  }
+};
+
+template <int NDIMS, class Fetch>
+__global__ void __launch_bounds__(kProjThreads)
+project_direct_kernel(Fetch fetch, float2* __restrict__ proj, const float* __restrict__ mats,
+                      ProjArgs a) {
+  const int slice = blockIdx.x / a.tiles;
+  const int tile = blockIdx.x - slice * a.tiles;
+  float m[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) m[i] = __ldg(mats + 9 * (int64_t)slice + i);
+  float2* out = proj + a.elements * slice;
+  const int half = a.n / 2;
+
+#pragma unroll
+  for (int k = 0; k < kProjPerThread; k++) {
+    int64_t id = (int64_t)tile * kProjTile + k * kProjThreads + threadIdx.x;
+    if (id >= a.elements) break;
+    int idx = (int)(id % a.dimft);
+    int idy = (int)((NDIMS == 3 ? id % a.area : id) / a.dimft);
+    int idz = NDIMS == 3 ? (int)(id / a.area) : 0;
+    int x = idx;
+    int y = idy <= half ? idy : idy - a.n;
+    int z = idz <= half ? idz : idz - a.n;
+    int r2 = NDIMS == 3 ? z * z + y * y + x * x : y * y + x * x;
+    if (r2 > a.rmax2) {
+      out[id] = make_float2(0.f, 0.f);
+      continue;
+    }
+    float3 pos = mat_apply(m, (float)x, (float)y, (float)z);
+    float sign = 1.f;
+    if (pos.x < -1e-5f) {  // Friedel mate: only x >= 0 is stored
+      pos.x = fabsf(pos.x);
+      pos.y = -pos.y;
+      pos.z = -pos.z;
+      sign = -1.f;
+    }
+    float fx0 = floorf(pos.x + 1e-5f);
+    int x0 = (int)fx0, x1 = x0 + 1;
+    float fx = pos.x - fx0;
+    float fy0 = floorf(pos.y);
+    int y0 = (int)fy0, y1 = y0 + 1;
+    if (y0 < 0) y0 += a.P;
+    if (y1 < 0) y1 += a.P;
+    float fy = pos.y - fy0;
+    float fz0 = floorf(pos.z);
+    int z0 = (int)fz0, z1 = z0 + 1;
+    if (z0 < 0) z0 += a.P;
+    if (z1 < 0) z1 += a.P;
+    float fz = pos.z - fz0;
+
+    float2 d000 = fetch(x0, y0, z0), d001 = fetch(x1, y0, z0);
+    float2 d010 = fetch(x0, y1, z0), d011 = fetch(x1, y1, z0);
+    float2 d100 = fetch(x0, y0, z1), d101 = fetch(x1, y0, z1);
+    float2 d110 = fetch(x0, y1, z1), d111 = fetch(x1, y1, z1);
+
+    float rx00 = lerpf(d000.x, d001.x, fx), ix00 = lerpf(d000.y, d001.y, fx);
+    float rx01 = lerpf(d010.x, d011.x, fx), ix01 = lerpf(d010.y, d011.y, fx);
+    float rx10 = lerpf(d100.x, d101.x, fx), ix10 = lerpf(d100.y, d101.y, fx);
+    float rx11 = lerpf(d110.x, d111.x, fx), ix11 = lerpf(d110.y, d111.y, fx);
+    float rxy0 = lerpf(rx00, rx01, fy), ixy0 = lerpf(ix00, ix01, fy);
+    float rxy1 = lerpf(rx10, rx11, fy), ixy1 = lerpf(ix10, ix11, fy);
+    float2 v = make_float2(lerpf(rxy0, rxy1, fz), lerpf(ixy0, ixy1, fz) * sign);
+    out[id] = v;
+  }
+}
+
+// Validates dimensions the way Project.cu:27-32 does and fills ProjArgs.
+static int project_setup(int vx, int vy, int vz, int px, int py, int pz, unsigned rmax,
+                         unsigned batch, ProjArgs* a, int* ndims_proj) {
+  int ndv = dimension_count(vx, vy, vz), ndp = dimension_count(px, py, pz);
+  if (ndv < ndp)
+    return set_error(GTOMRLN_ERR_INVALID,
+                     "project: volume has %d dimensions, projections %d (reference throws)", ndv,
+                     ndp);
+  if (ndp != 2 && ndp != 3)
+    return set_error(GTOMRLN_ERR_INVALID, "project: projections must be 2D or 3D (got %dD)", ndp);
+  if (vx <= 0 || px <= 0)
+    return set_error(GTOMRLN_ERR_INVALID, "project: non-positive dimension");
+  if (rmax > (unsigned)(px / 2)) rmax = px / 2;
+  a->n = px;
+  a->dimft = px / 2 + 1;
+  a->area = (int64_t)a->dimft * px;
+  a->elements = ndp == 3 ? a->area * px : a->area;
+  a->tiles = (int)((a->elements + kProjTile - 1) / kProjTile);
+  a->rmax2 = (int)(rmax * rmax);
+  a->P = vx;
+  a->nvox = (int64_t)(vx / 2 + 1) * vx * vx;
+  *ndims_proj = ndp;
+  if ((int64_t)a->tiles * batch > 0x7fffffffLL)
+    return set_error(GTOMRLN_ERR_INVALID, "project: batch too large for one launch");
+  return GTOMRLN_OK;
+}
+
+template <class Fetch>
+static int launch_project(Fetch f, int ndp, float* d_proj, const float* d_mats, const ProjArgs& a,
+                          unsigned batch, cudaStream_t stream) {
+  if (batch == 0) return GTOMRLN_OK;
+  dim3 grid((unsigned)(a.tiles * (int64_t)batch));
+  if (ndp == 2)
+    project_direct_kernel<2, Fetch><<<grid, kProjThreads, 0, stream>>>(f, (float2*)d_proj, d_mats, a);
+  else
+    project_direct_kernel<3, Fetch><<<grid, kProjThreads, 0, stream>>>(f, (float2*)d_proj, d_mats, a);
+  GTOMRLN_LAUNCH_CHECK("project_direct_kernel");
+  return GTOMRLN_OK;
+}
+
+}  // namespace gtomrln
+
+using namespace gtomrln;
+
+extern "C" {
+
+int gtomrln_project(const float* d_volumeft, int vx, int vy, int vz, float* d_proj, int px, int py,
+                    int pz, unsigned rmax, const float* d_matrices, unsigned batch, void* stream) {
+  clear_error();
+  ProjArgs a;
+  int ndp;
+  int st = project_setup(vx, vy, vz, px, py, pz, rmax, batch, &a, &ndp);
+  if (st) return st;
+  if (batch && (!d_volumeft || !d_proj || !d_matrices))
+    return set_error(GTOMRLN_ERR_INVALID, "project: NULL device pointer");
+  ArrayFetch f{(const float2*)d_volumeft, a.P, a.P / 2 + 1, a.nvox - 1};
+  return launch_project(f, ndp, d_proj, d_matrices, a, batch, (cudaStream_t)stream);
+}
+
+int gtomrln_project_angles(const float* d_volumeft, int vx, int vy, int vz, float* d_proj, int px,
+                           int py, int pz, const float* h_angles, float supersample, unsigned batch,
+                           void* stream) {
+  clear_error();
+  return with_device_matrices(h_angles, supersample, batch, (cudaStream_t)stream,
+                              [&](const float* d_m) {
+                                return gtomrln_project(d_volumeft, vx, vy, vz, d_proj, px, py, pz,
+                                                       (unsigned)(px / 2), d_m, batch, stream);
+                              });
+}
+
+int gtomrln_project_tex(unsigned long long t_re, unsigned long long t_im, int vx, int vy, int vz,
+                        float* d_proj, int px, int py, int pz, unsigned rmax,
+                        const float* d_matrices, unsigned batch, void* stream) {
+  clear_error();
+  ProjArgs a;
+  int ndp;
+  int st = project_setup(vx, vy, vz, px, py, pz, rmax, batch, &a, &ndp);
+  if (st) return st;
+  if (batch && (!d_proj || !d_matrices))
+    return set_error(GTOMRLN_ERR_INVALID, "project_tex: NULL device pointer");
+  TexFetch f{(cudaTextureObject_t)t_re, (cudaTextureObject_t)t_im};
+  return launch_project(f, ndp, d_proj, d_matrices, a, batch, (cudaStream_t)stream);
+}
+
+int gtomrln_project_tex_angles(unsigned long long t_re, unsigned long long t_im, int vx, int vy,
+                               int vz, float* d_proj, int px, int py, int pz,
+                               const float* h_angles, float supersample, unsigned batch,
+                               void* stream) {
+  clear_error();
+  return with_device_matrices(h_angles, supersample, batch, (cudaStream_t)stream,
+                              [&](const float* d_m) {
+                                return gtomrln_project_tex(t_re, t_im, vx, vy, vz, d_proj, px, py,
+                                                           pz, (unsigned)(px / 2), d_m, batch,
+                                                           stream);
+                              });
+}
+
+}  // extern "C"

@@ -1,0 +1,217 @@
+"""Python mirror of gtom's RELION projector / backprojector / gridding API.
+
+The functions keep the reference's names, argument order and meaning
+(include/Relion.cuh:9-10,34-37 and include/Reconstruction.cuh:16 of
+dtegunov/gtom); C++ overloads become one function that dispatches on the
+kind of its arguments.  Device buffers are CUDA torch tensors (complex64 for
+``tcomplex*``, float32 for ``tfloat*``), host arrays are numpy arrays, dims
+are 3-tuples (x, y, z).  Every call goes through the C ABI of
+libgtomrln.so (gtom_b200/_lib.py) on torch's current stream; a non-zero
+status raises GtomError where the reference would throw.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+
+Dims = Sequence[int]
+
+
+def elements_fft(dims: Dims) -> int:
+    """ElementsFFT (include/Prerequisites.cuh:224): (x/2+1) * y * z."""
+    return (dims[0] // 2 + 1) * dims[1] * max(dims[2], 1)
+
+
+def _stream(stream) -> C.c_void_p:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    if isinstance(stream, torch.cuda.Stream):
+        return C.c_void_p(stream.cuda_stream)
+    return C.c_void_p(int(stream))
+
+
+def _dev_ptr(t, name: str, dtype: torch.dtype | None = None, min_numel: int = 0,
+             optional: bool = False) -> C.c_void_p:
+    if t is None:
+        if optional:
+            return C.c_void_p(0)
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if dtype is not None and t.dtype != dtype:
+        raise ValueError(f"{name} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if t.numel() < min_numel:
+        raise ValueError(f"{name} holds {t.numel()} elements, needs {min_numel}")
+    return C.c_void_p(t.data_ptr())
+
+
+def _host_f32(a, name: str, min_numel: int) -> np.ndarray:
+    arr = np.ascontiguousarray(np.asarray(a if not isinstance(a, torch.Tensor) else a.cpu().numpy(),
+                                          dtype=np.float32))
+    if arr.size < min_numel:
+        raise ValueError(f"{name} holds {arr.size} values, needs {min_numel}")
+    return arr
+
+
+def _is_host(a) -> bool:
+    return isinstance(a, (np.ndarray, list, tuple)) or (isinstance(a, torch.Tensor) and not a.is_cuda)
+
+
+def matrices_from_angles(h_angles, supersample: float = 1.0) -> np.ndarray:
+    """transpose(Matrix3Euler(angles)) * supersample per slice, (batch, 9)
+    column-major float32 (src/Relion/Project.cu:14-16)."""
+    ang = _host_f32(h_angles, "h_angles", 0).reshape(-1, 3)
+    out = np.empty((ang.shape[0], 9), np.float32)
+    _lib.call("gtomrln_matrices_from_angles", ang.ctypes.data, C.c_float(supersample),
+              ang.shape[0], out.ctypes.data)
+    return out
+
+
+def d_rlnProject(volumeft, dimsvolume: Dims, proj: torch.Tensor, dimsproj: Dims, *args,
+                 stream=None) -> None:
+    """Central-slice gather (include/Relion.cuh:34-37).
+
+    Overloads, after ``(volumeft, dimsvolume, d_proj, dimsproj)``:
+      ``(h_angles, supersample, batch)``  — Project.cu:12-23
+      ``(rmax, d_matrices, batch)``       — Project.cu:25-43
+    ``volumeft`` is a complex64 CUDA tensor of the decentred half volume, or
+    a ``(t_volumeRe, t_volumeIm)`` pair of texture object handles
+    (Project.cu:45-87).
+    """
+    if len(args) != 3:
+        raise TypeError("d_rlnProject expects (h_angles, supersample, batch) or "
+                        "(rmax, d_matrices, batch) after dimsproj")
+    vx, vy, vz = (int(v) for v in dimsvolume)
+    px, py, pz = (int(v) for v in dimsproj)
+    batch = int(args[2])
+    e = elements_fft((px, py, pz))
+    pp = _dev_ptr(proj, "d_proj", torch.complex64, e * batch)
+    tex = isinstance(volumeft, tuple)
+    if not tex:
+        vp = _dev_ptr(volumeft, "d_volumeft", torch.complex64, elements_fft((vx, vy, vz)))
+    s = _stream(stream)
+    if _is_host(args[0]):
+        ang = _host_f32(args[0], "h_angles", 3 * batch)
+        if tex:
+            _lib.call("gtomrln_project_tex_angles", int(volumeft[0]), int(volumeft[1]), vx, vy, vz,
+                      pp, px, py, pz, ang.ctypes.data, C.c_float(args[1]), batch, s)
+        else:
+            _lib.call("gtomrln_project_angles", vp, vx, vy, vz, pp, px, py, pz, ang.ctypes.data,
+                      C.c_float(args[1]), batch, s)
+    else:
+        rmax = int(args[0])
+        mp = _dev_ptr(args[1], "d_matrices", torch.float32, 9 * batch)
+        if tex:
+            _lib.call("gtomrln_project_tex", int(volumeft[0]), int(volumeft[1]), vx, vy, vz, pp, px,
+                      py, pz, rmax, mp, batch, s)
+        else:
+            _lib.call("gtomrln_project", vp, vx, vy, vz, pp, px, py, pz, rmax, mp, batch, s)
+
+
+def d_rlnBackproject(volumeft, volumeweights, dimsvolume: Dims, projft, projweights,
+                     dimsproj: Dims, rmax: int, *args, stream=None) -> None:
+    """Trilinear scatter-insert, accumulating in place (include/Relion.cuh:9-10).
+
+    Overloads, after ``(..., dimsproj, rmax)``:
+      ``(d_matrices, d_ivolume, magnification, ewaldradiussuper,
+         outputdecentered, squareinterpweights, batch)``     — Backproject.cu:48-124
+      ``(h_angles, h_ivolume, magnification, ewaldradius, supersample,
+         outputdecentered, squareinterpweights, batch)``     — Backproject.cu:23-46
+    ``magnification`` is the float4 (x, y, z, w) of the 2x2 matrix columns.
+    """
+    vx, vy, vz = (int(v) for v in dimsvolume)
+    px, py, pz = (int(v) for v in dimsproj)
+    nvol = elements_fft((vx, vy, vz))
+    s = _stream(stream)
+    if len(args) == 7:
+        mats, ivol, mag, ewald, dec, sq, batch = args
+        batch = int(batch)
+        e = elements_fft((px, py, pz))
+        _lib.call("gtomrln_backproject",
+                  _dev_ptr(volumeft, "d_volumeft", torch.complex64, nvol, optional=True),
+                  _dev_ptr(volumeweights, "d_volumeweights", torch.float32, nvol, optional=True),
+                  vx, vy, vz,
+                  _dev_ptr(projft, "d_projft", torch.complex64, e * batch, optional=True),
+                  _dev_ptr(projweights, "d_projweights", torch.float32, e * batch, optional=True),
+                  px, py, pz, int(rmax),
+                  _dev_ptr(mats, "d_matrices", torch.float32, 9 * batch),
+                  _dev_ptr(ivol, "d_ivolume", torch.int32, batch, optional=True),
+                  *(C.c_float(float(m)) for m in mag), C.c_float(float(ewald)), int(bool(dec)),
+                  int(bool(sq)), batch, s)
+    elif len(args) == 8:
+        ang, ivol, mag, ewald, ss, dec, sq, batch = args
+        batch = int(batch)
+        e = elements_fft((px, py, pz))
+        ang = _host_f32(ang, "h_angles", 3 * batch)
+        iv = None
+        if ivol is not None:
+            iv = np.ascontiguousarray(np.asarray(ivol, dtype=np.int32))
+            if iv.size < batch:
+                raise ValueError("h_ivolume shorter than batch")
+        _lib.call("gtomrln_backproject_angles",
+                  _dev_ptr(volumeft, "d_volumeft", torch.complex64, nvol, optional=True),
+                  _dev_ptr(volumeweights, "d_volumeweights", torch.float32, nvol, optional=True),
+                  vx, vy, vz,
+                  _dev_ptr(projft, "d_projft", torch.complex64, e * batch, optional=True),
+                  _dev_ptr(projweights, "d_projweights", torch.float32, e * batch, optional=True),
+                  px, py, pz, int(rmax), ang.ctypes.data,
+                  C.c_void_p(iv.ctypes.data if iv is not None else 0),
+                  *(C.c_float(float(m)) for m in mag), C.c_float(float(ewald)),
+                  C.c_float(float(ss)), int(bool(dec)), int(bool(sq)), batch, s)
+    else:
+        raise TypeError("d_rlnBackproject: unexpected number of arguments")
+
+
+def d_ReconstructGridding(dataft, weight, reconstructed, dimsori: Dims, dimspadded: Dims,
+                          paddingfactor: int = 2, pre_planforw: int = 0, pre_planback: int = 0,
+                          iterations: int = 10, blobradius: float = 1.9, bloborder: int = 0,
+                          blobalpha: float = 15.0, stream=None) -> None:
+    """Gridding-corrected reconstruction (include/Reconstruction.cuh:16)."""
+    ox, oy, oz = (int(v) for v in dimsori)
+    qx, qy, qz = (int(v) for v in dimspadded)
+    npad = elements_fft((qx, qy, qz))
+    _lib.call("gtomrln_reconstruct_gridding",
+              _dev_ptr(dataft, "d_dataft", torch.complex64, npad),
+              _dev_ptr(weight, "d_weight", torch.float32, npad),
+              _dev_ptr(reconstructed, "d_reconstructed", torch.float32, ox * oy * oz),
+              ox, oy, oz, qx, qy, qz, int(paddingfactor), int(pre_planforw or 0),
+              int(pre_planback or 0), int(iterations), float(blobradius), int(bloborder),
+              float(blobalpha), _stream(stream))
+
+
+def reconstruct_gridding_tol(dataft, weight, reconstructed, dimsori: Dims, dimspadded: Dims,
+                             paddingfactor: int = 2, max_iterations: int = 100,
+                             tolerance: float = 1e-4, blobradius: float = 1.9,
+                             bloborder: int = 0, blobalpha: float = 15.0,
+                             stream=None) -> tuple[int, float]:
+    """d_ReconstructGridding with a convergence test on the relative change of
+    the gridding weights; returns (iterations run, last relative change)."""
+    ox, oy, oz = (int(v) for v in dimsori)
+    qx, qy, qz = (int(v) for v in dimspadded)
+    npad = elements_fft((qx, qy, qz))
+    it = C.c_int(0)
+    ch = C.c_double(0)
+    _lib.call("gtomrln_reconstruct_gridding_tol",
+              _dev_ptr(dataft, "d_dataft", torch.complex64, npad),
+              _dev_ptr(weight, "d_weight", torch.float32, npad),
+              _dev_ptr(reconstructed, "d_reconstructed", torch.float32, ox * oy * oz),
+              ox, oy, oz, qx, qy, qz, int(paddingfactor), int(max_iterations), float(tolerance),
+              float(blobradius), int(bloborder), float(blobalpha), C.byref(it), C.byref(ch),
+              _stream(stream))
+    return it.value, ch.value
+
+
+def kaiser_bessel_table(radius: float, alpha: float, order: int = 0,
+                        nsamples: int = 10000) -> np.ndarray:
+    """The normalised blob table of the gridding correction."""
+    out = np.empty(nsamples, np.float32)
+    _lib.call("gtomrln_kaiser_bessel_table", float(radius), float(alpha), int(order),
+              int(nsamples), out.ctypes.data)
+    return out

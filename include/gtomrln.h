@@ -1,0 +1,200 @@
+/*
+ * gtomrln.h — C ABI of the B200 RELION-style Fourier projector, backprojector
+ * and gridding reconstructor.
+ *
+ * Every entry point is a drop-in for one overload of gtom's C++ API
+ * (namespace gtom, include/Relion.cuh and include/Reconstruction.cuh of
+ * dtegunov/gtom); the reference declaration it replaces is cited above each
+ * one.  The arguments keep the reference's meaning and order; C types replace
+ * the C++ ones:
+ *
+ *   tcomplex*      -> float*  interleaved (re, im) pairs, 8-byte aligned
+ *   tfloat*        -> float*
+ *   int3 dims      -> three ints (x, y, z); a 2D slice has z == 1
+ *   glm::mat3*     -> float*  9 floats per matrix, column-major (glm layout)
+ *   tfloat3* angles-> float*  3 floats per slice: rot, tilt, psi in radians
+ *   float4 mag     -> four floats (the columns of the 2x2 magnification)
+ *   cudaTex        -> unsigned long long (cudaTextureObject_t)
+ *   cufftHandle    -> int (0 = let the library plan)
+ *
+ * One argument is added at the end of each call: a cudaStream_t passed as
+ * void* (NULL = the legacy default stream).  The reference runs on the
+ * default stream and returns only after its work is done; the entry points
+ * here enqueue on the given stream and return once the work is enqueued, so
+ * a caller that reads results on the host synchronises the stream first.
+ *
+ * Errors: every entry point returns GTOMRLN_OK (0) or a negative status and
+ * never throws or terminates; gtomrln_last_error() returns the calling
+ * thread's last message.  Where the reference calls `throw;` (which
+ * terminates the process) on inconsistent dimensions, these return
+ * GTOMRLN_ERR_INVALID.
+ *
+ * Memory: d_* pointers are caller-owned device buffers, h_* are caller-owned
+ * host arrays read during the call.  Backprojection accumulates into
+ * d_volumeft / d_volumeweights in place (the caller zeroes them first).
+ */
+#ifndef GTOMRLN_H
+#define GTOMRLN_H
+
+#if defined(__GNUC__)
+#define GTOMRLN_API __attribute__((visibility("default")))
+#else
+#define GTOMRLN_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GTOMRLN_OK 0
+#define GTOMRLN_ERR_INVALID -1 /* inconsistent dimensions or arguments */
+#define GTOMRLN_ERR_CUDA -2    /* a CUDA runtime call or launch failed */
+#define GTOMRLN_ERR_CUFFT -3   /* cuFFT planning or execution failed */
+#define GTOMRLN_ERR_ALLOC -4   /* device memory could not be allocated */
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+GTOMRLN_API int gtomrln_version(void);
+
+/* Message of the calling thread's last failed call ("" if none). */
+GTOMRLN_API const char* gtomrln_last_error(void);
+
+/* Release cached cuFFT plans and the library's memory pool on the current
+ * device.  Not required; the caches are also released at process exit. */
+GTOMRLN_API int gtomrln_release_caches(void);
+
+/* Host helper: M_b = transpose(Matrix3Euler(angles_b)) * supersample, the
+ * matrices the h_angles overloads build (src/Relion/Project.cu:14-16,
+ * src/Helpers/Euler.cu:39-68).  Writes 9 * batch floats, column-major. */
+GTOMRLN_API int gtomrln_matrices_from_angles(const float* h_angles, float supersample, unsigned batch,
+                                 float* h_matrices);
+
+/* ---------------------------------------------------------------------------
+ * Projector: trilinear central-slice gather from a decentred half-complex
+ * volume of (dimsvolume.x/2+1) x dimsvolume.y x dimsvolume.z.  Output slices
+ * are half-complex (dimsproj.x/2+1) x dimsproj.y [x dimsproj.z], one after
+ * another; elements with x^2+y^2 > rmax^2 are written as 0.
+ * ------------------------------------------------------------------------- */
+
+/* gtom::d_rlnProject(tcomplex* d_volumeft, int3 dimsvolume, tcomplex* d_proj,
+ *     int3 dimsproj, uint rmax, glm::mat3* d_matrices, uint batch)
+ * include/Relion.cuh:35, src/Relion/Project.cu:25-43 */
+GTOMRLN_API int gtomrln_project(const float* d_volumeft, int vx, int vy, int vz, float* d_proj, int px,
+                    int py, int pz, unsigned rmax, const float* d_matrices, unsigned batch,
+                    void* stream);
+
+/* gtom::d_rlnProject(tcomplex* d_volumeft, int3 dimsvolume, tcomplex* d_proj,
+ *     int3 dimsproj, tfloat3* h_angles, float supersample, uint batch)
+ * include/Relion.cuh:34, src/Relion/Project.cu:12-23 (rmax = dimsproj.x/2) */
+GTOMRLN_API int gtomrln_project_angles(const float* d_volumeft, int vx, int vy, int vz, float* d_proj,
+                           int px, int py, int pz, const float* h_angles, float supersample,
+                           unsigned batch, void* stream);
+
+/* gtom::d_rlnProject(cudaTex t_volumeRe, cudaTex t_volumeIm, int3 dimsvolume,
+ *     tcomplex* d_proj, int3 dimsproj, uint rmax, glm::mat3* d_matrices, uint batch)
+ * include/Relion.cuh:37, src/Relion/Project.cu:58-87.  The textures are read
+ * at the same integer coordinates as the reference, so their filter and
+ * address modes (set by the caller) act identically. */
+GTOMRLN_API int gtomrln_project_tex(unsigned long long t_volumeRe, unsigned long long t_volumeIm, int vx,
+                        int vy, int vz, float* d_proj, int px, int py, int pz, unsigned rmax,
+                        const float* d_matrices, unsigned batch, void* stream);
+
+/* gtom::d_rlnProject(cudaTex t_volumeRe, cudaTex t_volumeIm, int3 dimsvolume,
+ *     tcomplex* d_proj, int3 dimsproj, tfloat3* h_angles, float supersample, uint batch)
+ * include/Relion.cuh:36, src/Relion/Project.cu:45-56 */
+GTOMRLN_API int gtomrln_project_tex_angles(unsigned long long t_volumeRe, unsigned long long t_volumeIm,
+                               int vx, int vy, int vz, float* d_proj, int px, int py, int pz,
+                               const float* h_angles, float supersample, unsigned batch,
+                               void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Backprojector: trilinear scatter-insert of half-complex slices and their
+ * per-pixel weights (CTF-weighted data and CTF^2, applied by the caller) into
+ * a half-complex volume and a weight volume, accumulated in place.
+ * d_projft == NULL inserts (1, 0); d_projweights == NULL inserts weight 1;
+ * d_volumeft or d_volumeweights == NULL skips that output.  d_ivolume
+ * (optional) selects a target volume per slice.  The trilinear weights are
+ * rounded through binary16 exactly as the reference does
+ * (src/Relion/Backproject.cu:224-238).
+ * ------------------------------------------------------------------------- */
+
+/* gtom::d_rlnBackproject(tcomplex* d_volumeft, tfloat* d_volumeweights,
+ *     int3 dimsvolume, tcomplex* d_projft, tfloat* d_projweights, int3 dimsproj,
+ *     uint rmax, glm::mat3* d_matrices, int* d_ivolume, float4 magnification,
+ *     float ewaldradiussuper, bool outputdecentered, bool squareinterpweights,
+ *     uint batch)
+ * include/Relion.cuh:9, src/Relion/Backproject.cu:48-124 */
+GTOMRLN_API int gtomrln_backproject(float* d_volumeft, float* d_volumeweights, int vx, int vy, int vz,
+                        const float* d_projft, const float* d_projweights, int px, int py,
+                        int pz, unsigned rmax, const float* d_matrices, const int* d_ivolume,
+                        float mag_x, float mag_y, float mag_z, float mag_w,
+                        float ewaldradiussuper, int outputdecentered, int squareinterpweights,
+                        unsigned batch, void* stream);
+
+/* gtom::d_rlnBackproject(tcomplex* d_volumeft, tfloat* d_volumeweights,
+ *     int3 dimsvolume, tcomplex* d_projft, tfloat* d_projweights, int3 dimsproj,
+ *     uint rmax, tfloat3* h_angles, int* h_ivolume, float4 magnification,
+ *     float ewaldradius, float supersample, bool outputdecentered,
+ *     bool squareinterpweights, uint batch)
+ * include/Relion.cuh:10, src/Relion/Backproject.cu:23-46 */
+GTOMRLN_API int gtomrln_backproject_angles(float* d_volumeft, float* d_volumeweights, int vx, int vy,
+                               int vz, const float* d_projft, const float* d_projweights,
+                               int px, int py, int pz, unsigned rmax, const float* h_angles,
+                               const int* h_ivolume, float mag_x, float mag_y, float mag_z,
+                               float mag_w, float ewaldradius, float supersample,
+                               int outputdecentered, int squareinterpweights, unsigned batch,
+                               void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Gridding reconstructor: RELION-style iterative gridding-weight correction
+ * with a Kaiser-Bessel blob, then the inverse FFT, crop and sinc^2 correction.
+ * d_dataft / d_weight are CENTRED half-complex volumes of dimspadded (the
+ * output of a centred backprojection); the working grid is
+ * P = dimsori.x * paddingfactor.  d_reconstructed receives the real ori^3
+ * map, centred.  Inputs are not modified.  dimspadded.x must be at least
+ * P + 1: with a smaller box the reference reads outside its input (its
+ * DecenterKernel, RecFourier.cu:264-285); here such reads are not made and
+ * the masked values they would feed count as 0.
+ * ------------------------------------------------------------------------- */
+
+/* gtom::d_ReconstructGridding(tcomplex* d_dataft, tfloat* d_weight,
+ *     tfloat* d_reconstructed, int3 dimsori, int3 dimspadded, int paddingfactor = 2,
+ *     cufftHandle pre_planforw = NULL, cufftHandle pre_planback = NULL,
+ *     int iterations = 10, double blobradius = 1.9, int bloborder = 0,
+ *     double blobalpha = 15)
+ * include/Reconstruction.cuh:16, src/Reconstruction/RecFourier.cu:98-241.
+ * pre_planforw / pre_planback: 0 lets the library use its own cached plans
+ * for the P^3 R2C / C2R transforms; otherwise they must be such plans. */
+GTOMRLN_API int gtomrln_reconstruct_gridding(const float* d_dataft, const float* d_weight,
+                                 float* d_reconstructed, int ox, int oy, int oz, int padx,
+                                 int pady, int padz, int paddingfactor, int pre_planforw,
+                                 int pre_planback, int iterations, double blobradius,
+                                 int bloborder, double blobalpha, void* stream);
+
+/* Extension (no reference counterpart): the same reconstruction with a
+ * convergence test.  Iterates at most max_iterations times and stops early
+ * once the relative L2 change of the corrected weights Fweight * Fnewweight
+ * between two iterations, ||Fw (Fnw' - Fnw)|| / ||Fw Fnw||, is <= tolerance
+ * (voxels that received no weight do not count; their Fnewweight only grows
+ * towards the 1e20 clamp).  tolerance <= 0 disables the test, which then
+ * equals gtomrln_reconstruct_gridding).  *iterations_done and
+ * *final_change (either may be NULL) receive the count and the last
+ * relative change.  Synchronises the stream once per iteration. */
+GTOMRLN_API int gtomrln_reconstruct_gridding_tol(const float* d_dataft, const float* d_weight,
+                                     float* d_reconstructed, int ox, int oy, int oz, int padx,
+                                     int pady, int padz, int paddingfactor, int max_iterations,
+                                     double tolerance, double blobradius, int bloborder,
+                                     double blobalpha, int* iterations_done,
+                                     double* final_change, void* stream);
+
+/* The normalised Kaiser-Bessel table the gridding uses: nsamples values of
+ * kaiser_Fourier_value(i * 0.5 / nsamples, radius, alpha, order) divided by
+ * the value at 0 (src/Helpers/KaiserBessel.cpp:357-376,
+ * src/Reconstruction/RecFourier.cu:104-116).  order must be 0 or 2. */
+GTOMRLN_API int gtomrln_kaiser_bessel_table(double radius, double alpha, int order, int nsamples,
+                                float* h_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GTOMRLN_H */

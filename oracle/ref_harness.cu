@@ -1,0 +1,85 @@
+// C entry points over the reference's own CUDA implementation of the
+// projector / backprojector / gridding reconstructor, compiled from the
+// reference sources by oracle/Makefile into oracle/_ref/libgtomref.so.
+//
+// TEST INFRASTRUCTURE ONLY: used to pin the CPU oracle and to generate the
+// golden fixtures in tests/golden/.  The product library never links it.
+//
+// Each wrapper calls the reference overload named beside it unchanged and
+// returns cudaGetLastError() after a device synchronise.
+#include "Prerequisites.cuh"
+#include "Angles.cuh"
+#include "Helper.cuh"
+#include "Relion.cuh"
+#include "Reconstruction.cuh"
+
+using namespace gtom;
+
+extern "C" {
+
+// include/Relion.cuh:35 -> src/Relion/Project.cu:25-43
+int ref_project(float* d_volumeft, int P, float* d_proj, int n, int ndims, int rmax,
+                float* d_matrices, int batch) {
+  int3 dv = toInt3(P, P, P);
+  int3 dp = toInt3(n, n, ndims == 3 ? n : 1);
+  d_rlnProject((tcomplex*)d_volumeft, dv, (tcomplex*)d_proj, dp, (uint)rmax,
+               (glm::mat3*)d_matrices, (uint)batch);
+  cudaDeviceSynchronize();
+  return (int)cudaGetLastError();
+}
+
+// include/Relion.cuh:34 -> src/Relion/Project.cu:12-23
+int ref_project_angles(float* d_volumeft, int P, float* d_proj, int n, int ndims,
+                       float* h_angles, float supersample, int batch) {
+  int3 dv = toInt3(P, P, P);
+  int3 dp = toInt3(n, n, ndims == 3 ? n : 1);
+  d_rlnProject((tcomplex*)d_volumeft, dv, (tcomplex*)d_proj, dp, (tfloat3*)h_angles,
+               supersample, (uint)batch);
+  cudaDeviceSynchronize();
+  return (int)cudaGetLastError();
+}
+
+// include/Relion.cuh:9 -> src/Relion/Backproject.cu:48-124
+int ref_backproject(float* d_volumeft, float* d_volumeweights, int P, float* d_projft,
+                    float* d_projweights, int n, int ndims, int rmax, float* d_matrices,
+                    int* d_ivolume, float mx, float my, float mz, float mw,
+                    float ewaldradiussuper, int outputdecentered, int squareinterpweights,
+                    int batch) {
+  int3 dv = toInt3(P, P, P);
+  int3 dp = toInt3(n, n, ndims == 3 ? n : 1);
+  d_rlnBackproject((tcomplex*)d_volumeft, d_volumeweights, dv, (tcomplex*)d_projft,
+                   d_projweights, dp, (uint)rmax, (glm::mat3*)d_matrices, d_ivolume,
+                   make_float4(mx, my, mz, mw), ewaldradiussuper, outputdecentered != 0,
+                   squareinterpweights != 0, (uint)batch);
+  cudaDeviceSynchronize();
+  return (int)cudaGetLastError();
+}
+
+// include/Relion.cuh:10 -> src/Relion/Backproject.cu:23-46
+int ref_backproject_angles(float* d_volumeft, float* d_volumeweights, int P, float* d_projft,
+                           float* d_projweights, int n, int ndims, int rmax, float* h_angles,
+                           int* h_ivolume, float mx, float my, float mz, float mw,
+                           float ewaldradius, float supersample, int outputdecentered,
+                           int squareinterpweights, int batch) {
+  int3 dv = toInt3(P, P, P);
+  int3 dp = toInt3(n, n, ndims == 3 ? n : 1);
+  d_rlnBackproject((tcomplex*)d_volumeft, d_volumeweights, dv, (tcomplex*)d_projft,
+                   d_projweights, dp, (uint)rmax, (tfloat3*)h_angles, h_ivolume,
+                   make_float4(mx, my, mz, mw), ewaldradius, supersample,
+                   outputdecentered != 0, squareinterpweights != 0, (uint)batch);
+  cudaDeviceSynchronize();
+  return (int)cudaGetLastError();
+}
+
+// include/Reconstruction.cuh:16 -> src/Reconstruction/RecFourier.cu:98-241
+int ref_reconstruct_gridding(float* d_dataft, float* d_weight, float* d_reconstructed, int ori,
+                             int padded, int paddingfactor, int iterations, double blobradius,
+                             int bloborder, double blobalpha) {
+  d_ReconstructGridding((tcomplex*)d_dataft, d_weight, d_reconstructed, toInt3(ori, ori, ori),
+                        toInt3(padded, padded, padded), paddingfactor, NULL, NULL, iterations,
+                        blobradius, bloborder, blobalpha);
+  cudaDeviceSynchronize();
+  return (int)cudaGetLastError();
+}
+
+}  // extern "C"

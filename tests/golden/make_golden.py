@@ -1,0 +1,151 @@
+"""Generates the golden fixtures of tests/golden/ from the reference itself.
+
+Runs the reference's own CUDA implementation (oracle/_ref/libgtomref.so,
+compiled from the reference sources by `make -C oracle ref`) on seeded
+inputs and stores inputs and outputs as compressed .npz files:
+
+    python tests/golden/make_golden.py [outdir]      # needs a GPU
+
+The fixtures pin the CPU oracle (tests/test_oracle_golden.py) and the CUDA
+library (tests/test_parity_gpu.py) to the reference's results.  Buffers
+handed to the reference projector are over-allocated by 64 elements because
+its x1 = P/2+1 read (src/Relion/Project.cu:155) can touch one element past
+the end of the volume; the extra elements are zero and never reach a result
+that the fixtures keep.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import sys
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from oracle import oracle as O  # noqa: E402
+from tests.synthdata import blob_volume_ft, random_angles  # noqa: E402
+
+REF = C.CDLL(str(O.REF_PATH))
+_p, _i, _f, _d = C.c_void_p, C.c_int, C.c_float, C.c_double
+REF.ref_project.argtypes = [_p, _i, _p, _i, _i, _i, _p, _i]
+REF.ref_project_angles.argtypes = [_p, _i, _p, _i, _i, _p, _f, _i]
+REF.ref_backproject.argtypes = [_p, _p, _i, _p, _p, _i, _i, _i, _p, _p, _f, _f, _f, _f, _f, _i, _i, _i]
+REF.ref_backproject_angles.argtypes = [_p, _p, _i, _p, _p, _i, _i, _i, _p, _p, _f, _f, _f, _f, _f,
+                                       _f, _i, _i, _i]
+REF.ref_reconstruct_gridding.argtypes = [_p, _p, _p, _i, _i, _i, _i, _d, _i, _d]
+
+
+def _ok(rc: int, what: str) -> None:
+    if rc != 0:
+        raise RuntimeError(f"{what}: CUDA error {rc}")
+
+
+def dev(a: np.ndarray, extra: int = 0) -> torch.Tensor:
+    flat = torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).reshape(-1).copy())
+    t = torch.zeros(flat.numel() + extra * 8, dtype=torch.uint8, device="cuda")
+    t[: flat.numel()] = flat.cuda()
+    return t
+
+
+def host(t: torch.Tensor, dtype, count: int) -> np.ndarray:
+    return t.cpu().numpy().view(dtype)[:count].copy()
+
+
+def gen_project(out: Path, rng) -> None:
+    for name, n, ndims, batch, rmax in (("project_2d", 16, 2, 24, 8), ("project_2d_rmax", 16, 2, 12, 5),
+                                        ("project_3d", 8, 3, 3, 4)):
+        P = 2 * n
+        vol = blob_volume_ft(rng, n, P, 12)
+        vol = (vol + (rng.normal(size=vol.shape) + 1j * rng.normal(size=vol.shape)).astype(np.complex64) * 0.05 * np.abs(vol).max()).astype(np.complex64)
+        ang = random_angles(rng, batch)
+        mats = O.matrices_f64(ang, 2.0).astype(np.float32)
+        e = O.elements_fft(n, ndims)
+        dv = dev(vol, extra=64)
+        dm = dev(mats)
+        dp = torch.zeros(e * batch * 8, dtype=torch.uint8, device="cuda")
+        _ok(REF.ref_project(dv.data_ptr(), P, dp.data_ptr(), n, ndims, rmax, dm.data_ptr(), batch), name)
+        proj = host(dp, np.complex64, e * batch).reshape(batch, e)
+        dp2 = torch.zeros_like(dp)
+        _ok(REF.ref_project_angles(dv.data_ptr(), P, dp2.data_ptr(), n, ndims, ang.ctypes.data, 2.0, batch),
+            name + "_angles")
+        proj_ang = host(dp2, np.complex64, e * batch).reshape(batch, e)
+        np.savez_compressed(out / f"{name}.npz", volume=vol, P=P, n=n, ndims=ndims, rmax=rmax,
+                            angles=ang, matrices=mats, proj=proj, proj_angles=proj_ang)
+        print(name, np.abs(proj).max())
+
+
+def gen_backproject(out: Path, rng) -> None:
+    cases = (
+        # name, n, ndims, P, batch, decentred, square, mag, ewaldradius(super), nvol
+        ("bp_dec", 16, 2, 32, 40, True, False, (1, 0, 0, 1), 0.0, 1),
+        ("bp_cen_sq_mag", 16, 2, 33, 40, False, True, (1.03, 0.02, -0.01, 0.97), 40.0, 2),
+        ("bp_3d", 8, 3, 16, 3, True, False, (1, 0, 0, 1), 0.0, 1),
+    )
+    for name, n, ndims, P, batch, dec, sq, mag, ewald, nvol in cases:
+        ang = random_angles(rng, batch)
+        mats = O.matrices_f64(ang, 2.0).astype(np.float32)
+        e = O.elements_fft(n, ndims)
+        projft = (rng.normal(size=(batch, e)) + 1j * rng.normal(size=(batch, e))).astype(np.complex64)
+        projw = rng.uniform(0.1, 1.0, size=(batch, e)).astype(np.float32)
+        ivol = rng.integers(0, nvol, size=batch).astype(np.int32) if nvol > 1 else None
+        nv = (P // 2 + 1) * P * P
+        dvf = torch.zeros(nv * nvol * 8, dtype=torch.uint8, device="cuda")
+        dvw = torch.zeros(nv * nvol * 4, dtype=torch.uint8, device="cuda")
+        dpf, dpw, dm = dev(projft), dev(projw), dev(mats)
+        div = dev(ivol) if ivol is not None else None
+        rmax = n // 2
+        _ok(REF.ref_backproject(dvf.data_ptr(), dvw.data_ptr(), P, dpf.data_ptr(), dpw.data_ptr(), n, ndims,
+                                rmax, dm.data_ptr(), div.data_ptr() if div is not None else None,
+                                *mag, ewald, int(dec), int(sq), batch), name)
+        volft = host(dvf, np.complex64, nv * nvol)
+        volw = host(dvw, np.float32, nv * nvol)
+        np.savez_compressed(out / f"{name}.npz", P=P, n=n, ndims=ndims, rmax=rmax, angles=ang, matrices=mats,
+                            projft=projft, projw=projw, ivolume=ivol if ivol is not None else np.zeros(0, np.int32),
+                            nvol=nvol, mag=np.array(mag, np.float32), ewald=ewald, decentered=dec,
+                            square=sq, volft=volft, volw=volw)
+        print(name, np.abs(volft).max(), volw.max())
+
+
+def gen_gridding(out: Path, rng) -> None:
+    for name, ori, pad, nproj, iters in (("grid_it10", 16, 2, 300, 10), ("grid_it0", 16, 2, 300, 0),
+                                         ("grid_it3_pad3", 12, 3, 200, 3)):
+        P = ori * pad
+        dpad = P + 1
+        vol = blob_volume_ft(rng, ori, P, 10)
+        ang = random_angles(rng, nproj)
+        mats = O.matrices_f64(ang, float(pad)).astype(np.float32)
+        e = O.elements_fft(ori)
+        dv = dev(vol, extra=64)
+        dm = dev(mats)
+        dp = torch.zeros(e * nproj * 8, dtype=torch.uint8, device="cuda")
+        _ok(REF.ref_project(dv.data_ptr(), P, dp.data_ptr(), ori, 2, ori // 2, dm.data_ptr(), nproj), name)
+        nv = (dpad // 2 + 1) * dpad * dpad
+        dvf = torch.zeros(nv * 8, dtype=torch.uint8, device="cuda")
+        dvw = torch.zeros(nv * 4, dtype=torch.uint8, device="cuda")
+        _ok(REF.ref_backproject(dvf.data_ptr(), dvw.data_ptr(), dpad, dp.data_ptr(), None, ori, 2, ori // 2,
+                                dm.data_ptr(), None, 1, 0, 0, 1, 0.0, 0, 0, nproj), name + " bp")
+        dataft = host(dvf, np.complex64, nv)
+        weight = host(dvw, np.float32, nv)
+        drec = torch.zeros(ori ** 3 * 4, dtype=torch.uint8, device="cuda")
+        _ok(REF.ref_reconstruct_gridding(dvf.data_ptr(), dvw.data_ptr(), drec.data_ptr(), ori, dpad, pad,
+                                         iters, 1.9, 0, 15.0), name + " grid")
+        rec = host(drec, np.float32, ori ** 3).reshape(ori, ori, ori)
+        np.savez_compressed(out / f"{name}.npz", ori=ori, pad=pad, dimspadded=dpad, iterations=iters,
+                            dataft=dataft, weight=weight, reconstructed=rec)
+        print(name, np.abs(rec).max())
+
+
+def main() -> None:
+    out = Path(sys.argv[1]) if len(sys.argv) > 1 else Path(__file__).resolve().parent
+    out.mkdir(parents=True, exist_ok=True)
+    rng = np.random.default_rng(20261203)
+    gen_project(out, rng)
+    gen_backproject(out, rng)
+    gen_gridding(out, rng)
+
+
+if __name__ == "__main__":
+    main()
