@@ -11,4 +11,5 @@ from .relion import (  # noqa: F401
     kaiser_bessel_table,
     matrices_from_angles,
     reconstruct_gridding_tol,
+    set_path,
 )

@@ -46,6 +46,7 @@ SIGNATURES: dict[str, list] = {
     "gtomrln_version": [],
     "gtomrln_last_error": [],
     "gtomrln_release_caches": [],
+    "gtomrln_set_path": [_i, _i],
     "gtomrln_matrices_from_angles": [_p, _f, _u, _p],
     "gtomrln_project": [_p, _i, _i, _i, _p, _i, _i, _i, _u, _p, _u, _p],
     "gtomrln_project_angles": [_p, _i, _i, _i, _p, _i, _i, _i, _p, _f, _u, _p],

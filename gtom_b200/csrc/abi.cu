@@ -1,6 +1,7 @@
 // Library-wide pieces of the C ABI: error state, version, the device memory
 // pool for per-call scratch, and the host matrix builder.
 #include <cmath>
+#include <atomic>
 #include <cstdarg>
 #include <mutex>
 #include <vector>
@@ -91,6 +92,10 @@ int pool_free(void* ptr, cudaStream_t stream) {
 
 int release_gridding_plans();  // gridding.cu
 
+static std::atomic<int> g_path[2] = {{GTOMRLN_PATH_AUTO}, {GTOMRLN_PATH_AUTO}};
+
+int path_choice(int op) { return (op == 0 || op == 1) ? g_path[op].load() : GTOMRLN_PATH_AUTO; }
+
 }  // namespace gtomrln
 
 using namespace gtomrln;
@@ -111,6 +116,15 @@ int gtomrln_release_caches(void) {
     GTOMRLN_CUDA_TRY(cudaDeviceSynchronize());
     GTOMRLN_CUDA_TRY(cudaMemPoolTrimTo(g_pools[dev], 0));
   }
+  return GTOMRLN_OK;
+}
+
+int gtomrln_set_path(int op, int path) {
+  clear_error();
+  if ((op != GTOMRLN_OP_PROJECT && op != GTOMRLN_OP_BACKPROJECT) || path < GTOMRLN_PATH_AUTO ||
+      path > GTOMRLN_PATH_BRICK)
+    return set_error(GTOMRLN_ERR_INVALID, "set_path: unknown op %d or path %d", op, path);
+  g_path[op].store(path);
   return GTOMRLN_OK;
 }
 

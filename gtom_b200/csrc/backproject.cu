@@ -8,6 +8,10 @@
 // atomics; the weight as one scalar reduction.  Geometry, binary16 rounding
 // of the trilinear weights, Friedel mirroring, the second insertion on the
 // x = 0 plane and the clamps are the reference's, step for step.
+#include <algorithm>
+#include <cmath>
+
+#include "brick.cuh"
 #include "common.cuh"
 
 namespace gtomrln {
@@ -129,6 +133,180 @@ backproject_direct_kernel(float2* __restrict__ volft, float* __restrict__ volw,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Brick-major backprojector: insertion privatised per shared-memory brick.
+// A work item owns one 16^3 brick of the (signed-coordinate) volume as three
+// FP32 accumulators (re, im, weight) in shared memory.  Each warp takes one
+// of the item's slices and walks the pixels whose sample, or whose Friedel
+// mate's sample, lies within one voxel of the brick; per pixel it evaluates
+// the reference's eight binary16-rounded trilinear weights, Friedel mirroring
+// and the second insertion on the x = 0 plane, and adds the targets that
+// fall inside the brick to shared memory.  At the end of the item the brick
+// is added to the volume once: with plain read-add-write when the item is
+// the brick's only one and the voxel has no alias (decentred y or z = +-V/2
+// share storage), otherwise with vector L2 reductions.
+// ---------------------------------------------------------------------------
+constexpr int kBrickThreads = 256;
+constexpr int kBrickEdge = 16;
+constexpr unsigned kBrickMinBatch = 32;
+int brick_chunk_default();  // project.cu
+
+template <bool DECENTERED, bool SQUARE>
+__global__ void __launch_bounds__(kBrickThreads)
+backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
+                         const float2* __restrict__ projft, const float* __restrict__ projw,
+                         const float* __restrict__ mats, BpArgs a, BrickGrid g,
+                         const BrickItem* __restrict__ items, int nitems,
+                         const int* __restrict__ lists, int* __restrict__ counter) {
+  extern __shared__ float acc[];
+  __shared__ int item_s;
+  const int B = g.B, B3 = g.B * g.B * g.B;
+  float* are = acc;
+  float* aim = acc + B3;
+  float* aw = acc + 2 * B3;
+  const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int V = a.P;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) item_s = atomicAdd(counter, 1);
+    for (int k = threadIdx.x; k < 3 * B3; k += blockDim.x) acc[k] = 0.f;
+    __syncthreads();
+    const int w = item_s;
+    if (w >= nitems) break;
+    const BrickItem it = items[w];
+    const int3 o = brick_origin(g, it.brick);
+    float3 qlo, qhi;
+    brick_box(g, it.brick, qlo, qhi);
+
+    for (int j = warp; j < it.count; j += nwarps) {
+      const int slice = __ldg(lists + it.offset + j);
+      float m[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
+      for_each_footprint_pixel(m, qlo, qhi, a.rmax2 - 1, [&](int u, int v) {
+        // pixel (u, v): r^2 < rmax^2 and not (u == 0 && v < 0) by construction
+        int idy = v >= 0 ? v : v + a.n;
+        int64_t id = a.elements * slice + (int64_t)idy * a.dimft + u;
+        float3 pos = mat_apply(m, (float)u, (float)v, 0.f);
+        int x0 = (short)floorf(pos.x + 1e-5f);
+        int y0 = (short)floorf(pos.y);
+        int z0 = (short)floorf(pos.z);
+        float fx = pos.x - (float)x0, fy = pos.y - (float)y0, fz = pos.z - (float)z0;
+        float c0 = 1.f - fz, c1 = fz;
+        float c00 = half_round((1.f - fy) * c0), c10 = half_round(fy * c0);
+        float c01 = half_round((1.f - fy) * c1), c11 = half_round(fy * c1);
+        float wt[8];
+        wt[0] = half_round((1.f - fx) * c00); wt[1] = half_round(fx * c00);
+        wt[2] = half_round((1.f - fx) * c10); wt[3] = half_round(fx * c10);
+        wt[4] = half_round((1.f - fx) * c01); wt[5] = half_round(fx * c01);
+        wt[6] = half_round((1.f - fx) * c11); wt[7] = half_round(fx * c11);
+        float2 val = projft ? __ldg(projft + id) : make_float2(1.f, 0.f);
+        float pw = projw ? __ldg(projw + id) : 1.f;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          int nx = x0 + (i & 1), ny = y0 + ((i >> 1) & 1), nz = z0 + ((i >> 2) & 1);
+          float iw = wt[i];
+          if (SQUARE) iw *= iw;
+          int tx = nx, ty = ny, tz = nz;
+          float sim = val.y;
+          if (tx < 0) {
+            tx = -tx; ty = -ty; tz = -tz;
+            sim = -sim;
+          }
+          int lx = tx - o.x, ly = ty - o.y, lz = tz - o.z;
+          if ((unsigned)lx < (unsigned)B && (unsigned)ly < (unsigned)B && (unsigned)lz < (unsigned)B) {
+            int k = (lz * B + ly) * B + lx;
+            atomicAdd(are + k, iw * val.x);
+            atomicAdd(aim + k, iw * sim);
+            atomicAdd(aw + k, iw * pw);
+          }
+          if (nx == 0 && (ny != 0 || nz != 0)) {  // second insertion on the x = 0 plane
+            lx = -o.x; ly = -ny - o.y; lz = -nz - o.z;
+            if ((unsigned)lx < (unsigned)B && (unsigned)ly < (unsigned)B && (unsigned)lz < (unsigned)B) {
+              int k = (lz * B + ly) * B + lx;
+              atomicAdd(are + k, iw * val.x);
+              atomicAdd(aim + k, iw * -sim);
+              atomicAdd(aw + k, iw * pw);
+            }
+          }
+        }
+      });
+    }
+    __syncthreads();
+
+    // flush the brick into the volume
+    const int rowlen = a.rowlen;
+    for (int k = threadIdx.x; k < B3; k += blockDim.x) {
+      float r = are[k], im = aim[k], ww = aw[k];
+      if (r == 0.f && im == 0.f && ww == 0.f) continue;
+      int lx = k % B, t = k / B, ly = t % B, lz = t / B;
+      int x = o.x + lx, y = o.y + ly, z = o.z + lz;
+      int ys, zs;
+      bool alias;
+      if (DECENTERED) {
+        ys = y < 0 ? y + V : y;
+        zs = z < 0 ? z + V : z;
+        alias = (y == V / 2 || y == -(V / 2) || z == V / 2 || z == -(V / 2));
+      } else {
+        ys = y + V / 2;
+        zs = z + V / 2;
+        alias = false;
+      }
+      if ((unsigned)x > (unsigned)(V / 2) || (unsigned)ys >= (unsigned)V || (unsigned)zs >= (unsigned)V)
+        continue;  // outside the volume: nothing can have been added here
+      int64_t idx = ((int64_t)zs * V + ys) * rowlen + x;
+      if (it.exclusive && !alias) {
+        if (volft) {
+          float2 c = volft[idx];
+          volft[idx] = make_float2(c.x + r, c.y + im);
+        }
+        if (volw) volw[idx] += ww;
+      } else {
+        if (volft) red_add2((float*)(volft + idx), r, im);
+        if (volw) red_add(volw + idx, ww);
+      }
+    }
+  }
+}
+
+static int backproject_brick(float* d_volumeft, float* d_volumeweights, const float* d_projft,
+                             const float* d_projweights, const float* d_mats, const BpArgs& a,
+                             int rmax, int decentered, int square, unsigned batch, cudaStream_t stream,
+                             bool* done) {
+  *done = false;
+  const int V = a.P;
+  // Neighbours stay inside x [0, V/2] and y, z [-V/2, yhi] (no clamp, no
+  // wrap beyond the reference's) while every sample radius is below limit.
+  const int yhi = decentered ? V / 2 : V - 1 - V / 2;
+  const float limit = (float)std::min(V / 2, yhi) - 1e-4f;
+  BrickGrid g = make_brick_grid(V, kBrickEdge, V / 2, -(V / 2), yhi);
+  BrickPlan plan;
+  bool fits = false;
+  float pmax = std::sqrt((float)std::max(0, rmax * rmax - 1));
+  int st = build_brick_plan(d_mats, (int)batch, g, pmax, limit, brick_chunk_default(), stream, &plan, &fits);
+  if (st || !fits) return st;
+  size_t smem = sizeof(float) * 3 * (size_t)kBrickEdge * kBrickEdge * kBrickEdge;
+  auto kern = decentered ? (square ? backproject_brick_kernel<true, true> : backproject_brick_kernel<true, false>)
+                         : (square ? backproject_brick_kernel<false, true> : backproject_brick_kernel<false, false>);
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int dev = 0, sms = 148, occ = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBrickThreads, smem);
+  int grid = std::max(1, std::min(plan.nitems, sms * std::max(occ, 1)));
+  if (plan.nitems > 0)
+    kern<<<grid, kBrickThreads, smem, stream>>>((float2*)d_volumeft, d_volumeweights,
+                                                 (const float2*)d_projft, d_projweights, d_mats, a, g,
+                                                 plan.items, plan.nitems, plan.lists, plan.counter);
+  cudaError_t e = cudaGetLastError();
+  free_brick_plan(&plan, stream);
+  if (e != cudaSuccess)
+    return set_error(GTOMRLN_ERR_CUDA, "launch of backproject_brick_kernel failed: %s",
+                     cudaGetErrorString(e));
+  *done = true;
+  return GTOMRLN_OK;
+}
+
 static int backproject_launch(float* d_volumeft, float* d_volumeweights, int vx, int vy, int vz,
                               const float* d_projft, const float* d_projweights, int px, int py,
                               int pz, unsigned rmax, const float* d_matrices, const int* d_ivolume,
@@ -161,6 +339,16 @@ static int backproject_launch(float* d_volumeft, float* d_volumeweights, int vx,
   a.ewalddiaminv = ewaldradiussuper == 0 ? 0.f : 1.0f / (2.0f * ewaldradiussuper);
   if ((int64_t)a.tiles * batch > 0x7fffffffLL)
     return set_error(GTOMRLN_ERR_INVALID, "backproject: batch too large for one launch");
+
+  const int choice = path_choice(GTOMRLN_OP_BACKPROJECT);
+  if (ndp == 2 && vx == vy && vx == vz && vx >= 4 && !d_ivolume && mag.x == 1.f && mag.y == 0.f &&
+      mag.z == 0.f && mag.w == 1.f && a.ewalddiaminv == 0.f && (d_volumeft || d_volumeweights) &&
+      (choice == GTOMRLN_PATH_BRICK || (choice == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch))) {
+    bool done = false;
+    int st = backproject_brick(d_volumeft, d_volumeweights, d_projft, d_projweights, d_matrices, a,
+                               (int)rmax, decentered, square, batch, stream, &done);
+    if (st || done) return st;
+  }
 
   dim3 grid((unsigned)(a.tiles * (int64_t)batch));
   float2* vf = (float2*)d_volumeft;

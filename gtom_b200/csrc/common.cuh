@@ -44,6 +44,9 @@ inline int dimension_count(int x, int y, int z) {
 // Host matrices exactly as Project.cu:14-16 builds them (single precision).
 void matrices_from_angles(const float* angles, float supersample, unsigned batch, float* out);
 
+// Implementation chosen for op (GTOMRLN_OP_*) by gtomrln_set_path.
+int path_choice(int op);
+
 // Stream-ordered device scratch from the library's memory pool.
 int pool_alloc(void** ptr, size_t bytes, cudaStream_t stream);
 int pool_free(void* ptr, cudaStream_t stream);

@@ -7,6 +7,11 @@
 // read-only path so that consecutive slices of similar orientation hit L2.
 // The per-sample arithmetic is the reference's, operation for operation, so
 // the result is the same for the same inputs.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+
+#include "brick.cuh"
 #include "common.cuh"
 
 namespace gtomrln {
@@ -22,6 +27,7 @@ struct ProjArgs {
   int64_t elements;
   int tiles;      // tiles per slice
   int rmax2;
+  int rmax;
   int P;          // dimsvolume.x
   int64_t nvox;   // (P/2+1) * P * P
 };
@@ -113,6 +119,150 @@ project_direct_kernel(Fetch fetch, float2* __restrict__ proj, const float* __res
   }
 }
 
+// ---------------------------------------------------------------------------
+// Brick-major projector.  Each work item stages one brick of the volume
+// (16^3 voxels plus a one-voxel halo, in signed coordinates, wrapped into the
+// decentred layout exactly as the reference's index arithmetic wraps them)
+// in shared memory, then every warp takes one of the brick's slices and
+// evaluates the pixels whose interpolation base voxel (x0, y0, z0) lies in
+// the brick.  Each in-disk pixel has exactly one such brick, so it is
+// written exactly once, with the direct kernel's arithmetic on the same
+// voxel values: the results are identical.  Pixels outside rmax are zeroed
+// by project_zero_kernel.
+// ---------------------------------------------------------------------------
+constexpr int kBrickThreads = 256;
+
+__global__ void __launch_bounds__(kBrickThreads)
+project_brick_kernel(const float2* __restrict__ vol, float2* __restrict__ proj,
+                     const float* __restrict__ mats, ProjArgs a, BrickGrid g,
+                     const BrickItem* __restrict__ items, int nitems, const int* __restrict__ lists,
+                     int* __restrict__ counter) {
+  extern __shared__ float2 tile[];
+  __shared__ int item_s;
+  const int B = g.B, T = g.B + 1;
+  const int rowlen = a.P / 2 + 1;
+  const int64_t last = a.nvox - 1;
+  const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (;;) {
+    __syncthreads();  // previous item done with the tile
+    if (threadIdx.x == 0) item_s = atomicAdd(counter, 1);
+    __syncthreads();
+    const int w = item_s;
+    if (w >= nitems) break;
+    const BrickItem it = items[w];
+    const int3 o = brick_origin(g, it.brick);
+    for (int k = threadIdx.x; k < T * T * T; k += blockDim.x) {
+      int tx = k % T, t2 = k / T, ty = t2 % T, tz = t2 / T;
+      int x = o.x + tx, y = o.y + ty, z = o.z + tz;
+      int ys = y < 0 ? y + a.P : y, zs = z < 0 ? z + a.P : z;
+      int64_t i = ((int64_t)zs * a.P + ys) * rowlen + x;
+      i = i < 0 ? 0 : (i > last ? last : i);
+      tile[k] = __ldg(vol + i);
+    }
+    __syncthreads();
+    float3 qlo, qhi;
+    brick_box(g, it.brick, qlo, qhi);
+    for (int j = warp; j < it.count; j += nwarps) {
+      const int slice = __ldg(lists + it.offset + j);
+      float m[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
+      float2* out = proj + a.elements * slice;
+      for_each_footprint_pixel(m, qlo, qhi, a.rmax2, [&](int u, int v) {
+        float3 pos = mat_apply(m, (float)u, (float)v, 0.f);
+        float sign = 1.f;
+        if (pos.x < -1e-5f) {
+          pos.x = fabsf(pos.x);
+          pos.y = -pos.y;
+          pos.z = -pos.z;
+          sign = -1.f;
+        }
+        float fx0 = floorf(pos.x + 1e-5f), fy0 = floorf(pos.y), fz0 = floorf(pos.z);
+        int lx = (int)fx0 - o.x, ly = (int)fy0 - o.y, lz = (int)fz0 - o.z;
+        if ((unsigned)lx >= (unsigned)B || (unsigned)ly >= (unsigned)B || (unsigned)lz >= (unsigned)B)
+          return;  // another brick owns this pixel
+        float fx = pos.x - fx0, fy = pos.y - fy0, fz = pos.z - fz0;
+        const float2* c = tile + (lz * T + ly) * T + lx;
+        float2 d000 = c[0], d001 = c[1], d010 = c[T], d011 = c[T + 1];
+        float2 d100 = c[T * T], d101 = c[T * T + 1], d110 = c[T * T + T], d111 = c[T * T + T + 1];
+        float rx00 = lerpf(d000.x, d001.x, fx), ix00 = lerpf(d000.y, d001.y, fx);
+        float rx01 = lerpf(d010.x, d011.x, fx), ix01 = lerpf(d010.y, d011.y, fx);
+        float rx10 = lerpf(d100.x, d101.x, fx), ix10 = lerpf(d100.y, d101.y, fx);
+        float rx11 = lerpf(d110.x, d111.x, fx), ix11 = lerpf(d110.y, d111.y, fx);
+        float rxy0 = lerpf(rx00, rx01, fy), ixy0 = lerpf(ix00, ix01, fy);
+        float rxy1 = lerpf(rx10, rx11, fy), ixy1 = lerpf(ix10, ix11, fy);
+        int idy = v >= 0 ? v : v + a.n;
+        out[(int64_t)idy * a.dimft + u] =
+            make_float2(lerpf(rxy0, rxy1, fz), lerpf(ixy0, ixy1, fz) * sign);
+      });
+    }
+  }
+}
+
+// Zeroes the elements outside rmax (Project.cu:111-115) for the brick path.
+__global__ void project_zero_kernel(float2* __restrict__ proj, ProjArgs a, int64_t total) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t id = i % a.elements;
+    int x = (int)(id % a.dimft);
+    int idy = (int)(id / a.dimft);
+    int y = idy <= a.n / 2 ? idy : idy - a.n;
+    if (x * x + y * y > a.rmax2) proj[i] = make_float2(0.f, 0.f);
+  }
+}
+
+// Brick edge and slices per work item of the brick paths.  Chosen for the
+// B200 (see the autotuner notes); overridable for experiments through
+// GTOMRLN_BRICK_CHUNK.
+int brick_chunk_default() {
+  static int chunk = [] {
+    const char* e = getenv("GTOMRLN_BRICK_CHUNK");
+    int c = e ? atoi(e) : 0;
+    return c > 0 ? c : 512;
+  }();
+  return chunk;
+}
+constexpr int kBrickEdge = 16;
+constexpr unsigned kBrickMinBatch = 32;
+
+// Runs the brick path if the geometry allows it; *done tells whether it did.
+static int project_brick(const float* d_volumeft, float* d_proj, const float* d_mats, const ProjArgs& a,
+                         unsigned rmax, unsigned batch, cudaStream_t stream, bool* done) {
+  *done = false;
+  const int P = a.P;
+  // While every sample radius stays below P/2 + 0.99, the base voxels lie in
+  // x [0, P/2] and y, z [-P/2 - 1, P/2].
+  BrickGrid g = make_brick_grid(P, kBrickEdge, P / 2, -(P / 2) - 1, P / 2);
+  BrickPlan plan;
+  bool fits = false;
+  int st = build_brick_plan(d_mats, (int)batch, g, (float)rmax, (float)(P / 2) + 0.99f,
+                            brick_chunk_default(), stream, &plan, &fits);
+  if (st || !fits) return st;
+  size_t smem = sizeof(float2) * (size_t)(kBrickEdge + 1) * (kBrickEdge + 1) * (kBrickEdge + 1);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(project_brick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  int dev = 0, sms = 148, occ = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, project_brick_kernel, kBrickThreads, smem);
+  int grid = std::max(1, std::min(plan.nitems, sms * std::max(occ, 1)));
+  int64_t total = a.elements * (int64_t)batch;
+  project_zero_kernel<<<sms * 8, 256, 0, stream>>>((float2*)d_proj, a, total);
+  if (plan.nitems > 0)
+    project_brick_kernel<<<grid, kBrickThreads, smem, stream>>>(
+        (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, plan.items, plan.nitems, plan.lists,
+        plan.counter);
+  cudaError_t e = cudaGetLastError();
+  free_brick_plan(&plan, stream);
+  if (e != cudaSuccess)
+    return set_error(GTOMRLN_ERR_CUDA, "launch of project_brick_kernel failed: %s", cudaGetErrorString(e));
+  *done = true;
+  return GTOMRLN_OK;
+}
+
 // Validates dimensions the way Project.cu:27-32 does and fills ProjArgs.
 static int project_setup(int vx, int vy, int vz, int px, int py, int pz, unsigned rmax,
                          unsigned batch, ProjArgs* a, int* ndims_proj) {
@@ -132,6 +282,7 @@ static int project_setup(int vx, int vy, int vz, int px, int py, int pz, unsigne
   a->elements = ndp == 3 ? a->area * px : a->area;
   a->tiles = (int)((a->elements + kProjTile - 1) / kProjTile);
   a->rmax2 = (int)(rmax * rmax);
+  a->rmax = (int)rmax;
   a->P = vx;
   a->nvox = (int64_t)(vx / 2 + 1) * vx * vx;
   *ndims_proj = ndp;
@@ -168,6 +319,13 @@ int gtomrln_project(const float* d_volumeft, int vx, int vy, int vz, float* d_pr
   if (st) return st;
   if (batch && (!d_volumeft || !d_proj || !d_matrices))
     return set_error(GTOMRLN_ERR_INVALID, "project: NULL device pointer");
+  if (ndp == 2 && vx == vy && vx == vz && vx >= 4 &&
+      (path_choice(0) == GTOMRLN_PATH_BRICK || (path_choice(0) == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch))) {
+    bool done = false;
+    st = project_brick(d_volumeft, d_proj, d_matrices, a, (unsigned)a.rmax, batch, (cudaStream_t)stream,
+                       &done);
+    if (st || done) return st;
+  }
   ArrayFetch f{(const float2*)d_volumeft, a.P, a.P / 2 + 1, a.nvox - 1};
   return launch_project(f, ndp, d_proj, d_matrices, a, batch, (cudaStream_t)stream);
 }

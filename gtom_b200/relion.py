@@ -208,6 +208,16 @@ def reconstruct_gridding_tol(dataft, weight, reconstructed, dimsori: Dims, dimsp
     return it.value, ch.value
 
 
+_OPS = {"project": 0, "backproject": 1}
+_PATHS = {"auto": 0, "direct": 1, "brick": 2}
+
+
+def set_path(op: str, path: str) -> None:
+    """Selects the implementation of "project" or "backproject" for this
+    process: "auto" (default), "direct" or "brick" (gtomrln_set_path)."""
+    _lib.call("gtomrln_set_path", _OPS[op], _PATHS[path])
+
+
 def kaiser_bessel_table(radius: float, alpha: float, order: int = 0,
                         nsamples: int = 10000) -> np.ndarray:
     """The normalised blob table of the gridding correction."""

@@ -62,6 +62,21 @@ GTOMRLN_API const char* gtomrln_last_error(void);
  * device.  Not required; the caches are also released at process exit. */
 GTOMRLN_API int gtomrln_release_caches(void);
 
+/* Extension (no reference counterpart): choose the implementation of an
+ * operation for the calling process.  op: GTOMRLN_OP_PROJECT or
+ * GTOMRLN_OP_BACKPROJECT; path: GTOMRLN_PATH_AUTO (default: brick-major for
+ * batches of 32 or more 2D slices whose geometry allows it, else direct),
+ * GTOMRLN_PATH_DIRECT (one thread per slice element, global gathers /
+ * reductions) or GTOMRLN_PATH_BRICK (brick-major, shared-memory staging;
+ * falls back to direct where the geometry does not allow it).  Both paths
+ * compute the same per-sample arithmetic. */
+#define GTOMRLN_OP_PROJECT 0
+#define GTOMRLN_OP_BACKPROJECT 1
+#define GTOMRLN_PATH_AUTO 0
+#define GTOMRLN_PATH_DIRECT 1
+#define GTOMRLN_PATH_BRICK 2
+GTOMRLN_API int gtomrln_set_path(int op, int path);
+
 /* Host helper: M_b = transpose(Matrix3Euler(angles_b)) * supersample, the
  * matrices the h_angles overloads build (src/Relion/Project.cu:14-16,
  * src/Helpers/Euler.cu:39-68).  Writes 9 * batch floats, column-major. */

@@ -1,0 +1,123 @@
+"""The brick-major kernels against the direct ones on larger batches.
+
+The brick projector evaluates every pixel with the direct kernel's
+arithmetic on the same voxel values, so the two must agree bit for bit.  The
+brick backprojector sums the same contributions in another order (shared
+memory first, then one reduction per brick), so the two agree to FP32
+rounding of the sums."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests.helpers import rel_l2
+from tests.synthdata import blob_volume_ft, random_angles
+
+pytestmark = pytest.mark.gpu
+
+
+def _paths(p, b):
+    from gtom_b200 import set_path
+    set_path("project", p)
+    set_path("backproject", b)
+
+
+@pytest.fixture(autouse=True)
+def _reset(gtom_lib):
+    yield
+    _paths("auto", "auto")
+
+
+def _angles(rng, batch, kind):
+    if kind == "uniform":
+        return random_angles(rng, batch)
+    if kind == "near_identity":  # planes close to z = 0: many samples on the x = 0 plane boundary
+        return (rng.normal(size=(batch, 3)) * 0.05).astype(np.float32)
+    if kind == "axis_aligned":  # exact multiples of 90 degrees: samples on voxel faces
+        return (rng.integers(0, 4, size=(batch, 3)) * (np.pi / 2)).astype(np.float32)
+    raise ValueError(kind)
+
+
+@pytest.mark.parametrize("n,scale,batch,kind", [(64, 2, 300, "uniform"), (32, 2, 200, "near_identity"),
+                                                 (32, 2, 64, "axis_aligned"), (48, 3, 100, "uniform"),
+                                                 (96, 2, 64, "uniform")])
+def test_brick_projector_is_bit_identical(cuda, n, scale, batch, kind):
+    from gtom_b200 import d_rlnProject, matrices_from_angles
+    rng = np.random.default_rng(n * 7 + batch)
+    P = scale * n
+    vol = blob_volume_ft(rng, n, P, 20)
+    vol = (vol + 0.01 * np.abs(vol).max() * (rng.normal(size=vol.shape) + 1j * rng.normal(size=vol.shape))).astype(np.complex64)
+    mats = torch.from_numpy(matrices_from_angles(_angles(rng, batch, kind), float(scale))).cuda().reshape(-1)
+    e = (n // 2 + 1) * n
+    dv = torch.from_numpy(vol).cuda().reshape(-1)
+    outs = {}
+    for p in ("direct", "brick"):
+        _paths(p, "auto")
+        out = torch.full((batch * e,), complex(np.nan, np.nan), dtype=torch.complex64, device="cuda")
+        d_rlnProject(dv, (P, P, P), out, (n, n, 1), n // 2, mats, batch)
+        torch.cuda.synchronize()
+        outs[p] = out
+    assert torch.isfinite(torch.view_as_real(outs["brick"])).all()
+    assert torch.equal(outs["direct"], outs["brick"])
+
+
+@pytest.mark.parametrize("n,V,batch,kind,dec,sq", [(64, 129, 300, "uniform", False, False),
+                                                   (64, 128, 300, "uniform", True, False),
+                                                   (32, 64, 200, "near_identity", True, True),
+                                                   (32, 65, 64, "axis_aligned", False, False),
+                                                   (48, 97, 100, "uniform", False, True),
+                                                   (32, 64, 64, "uniform", False, False)])
+def test_brick_backprojector_matches_direct(cuda, n, V, batch, kind, dec, sq):
+    from gtom_b200 import d_rlnBackproject, matrices_from_angles
+    rng = np.random.default_rng(n * 11 + batch)
+    e = (n // 2 + 1) * n
+    scale = 2.0 if V < 3 * n else 3.0
+    ang = _angles(rng, batch, kind)
+    m_host = matrices_from_angles(ang, scale)
+    mats = torch.from_numpy(m_host).cuda().reshape(-1)
+    projft = (rng.normal(size=(batch, e)) + 1j * rng.normal(size=(batch, e))).astype(np.complex64)
+    projw = rng.uniform(0.1, 1, size=(batch, e)).astype(np.float32)
+    dpf = torch.from_numpy(projft).cuda().reshape(-1)
+    dpw = torch.from_numpy(projw).cuda().reshape(-1)
+    nv = (V // 2 + 1) * V * V
+    res = {}
+    for b in ("direct", "brick"):
+        _paths("auto", b)
+        vf = torch.zeros(nv, dtype=torch.complex64, device="cuda")
+        vw = torch.zeros(nv, dtype=torch.float32, device="cuda")
+        d_rlnBackproject(vf, vw, (V, V, V), dpf, dpw, (n, n, 1), n // 2, mats, None, (1, 0, 0, 1), 0.0, dec, sq,
+                         batch)
+        torch.cuda.synchronize()
+        res[b] = (vf.cpu().numpy(), vw.cpu().numpy())
+    assert rel_l2(res["brick"][0], res["direct"][0]) <= 1e-6
+    assert rel_l2(res["brick"][1], res["direct"][1]) <= 1e-6
+    of, ow = np.zeros(nv, np.complex64), np.zeros(nv, np.float32)
+    O.backproject(of, ow, V, projft, projw, n, n // 2, m_host, decentered=dec, square=sq, fp32=True)
+    assert rel_l2(res["brick"][0], of) <= 1e-5 and rel_l2(res["brick"][1], ow) <= 1e-5
+    # the voxels that received nothing are exactly the same ones
+    assert np.array_equal(res["brick"][1] == 0, res["direct"][1] == 0)
+
+
+def test_brick_backprojector_accumulates_across_calls(cuda):
+    """Two calls into the same accumulators equal one call over both batches."""
+    from gtom_b200 import d_rlnBackproject, matrices_from_angles
+    rng = np.random.default_rng(5)
+    n, V, batch = 32, 65, 120
+    e = (n // 2 + 1) * n
+    mats = torch.from_numpy(matrices_from_angles(random_angles(rng, batch), 2.0)).cuda()
+    pf = torch.from_numpy((rng.normal(size=(batch, e)) + 1j * rng.normal(size=(batch, e))).astype(np.complex64)).cuda()
+    nv = (V // 2 + 1) * V * V
+    _paths("auto", "brick")
+    a_f = torch.zeros(nv, dtype=torch.complex64, device="cuda")
+    a_w = torch.zeros(nv, dtype=torch.float32, device="cuda")
+    h = batch // 2
+    for s in (slice(0, h), slice(h, batch)):
+        d_rlnBackproject(a_f, a_w, (V, V, V), pf[s].reshape(-1), None, (n, n, 1), n // 2,
+                         mats[s].reshape(-1).contiguous(), None, (1, 0, 0, 1), 0.0, False, False, s.stop - s.start)
+    b_f = torch.zeros_like(a_f)
+    b_w = torch.zeros_like(a_w)
+    d_rlnBackproject(b_f, b_w, (V, V, V), pf.reshape(-1), None, (n, n, 1), n // 2, mats.reshape(-1), None,
+                     (1, 0, 0, 1), 0.0, False, False, batch)
+    torch.cuda.synchronize()
+    assert rel_l2(a_f.cpu().numpy(), b_f.cpu().numpy()) <= 1e-6
+    assert rel_l2(a_w.cpu().numpy(), b_w.cpu().numpy()) <= 1e-6
