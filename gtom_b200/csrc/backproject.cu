@@ -183,7 +183,8 @@ backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
       float m[9];
 #pragma unroll
       for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
-      for_each_footprint_pixel(m, qlo, qhi, a.rmax2 - 1, [&](int u, int v) {
+      for_each_footprint_pixel<false>(m, qlo, qhi, a.rmax2 - 1, a.n / 2 + 1 - a.n, a.n / 2,
+                                      [&](int u, int v) {
         // pixel (u, v): r^2 < rmax^2 and not (u == 0 && v < 0) by construction
         int idy = v >= 0 ? v : v + a.n;
         int64_t id = a.elements * slice + (int64_t)idy * a.dimft + u;

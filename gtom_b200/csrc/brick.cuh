@@ -134,14 +134,23 @@ __device__ __forceinline__ void v_range(const PlaneFrame& f, float3 qlo, float3 
   v1 = min(rmax, (int)floorf(vmax + 1e-3f));
 }
 
-// Warp-cooperative walk over the stored half-plane pixels p = (u, v)
-// (u > 0, or u == 0 and v >= 0) with u^2 + v^2 <= r2max whose sample M p, or
-// whose mate's sample M(-p), lies in Q.  Each such pixel is visited exactly
-// once per call.  All 32 lanes must call this; visit(u, v) runs on the lane
-// that owns the pixel.
-template <class Visit>
+// Stored pixels of a half-complex slice: rows v in [vlo, vhi] (FFT order
+// holds y = n/2 but not -n/2 for even n), columns u >= 0.  The projector
+// evaluates the whole u = 0 column; the backprojector skips u = 0, v < 0
+// (Backproject.cu:177), whose samples are the mirrors of u = 0, v > 0.
+template <bool FULL_X0>
+__device__ __forceinline__ bool stored_pixel(int u, int v, int vlo, int vhi) {
+  if (v < vlo || v > vhi) return false;
+  return FULL_X0 ? u >= 0 : (u > 0 || (u == 0 && v >= 0));
+}
+
+// Warp-cooperative walk over the stored pixels p = (u, v) with
+// u^2 + v^2 <= r2max whose sample M p, or whose Friedel mate's sample
+// M(-p), lies in Q.  Each such pixel is visited exactly once per call.  All
+// 32 lanes must call this; visit(u, v) runs on the lane that owns the pixel.
+template <bool FULL_X0, class Visit>
 __device__ __forceinline__ void for_each_footprint_pixel(const float* m, float3 qlo, float3 qhi,
-                                                         int r2max, Visit&& visit) {
+                                                         int r2max, int vlo, int vhi, Visit&& visit) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   PlaneFrame f = plane_frame(m);
@@ -172,13 +181,14 @@ __device__ __forceinline__ void for_each_footprint_pixel(const float* m, float3 
       int len_r = __shfl_sync(FULL, len, r);
       int ua_r = __shfl_sync(FULL, ua, r);
       if (t < total) {
+        // q = (qu, qv) has M q in Q.  Visit q if it is stored, and its
+        // Friedel mate p = -q (whose mirrored sample M q lies in Q) if that is
+        // stored and is not itself on the walk (it is then visited as a q).
         int qu = ua_r + (t - (incl_r - len_r));
         int qv = vb + r;
-        if (qu > 0 || (qu == 0 && qv >= 0)) {
-          visit(qu, qv);
-        } else {
-          // Friedel mate p = -q; skip it if p itself lies on the walk.
-          int pu = -qu, pv = -qv;
+        if (stored_pixel<FULL_X0>(qu, qv, vlo, vhi)) visit(qu, qv);
+        int pu = -qu, pv = -qv;
+        if ((pu != qu || pv != qv) && stored_pixel<FULL_X0>(pu, pv, vlo, vhi)) {
           bool direct = false;
           if (pv >= v0 && pv <= v1) {
             int a, bnd;

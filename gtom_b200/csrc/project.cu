@@ -168,7 +168,7 @@ project_brick_kernel(const float2* __restrict__ vol, float2* __restrict__ proj,
 #pragma unroll
       for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
       float2* out = proj + a.elements * slice;
-      for_each_footprint_pixel(m, qlo, qhi, a.rmax2, [&](int u, int v) {
+      for_each_footprint_pixel<true>(m, qlo, qhi, a.rmax2, a.n / 2 + 1 - a.n, a.n / 2, [&](int u, int v) {
         float3 pos = mat_apply(m, (float)u, (float)v, 0.f);
         float sign = 1.f;
         if (pos.x < -1e-5f) {
