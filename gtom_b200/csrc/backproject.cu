@@ -52,12 +52,19 @@ __device__ __forceinline__ int64_t place(int x, int y, int z, int P, int rowlen)
 
 template <int NDIMS, bool DECENTERED, bool SQUARE>
 __global__ void __launch_bounds__(kBpThreads)
-backproject_direct_kernel(float2* __restrict__ volft, float* __restrict__ volw,
+backproject_direct_kernel(float2* __restrict__ volft_base, float* __restrict__ volw_base,
                           const float2* __restrict__ projft, const float* __restrict__ projw,
                           const float* __restrict__ mats, const int* __restrict__ ivolume,
-                          BpArgs a) {
-  const int slice = blockIdx.x / a.tiles;
-  const int tile = blockIdx.x - slice * a.tiles;
+                          BpArgs a, const int* __restrict__ list, const int* __restrict__ nlist) {
+  // Without a list the grid covers every (slice, tile) once; with one (the
+  // slices a brick plan left over) a persistent grid strides over them.
+  const int64_t total = list ? (int64_t)(*nlist) * a.tiles : (int64_t)gridDim.x;
+  for (int64_t work = blockIdx.x; work < total; work += gridDim.x) {
+  const int entry = (int)(work / a.tiles);
+  const int tile = (int)(work - (int64_t)entry * a.tiles);
+  const int slice = list ? __ldg(list + entry) : entry;
+  float2* volft = volft_base;
+  float* volw = volw_base;
   float m[9];
 #pragma unroll
   for (int i = 0; i < 9; i++) m[i] = __ldg(mats + 9 * (int64_t)slice + i);
@@ -131,6 +138,7 @@ backproject_direct_kernel(float2* __restrict__ volft, float* __restrict__ volw,
       }
     }
   }
+  }  // work loop
 }
 
 // ---------------------------------------------------------------------------
@@ -156,10 +164,11 @@ __global__ void __launch_bounds__(kBrickThreads)
 backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
                          const float2* __restrict__ projft, const float* __restrict__ projw,
                          const float* __restrict__ mats, BpArgs a, BrickGrid g,
-                         const BrickItem* __restrict__ items, int nitems,
+                         const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
                          const int* __restrict__ lists, int* __restrict__ counter) {
   extern __shared__ float acc[];
   __shared__ int item_s;
+  const int nitems = *nitems_ptr;
   const int B = g.B, B3 = g.B * g.B * g.B;
   float* are = acc;
   float* aim = acc + B3;
@@ -270,11 +279,33 @@ backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
   }
 }
 
+template <bool DEC, bool SQ>
+static void launch_bp_direct(dim3 grid, cudaStream_t stream, float2* vf, float* vw, const float2* pf,
+                             const float* pw, const float* mats, const int* ivol, const BpArgs& a,
+                             const int* list, const int* nlist, int ndp) {
+  if (ndp == 2)
+    backproject_direct_kernel<2, DEC, SQ><<<grid, kBpThreads, 0, stream>>>(vf, vw, pf, pw, mats, ivol, a, list, nlist);
+  else
+    backproject_direct_kernel<3, DEC, SQ><<<grid, kBpThreads, 0, stream>>>(vf, vw, pf, pw, mats, ivol, a, list, nlist);
+}
+
+static void launch_bp_direct_any(dim3 grid, cudaStream_t stream, float2* vf, float* vw, const float2* pf,
+                                 const float* pw, const float* mats, const int* ivol, const BpArgs& a,
+                                 const int* list, const int* nlist, int ndp, int decentered, int square) {
+  if (decentered) {
+    if (square) launch_bp_direct<true, true>(grid, stream, vf, vw, pf, pw, mats, ivol, a, list, nlist, ndp);
+    else launch_bp_direct<true, false>(grid, stream, vf, vw, pf, pw, mats, ivol, a, list, nlist, ndp);
+  } else {
+    if (square) launch_bp_direct<false, true>(grid, stream, vf, vw, pf, pw, mats, ivol, a, list, nlist, ndp);
+    else launch_bp_direct<false, false>(grid, stream, vf, vw, pf, pw, mats, ivol, a, list, nlist, ndp);
+  }
+}
+
+// The brick path: plan, brick kernel, and the direct kernel for any slice the
+// plan could not take.  Nothing synchronises.
 static int backproject_brick(float* d_volumeft, float* d_volumeweights, const float* d_projft,
                              const float* d_projweights, const float* d_mats, const BpArgs& a,
-                             int rmax, int decentered, int square, unsigned batch, cudaStream_t stream,
-                             bool* done) {
-  *done = false;
+                             int rmax, int decentered, int square, unsigned batch, cudaStream_t stream) {
   const int V = a.P;
   // Neighbours stay inside x [0, V/2] and y, z [-V/2, yhi] (no clamp, no
   // wrap beyond the reference's) while every sample radius is below limit.
@@ -282,10 +313,9 @@ static int backproject_brick(float* d_volumeft, float* d_volumeweights, const fl
   const float limit = (float)std::min(V / 2, yhi) - 1e-4f;
   BrickGrid g = make_brick_grid(V, kBrickEdge, V / 2, -(V / 2), yhi);
   BrickPlan plan;
-  bool fits = false;
   float pmax = std::sqrt((float)std::max(0, rmax * rmax - 1));
-  int st = build_brick_plan(d_mats, (int)batch, g, pmax, limit, brick_chunk_default(), stream, &plan, &fits);
-  if (st || !fits) return st;
+  int st = build_brick_plan(d_mats, (int)batch, g, pmax, limit, brick_chunk_default(), stream, &plan);
+  if (st) return st;
   size_t smem = sizeof(float) * 3 * (size_t)kBrickEdge * kBrickEdge * kBrickEdge;
   auto kern = decentered ? (square ? backproject_brick_kernel<true, true> : backproject_brick_kernel<true, false>)
                          : (square ? backproject_brick_kernel<false, true> : backproject_brick_kernel<false, false>);
@@ -294,17 +324,15 @@ static int backproject_brick(float* d_volumeft, float* d_volumeweights, const fl
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBrickThreads, smem);
-  int grid = std::max(1, std::min(plan.nitems, sms * std::max(occ, 1)));
-  if (plan.nitems > 0)
-    kern<<<grid, kBrickThreads, smem, stream>>>((float2*)d_volumeft, d_volumeweights,
-                                                 (const float2*)d_projft, d_projweights, d_mats, a, g,
-                                                 plan.items, plan.nitems, plan.lists, plan.counter);
+  kern<<<sms * std::max(occ, 1), kBrickThreads, smem, stream>>>(
+      (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, a, g, plan.items,
+      plan.nitems, plan.lists, plan.counter);
+  launch_bp_direct_any(dim3(sms * 4), stream, (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft,
+                       d_projweights, d_mats, nullptr, a, plan.fallback, plan.nfallback, 2, decentered, square);
   cudaError_t e = cudaGetLastError();
   free_brick_plan(&plan, stream);
   if (e != cudaSuccess)
-    return set_error(GTOMRLN_ERR_CUDA, "launch of backproject_brick_kernel failed: %s",
-                     cudaGetErrorString(e));
-  *done = true;
+    return set_error(GTOMRLN_ERR_CUDA, "launch of the brick backprojector failed: %s", cudaGetErrorString(e));
   return GTOMRLN_OK;
 }
 
@@ -344,28 +372,13 @@ static int backproject_launch(float* d_volumeft, float* d_volumeweights, int vx,
   const int choice = path_choice(GTOMRLN_OP_BACKPROJECT);
   if (ndp == 2 && vx == vy && vx == vz && vx >= 4 && !d_ivolume && mag.x == 1.f && mag.y == 0.f &&
       mag.z == 0.f && mag.w == 1.f && a.ewalddiaminv == 0.f && (d_volumeft || d_volumeweights) &&
-      (choice == GTOMRLN_PATH_BRICK || (choice == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch))) {
-    bool done = false;
-    int st = backproject_brick(d_volumeft, d_volumeweights, d_projft, d_projweights, d_matrices, a,
-                               (int)rmax, decentered, square, batch, stream, &done);
-    if (st || done) return st;
-  }
+      (choice == GTOMRLN_PATH_BRICK || (choice == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch)))
+    return backproject_brick(d_volumeft, d_volumeweights, d_projft, d_projweights, d_matrices, a, (int)rmax,
+                             decentered, square, batch, stream);
 
-  dim3 grid((unsigned)(a.tiles * (int64_t)batch));
-  float2* vf = (float2*)d_volumeft;
-  const float2* pf = (const float2*)d_projft;
-#define GTOMRLN_BP(ND, DEC, SQ)                                                           \
-  backproject_direct_kernel<ND, DEC, SQ><<<grid, kBpThreads, 0, stream>>>(vf, d_volumeweights, \
-                                                                         pf, d_projweights,  \
-                                                                         d_matrices, d_ivolume, a)
-  if (ndp == 2) {
-    if (decentered) { if (square) GTOMRLN_BP(2, true, true); else GTOMRLN_BP(2, true, false); }
-    else            { if (square) GTOMRLN_BP(2, false, true); else GTOMRLN_BP(2, false, false); }
-  } else {
-    if (decentered) { if (square) GTOMRLN_BP(3, true, true); else GTOMRLN_BP(3, true, false); }
-    else            { if (square) GTOMRLN_BP(3, false, true); else GTOMRLN_BP(3, false, false); }
-  }
-#undef GTOMRLN_BP
+  launch_bp_direct_any(dim3((unsigned)(a.tiles * (int64_t)batch)), stream, (float2*)d_volumeft, d_volumeweights,
+                       (const float2*)d_projft, d_projweights, d_matrices, d_ivolume, a, nullptr, nullptr, ndp,
+                       decentered, square);
   GTOMRLN_LAUNCH_CHECK("backproject_direct_kernel");
   return GTOMRLN_OK;
 }

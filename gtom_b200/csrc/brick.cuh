@@ -202,25 +202,30 @@ __device__ __forceinline__ void for_each_footprint_pixel(const float* m, float3 
   }
 }
 
-// Per-call plan: slice lists per brick and the work items over them.
+// Per-call plan, all in device memory: slice lists per brick, the work items
+// over them, and the slices left to the direct kernels.
 struct BrickPlan {
   BrickGrid g;
-  int nitems = 0;
-  BrickItem* items = nullptr;  // device
-  int* lists = nullptr;        // device
-  int* counter = nullptr;      // device work counter
-  void* scratch = nullptr;     // one pool allocation holding all of the above
+  int batch = 0;
+  int max_items = 0;
+  BrickItem* items = nullptr;
+  int* nitems = nullptr;     // number of valid items
+  int* lists = nullptr;
+  int* counter = nullptr;    // work counter of the persistent kernel (starts at 0)
+  int* fallback = nullptr;   // slices for the direct kernels
+  int* nfallback = nullptr;
+  void* scratch = nullptr;   // one pool allocation holding all of the above
 };
 
-// Builds the plan for `batch` matrices (device, 9 floats each).  pmax is
-// the largest pixel radius of the slice (its samples lie within
-// sigma * pmax of the origin, sigma the largest singular value of the
-// matrix's first two columns).  If some sample could lie at or beyond
-// `limit`, no plan is built and *fits is set to false: the caller then takes
-// the direct path, whose clamps and wraps cover every geometry.  chunk caps
-// the slices per work item.  Synchronises the stream twice.
+// Enqueues the construction of the plan for `batch` matrices (device, 9
+// floats each) on `stream`; nothing is synchronised.  pmax is the largest
+// pixel radius of a slice: its samples lie within sigma * pmax of the origin
+// (sigma = largest singular value of the matrix's first two columns).  A
+// slice whose bound reaches `limit` is not planned but listed in
+// plan->fallback, for the direct kernels, whose clamps and wraps cover every
+// geometry.  chunk caps the slices per work item.
 int build_brick_plan(const float* d_mats, int batch, const BrickGrid& g, float pmax, float limit,
-                     int chunk, cudaStream_t stream, BrickPlan* plan, bool* fits);
+                     int chunk, cudaStream_t stream, BrickPlan* plan);
 int free_brick_plan(BrickPlan* plan, cudaStream_t stream);
 
 // Largest singular value of the first two columns of a matrix.

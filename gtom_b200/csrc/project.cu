@@ -55,11 +55,9 @@ struct TexFetch {
 };
 
 template <int NDIMS, class Fetch>
-__global__ void __launch_bounds__(kProjThreads)
-project_direct_kernel(Fetch fetch, float2* __restrict__ proj, const float* __restrict__ mats,
-                      ProjArgs a) {
-  const int slice = blockIdx.x / a.tiles;
-  const int tile = blockIdx.x - slice * a.tiles;
+__device__ __forceinline__ void project_direct_tile(const Fetch& fetch, float2* __restrict__ proj,
+                                                    const float* __restrict__ mats, const ProjArgs& a,
+                                                    int slice, int tile) {
   float m[9];
 #pragma unroll
   for (int i = 0; i < 9; i++) m[i] = __ldg(mats + 9 * (int64_t)slice + i);
@@ -119,6 +117,24 @@ project_direct_kernel(Fetch fetch, float2* __restrict__ proj, const float* __res
   }
 }
 
+template <int NDIMS, class Fetch>
+__global__ void __launch_bounds__(kProjThreads)
+project_direct_kernel(Fetch fetch, float2* __restrict__ proj, const float* __restrict__ mats,
+                      ProjArgs a) {
+  const int slice = blockIdx.x / a.tiles;
+  project_direct_tile<NDIMS>(fetch, proj, mats, a, slice, blockIdx.x - slice * a.tiles);
+}
+
+// The direct kernel over the slices listed in list[0 .. *nlist), which the
+// brick plan left to it; a persistent grid strides over (slice, tile).
+__global__ void __launch_bounds__(kProjThreads)
+project_listed_kernel(ArrayFetch fetch, float2* __restrict__ proj, const float* __restrict__ mats,
+                      ProjArgs a, const int* __restrict__ list, const int* __restrict__ nlist) {
+  const int64_t total = (int64_t)(*nlist) * a.tiles;
+  for (int64_t w = blockIdx.x; w < total; w += gridDim.x)
+    project_direct_tile<2>(fetch, proj, mats, a, __ldg(list + w / a.tiles), (int)(w % a.tiles));
+}
+
 // ---------------------------------------------------------------------------
 // Brick-major projector.  Each work item stages one brick of the volume
 // (16^3 voxels plus a one-voxel halo, in signed coordinates, wrapped into the
@@ -135,10 +151,11 @@ constexpr int kBrickThreads = 256;
 __global__ void __launch_bounds__(kBrickThreads)
 project_brick_kernel(const float2* __restrict__ vol, float2* __restrict__ proj,
                      const float* __restrict__ mats, ProjArgs a, BrickGrid g,
-                     const BrickItem* __restrict__ items, int nitems, const int* __restrict__ lists,
-                     int* __restrict__ counter) {
+                     const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
+                     const int* __restrict__ lists, int* __restrict__ counter) {
   extern __shared__ float2 tile[];
   __shared__ int item_s;
+  const int nitems = *nitems_ptr;
   const int B = g.B, T = g.B + 1;
   const int rowlen = a.P / 2 + 1;
   const int64_t last = a.nvox - 1;
@@ -225,19 +242,18 @@ int brick_chunk_default() {
 constexpr int kBrickEdge = 16;
 constexpr unsigned kBrickMinBatch = 32;
 
-// Runs the brick path if the geometry allows it; *done tells whether it did.
+// The brick path: plan, zero fill outside rmax, brick kernel, and the direct
+// kernel for any slice the plan could not take.  Nothing synchronises.
 static int project_brick(const float* d_volumeft, float* d_proj, const float* d_mats, const ProjArgs& a,
-                         unsigned rmax, unsigned batch, cudaStream_t stream, bool* done) {
-  *done = false;
+                         unsigned batch, cudaStream_t stream) {
   const int P = a.P;
   // While every sample radius stays below P/2 + 0.99, the base voxels lie in
   // x [0, P/2] and y, z [-P/2 - 1, P/2].
   BrickGrid g = make_brick_grid(P, kBrickEdge, P / 2, -(P / 2) - 1, P / 2);
   BrickPlan plan;
-  bool fits = false;
-  int st = build_brick_plan(d_mats, (int)batch, g, (float)rmax, (float)(P / 2) + 0.99f,
-                            brick_chunk_default(), stream, &plan, &fits);
-  if (st || !fits) return st;
+  int st = build_brick_plan(d_mats, (int)batch, g, (float)a.rmax, (float)(P / 2) + 0.99f,
+                            brick_chunk_default(), stream, &plan);
+  if (st) return st;
   size_t smem = sizeof(float2) * (size_t)(kBrickEdge + 1) * (kBrickEdge + 1) * (kBrickEdge + 1);
   static bool attr = false;
   if (!attr) {
@@ -248,18 +264,18 @@ static int project_brick(const float* d_volumeft, float* d_proj, const float* d_
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, project_brick_kernel, kBrickThreads, smem);
-  int grid = std::max(1, std::min(plan.nitems, sms * std::max(occ, 1)));
   int64_t total = a.elements * (int64_t)batch;
   project_zero_kernel<<<sms * 8, 256, 0, stream>>>((float2*)d_proj, a, total);
-  if (plan.nitems > 0)
-    project_brick_kernel<<<grid, kBrickThreads, smem, stream>>>(
-        (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, plan.items, plan.nitems, plan.lists,
-        plan.counter);
+  project_brick_kernel<<<sms * std::max(occ, 1), kBrickThreads, smem, stream>>>(
+      (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, plan.items, plan.nitems, plan.lists,
+      plan.counter);
+  ArrayFetch f{(const float2*)d_volumeft, a.P, a.P / 2 + 1, a.nvox - 1};
+  project_listed_kernel<<<sms * 4, kProjThreads, 0, stream>>>(f, (float2*)d_proj, d_mats, a, plan.fallback,
+                                                               plan.nfallback);
   cudaError_t e = cudaGetLastError();
   free_brick_plan(&plan, stream);
   if (e != cudaSuccess)
-    return set_error(GTOMRLN_ERR_CUDA, "launch of project_brick_kernel failed: %s", cudaGetErrorString(e));
-  *done = true;
+    return set_error(GTOMRLN_ERR_CUDA, "launch of the brick projector failed: %s", cudaGetErrorString(e));
   return GTOMRLN_OK;
 }
 
@@ -320,12 +336,8 @@ int gtomrln_project(const float* d_volumeft, int vx, int vy, int vz, float* d_pr
   if (batch && (!d_volumeft || !d_proj || !d_matrices))
     return set_error(GTOMRLN_ERR_INVALID, "project: NULL device pointer");
   if (ndp == 2 && vx == vy && vx == vz && vx >= 4 &&
-      (path_choice(0) == GTOMRLN_PATH_BRICK || (path_choice(0) == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch))) {
-    bool done = false;
-    st = project_brick(d_volumeft, d_proj, d_matrices, a, (unsigned)a.rmax, batch, (cudaStream_t)stream,
-                       &done);
-    if (st || done) return st;
-  }
+      (path_choice(0) == GTOMRLN_PATH_BRICK || (path_choice(0) == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch)))
+    return project_brick(d_volumeft, d_proj, d_matrices, a, batch, (cudaStream_t)stream);
   ArrayFetch f{(const float2*)d_volumeft, a.P, a.P / 2 + 1, a.nvox - 1};
   return launch_project(f, ndp, d_proj, d_matrices, a, batch, (cudaStream_t)stream);
 }
