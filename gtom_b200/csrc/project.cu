@@ -217,14 +217,24 @@ project_brick_kernel(const float2* __restrict__ vol, float2* __restrict__ proj,
 }
 
 // Zeroes the elements outside rmax (Project.cu:111-115) for the brick path.
-__global__ void project_zero_kernel(float2* __restrict__ proj, ProjArgs a, int64_t total) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t id = i % a.elements;
-    int x = (int)(id % a.dimft);
-    int idy = (int)(id / a.dimft);
+// In each row they form the tail x > sqrt(rmax^2 - y^2); one warp writes
+// one row's tail, coalesced.
+__global__ void project_zero_kernel(float2* __restrict__ proj, ProjArgs a, int64_t rows) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rows; r += warps) {
+    int idy = (int)(r % a.n);
     int y = idy <= a.n / 2 ? idy : idy - a.n;
-    if (x * x + y * y > a.rmax2) proj[i] = make_float2(0.f, 0.f);
+    int rem = a.rmax2 - y * y;
+    int x0 = 0;
+    if (rem >= 0) {
+      x0 = (int)sqrtf((float)rem);
+      while (x0 * x0 > rem) x0--;
+      while ((x0 + 1) * (x0 + 1) <= rem) x0++;
+      x0++;  // first x with x^2 + y^2 > rmax^2
+    }
+    float2* row = proj + r * a.dimft;
+    for (int x = x0 + lane; x < a.dimft; x += 32) row[x] = make_float2(0.f, 0.f);
   }
 }
 
@@ -264,8 +274,8 @@ static int project_brick(const float* d_volumeft, float* d_proj, const float* d_
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, project_brick_kernel, kBrickThreads, smem);
-  int64_t total = a.elements * (int64_t)batch;
-  project_zero_kernel<<<sms * 8, 256, 0, stream>>>((float2*)d_proj, a, total);
+  int64_t rows = (int64_t)a.n * batch;  // 2D slices: n rows of dimft elements each
+  project_zero_kernel<<<sms * 8, 256, 0, stream>>>((float2*)d_proj, a, rows);
   project_brick_kernel<<<sms * std::max(occ, 1), kBrickThreads, smem, stream>>>(
       (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, plan.items, plan.nitems, plan.lists,
       plan.counter);
