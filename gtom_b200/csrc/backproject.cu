@@ -167,18 +167,25 @@ backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
                          const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
                          const int* __restrict__ lists, int* __restrict__ counter) {
   extern __shared__ float acc[];
-  __shared__ int item_s;
+  __shared__ int item_s, next_s;
   const int nitems = *nitems_ptr;
-  const int B = g.B, B3 = g.B * g.B * g.B;
+  // Accumulator layout: rows padded to B+1 and planes to (B+1)^2 floats, so
+  // that the lanes of a warp, whose samples step along an arbitrary
+  // direction, spread over the banks (unpadded, steps along y or z would
+  // land every lane in the same bank).
+  const int B = g.B, RS = g.B + 1, PS = (g.B + 1) * (g.B + 1), NA = g.B * PS;
   float* are = acc;
-  float* aim = acc + B3;
-  float* aw = acc + 2 * B3;
-  const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  float* aim = acc + NA;
+  float* aw = acc + 2 * NA;
+  const int lane = threadIdx.x & 31;
   const int V = a.P;
   for (;;) {
     __syncthreads();
-    if (threadIdx.x == 0) item_s = atomicAdd(counter, 1);
-    for (int k = threadIdx.x; k < 3 * B3; k += blockDim.x) acc[k] = 0.f;
+    if (threadIdx.x == 0) {
+      item_s = atomicAdd(counter, 1);
+      next_s = 0;
+    }
+    for (int k = threadIdx.x; k < 3 * NA; k += blockDim.x) acc[k] = 0.f;
     __syncthreads();
     const int w = item_s;
     if (w >= nitems) break;
@@ -187,7 +194,11 @@ backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
     float3 qlo, qhi;
     brick_box(g, it.brick, qlo, qhi);
 
-    for (int j = warp; j < it.count; j += nwarps) {
+    for (;;) {  // warps take the item's slices one at a time
+      int j = 0;
+      if (lane == 0) j = atomicAdd(&next_s, 1);
+      j = __shfl_sync(0xffffffffu, j, 0);
+      if (j >= it.count) break;
       const int slice = __ldg(lists + it.offset + j);
       float m[9];
 #pragma unroll
@@ -225,7 +236,7 @@ backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
           }
           int lx = tx - o.x, ly = ty - o.y, lz = tz - o.z;
           if ((unsigned)lx < (unsigned)B && (unsigned)ly < (unsigned)B && (unsigned)lz < (unsigned)B) {
-            int k = (lz * B + ly) * B + lx;
+            int k = lz * PS + ly * RS + lx;
             atomicAdd(are + k, iw * val.x);
             atomicAdd(aim + k, iw * sim);
             atomicAdd(aw + k, iw * pw);
@@ -233,7 +244,7 @@ backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
           if (nx == 0 && (ny != 0 || nz != 0)) {  // second insertion on the x = 0 plane
             lx = -o.x; ly = -ny - o.y; lz = -nz - o.z;
             if ((unsigned)lx < (unsigned)B && (unsigned)ly < (unsigned)B && (unsigned)lz < (unsigned)B) {
-              int k = (lz * B + ly) * B + lx;
+              int k = lz * PS + ly * RS + lx;
               atomicAdd(are + k, iw * val.x);
               atomicAdd(aim + k, iw * -sim);
               atomicAdd(aw + k, iw * pw);
@@ -246,10 +257,11 @@ backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
 
     // flush the brick into the volume
     const int rowlen = a.rowlen;
-    for (int k = threadIdx.x; k < B3; k += blockDim.x) {
+    for (int e = threadIdx.x; e < B * B * B; e += blockDim.x) {
+      int lx = e % B, t = e / B, ly = t % B, lz = t / B;
+      int k = lz * PS + ly * RS + lx;
       float r = are[k], im = aim[k], ww = aw[k];
       if (r == 0.f && im == 0.f && ww == 0.f) continue;
-      int lx = k % B, t = k / B, ly = t % B, lz = t / B;
       int x = o.x + lx, y = o.y + ly, z = o.z + lz;
       int ys, zs;
       bool alias;
@@ -316,7 +328,7 @@ static int backproject_brick(float* d_volumeft, float* d_volumeweights, const fl
   float pmax = std::sqrt((float)std::max(0, rmax * rmax - 1));
   int st = build_brick_plan(d_mats, (int)batch, g, pmax, limit, brick_chunk_default(), stream, &plan);
   if (st) return st;
-  size_t smem = sizeof(float) * 3 * (size_t)kBrickEdge * kBrickEdge * kBrickEdge;
+  size_t smem = sizeof(float) * 3 * (size_t)kBrickEdge * (kBrickEdge + 1) * (kBrickEdge + 1);
   auto kern = decentered ? (square ? backproject_brick_kernel<true, true> : backproject_brick_kernel<true, false>)
                          : (square ? backproject_brick_kernel<false, true> : backproject_brick_kernel<false, false>);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

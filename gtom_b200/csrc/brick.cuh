@@ -66,10 +66,13 @@ __device__ __forceinline__ bool plane_hits_box(const float* m, float3 qlo, float
 }
 
 // In-plane coordinates: pos = u * c0 + v * c1.  The dual vector d1 gives
-// v = pos . d1 for points on the plane.
+// v = pos . d1 for points on the plane; r0 holds 1 / c0 per axis (0 where
+// that component is negligible).
 struct PlaneFrame {
-  float3 c0, c1, d1;
+  float3 c0, c1, d1, r0;
 };
+
+__device__ __forceinline__ float safe_rcp(float a) { return fabsf(a) > 1e-6f ? 1.f / a : 0.f; }
 
 __device__ __forceinline__ PlaneFrame plane_frame(const float* m) {
   PlaneFrame f;
@@ -81,13 +84,15 @@ __device__ __forceinline__ PlaneFrame plane_frame(const float* m) {
   float inv = 1.f / (g00 * g11 - g01 * g01);
   f.d1 = make_float3((f.c1.x * g00 - f.c0.x * g01) * inv, (f.c1.y * g00 - f.c0.y * g01) * inv,
                      (f.c1.z * g00 - f.c0.z * g01) * inv);
+  f.r0 = make_float3(safe_rcp(f.c0.x), safe_rcp(f.c0.y), safe_rcp(f.c0.z));
   return f;
 }
 
-__device__ __forceinline__ void slab(float a, float b, float lo, float hi, float& ua, float& ub) {
-  // lo <= u * a + b <= hi
-  if (fabsf(a) > 1e-6f) {
-    float t0 = (lo - b) / a, t1 = (hi - b) / a;
+// Narrows [ua, ub] to the u with lo <= u * a + b <= hi (ra = 1/a, or 0 when
+// a is negligible: then b alone decides).
+__device__ __forceinline__ void slab(float ra, float b, float lo, float hi, float& ua, float& ub) {
+  if (ra != 0.f) {
+    float t0 = (lo - b) * ra, t1 = (hi - b) * ra;
     ua = fmaxf(ua, fminf(t0, t1));
     ub = fminf(ub, fmaxf(t0, t1));
   } else if (b < lo || b > hi) {
@@ -112,9 +117,9 @@ __device__ __forceinline__ void row_interval(const PlaneFrame& f, int v, float3 
   while ((umax + 1) * (umax + 1) <= rem) umax++;
   float fa = -1e30f, fb = 1e30f;
   float fv = (float)v;
-  slab(f.c0.x, fv * f.c1.x, qlo.x, qhi.x, fa, fb);
-  slab(f.c0.y, fv * f.c1.y, qlo.y, qhi.y, fa, fb);
-  slab(f.c0.z, fv * f.c1.z, qlo.z, qhi.z, fa, fb);
+  slab(f.r0.x, fv * f.c1.x, qlo.x, qhi.x, fa, fb);
+  slab(f.r0.y, fv * f.c1.y, qlo.y, qhi.y, fa, fb);
+  slab(f.r0.z, fv * f.c1.z, qlo.z, qhi.z, fa, fb);
   if (fa > fb) {
     ua = 1;
     ub = 0;
@@ -157,6 +162,10 @@ __device__ __forceinline__ void for_each_footprint_pixel(const float* m, float3 
   int rmax = (int)sqrtf((float)r2max) + 1;
   int v0, v1;
   v_range(f, qlo, qhi, rmax, v0, v1);
+  // A pixel and its mate can both lie on the walk only if Q and -Q overlap,
+  // i.e. Q straddles the origin on every axis (the few central bricks).
+  const bool dedupe = qlo.x <= 0.5f && qhi.x >= -0.5f && qlo.y <= 0.5f && qhi.y >= -0.5f &&
+                      qlo.z <= 0.5f && qhi.z >= -0.5f;
   for (int vb = v0; vb <= v1; vb += 32) {
     int v = vb + lane;
     int ua = 1, ub = 0;
@@ -190,7 +199,7 @@ __device__ __forceinline__ void for_each_footprint_pixel(const float* m, float3 
         int pu = -qu, pv = -qv;
         if ((pu != qu || pv != qv) && stored_pixel<FULL_X0>(pu, pv, vlo, vhi)) {
           bool direct = false;
-          if (pv >= v0 && pv <= v1) {
+          if (dedupe && pv >= v0 && pv <= v1) {
             int a, bnd;
             row_interval(f, pv, qlo, qhi, r2max, a, bnd);
             direct = pu >= a && pu <= bnd;

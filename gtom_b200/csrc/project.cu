@@ -154,15 +154,17 @@ project_brick_kernel(const float2* __restrict__ vol, float2* __restrict__ proj,
                      const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
                      const int* __restrict__ lists, int* __restrict__ counter) {
   extern __shared__ float2 tile[];
-  __shared__ int item_s;
+  __shared__ int item_s, next_s;
   const int nitems = *nitems_ptr;
   const int B = g.B, T = g.B + 1;
   const int rowlen = a.P / 2 + 1;
   const int64_t last = a.nvox - 1;
-  const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (;;) {
     __syncthreads();  // previous item done with the tile
-    if (threadIdx.x == 0) item_s = atomicAdd(counter, 1);
+    if (threadIdx.x == 0) {
+      item_s = atomicAdd(counter, 1);
+      next_s = 0;
+    }
     __syncthreads();
     const int w = item_s;
     if (w >= nitems) break;
@@ -179,7 +181,11 @@ project_brick_kernel(const float2* __restrict__ vol, float2* __restrict__ proj,
     __syncthreads();
     float3 qlo, qhi;
     brick_box(g, it.brick, qlo, qhi);
-    for (int j = warp; j < it.count; j += nwarps) {
+    for (;;) {  // warps take the item's slices one at a time
+      int j = 0;
+      if ((threadIdx.x & 31) == 0) j = atomicAdd(&next_s, 1);
+      j = __shfl_sync(0xffffffffu, j, 0);
+      if (j >= it.count) break;
       const int slice = __ldg(lists + it.offset + j);
       float m[9];
 #pragma unroll
@@ -245,7 +251,7 @@ int brick_chunk_default() {
   static int chunk = [] {
     const char* e = getenv("GTOMRLN_BRICK_CHUNK");
     int c = e ? atoi(e) : 0;
-    return c > 0 ? c : 512;
+    return c > 0 ? c : 2048;
   }();
   return chunk;
 }
