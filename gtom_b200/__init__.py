@@ -11,5 +11,6 @@ from .relion import (  # noqa: F401
     kaiser_bessel_table,
     matrices_from_angles,
     reconstruct_gridding_tol,
+    set_brick_tuning,
     set_path,
 )

@@ -47,6 +47,7 @@ SIGNATURES: dict[str, list] = {
     "gtomrln_last_error": [],
     "gtomrln_release_caches": [],
     "gtomrln_set_path": [_i, _i],
+    "gtomrln_set_brick_tuning": [_i, _i, _i, _i],
     "gtomrln_matrices_from_angles": [_p, _f, _u, _p],
     "gtomrln_project": [_p, _i, _i, _i, _p, _i, _i, _i, _u, _p, _u, _p],
     "gtomrln_project_angles": [_p, _i, _i, _i, _p, _i, _i, _i, _p, _f, _u, _p],

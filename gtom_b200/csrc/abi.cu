@@ -96,6 +96,17 @@ static std::atomic<int> g_path[2] = {{GTOMRLN_PATH_AUTO}, {GTOMRLN_PATH_AUTO}};
 
 int path_choice(int op) { return (op == 0 || op == 1) ? g_path[op].load() : GTOMRLN_PATH_AUTO; }
 
+// Defaults measured on the B200 at 256^3 (padding 2) with 10,000-slice
+// batches; the autotuner (gtom_b200/autotune.py) can replace them.
+static const BrickTuning kDefaultTuning[2] = {{24, 1024, 2048}, {24, 1024, 2048}};
+static std::mutex g_tuning_mutex;
+static BrickTuning g_tuning[2] = {kDefaultTuning[0], kDefaultTuning[1]};
+
+BrickTuning brick_tuning(int op) {
+  std::lock_guard<std::mutex> lock(g_tuning_mutex);
+  return g_tuning[op == 1 ? 1 : 0];
+}
+
 }  // namespace gtomrln
 
 using namespace gtomrln;
@@ -125,6 +136,27 @@ int gtomrln_set_path(int op, int path) {
       path > GTOMRLN_PATH_BRICK)
     return set_error(GTOMRLN_ERR_INVALID, "set_path: unknown op %d or path %d", op, path);
   g_path[op].store(path);
+  return GTOMRLN_OK;
+}
+
+int gtomrln_set_brick_tuning(int op, int edge, int threads, int chunk) {
+  clear_error();
+  if (op != GTOMRLN_OP_PROJECT && op != GTOMRLN_OP_BACKPROJECT)
+    return set_error(GTOMRLN_ERR_INVALID, "set_brick_tuning: unknown op %d", op);
+  BrickTuning t = kDefaultTuning[op];
+  if (edge) t.edge = edge;
+  if (threads) t.threads = threads;
+  if (chunk) t.chunk = chunk;
+  // Shared memory per CTA: the projector stages (edge+1)^3 complex voxels,
+  // the backprojector keeps 3 * edge * (edge+1)^2 floats; both <= 227 KB.
+  size_t smem = op == GTOMRLN_OP_PROJECT ? 8 * (size_t)(t.edge + 1) * (t.edge + 1) * (t.edge + 1)
+                                         : 12 * (size_t)t.edge * (t.edge + 1) * (t.edge + 1);
+  if (t.edge < 4 || t.edge > 64 || smem > 227 * 1024 || t.threads < 64 || t.threads > 1024 ||
+      t.threads % 32 || t.chunk < 1)
+    return set_error(GTOMRLN_ERR_INVALID, "set_brick_tuning: edge %d, threads %d, chunk %d out of range",
+                     t.edge, t.threads, t.chunk);
+  std::lock_guard<std::mutex> lock(g_tuning_mutex);
+  g_tuning[op] = t;
   return GTOMRLN_OK;
 }
 

@@ -154,13 +154,10 @@ backproject_direct_kernel(float2* __restrict__ volft_base, float* __restrict__ v
 // the brick's only one and the voxel has no alias (decentred y or z = +-V/2
 // share storage), otherwise with vector L2 reductions.
 // ---------------------------------------------------------------------------
-constexpr int kBrickThreads = 256;
-constexpr int kBrickEdge = 16;
 constexpr unsigned kBrickMinBatch = 32;
-int brick_chunk_default();  // project.cu
 
 template <bool DECENTERED, bool SQUARE>
-__global__ void __launch_bounds__(kBrickThreads)
+__global__ void __launch_bounds__(1024)
 backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
                          const float2* __restrict__ projft, const float* __restrict__ projw,
                          const float* __restrict__ mats, BpArgs a, BrickGrid g,
@@ -323,25 +320,29 @@ static int backproject_brick(float* d_volumeft, float* d_volumeweights, const fl
   // wrap beyond the reference's) while every sample radius is below limit.
   const int yhi = decentered ? V / 2 : V - 1 - V / 2;
   const float limit = (float)std::min(V / 2, yhi) - 1e-4f;
-  BrickGrid g = make_brick_grid(V, kBrickEdge, V / 2, -(V / 2), yhi);
-  BrickPlan plan;
-  float pmax = std::sqrt((float)std::max(0, rmax * rmax - 1));
-  int st = build_brick_plan(d_mats, (int)batch, g, pmax, limit, brick_chunk_default(), stream, &plan);
-  if (st) return st;
-  size_t smem = sizeof(float) * 3 * (size_t)kBrickEdge * (kBrickEdge + 1) * (kBrickEdge + 1);
+  const BrickTuning tune = brick_tuning(GTOMRLN_OP_BACKPROJECT);
+  BrickGrid g = make_brick_grid(V, tune.edge, V / 2, -(V / 2), yhi);
+  size_t smem = sizeof(float) * 3 * (size_t)tune.edge * (tune.edge + 1) * (tune.edge + 1);
   auto kern = decentered ? (square ? backproject_brick_kernel<true, true> : backproject_brick_kernel<true, false>)
                          : (square ? backproject_brick_kernel<false, true> : backproject_brick_kernel<false, false>);
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess)
+    return set_error(GTOMRLN_ERR_CUDA, "brick backprojector: %zu B of shared memory refused: %s", smem,
+                     cudaGetErrorString(e));
   int dev = 0, sms = 148, occ = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBrickThreads, smem);
-  kern<<<sms * std::max(occ, 1), kBrickThreads, smem, stream>>>(
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, tune.threads, smem);
+  BrickPlan plan;
+  float pmax = std::sqrt((float)std::max(0, rmax * rmax - 1));
+  int st = build_brick_plan(d_mats, (int)batch, g, pmax, limit, tune.chunk, stream, &plan);
+  if (st) return st;
+  kern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
       (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, a, g, plan.items,
       plan.nitems, plan.lists, plan.counter);
   launch_bp_direct_any(dim3(sms * 4), stream, (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft,
                        d_projweights, d_mats, nullptr, a, plan.fallback, plan.nfallback, 2, decentered, square);
-  cudaError_t e = cudaGetLastError();
+  e = cudaGetLastError();
   free_brick_plan(&plan, stream);
   if (e != cudaSuccess)
     return set_error(GTOMRLN_ERR_CUDA, "launch of the brick backprojector failed: %s", cudaGetErrorString(e));

@@ -47,6 +47,13 @@ void matrices_from_angles(const float* angles, float supersample, unsigned batch
 // Implementation chosen for op (GTOMRLN_OP_*) by gtomrln_set_path.
 int path_choice(int op);
 
+// Launch shape of the brick kernels for op: brick edge in voxels, threads
+// per CTA, and the most slices one work item takes (gtomrln_set_brick_tuning).
+struct BrickTuning {
+  int edge, threads, chunk;
+};
+BrickTuning brick_tuning(int op);
+
 // Stream-ordered device scratch from the library's memory pool.
 int pool_alloc(void** ptr, size_t bytes, cudaStream_t stream);
 int pool_free(void* ptr, cudaStream_t stream);

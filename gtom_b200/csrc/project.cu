@@ -146,9 +146,7 @@ project_listed_kernel(ArrayFetch fetch, float2* __restrict__ proj, const float* 
 // voxel values: the results are identical.  Pixels outside rmax are zeroed
 // by project_zero_kernel.
 // ---------------------------------------------------------------------------
-constexpr int kBrickThreads = 256;
-
-__global__ void __launch_bounds__(kBrickThreads)
+__global__ void __launch_bounds__(1024)
 project_brick_kernel(const float2* __restrict__ vol, float2* __restrict__ proj,
                      const float* __restrict__ mats, ProjArgs a, BrickGrid g,
                      const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
@@ -244,18 +242,6 @@ __global__ void project_zero_kernel(float2* __restrict__ proj, ProjArgs a, int64
   }
 }
 
-// Brick edge and slices per work item of the brick paths.  Chosen for the
-// B200 (see the autotuner notes); overridable for experiments through
-// GTOMRLN_BRICK_CHUNK.
-int brick_chunk_default() {
-  static int chunk = [] {
-    const char* e = getenv("GTOMRLN_BRICK_CHUNK");
-    int c = e ? atoi(e) : 0;
-    return c > 0 ? c : 2048;
-  }();
-  return chunk;
-}
-constexpr int kBrickEdge = 16;
 constexpr unsigned kBrickMinBatch = 32;
 
 // The brick path: plan, zero fill outside rmax, brick kernel, and the direct
@@ -263,32 +249,33 @@ constexpr unsigned kBrickMinBatch = 32;
 static int project_brick(const float* d_volumeft, float* d_proj, const float* d_mats, const ProjArgs& a,
                          unsigned batch, cudaStream_t stream) {
   const int P = a.P;
+  const BrickTuning tune = brick_tuning(GTOMRLN_OP_PROJECT);
   // While every sample radius stays below P/2 + 0.99, the base voxels lie in
   // x [0, P/2] and y, z [-P/2 - 1, P/2].
-  BrickGrid g = make_brick_grid(P, kBrickEdge, P / 2, -(P / 2) - 1, P / 2);
-  BrickPlan plan;
-  int st = build_brick_plan(d_mats, (int)batch, g, (float)a.rmax, (float)(P / 2) + 0.99f,
-                            brick_chunk_default(), stream, &plan);
-  if (st) return st;
-  size_t smem = sizeof(float2) * (size_t)(kBrickEdge + 1) * (kBrickEdge + 1) * (kBrickEdge + 1);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(project_brick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
+  BrickGrid g = make_brick_grid(P, tune.edge, P / 2, -(P / 2) - 1, P / 2);
+  size_t smem = sizeof(float2) * (size_t)(tune.edge + 1) * (tune.edge + 1) * (tune.edge + 1);
+  cudaError_t e = cudaFuncSetAttribute(project_brick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess)
+    return set_error(GTOMRLN_ERR_CUDA, "brick projector: %zu B of shared memory refused: %s", smem,
+                     cudaGetErrorString(e));
   int dev = 0, sms = 148, occ = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, project_brick_kernel, kBrickThreads, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, project_brick_kernel, tune.threads, smem);
+  BrickPlan plan;
+  int st = build_brick_plan(d_mats, (int)batch, g, (float)a.rmax, (float)(P / 2) + 0.99f, tune.chunk, stream,
+                            &plan);
+  if (st) return st;
   int64_t rows = (int64_t)a.n * batch;  // 2D slices: n rows of dimft elements each
   project_zero_kernel<<<sms * 8, 256, 0, stream>>>((float2*)d_proj, a, rows);
-  project_brick_kernel<<<sms * std::max(occ, 1), kBrickThreads, smem, stream>>>(
+  project_brick_kernel<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
       (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, plan.items, plan.nitems, plan.lists,
       plan.counter);
   ArrayFetch f{(const float2*)d_volumeft, a.P, a.P / 2 + 1, a.nvox - 1};
   project_listed_kernel<<<sms * 4, kProjThreads, 0, stream>>>(f, (float2*)d_proj, d_mats, a, plan.fallback,
                                                                plan.nfallback);
-  cudaError_t e = cudaGetLastError();
+  e = cudaGetLastError();
   free_brick_plan(&plan, stream);
   if (e != cudaSuccess)
     return set_error(GTOMRLN_ERR_CUDA, "launch of the brick projector failed: %s", cudaGetErrorString(e));

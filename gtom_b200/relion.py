@@ -218,6 +218,12 @@ def set_path(op: str, path: str) -> None:
     _lib.call("gtomrln_set_path", _OPS[op], _PATHS[path])
 
 
+def set_brick_tuning(op: str, edge: int = 0, threads: int = 0, chunk: int = 0) -> None:
+    """Launch shape of the brick-major kernels of "project" or "backproject"
+    (gtomrln_set_brick_tuning); 0 keeps the default for a field."""
+    _lib.call("gtomrln_set_brick_tuning", _OPS[op], int(edge), int(threads), int(chunk))
+
+
 def kaiser_bessel_table(radius: float, alpha: float, order: int = 0,
                         nsamples: int = 10000) -> np.ndarray:
     """The normalised blob table of the gridding correction."""

@@ -77,6 +77,14 @@ GTOMRLN_API int gtomrln_release_caches(void);
 #define GTOMRLN_PATH_BRICK 2
 GTOMRLN_API int gtomrln_set_path(int op, int path);
 
+/* Extension (no reference counterpart): launch shape of the brick-major
+ * kernels of op for the calling process — brick edge in voxels, threads per
+ * CTA (multiple of 32, <= 1024) and the most slices one work item takes.
+ * 0 keeps the built-in default for that field.  Results do not depend on
+ * these (the projector's are bit-identical for any shape); speed does.
+ * Returns GTOMRLN_ERR_INVALID for shapes whose shared memory exceeds a CTA's. */
+GTOMRLN_API int gtomrln_set_brick_tuning(int op, int edge, int threads, int chunk);
+
 /* Host helper: M_b = transpose(Matrix3Euler(angles_b)) * supersample, the
  * matrices the h_angles overloads build (src/Relion/Project.cu:14-16,
  * src/Helpers/Euler.cu:39-68).  Writes 9 * batch floats, column-major. */
