@@ -13,6 +13,7 @@
 
 #include "brick.cuh"
 #include "common.cuh"
+#include "sample.cuh"
 
 namespace gtomrln {
 
@@ -143,13 +144,14 @@ backproject_direct_kernel(float2* __restrict__ volft_base, float* __restrict__ v
 
 // ---------------------------------------------------------------------------
 // Brick-major backprojector: insertion privatised per shared-memory brick.
-// A work item owns one 16^3 brick of the (signed-coordinate) volume as three
-// FP32 accumulators (re, im, weight) in shared memory.  Each warp takes one
-// of the item's slices and walks the pixels whose sample, or whose Friedel
-// mate's sample, lies within one voxel of the brick; per pixel it evaluates
-// the reference's eight binary16-rounded trilinear weights, Friedel mirroring
-// and the second insertion on the x = 0 plane, and adds the targets that
-// fall inside the brick to shared memory.  At the end of the item the brick
+// A work item owns one edge^3 brick of the (signed-coordinate) volume as
+// three FP32 accumulators (re, im, weight) in shared memory.  The warps take
+// the item's bins (slice, pixel run) one at a time: the plan binned every
+// pixel under each brick one of its targets falls into.  Per pixel a lane
+// evaluates the reference's eight binary16-rounded trilinear weights,
+// Friedel mirroring and the second insertion on the x = 0 plane, and adds
+// the targets inside the brick to shared memory (a whole 2x2x2 cube inside
+// the brick takes a path without per-target tests).  At the end of the item the brick
 // is added to the volume once: with plain read-add-write when the item is
 // the brick's only one and the voxel has no alias (decentred y or z = +-V/2
 // share storage), otherwise with vector L2 reductions.
@@ -162,7 +164,8 @@ backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
                          const float2* __restrict__ projft, const float* __restrict__ projw,
                          const float* __restrict__ mats, BpArgs a, BrickGrid g,
                          const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
-                         const int* __restrict__ lists, int* __restrict__ counter) {
+                         const int* __restrict__ pairs, const PixelBin* __restrict__ bins,
+                         const int* __restrict__ entries, int* __restrict__ counter) {
   extern __shared__ float acc[];
   __shared__ int item_s, next_s;
   const int nitems = *nitems_ptr;
@@ -188,67 +191,64 @@ backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
     if (w >= nitems) break;
     const BrickItem it = items[w];
     const int3 o = brick_origin(g, it.brick);
-    float3 qlo, qhi;
-    brick_box(g, it.brick, qlo, qhi);
 
-    for (;;) {  // warps take the item's slices one at a time
+    for (;;) {  // warps take the item's bins one at a time
       int j = 0;
       if (lane == 0) j = atomicAdd(&next_s, 1);
       j = __shfl_sync(0xffffffffu, j, 0);
       if (j >= it.count) break;
-      const int slice = __ldg(lists + it.offset + j);
+      const PixelBin bn = bins[__ldg(pairs + it.offset + j)];
       float m[9];
 #pragma unroll
-      for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
-      for_each_footprint_pixel<false>(m, qlo, qhi, a.rmax2 - 1, a.n / 2 + 1 - a.n, a.n / 2,
-                                      [&](int u, int v) {
-        // pixel (u, v): r^2 < rmax^2 and not (u == 0 && v < 0) by construction
-        int idy = v >= 0 ? v : v + a.n;
-        int64_t id = a.elements * slice + (int64_t)idy * a.dimft + u;
-        float3 pos = mat_apply(m, (float)u, (float)v, 0.f);
-        int x0 = (short)floorf(pos.x + 1e-5f);
-        int y0 = (short)floorf(pos.y);
-        int z0 = (short)floorf(pos.z);
-        float fx = pos.x - (float)x0, fy = pos.y - (float)y0, fz = pos.z - (float)z0;
-        float c0 = 1.f - fz, c1 = fz;
-        float c00 = half_round((1.f - fy) * c0), c10 = half_round(fy * c0);
-        float c01 = half_round((1.f - fy) * c1), c11 = half_round(fy * c1);
-        float wt[8];
-        wt[0] = half_round((1.f - fx) * c00); wt[1] = half_round(fx * c00);
-        wt[2] = half_round((1.f - fx) * c10); wt[3] = half_round(fx * c10);
-        wt[4] = half_round((1.f - fx) * c01); wt[5] = half_round(fx * c01);
-        wt[6] = half_round((1.f - fx) * c11); wt[7] = half_round(fx * c11);
+      for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)bn.slice + k);
+      for (int e = lane; e < bn.count; e += 32) {
+        const int pid = __ldg(entries + bn.start + e);
+        int u, v;
+        pixel_uv(pid, a.n, a.dimft, u, v);
+        const int64_t id = a.elements * bn.slice + pid;
+        BpSample s = backproject_sample(m, (float)u, (float)v, 0.f);
         float2 val = projft ? __ldg(projft + id) : make_float2(1.f, 0.f);
         float pw = projw ? __ldg(projw + id) : 1.f;
+        if (SQUARE) {
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-          int nx = x0 + (i & 1), ny = y0 + ((i >> 1) & 1), nz = z0 + ((i >> 2) & 1);
-          float iw = wt[i];
-          if (SQUARE) iw *= iw;
-          int tx = nx, ty = ny, tz = nz;
-          float sim = val.y;
-          if (tx < 0) {
-            tx = -tx; ty = -ty; tz = -tz;
-            sim = -sim;
+          for (int i = 0; i < 8; i++) s.w[i] *= s.w[i];
+        }
+        const int lx0 = s.x0 - o.x, ly0 = s.y0 - o.y, lz0 = s.z0 - o.z;
+        const int mx0 = -s.x0 - 1 - o.x, my0 = -s.y0 - 1 - o.y, mz0 = -s.z0 - 1 - o.z;
+        if (s.x0 >= 1 && (unsigned)lx0 < (unsigned)(B - 1) && (unsigned)ly0 < (unsigned)(B - 1) &&
+            (unsigned)lz0 < (unsigned)(B - 1)) {
+          // whole 2x2x2 cube inside the brick, no mirroring, no x = 0 plane
+          const int k0 = lz0 * PS + ly0 * RS + lx0;
+#pragma unroll
+          for (int i = 0; i < 8; i++) {
+            int k = k0 + (i & 1) + ((i >> 1) & 1) * RS + ((i >> 2) & 1) * PS;
+            atomicAdd(are + k, s.w[i] * val.x);
+            atomicAdd(aim + k, s.w[i] * val.y);
+            atomicAdd(aw + k, s.w[i] * pw);
           }
-          int lx = tx - o.x, ly = ty - o.y, lz = tz - o.z;
-          if ((unsigned)lx < (unsigned)B && (unsigned)ly < (unsigned)B && (unsigned)lz < (unsigned)B) {
-            int k = lz * PS + ly * RS + lx;
-            atomicAdd(are + k, iw * val.x);
-            atomicAdd(aim + k, iw * sim);
-            atomicAdd(aw + k, iw * pw);
+        } else if (s.x0 <= -2 && (unsigned)mx0 < (unsigned)(B - 1) && (unsigned)my0 < (unsigned)(B - 1) &&
+                   (unsigned)mz0 < (unsigned)(B - 1)) {
+          // whole cube mirrored to (-x0-1 .. -x0, ...) inside the brick, conjugated
+          const int k0 = mz0 * PS + my0 * RS + mx0;
+#pragma unroll
+          for (int i = 0; i < 8; i++) {
+            int k = k0 + (1 - (i & 1)) + (1 - ((i >> 1) & 1)) * RS + (1 - ((i >> 2) & 1)) * PS;
+            atomicAdd(are + k, s.w[i] * val.x);
+            atomicAdd(aim + k, s.w[i] * -val.y);
+            atomicAdd(aw + k, s.w[i] * pw);
           }
-          if (nx == 0 && (ny != 0 || nz != 0)) {  // second insertion on the x = 0 plane
-            lx = -o.x; ly = -ny - o.y; lz = -nz - o.z;
+        } else {
+          for_each_target(s.x0, s.y0, s.z0, [&](int i, int x, int y, int z, bool conj) {
+            int lx = x - o.x, ly = y - o.y, lz = z - o.z;
             if ((unsigned)lx < (unsigned)B && (unsigned)ly < (unsigned)B && (unsigned)lz < (unsigned)B) {
               int k = lz * PS + ly * RS + lx;
-              atomicAdd(are + k, iw * val.x);
-              atomicAdd(aim + k, iw * -sim);
-              atomicAdd(aw + k, iw * pw);
+              atomicAdd(are + k, s.w[i] * val.x);
+              atomicAdd(aim + k, s.w[i] * (conj ? -val.y : val.y));
+              atomicAdd(aw + k, s.w[i] * pw);
             }
-          }
+          });
         }
-      });
+      }
     }
     __syncthreads();
 
@@ -333,13 +333,19 @@ static int backproject_brick(float* d_volumeft, float* d_volumeweights, const fl
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, tune.threads, smem);
+  PixelSet px;
+  px.n = a.n;
+  px.dimft = a.dimft;
+  px.elements = a.elements;
+  px.rmax2 = a.rmax2;
+  px.strict = 1;
+  px.pmax = std::sqrt((float)std::max(0, rmax * rmax - 1));
   BrickPlan plan;
-  float pmax = std::sqrt((float)std::max(0, rmax * rmax - 1));
-  int st = build_brick_plan(d_mats, (int)batch, g, pmax, limit, tune.chunk, stream, &plan);
+  int st = build_brick_plan(GTOMRLN_OP_BACKPROJECT, d_mats, (int)batch, g, px, limit, tune.chunk, stream, &plan);
   if (st) return st;
   kern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
       (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, a, g, plan.items,
-      plan.nitems, plan.lists, plan.counter);
+      plan.nitems, plan.pairs, plan.bins, plan.entries, plan.counter);
   launch_bp_direct_any(dim3(sms * 4), stream, (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft,
                        d_projweights, d_mats, nullptr, a, plan.fallback, plan.nfallback, 2, decentered, square);
   e = cudaGetLastError();

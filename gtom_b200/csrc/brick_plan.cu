@@ -1,123 +1,175 @@
-// Plan construction for the brick-major kernels, entirely on the device (no
-// host synchronisation, so a call can be captured in a CUDA graph):
+// Binning plan for the brick-major kernels (see brick.cuh), built entirely
+// on the device so that a call never synchronises with the host.
 //
-//  1. bin_count: one warp per slice rasterises the slice's central plane
-//     over the brick grid (columns along the plane normal's dominant axis)
-//     and counts, per brick, the slices that cross it.  Slices whose samples
-//     could leave the region the brick kernels handle (larger radius than
-//     `limit`) go to a fallback list for the direct kernels instead.
-//  2. plan_scan: one block turns the counts into list offsets and work
-//     items (at most `chunk` slices each), bricks in order of increasing
-//     distance from the origin so that the heaviest items start first.
-//  3. bin_fill: the same rasterisation writes each slice into its bricks'
-//     lists.
-//  4. plan_items: one thread per brick writes its items.
+//   bin_slices_kernel   one CTA per slice: brick(s) of every pixel, a
+//                       shared-memory histogram over bricks, the slice's bins
+//                       and its pixel ids sorted by brick;
+//   pairs_scan_kernel   one CTA: per-brick bin offsets and work items, bricks
+//                       in order of increasing distance from the origin so
+//                       that the heaviest items start first;
+//   pairs_fill_kernel   groups the bins by brick;
+//   plan_items_kernel   writes the work items.
 #include <algorithm>
 #include <cmath>
-#include <cstring>
 #include <map>
 #include <mutex>
 #include <numeric>
 #include <tuple>
 
 #include "brick.cuh"
+#include "sample.cuh"
 
 namespace gtomrln {
 
-constexpr int kBinWarps = 8;  // warps (slices) per block of the binning kernels
+constexpr int kBinThreads = 512;
+constexpr int kMaxBinsPerSlice = 2048;  // bins reserved per slice on average
+constexpr int kMaxPixelBricks = 16;
 
-__device__ __forceinline__ bool box_within_disk(float3 qlo, float3 qhi, float rdisk) {
-  float px = fminf(fmaxf(0.f, qlo.x), qhi.x), py = fminf(fmaxf(0.f, qlo.y), qhi.y),
-        pz = fminf(fmaxf(0.f, qlo.z), qhi.z);
-  return px * px + py * py + pz * pz <= rdisk * rdisk;
+__device__ __forceinline__ bool in_pixel_set(const PixelSet& px, int u, int v) {
+  int r2 = u * u + v * v;
+  if (px.strict) return r2 < px.rmax2 && !(u == 0 && v < 0);
+  return r2 <= px.rmax2;
 }
 
-// Calls hit(b) for every brick b whose dilated box the slice's plane
-// crosses within its disk (the same test as plane_hits_box).  Warp-wide:
-// the lanes split the columns.
-template <class Hit>
-__device__ __forceinline__ void for_each_crossed_brick(const float* m, const BrickGrid& g, float rdisk,
-                                                       Hit&& hit) {
-  const int lane = threadIdx.x & 31;
-  float3 c0 = make_float3(m[0], m[1], m[2]), c1 = make_float3(m[3], m[4], m[5]);
-  float n[3] = {c0.y * c1.z - c0.z * c1.y, c0.z * c1.x - c0.x * c1.z, c0.x * c1.y - c0.y * c1.x};
-  float an[3] = {fabsf(n[0]), fabsf(n[1]), fabsf(n[2])};
-  int k = an[0] >= an[1] ? (an[0] >= an[2] ? 0 : 2) : (an[1] >= an[2] ? 1 : 2);  // dominant axis
-  int i = k == 0 ? 1 : 0, j = k == 2 ? 1 : 2;
-  const int nb[3] = {g.nbx, g.nby, g.nbz};
-  const int lo0[3] = {0, g.ylo, g.zlo};
-  const float guard = 1.0f + 1e-2f;
-  // Covers plane_hits_box's own tolerance (1e-3 |n| (1 + |c|_1) along n,
-  // at most sqrt(3) times that along the dominant axis).
-  const float tol = 4e-3f;
-  int ncols = nb[i] * nb[j];
-  for (int col = lane; col < ncols; col += 32) {
-    int bi = col % nb[i], bj = col / nb[i];
-    float ilo = lo0[i] + bi * g.B - guard, ihi = lo0[i] + bi * g.B + g.B - 1 + guard;
-    float jlo = lo0[j] + bj * g.B - guard, jhi = lo0[j] + bj * g.B + g.B - 1 + guard;
-    // plane: n_k x_k = -(n_i x_i + n_j x_j); its x_k range over the column's rectangle
-    float a0 = n[i] * ilo, a1 = n[i] * ihi, b0 = n[j] * jlo, b1 = n[j] * jhi;
-    float smin = fminf(a0, a1) + fminf(b0, b1), smax = fmaxf(a0, a1) + fmaxf(b0, b1);
-    float kmin = fminf(-smin / n[k], -smax / n[k]), kmax = fmaxf(-smin / n[k], -smax / n[k]);
-    float pad = guard + tol * (1.f + fabsf(kmin) + fabsf(kmax) + fmaxf(fabsf(ilo), fabsf(ihi)) +
-                               fmaxf(fabsf(jlo), fabsf(jhi)));
-    int b_lo = (int)floorf((kmin - pad - lo0[k]) / g.B);
-    int b_hi = (int)floorf((kmax + pad - lo0[k]) / g.B);
-    b_lo = max(b_lo, 0);
-    b_hi = min(b_hi, nb[k] - 1);
-    for (int bk = b_lo; bk <= b_hi; bk++) {
-      int idx[3];
-      idx[i] = bi;
-      idx[j] = bj;
-      idx[k] = bk;
-      int b = (idx[2] * g.nby + idx[1]) * g.nbx + idx[0];
-      float3 qlo, qhi;
-      brick_box(g, b, qlo, qhi);
-      if (box_within_disk(qlo, qhi, rdisk) && plane_hits_box(m, qlo, qhi, rdisk)) hit(b);
-    }
+// The bricks pixel (u, v) of a slice with matrix m reads from (projector)
+// or adds to (backprojector), without repeats.  Returns the count, or -1 if
+// some voxel falls outside the grid (the slice must then take the direct path).
+template <int OP>
+__device__ __forceinline__ int pixel_bricks(const float* m, int u, int v, const BrickGrid& g,
+                                            int (&out)[kMaxPixelBricks]) {
+  if (OP == GTOMRLN_OP_PROJECT) {
+    ProjSample s = project_sample(m, u, v, 0);
+    int b = brick_of(g, s.x0, s.y0, s.z0);
+    out[0] = b;
+    return b < 0 ? -1 : 1;
+  } else {
+    BpSample s = backproject_sample(m, (float)u, (float)v, 0.f);
+    int n = 0;
+    bool bad = false;
+    for_each_target(s.x0, s.y0, s.z0, [&](int, int x, int y, int z, bool) {
+      int b = brick_of(g, x, y, z);
+      if (b < 0) {
+        bad = true;
+        return;
+      }
+      for (int k = 0; k < n; k++)
+        if (out[k] == b) return;
+      out[n++] = b;
+    });
+    return bad ? -1 : n;
   }
 }
 
-__global__ void __launch_bounds__(kBinWarps * 32)
-bin_count_kernel(const float* __restrict__ mats, int batch, BrickGrid g, float pmax, float limit,
-                 int* __restrict__ counts, int* __restrict__ fallback, int* __restrict__ nfallback) {
-  const int slice = blockIdx.x * kBinWarps + (threadIdx.x >> 5);
-  if (slice >= batch) return;
+template <int OP>
+__global__ void __launch_bounds__(kBinThreads)
+bin_slices_kernel(const float* __restrict__ mats, BrickGrid g, PixelSet px, float limit,
+                  int* __restrict__ entries, int64_t entries_cap, PixelBin* __restrict__ bins,
+                  int64_t bins_cap, unsigned long long* __restrict__ counters,
+                  int* __restrict__ brick_pairs, int* __restrict__ fallback, int* __restrict__ nfallback) {
+  extern __shared__ int hist[];  // nbricks
+  __shared__ int s_bad, s_sum[kBinThreads / 32], s_nz[kBinThreads / 32];
+  __shared__ long long s_base_e, s_base_b;
+  const int slice = blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   float m[9];
 #pragma unroll
   for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
-  float r = plane_scale(m) * pmax;
-  if (!(r < limit)) {
-    if ((threadIdx.x & 31) == 0) fallback[atomicAdd(nfallback, 1)] = slice;
+  if (!(plane_scale(m) * px.pmax < limit)) {  // uniform over the block
+    if (tid == 0) fallback[atomicAdd(nfallback, 1)] = slice;
     return;
   }
-  for_each_crossed_brick(m, g, r + 1e-2f, [&](int b) { atomicAdd(counts + b, 1); });
-}
-
-__global__ void __launch_bounds__(kBinWarps * 32)
-bin_fill_kernel(const float* __restrict__ mats, int batch, BrickGrid g, float pmax, float limit,
-                const int* __restrict__ offsets, const int* __restrict__ counts,
-                int* __restrict__ cursor, int* __restrict__ lists) {
-  const int slice = blockIdx.x * kBinWarps + (threadIdx.x >> 5);
-  if (slice >= batch) return;
-  float m[9];
+  for (int b = tid; b < g.nbricks; b += kBinThreads) hist[b] = 0;
+  if (tid == 0) s_bad = 0;
+  __syncthreads();
+  for (int id = tid; id < px.elements; id += kBinThreads) {
+    int u, v;
+    pixel_uv(id, px.n, px.dimft, u, v);
+    if (!in_pixel_set(px, u, v)) continue;
+    int bl[kMaxPixelBricks];
+    int nb = pixel_bricks<OP>(m, u, v, g, bl);
+    if (nb < 0) {
+      s_bad = 1;
+      continue;
+    }
+    for (int k = 0; k < nb; k++) atomicAdd(&hist[bl[k]], 1);
+  }
+  __syncthreads();
+  if (s_bad) {
+    if (tid == 0) fallback[atomicAdd(nfallback, 1)] = slice;
+    return;
+  }
+  // Each thread owns a contiguous run of bricks: sum its counts and nonzero
+  // bins, scan those over the block, then turn counts into offsets.
+  const int per = (g.nbricks + kBinThreads - 1) / kBinThreads;
+  const int b0 = min(tid * per, g.nbricks), b1 = min(b0 + per, g.nbricks);
+  int sum = 0, nz = 0;
+  for (int b = b0; b < b1; b++) {
+    sum += hist[b];
+    nz += hist[b] > 0;
+  }
+  int isum = sum, inz = nz;
 #pragma unroll
-  for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
-  float r = plane_scale(m) * pmax;
-  if (!(r < limit)) return;
-  for_each_crossed_brick(m, g, r + 1e-2f, [&](int b) {
-    int s = atomicAdd(cursor + b, 1);
-    if (s < counts[b]) lists[offsets[b] + s] = slice;  // never past the brick's share
-  });
+  for (int o = 1; o < 32; o <<= 1) {
+    int a = __shfl_up_sync(0xffffffffu, isum, o), c = __shfl_up_sync(0xffffffffu, inz, o);
+    if (lane >= o) {
+      isum += a;
+      inz += c;
+    }
+  }
+  if (lane == 31) {
+    s_sum[warp] = isum;
+    s_nz[warp] = inz;
+  }
+  __syncthreads();
+  int wsum = 0, wnz = 0, tsum = 0, tnz = 0;
+  for (int w = 0; w < kBinThreads / 32; w++) {
+    if (w < warp) {
+      wsum += s_sum[w];
+      wnz += s_nz[w];
+    }
+    tsum += s_sum[w];
+    tnz += s_nz[w];
+  }
+  if (tid == 0) {
+    s_base_e = (long long)atomicAdd(counters + 0, (unsigned long long)tsum);
+    s_base_b = (long long)atomicAdd(counters + 1, (unsigned long long)tnz);
+  }
+  __syncthreads();
+  if (s_base_e + tsum > entries_cap || s_base_b + tnz > bins_cap) {  // out of room: direct path
+    for (long long k = s_base_b + tid; k < s_base_b + tnz && k < bins_cap; k += kBinThreads)
+      bins[k].brick = -1;  // reserved but empty
+    if (tid == 0) fallback[atomicAdd(nfallback, 1)] = slice;
+    return;
+  }
+  int off = wsum + isum - sum, bi = wnz + inz - nz;
+  for (int b = b0; b < b1; b++) {
+    int c = hist[b];
+    hist[b] = off;
+    if (c > 0) {
+      bins[s_base_b + bi] = {slice, (int)(s_base_e + off), c, b};
+      atomicAdd(brick_pairs + b, 1);
+      bi++;
+    }
+    off += c;
+  }
+  __syncthreads();
+  for (int id = tid; id < px.elements; id += kBinThreads) {
+    int u, v;
+    pixel_uv(id, px.n, px.dimft, u, v);
+    if (!in_pixel_set(px, u, v)) continue;
+    int bl[kMaxPixelBricks];
+    int nb = pixel_bricks<OP>(m, u, v, g, bl);
+    for (int k = 0; k < nb; k++) entries[s_base_e + atomicAdd(&hist[bl[k]], 1)] = id;
+  }
 }
 
-// Single block.  Bricks are visited in `order` (increasing distance from
-// the origin); writes list offsets, per-brick item offsets and the item count.
+// Single block.  Bricks are visited in `order` (increasing distance from the
+// origin); writes bin-list offsets, per-brick item offsets and the item count.
 constexpr int kScanThreads = 1024;
 __global__ void __launch_bounds__(kScanThreads)
-plan_scan_kernel(const int* __restrict__ counts, const int* __restrict__ order, int nbricks, int chunk,
-                 int* __restrict__ offsets, int* __restrict__ item_off, int* __restrict__ cursor,
-                 int* __restrict__ nitems) {
+pairs_scan_kernel(const int* __restrict__ counts, const int* __restrict__ order, int nbricks, int chunk,
+                  int* __restrict__ offsets, int* __restrict__ item_off, int* __restrict__ cursor,
+                  int* __restrict__ nitems) {
   __shared__ int s_c[kScanThreads], s_i[kScanThreads];
   __shared__ int carry_c, carry_i;
   if (threadIdx.x == 0) carry_c = carry_i = 0;
@@ -151,6 +203,20 @@ plan_scan_kernel(const int* __restrict__ counts, const int* __restrict__ order, 
     __syncthreads();
   }
   if (threadIdx.x == 0) *nitems = carry_i;
+}
+
+__global__ void pairs_fill_kernel(const PixelBin* __restrict__ bins,
+                                  const unsigned long long* __restrict__ counters, int64_t bins_cap,
+                                  const int* __restrict__ counts, const int* __restrict__ offsets,
+                                  int* __restrict__ cursor, int* __restrict__ pairs) {
+  int64_t nb = (int64_t)min(counters[1], (unsigned long long)bins_cap);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int b = bins[i].brick;
+    if (b < 0) continue;  // reserved by a slice that fell back
+    int s = atomicAdd(cursor + b, 1);
+    if (s < counts[b]) pairs[offsets[b] + s] = (int)i;
+  }
 }
 
 __global__ void plan_items_kernel(const int* __restrict__ counts, const int* __restrict__ offsets,
@@ -196,60 +262,82 @@ static int brick_order(const BrickGrid& g, const int** out) {
   return GTOMRLN_OK;
 }
 
-int build_brick_plan(const float* d_mats, int batch, const BrickGrid& g, float pmax, float limit,
-                     int chunk, cudaStream_t stream, BrickPlan* plan) {
+int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g, const PixelSet& px,
+                     float limit, int chunk, cudaStream_t stream, BrickPlan* plan) {
   plan->g = g;
   plan->batch = batch;
+  size_t hist_bytes = sizeof(int) * (size_t)g.nbricks;
+  if (hist_bytes > 200 * 1024)
+    return set_error(GTOMRLN_ERR_INVALID, "brick grid of %d bricks too fine for the binning plan", g.nbricks);
   const int* d_order = nullptr;
   int st = brick_order(g, &d_order);
   if (st) return st;
-  // Upper bound of the bricks one plane can cross: per column along the
-  // dominant axis of its normal the plane spans at most 3 (B + 2.02) voxels
-  // (the other two slopes are <= 1), i.e. at most 5 bricks.
-  int64_t cols = std::max({(int64_t)g.nby * g.nbz, (int64_t)g.nbx * g.nbz, (int64_t)g.nbx * g.nby});
-  int64_t cap_lists = std::max<int64_t>(1, (int64_t)batch * cols * 5);
-  int64_t cap_items = (int64_t)g.nbricks + cap_lists / chunk + 1;
-  if (cap_lists > 0x7fffffffLL)
+  // Capacities: the projector bins each pixel once; the backprojector's
+  // pixels land in ~1.2-1.5 bricks on average (8 at most), so twice the
+  // pixel count is reserved.  A slice that does not fit takes the direct path.
+  int64_t npix = px.elements;
+  int64_t entries_cap = std::max<int64_t>(1, (int64_t)batch * npix * (op == GTOMRLN_OP_PROJECT ? 1 : 2));
+  int64_t bins_cap = std::max<int64_t>(1, (int64_t)batch * std::min(g.nbricks, kMaxBinsPerSlice));
+  if (entries_cap > 0x7fffffffLL || bins_cap > 0x7fffffffLL)
     return set_error(GTOMRLN_ERR_INVALID, "brick plan too large for one call; split the batch");
+  int64_t cap_items = (int64_t)g.nbricks + bins_cap / chunk + 1;
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   size_t nb = (size_t)g.nbricks;
-  size_t off_counts = 0;
-  size_t off_offsets = off_counts + al(nb * 4);
-  size_t off_itemoff = off_offsets + al(nb * 4);
-  size_t off_cursor = off_itemoff + al(nb * 4);
-  size_t off_misc = off_cursor + al(nb * 4);                // counter, nitems, nfallback
-  size_t off_fallback = off_misc + 256;
-  size_t off_items = off_fallback + al((size_t)std::max(batch, 1) * 4);
-  size_t off_lists = off_items + al((size_t)cap_items * sizeof(BrickItem));
-  size_t bytes = off_lists + al((size_t)cap_lists * 4);
+  size_t o_counts = 0;
+  size_t o_offsets = o_counts + al(nb * 4);
+  size_t o_itemoff = o_offsets + al(nb * 4);
+  size_t o_cursor = o_itemoff + al(nb * 4);
+  size_t o_misc = o_cursor + al(nb * 4);  // counters (2 x u64), work counter, nitems, nfallback
+  size_t o_fallback = o_misc + 256;
+  size_t o_items = o_fallback + al((size_t)std::max(batch, 1) * 4);
+  size_t o_bins = o_items + al((size_t)cap_items * sizeof(BrickItem));
+  size_t o_pairs = o_bins + al((size_t)bins_cap * sizeof(PixelBin));
+  size_t o_entries = o_pairs + al((size_t)bins_cap * 4);
+  size_t bytes = o_entries + al((size_t)entries_cap * 4);
   char* base = nullptr;
   st = pool_alloc((void**)&base, bytes, stream);
   if (st) return st;
   plan->scratch = base;
-  int* counts = (int*)(base + off_counts);
-  int* offsets = (int*)(base + off_offsets);
-  int* item_off = (int*)(base + off_itemoff);
-  int* cursor = (int*)(base + off_cursor);
-  plan->counter = (int*)(base + off_misc);
-  plan->nitems = (int*)(base + off_misc) + 1;
-  plan->nfallback = (int*)(base + off_misc) + 2;
-  plan->fallback = (int*)(base + off_fallback);
-  plan->items = (BrickItem*)(base + off_items);
-  plan->lists = (int*)(base + off_lists);
+  int* counts = (int*)(base + o_counts);
+  int* offsets = (int*)(base + o_offsets);
+  int* item_off = (int*)(base + o_itemoff);
+  int* cursor = (int*)(base + o_cursor);
+  unsigned long long* counters = (unsigned long long*)(base + o_misc);
+  plan->counter = (int*)(base + o_misc + 16);
+  plan->nitems = (int*)(base + o_misc + 20);
+  plan->nfallback = (int*)(base + o_misc + 24);
+  plan->fallback = (int*)(base + o_fallback);
+  plan->items = (BrickItem*)(base + o_items);
+  plan->bins = (PixelBin*)(base + o_bins);
+  plan->pairs = (int*)(base + o_pairs);
+  plan->entries = (int*)(base + o_entries);
   plan->max_items = (int)std::min<int64_t>(cap_items, 0x7fffffff);
 
   cudaError_t e = cudaMemsetAsync(counts, 0, nb * 4, stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(base + off_misc, 0, 256, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(base + o_misc, 0, 256, stream);
   if (e == cudaSuccess && batch > 0) {
-    int blocks = (batch + kBinWarps - 1) / kBinWarps;
-    bin_count_kernel<<<blocks, kBinWarps * 32, 0, stream>>>(d_mats, batch, g, pmax, limit, counts,
-                                                            plan->fallback, plan->nfallback);
-    plan_scan_kernel<<<1, kScanThreads, 0, stream>>>(counts, d_order, g.nbricks, chunk, offsets, item_off,
-                                                     cursor, plan->nitems);
-    bin_fill_kernel<<<blocks, kBinWarps * 32, 0, stream>>>(d_mats, batch, g, pmax, limit, offsets, counts,
-                                                           cursor, plan->lists);
-    plan_items_kernel<<<(g.nbricks + 255) / 256, 256, 0, stream>>>(counts, offsets, item_off, g.nbricks,
-                                                                   chunk, plan->items);
+    if (op == GTOMRLN_OP_PROJECT) {
+      cudaFuncSetAttribute(bin_slices_kernel<GTOMRLN_OP_PROJECT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)hist_bytes);
+      bin_slices_kernel<GTOMRLN_OP_PROJECT><<<batch, kBinThreads, hist_bytes, stream>>>(
+          d_mats, g, px, limit, plan->entries, entries_cap, plan->bins, bins_cap, counters, counts,
+          plan->fallback, plan->nfallback);
+    } else {
+      cudaFuncSetAttribute(bin_slices_kernel<GTOMRLN_OP_BACKPROJECT>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_bytes);
+      bin_slices_kernel<GTOMRLN_OP_BACKPROJECT><<<batch, kBinThreads, hist_bytes, stream>>>(
+          d_mats, g, px, limit, plan->entries, entries_cap, plan->bins, bins_cap, counters, counts,
+          plan->fallback, plan->nfallback);
+    }
+    pairs_scan_kernel<<<1, kScanThreads, 0, stream>>>(counts, d_order, g.nbricks, chunk, offsets, item_off,
+                                                      cursor, plan->nitems);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    pairs_fill_kernel<<<sms * 4, 256, 0, stream>>>(plan->bins, counters, bins_cap, counts, offsets, cursor,
+                                                   plan->pairs);
+    plan_items_kernel<<<(g.nbricks + 255) / 256, 256, 0, stream>>>(counts, offsets, item_off, g.nbricks, chunk,
+                                                                   plan->items);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess) {

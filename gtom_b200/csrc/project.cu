@@ -13,6 +13,7 @@
 
 #include "brick.cuh"
 #include "common.cuh"
+#include "sample.cuh"
 
 namespace gtomrln {
 
@@ -137,20 +138,21 @@ project_listed_kernel(ArrayFetch fetch, float2* __restrict__ proj, const float* 
 
 // ---------------------------------------------------------------------------
 // Brick-major projector.  Each work item stages one brick of the volume
-// (16^3 voxels plus a one-voxel halo, in signed coordinates, wrapped into the
-// decentred layout exactly as the reference's index arithmetic wraps them)
-// in shared memory, then every warp takes one of the brick's slices and
-// evaluates the pixels whose interpolation base voxel (x0, y0, z0) lies in
-// the brick.  Each in-disk pixel has exactly one such brick, so it is
-// written exactly once, with the direct kernel's arithmetic on the same
-// voxel values: the results are identical.  Pixels outside rmax are zeroed
-// by project_zero_kernel.
+// (edge^3 voxels plus a one-voxel halo, in signed coordinates, wrapped into
+// the decentred layout exactly as the reference's index arithmetic wraps
+// them) in shared memory, then the warps take the item's bins (slice, pixel
+// run) one at a time and evaluate those pixels — the plan put every in-disk
+// pixel into the bin of the brick holding its interpolation base voxel
+// (x0, y0, z0), so each is written exactly once, with the direct kernel's
+// arithmetic on the same voxel values: the results are identical.  Pixels
+// outside rmax are zeroed by project_zero_kernel.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024)
 project_brick_kernel(const float2* __restrict__ vol, float2* __restrict__ proj,
                      const float* __restrict__ mats, ProjArgs a, BrickGrid g,
                      const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
-                     const int* __restrict__ lists, int* __restrict__ counter) {
+                     const int* __restrict__ pairs, const PixelBin* __restrict__ bins,
+                     const int* __restrict__ entries, int* __restrict__ counter) {
   extern __shared__ float2 tile[];
   __shared__ int item_s, next_s;
   const int nitems = *nitems_ptr;
@@ -177,45 +179,28 @@ project_brick_kernel(const float2* __restrict__ vol, float2* __restrict__ proj,
       tile[k] = __ldg(vol + i);
     }
     __syncthreads();
-    float3 qlo, qhi;
-    brick_box(g, it.brick, qlo, qhi);
-    for (;;) {  // warps take the item's slices one at a time
+    for (;;) {  // warps take the item's bins one at a time
       int j = 0;
       if ((threadIdx.x & 31) == 0) j = atomicAdd(&next_s, 1);
       j = __shfl_sync(0xffffffffu, j, 0);
       if (j >= it.count) break;
-      const int slice = __ldg(lists + it.offset + j);
+      const PixelBin bn = bins[__ldg(pairs + it.offset + j)];
       float m[9];
 #pragma unroll
-      for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
-      float2* out = proj + a.elements * slice;
-      for_each_footprint_pixel<true>(m, qlo, qhi, a.rmax2, a.n / 2 + 1 - a.n, a.n / 2, [&](int u, int v) {
-        float3 pos = mat_apply(m, (float)u, (float)v, 0.f);
-        float sign = 1.f;
-        if (pos.x < -1e-5f) {
-          pos.x = fabsf(pos.x);
-          pos.y = -pos.y;
-          pos.z = -pos.z;
-          sign = -1.f;
-        }
-        float fx0 = floorf(pos.x + 1e-5f), fy0 = floorf(pos.y), fz0 = floorf(pos.z);
-        int lx = (int)fx0 - o.x, ly = (int)fy0 - o.y, lz = (int)fz0 - o.z;
+      for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)bn.slice + k);
+      float2* out = proj + a.elements * bn.slice;
+      for (int k = threadIdx.x & 31; k < bn.count; k += 32) {
+        const int id = __ldg(entries + bn.start + k);
+        int u, v;
+        pixel_uv(id, a.n, a.dimft, u, v);
+        ProjSample s = project_sample(m, u, v, 0);
+        int lx = s.x0 - o.x, ly = s.y0 - o.y, lz = s.z0 - o.z;
         if ((unsigned)lx >= (unsigned)B || (unsigned)ly >= (unsigned)B || (unsigned)lz >= (unsigned)B)
-          return;  // another brick owns this pixel
-        float fx = pos.x - fx0, fy = pos.y - fy0, fz = pos.z - fz0;
+          continue;  // cannot happen: the plan used the same arithmetic
         const float2* c = tile + (lz * T + ly) * T + lx;
-        float2 d000 = c[0], d001 = c[1], d010 = c[T], d011 = c[T + 1];
-        float2 d100 = c[T * T], d101 = c[T * T + 1], d110 = c[T * T + T], d111 = c[T * T + T + 1];
-        float rx00 = lerpf(d000.x, d001.x, fx), ix00 = lerpf(d000.y, d001.y, fx);
-        float rx01 = lerpf(d010.x, d011.x, fx), ix01 = lerpf(d010.y, d011.y, fx);
-        float rx10 = lerpf(d100.x, d101.x, fx), ix10 = lerpf(d100.y, d101.y, fx);
-        float rx11 = lerpf(d110.x, d111.x, fx), ix11 = lerpf(d110.y, d111.y, fx);
-        float rxy0 = lerpf(rx00, rx01, fy), ixy0 = lerpf(ix00, ix01, fy);
-        float rxy1 = lerpf(rx10, rx11, fy), ixy1 = lerpf(ix10, ix11, fy);
-        int idy = v >= 0 ? v : v + a.n;
-        out[(int64_t)idy * a.dimft + u] =
-            make_float2(lerpf(rxy0, rxy1, fz), lerpf(ixy0, ixy1, fz) * sign);
-      });
+        out[id] = trilerp(s, c[0], c[1], c[T], c[T + 1], c[T * T], c[T * T + 1], c[T * T + T],
+                          c[T * T + T + 1]);
+      }
     }
   }
 }
@@ -263,15 +248,22 @@ static int project_brick(const float* d_volumeft, float* d_proj, const float* d_
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, project_brick_kernel, tune.threads, smem);
+  PixelSet px;
+  px.n = a.n;
+  px.dimft = a.dimft;
+  px.elements = a.elements;
+  px.rmax2 = a.rmax2;
+  px.strict = 0;
+  px.pmax = (float)a.rmax;
   BrickPlan plan;
-  int st = build_brick_plan(d_mats, (int)batch, g, (float)a.rmax, (float)(P / 2) + 0.99f, tune.chunk, stream,
-                            &plan);
+  int st = build_brick_plan(GTOMRLN_OP_PROJECT, d_mats, (int)batch, g, px, (float)(P / 2) + 0.99f, tune.chunk,
+                            stream, &plan);
   if (st) return st;
   int64_t rows = (int64_t)a.n * batch;  // 2D slices: n rows of dimft elements each
   project_zero_kernel<<<sms * 8, 256, 0, stream>>>((float2*)d_proj, a, rows);
   project_brick_kernel<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
-      (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, plan.items, plan.nitems, plan.lists,
-      plan.counter);
+      (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, plan.items, plan.nitems, plan.pairs, plan.bins,
+      plan.entries, plan.counter);
   ArrayFetch f{(const float2*)d_volumeft, a.P, a.P / 2 + 1, a.nvox - 1};
   project_listed_kernel<<<sms * 4, kProjThreads, 0, stream>>>(f, (float2*)d_proj, d_mats, a, plan.fallback,
                                                                plan.nfallback);
