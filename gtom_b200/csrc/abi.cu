@@ -45,8 +45,9 @@ void matrices_from_angles(const float* angles, float s, unsigned batch, float* o
   }
 }
 
-// One pool per device; its release threshold keeps up to 4 GiB of freed
-// scratch mapped so that repeated calls do not remap it.
+// One pool per device.  Freed scratch stays mapped in the pool (no release
+// threshold) so that repeated calls reuse it instead of remapping gigabytes
+// each time; gtomrln_release_caches() returns it to the device.
 static std::mutex g_pool_mutex;
 static std::vector<cudaMemPool_t> g_pools;
 
@@ -62,7 +63,7 @@ static int get_pool(cudaMemPool_t* out) {
     props.location.id = dev;
     cudaMemPool_t pool;
     GTOMRLN_CUDA_TRY(cudaMemPoolCreate(&pool, &props));
-    uint64_t threshold = 4ull << 30;
+    uint64_t threshold = UINT64_MAX;
     GTOMRLN_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
     g_pools[dev] = pool;
   }

@@ -23,7 +23,6 @@ namespace gtomrln {
 
 constexpr int kBinThreads = 512;
 constexpr int kMaxBinsPerSlice = 2048;  // bins reserved per slice on average
-constexpr int kMaxPixelBricks = 16;
 
 __device__ __forceinline__ bool in_pixel_set(const PixelSet& px, int u, int v) {
   int r2 = u * u + v * v;
@@ -31,32 +30,83 @@ __device__ __forceinline__ bool in_pixel_set(const PixelSet& px, int u, int v) {
   return r2 <= px.rmax2;
 }
 
-// The bricks pixel (u, v) of a slice with matrix m reads from (projector)
-// or adds to (backprojector), without repeats.  Returns the count, or -1 if
-// some voxel falls outside the grid (the slice must then take the direct path).
-template <int OP>
-__device__ __forceinline__ int pixel_bricks(const float* m, int u, int v, const BrickGrid& g,
-                                            int (&out)[kMaxPixelBricks]) {
+// Brick indices along each axis spanned by the 2x2x2 voxel cube with lowest
+// corner (x, y, z) (index 1 equals index 0 when the cube does not cross a
+// brick face).
+struct CubeBricks {
+  int bx0, bx1, by0, by1, bz0, bz1;
+};
+
+__device__ __forceinline__ bool cube_bricks(const BrickGrid& g, int x, int y, int z, CubeBricks& c) {
+  int dy = y - g.ylo, dz = z - g.zlo;
+  if (x < 0 || dy < 0 || dz < 0) return false;
+  c.bx0 = x / g.B;
+  c.bx1 = (x + 1) / g.B;
+  c.by0 = dy / g.B;
+  c.by1 = (dy + 1) / g.B;
+  c.bz0 = dz / g.B;
+  c.bz1 = (dz + 1) / g.B;
+  return c.bx1 < g.nbx && c.by1 < g.nby && c.bz1 < g.nbz;
+}
+
+__device__ __forceinline__ bool cube_has(const CubeBricks& c, int bx, int by, int bz) {
+  return (bx == c.bx0 || bx == c.bx1) && (by == c.by0 || by == c.by1) && (bz == c.bz0 || bz == c.bz1);
+}
+
+// f(b) for every brick of cube c, each once, skipping those of `skip`.
+template <class F>
+__device__ __forceinline__ void for_each_cube_brick(const BrickGrid& g, const CubeBricks& c,
+                                                    const CubeBricks* skip, F&& f) {
+#pragma unroll
+  for (int iz = 0; iz < 2; iz++) {
+    int bz = iz ? c.bz1 : c.bz0;
+    if (iz && bz == c.bz0) continue;
+#pragma unroll
+    for (int iy = 0; iy < 2; iy++) {
+      int by = iy ? c.by1 : c.by0;
+      if (iy && by == c.by0) continue;
+#pragma unroll
+      for (int ix = 0; ix < 2; ix++) {
+        int bx = ix ? c.bx1 : c.bx0;
+        if (ix && bx == c.bx0) continue;
+        if (skip && cube_has(*skip, bx, by, bz)) continue;
+        f((bz * g.nby + by) * g.nbx + bx);
+      }
+    }
+  }
+}
+
+// f(b) for every brick pixel (u, v) of a slice with matrix m reads from (the
+// projector: the brick of its base voxel) or adds to (the backprojector:
+// the bricks of its target cube — for x0 >= 1 the cube at (x0, y0, z0), for
+// x0 <= -2 the mirrored cube at (-x0-1, -y0-1, -z0-1), and near x = 0 both
+// cubes with x in {0, 1}, which hold every direct, mirrored and second-plane
+// target), each brick once.  Returns false if a voxel falls outside the grid
+// (the slice must then take the direct path).  A brick may receive a pixel
+// none of whose targets it holds; the brick kernel adds only its own targets.
+template <int OP, class F>
+__device__ __forceinline__ bool pixel_bricks(const float* m, int u, int v, const BrickGrid& g, F&& f) {
   if (OP == GTOMRLN_OP_PROJECT) {
     ProjSample s = project_sample(m, u, v, 0);
     int b = brick_of(g, s.x0, s.y0, s.z0);
-    out[0] = b;
-    return b < 0 ? -1 : 1;
+    if (b < 0) return false;
+    f(b);
+    return true;
   } else {
     BpSample s = backproject_sample(m, (float)u, (float)v, 0.f);
-    int n = 0;
-    bool bad = false;
-    for_each_target(s.x0, s.y0, s.z0, [&](int, int x, int y, int z, bool) {
-      int b = brick_of(g, x, y, z);
-      if (b < 0) {
-        bad = true;
-        return;
-      }
-      for (int k = 0; k < n; k++)
-        if (out[k] == b) return;
-      out[n++] = b;
-    });
-    return bad ? -1 : n;
+    CubeBricks c1, c2;
+    if (s.x0 >= 1) {
+      if (!cube_bricks(g, s.x0, s.y0, s.z0, c1)) return false;
+      for_each_cube_brick(g, c1, nullptr, f);
+    } else if (s.x0 <= -2) {
+      if (!cube_bricks(g, -s.x0 - 1, -s.y0 - 1, -s.z0 - 1, c1)) return false;
+      for_each_cube_brick(g, c1, nullptr, f);
+    } else {
+      if (!cube_bricks(g, 0, s.y0, s.z0, c1) || !cube_bricks(g, 0, -s.y0 - 1, -s.z0 - 1, c2)) return false;
+      for_each_cube_brick(g, c1, nullptr, f);
+      for_each_cube_brick(g, c2, &c1, f);
+    }
+    return true;
   }
 }
 
@@ -85,13 +135,7 @@ bin_slices_kernel(const float* __restrict__ mats, BrickGrid g, PixelSet px, floa
     int u, v;
     pixel_uv(id, px.n, px.dimft, u, v);
     if (!in_pixel_set(px, u, v)) continue;
-    int bl[kMaxPixelBricks];
-    int nb = pixel_bricks<OP>(m, u, v, g, bl);
-    if (nb < 0) {
-      s_bad = 1;
-      continue;
-    }
-    for (int k = 0; k < nb; k++) atomicAdd(&hist[bl[k]], 1);
+    if (!pixel_bricks<OP>(m, u, v, g, [&](int b) { atomicAdd(&hist[b], 1); })) s_bad = 1;
   }
   __syncthreads();
   if (s_bad) {
@@ -157,9 +201,7 @@ bin_slices_kernel(const float* __restrict__ mats, BrickGrid g, PixelSet px, floa
     int u, v;
     pixel_uv(id, px.n, px.dimft, u, v);
     if (!in_pixel_set(px, u, v)) continue;
-    int bl[kMaxPixelBricks];
-    int nb = pixel_bricks<OP>(m, u, v, g, bl);
-    for (int k = 0; k < nb; k++) entries[s_base_e + atomicAdd(&hist[bl[k]], 1)] = id;
+    pixel_bricks<OP>(m, u, v, g, [&](int b) { entries[s_base_e + atomicAdd(&hist[b], 1)] = id; });
   }
 }
 
@@ -275,7 +317,14 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
   // Capacities: the projector bins each pixel once; the backprojector's
   // pixels land in ~1.2-1.5 bricks on average (8 at most), so twice the
   // pixel count is reserved.  A slice that does not fit takes the direct path.
-  int64_t npix = px.elements;
+  int64_t npix = 0;
+  for (int idy = 0; idy < px.n; idy++) {
+    int v = idy <= px.n / 2 ? idy : idy - px.n;
+    for (int u = 0; u < px.dimft; u++) {
+      int r2 = u * u + v * v;
+      npix += px.strict ? (r2 < px.rmax2 && !(u == 0 && v < 0)) : (r2 <= px.rmax2);
+    }
+  }
   int64_t entries_cap = std::max<int64_t>(1, (int64_t)batch * npix * (op == GTOMRLN_OP_PROJECT ? 1 : 2));
   int64_t bins_cap = std::max<int64_t>(1, (int64_t)batch * std::min(g.nbricks, kMaxBinsPerSlice));
   if (entries_cap > 0x7fffffffLL || bins_cap > 0x7fffffffLL)
