@@ -201,7 +201,10 @@ backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
       float m[9];
 #pragma unroll
       for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)bn.slice + k);
-      for (int e = lane; e < bn.count; e += 32) {
+      // Interior entries: the whole target cube lies in this brick, either
+      // direct (x0 >= 1) or mirrored to -n and conjugated (x0 <= -2).  One
+      // branch-free path: corner kb and direction sg (+1 or -1).
+      for (int e = lane; e < bn.interior; e += 32) {
         const int pid = __ldg(entries + bn.start + e);
         int u, v;
         pixel_uv(pid, a.n, a.dimft, u, v);
@@ -209,45 +212,38 @@ backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
         BpSample s = backproject_sample(m, (float)u, (float)v, 0.f);
         float2 val = projft ? __ldg(projft + id) : make_float2(1.f, 0.f);
         float pw = projw ? __ldg(projw + id) : 1.f;
-        if (SQUARE) {
+        const int sg = s.x0 >= 1 ? 1 : -1;
+        const int kb = (sg * s.z0 - o.z) * PS + (sg * s.y0 - o.y) * RS + (sg * s.x0 - o.x);
+        const float im = sg * val.y;
 #pragma unroll
-          for (int i = 0; i < 8; i++) s.w[i] *= s.w[i];
+        for (int i = 0; i < 8; i++) {
+          float w = SQUARE ? s.w[i] * s.w[i] : s.w[i];
+          int k = kb + sg * ((i & 1) + ((i >> 1) & 1) * RS + ((i >> 2) & 1) * PS);
+          atomicAdd(are + k, w * val.x);
+          atomicAdd(aim + k, w * im);
+          atomicAdd(aw + k, w * pw);
         }
-        const int lx0 = s.x0 - o.x, ly0 = s.y0 - o.y, lz0 = s.z0 - o.z;
-        const int mx0 = -s.x0 - 1 - o.x, my0 = -s.y0 - 1 - o.y, mz0 = -s.z0 - 1 - o.z;
-        if (s.x0 >= 1 && (unsigned)lx0 < (unsigned)(B - 1) && (unsigned)ly0 < (unsigned)(B - 1) &&
-            (unsigned)lz0 < (unsigned)(B - 1)) {
-          // whole 2x2x2 cube inside the brick, no mirroring, no x = 0 plane
-          const int k0 = lz0 * PS + ly0 * RS + lx0;
-#pragma unroll
-          for (int i = 0; i < 8; i++) {
-            int k = k0 + (i & 1) + ((i >> 1) & 1) * RS + ((i >> 2) & 1) * PS;
-            atomicAdd(are + k, s.w[i] * val.x);
-            atomicAdd(aim + k, s.w[i] * val.y);
-            atomicAdd(aw + k, s.w[i] * pw);
+      }
+      // Boundary entries: the cube crosses a brick face or the x = 0 plane;
+      // every target is tested.
+      for (int e = bn.interior + lane; e < bn.count; e += 32) {
+        const int pid = __ldg(entries + bn.start + e);
+        int u, v;
+        pixel_uv(pid, a.n, a.dimft, u, v);
+        const int64_t id = a.elements * bn.slice + pid;
+        BpSample s = backproject_sample(m, (float)u, (float)v, 0.f);
+        float2 val = projft ? __ldg(projft + id) : make_float2(1.f, 0.f);
+        float pw = projw ? __ldg(projw + id) : 1.f;
+        for_each_target(s.x0, s.y0, s.z0, [&](int i, int x, int y, int z, bool conj) {
+          int lx = x - o.x, ly = y - o.y, lz = z - o.z;
+          if ((unsigned)lx < (unsigned)B && (unsigned)ly < (unsigned)B && (unsigned)lz < (unsigned)B) {
+            float w = SQUARE ? s.w[i] * s.w[i] : s.w[i];
+            int k = lz * PS + ly * RS + lx;
+            atomicAdd(are + k, w * val.x);
+            atomicAdd(aim + k, w * (conj ? -val.y : val.y));
+            atomicAdd(aw + k, w * pw);
           }
-        } else if (s.x0 <= -2 && (unsigned)mx0 < (unsigned)(B - 1) && (unsigned)my0 < (unsigned)(B - 1) &&
-                   (unsigned)mz0 < (unsigned)(B - 1)) {
-          // whole cube mirrored to (-x0-1 .. -x0, ...) inside the brick, conjugated
-          const int k0 = mz0 * PS + my0 * RS + mx0;
-#pragma unroll
-          for (int i = 0; i < 8; i++) {
-            int k = k0 + (1 - (i & 1)) + (1 - ((i >> 1) & 1)) * RS + (1 - ((i >> 2) & 1)) * PS;
-            atomicAdd(are + k, s.w[i] * val.x);
-            atomicAdd(aim + k, s.w[i] * -val.y);
-            atomicAdd(aw + k, s.w[i] * pw);
-          }
-        } else {
-          for_each_target(s.x0, s.y0, s.z0, [&](int i, int x, int y, int z, bool conj) {
-            int lx = x - o.x, ly = y - o.y, lz = z - o.z;
-            if ((unsigned)lx < (unsigned)B && (unsigned)ly < (unsigned)B && (unsigned)lz < (unsigned)B) {
-              int k = lz * PS + ly * RS + lx;
-              atomicAdd(are + k, s.w[i] * val.x);
-              atomicAdd(aim + k, s.w[i] * (conj ? -val.y : val.y));
-              atomicAdd(aw + k, s.w[i] * pw);
-            }
-          });
-        }
+        });
       }
     }
     __syncthreads();

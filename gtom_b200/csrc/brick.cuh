@@ -36,9 +36,12 @@ struct BrickItem {
   int exclusive;  // 1 if this is the brick's only item (no other CTA writes it)
 };
 
-// A (slice, brick) bin: `count` pixel ids starting at entries[start].
+// A (slice, brick) bin: `count` pixel ids starting at entries[start]; the
+// first `interior` of them are pixels whose whole 2x2x2 target cube (direct
+// or mirrored, away from the x = 0 plane) lies inside the brick, so a warp
+// can treat them with one branch-free path.
 struct PixelBin {
-  int slice, start, count, brick;
+  int slice, start, count, brick, interior, pad0, pad1, pad2;
 };
 
 __host__ __device__ inline int3 brick_origin(const BrickGrid& g, int b) {
@@ -49,13 +52,21 @@ __host__ __device__ inline int3 brick_origin(const BrickGrid& g, int b) {
   return make_int3(bx * g.B, g.ylo + by * g.B, g.zlo + bz * g.B);
 }
 
+// floor(x / B) for 0 <= x < 2^20 without an integer division: a float
+// estimate corrected by one step either way.
+__device__ __forceinline__ int div_brick(int x, int B, float invB) {
+  int q = (int)((float)x * invB);
+  q -= q * B > x;
+  q += (q + 1) * B <= x;
+  return q;
+}
+
 // Brick holding signed voxel (x, y, z), or -1 outside the grid.
 __device__ __forceinline__ int brick_of(const BrickGrid& g, int x, int y, int z) {
-  if (x < 0) return -1;
-  int bx = x / g.B;
   int dy = y - g.ylo, dz = z - g.zlo;
-  if (dy < 0 || dz < 0) return -1;
-  int by = dy / g.B, bz = dz / g.B;
+  if (x < 0 || dy < 0 || dz < 0) return -1;
+  const float inv = 1.f / (float)g.B;
+  int bx = div_brick(x, g.B, inv), by = div_brick(dy, g.B, inv), bz = div_brick(dz, g.B, inv);
   if (bx >= g.nbx || by >= g.nby || bz >= g.nbz) return -1;
   return (bz * g.nby + by) * g.nbx + bx;
 }

@@ -40,17 +40,22 @@ struct CubeBricks {
 __device__ __forceinline__ bool cube_bricks(const BrickGrid& g, int x, int y, int z, CubeBricks& c) {
   int dy = y - g.ylo, dz = z - g.zlo;
   if (x < 0 || dy < 0 || dz < 0) return false;
-  c.bx0 = x / g.B;
-  c.bx1 = (x + 1) / g.B;
-  c.by0 = dy / g.B;
-  c.by1 = (dy + 1) / g.B;
-  c.bz0 = dz / g.B;
-  c.bz1 = (dz + 1) / g.B;
+  const float inv = 1.f / (float)g.B;
+  c.bx0 = div_brick(x, g.B, inv);
+  c.bx1 = div_brick(x + 1, g.B, inv);
+  c.by0 = div_brick(dy, g.B, inv);
+  c.by1 = div_brick(dy + 1, g.B, inv);
+  c.bz0 = div_brick(dz, g.B, inv);
+  c.bz1 = div_brick(dz + 1, g.B, inv);
   return c.bx1 < g.nbx && c.by1 < g.nby && c.bz1 < g.nbz;
 }
 
 __device__ __forceinline__ bool cube_has(const CubeBricks& c, int bx, int by, int bz) {
   return (bx == c.bx0 || bx == c.bx1) && (by == c.by0 || by == c.by1) && (bz == c.bz0 || bz == c.bz1);
+}
+
+__device__ __forceinline__ bool cube_single(const CubeBricks& c) {
+  return c.bx0 == c.bx1 && c.by0 == c.by1 && c.bz0 == c.bz1;
 }
 
 // f(b) for every brick of cube c, each once, skipping those of `skip`.
@@ -76,37 +81,55 @@ __device__ __forceinline__ void for_each_cube_brick(const BrickGrid& g, const Cu
   }
 }
 
-// f(b) for every brick pixel (u, v) of a slice with matrix m reads from (the
-// projector: the brick of its base voxel) or adds to (the backprojector:
-// the bricks of its target cube — for x0 >= 1 the cube at (x0, y0, z0), for
-// x0 <= -2 the mirrored cube at (-x0-1, -y0-1, -z0-1), and near x = 0 both
-// cubes with x in {0, 1}, which hold every direct, mirrored and second-plane
-// target), each brick once.  Returns false if a voxel falls outside the grid
-// (the slice must then take the direct path).  A brick may receive a pixel
-// none of whose targets it holds; the brick kernel adds only its own targets.
+// f(b, interior) for every brick pixel (u, v) of a slice with matrix m reads
+// from (the projector: the brick of its base voxel) or adds to (the
+// backprojector: the bricks of its target cube — for x0 >= 1 the cube at
+// (x0, y0, z0), for x0 <= -2 the mirrored cube at (-x0-1, -y0-1, -z0-1), and
+// near x = 0 both cubes with x in {0, 1}, which hold every direct, mirrored
+// and second-plane target), each brick once.  interior: the pixel's whole
+// single cube lies in that brick.  Returns false if a voxel falls outside
+// the grid (the slice must then take the direct path).  A brick may receive
+// a pixel none of whose targets it holds; the brick kernel adds only its own.
 template <int OP, class F>
 __device__ __forceinline__ bool pixel_bricks(const float* m, int u, int v, const BrickGrid& g, F&& f) {
   if (OP == GTOMRLN_OP_PROJECT) {
     ProjSample s = project_sample(m, u, v, 0);
     int b = brick_of(g, s.x0, s.y0, s.z0);
     if (b < 0) return false;
-    f(b);
+    f(b, true);
     return true;
   } else {
     BpSample s = backproject_sample(m, (float)u, (float)v, 0.f);
     CubeBricks c1, c2;
-    if (s.x0 >= 1) {
-      if (!cube_bricks(g, s.x0, s.y0, s.z0, c1)) return false;
-      for_each_cube_brick(g, c1, nullptr, f);
-    } else if (s.x0 <= -2) {
-      if (!cube_bricks(g, -s.x0 - 1, -s.y0 - 1, -s.z0 - 1, c1)) return false;
-      for_each_cube_brick(g, c1, nullptr, f);
+    if (s.x0 >= 1 || s.x0 <= -2) {
+      bool ok = s.x0 >= 1 ? cube_bricks(g, s.x0, s.y0, s.z0, c1)
+                          : cube_bricks(g, -s.x0 - 1, -s.y0 - 1, -s.z0 - 1, c1);
+      if (!ok) return false;
+      const bool single = cube_single(c1);
+      for_each_cube_brick(g, c1, nullptr, [&](int b) { f(b, single); });
     } else {
       if (!cube_bricks(g, 0, s.y0, s.z0, c1) || !cube_bricks(g, 0, -s.y0 - 1, -s.z0 - 1, c2)) return false;
-      for_each_cube_brick(g, c1, nullptr, f);
-      for_each_cube_brick(g, c2, &c1, f);
+      for_each_cube_brick(g, c1, nullptr, [&](int b) { f(b, false); });
+      for_each_cube_brick(g, c2, &c1, [&](int b) { f(b, false); });
     }
     return true;
+  }
+}
+
+// Visits the slice's pixel set row by row (one warp per row, lanes along
+// the row), so that no pixel id needs a division.
+template <class F>
+__device__ __forceinline__ void for_each_set_pixel(const PixelSet& px, F&& f) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int idy = warp; idy < px.n; idy += nw) {
+    int v = idy <= px.n / 2 ? idy : idy - px.n;
+    int rem = (px.strict ? px.rmax2 - 1 : px.rmax2) - v * v;
+    if (rem < 0) continue;
+    int umax = (int)sqrtf((float)rem);
+    umax -= umax * umax > rem;
+    umax += (umax + 1) * (umax + 1) <= rem;
+    int u0 = (px.strict && v < 0) ? 1 : 0;
+    for (int u = u0 + lane; u <= umax && u < px.dimft; u += 32) f(idy * px.dimft + u, u, v);
   }
 }
 
@@ -116,7 +139,8 @@ bin_slices_kernel(const float* __restrict__ mats, BrickGrid g, PixelSet px, floa
                   int* __restrict__ entries, int64_t entries_cap, PixelBin* __restrict__ bins,
                   int64_t bins_cap, unsigned long long* __restrict__ counters,
                   int* __restrict__ brick_pairs, int* __restrict__ fallback, int* __restrict__ nfallback) {
-  extern __shared__ int hist[];  // nbricks
+  extern __shared__ int hist[];  // interior counts [nbricks], then boundary counts [nbricks]
+  int* hist_b = hist + g.nbricks;
   __shared__ int s_bad, s_sum[kBinThreads / 32], s_nz[kBinThreads / 32];
   __shared__ long long s_base_e, s_base_b;
   const int slice = blockIdx.x;
@@ -128,15 +152,13 @@ bin_slices_kernel(const float* __restrict__ mats, BrickGrid g, PixelSet px, floa
     if (tid == 0) fallback[atomicAdd(nfallback, 1)] = slice;
     return;
   }
-  for (int b = tid; b < g.nbricks; b += kBinThreads) hist[b] = 0;
+  for (int b = tid; b < 2 * g.nbricks; b += kBinThreads) hist[b] = 0;
   if (tid == 0) s_bad = 0;
   __syncthreads();
-  for (int id = tid; id < px.elements; id += kBinThreads) {
-    int u, v;
-    pixel_uv(id, px.n, px.dimft, u, v);
-    if (!in_pixel_set(px, u, v)) continue;
-    if (!pixel_bricks<OP>(m, u, v, g, [&](int b) { atomicAdd(&hist[b], 1); })) s_bad = 1;
-  }
+  for_each_set_pixel(px, [&](int, int u, int v) {
+    bool ok = pixel_bricks<OP>(m, u, v, g, [&](int b, bool in) { atomicAdd(in ? &hist[b] : &hist_b[b], 1); });
+    if (!ok) s_bad = 1;
+  });
   __syncthreads();
   if (s_bad) {
     if (tid == 0) fallback[atomicAdd(nfallback, 1)] = slice;
@@ -148,8 +170,9 @@ bin_slices_kernel(const float* __restrict__ mats, BrickGrid g, PixelSet px, floa
   const int b0 = min(tid * per, g.nbricks), b1 = min(b0 + per, g.nbricks);
   int sum = 0, nz = 0;
   for (int b = b0; b < b1; b++) {
-    sum += hist[b];
-    nz += hist[b] > 0;
+    int c = hist[b] + hist_b[b];
+    sum += c;
+    nz += c > 0;
   }
   int isum = sum, inz = nz;
 #pragma unroll
@@ -187,22 +210,22 @@ bin_slices_kernel(const float* __restrict__ mats, BrickGrid g, PixelSet px, floa
   }
   int off = wsum + isum - sum, bi = wnz + inz - nz;
   for (int b = b0; b < b1; b++) {
-    int c = hist[b];
-    hist[b] = off;
-    if (c > 0) {
-      bins[s_base_b + bi] = {slice, (int)(s_base_e + off), c, b};
+    int ci = hist[b], cb = hist_b[b];
+    hist[b] = off;  // next interior slot
+    hist_b[b] = off + ci;  // next boundary slot
+    if (ci + cb > 0) {
+      bins[s_base_b + bi] = {slice, (int)(s_base_e + off), ci + cb, b, ci, 0, 0, 0};
       atomicAdd(brick_pairs + b, 1);
       bi++;
     }
-    off += c;
+    off += ci + cb;
   }
   __syncthreads();
-  for (int id = tid; id < px.elements; id += kBinThreads) {
-    int u, v;
-    pixel_uv(id, px.n, px.dimft, u, v);
-    if (!in_pixel_set(px, u, v)) continue;
-    pixel_bricks<OP>(m, u, v, g, [&](int b) { entries[s_base_e + atomicAdd(&hist[b], 1)] = id; });
-  }
+  for_each_set_pixel(px, [&](int id, int u, int v) {
+    pixel_bricks<OP>(m, u, v, g, [&](int b, bool in) {
+      entries[s_base_e + atomicAdd(in ? &hist[b] : &hist_b[b], 1)] = id;
+    });
+  });
 }
 
 // Single block.  Bricks are visited in `order` (increasing distance from the
@@ -308,7 +331,7 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
                      float limit, int chunk, cudaStream_t stream, BrickPlan* plan) {
   plan->g = g;
   plan->batch = batch;
-  size_t hist_bytes = sizeof(int) * (size_t)g.nbricks;
+  size_t hist_bytes = 2 * sizeof(int) * (size_t)g.nbricks;
   if (hist_bytes > 200 * 1024)
     return set_error(GTOMRLN_ERR_INVALID, "brick grid of %d bricks too fine for the binning plan", g.nbricks);
   const int* d_order = nullptr;
