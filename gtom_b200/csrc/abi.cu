@@ -99,7 +99,7 @@ int path_choice(int op) { return (op == 0 || op == 1) ? g_path[op].load() : GTOM
 
 // Defaults measured on the B200 at 256^3 (padding 2) with 10,000-slice
 // batches; the autotuner (gtom_b200/autotune.py) can replace them.
-static const BrickTuning kDefaultTuning[2] = {{24, 1024, 2048}, {24, 1024, 2048}};
+static const BrickTuning kDefaultTuning[2] = {{28, 1024, 4096}, {24, 1024, 4096}};
 static std::mutex g_tuning_mutex;
 static BrickTuning g_tuning[2] = {kDefaultTuning[0], kDefaultTuning[1]};
 

@@ -57,9 +57,59 @@ __global__ void gather_probe_kernel(const float2* __restrict__ buf, uint32_t mas
   if (acc == 123.456f) sink[t] = acc;  // keeps the loads alive
 }
 
+// Shared-memory update rate: every thread adds to pseudo-random words of a
+// 12K-word (48 KB) array.  mode 0: FP32 atomicAdd, 1: int32 atomicAdd,
+// 2: plain FP32 read-add-write (no atomicity), 3: int64 atomicAdd.
+template <int MODE>
+__global__ void smem_probe_kernel(float* __restrict__ sink, int iters) {
+  __shared__ float s[12288];
+  for (int i = threadIdx.x; i < 12288; i += blockDim.x) s[i] = 0.f;
+  __syncthreads();
+  uint32_t h = hash32(blockIdx.x * blockDim.x + threadIdx.x);
+  for (int i = 0; i < iters; i++) {
+    h = h * 1664525u + 1013904223u;
+    uint32_t k = (h >> 8) % (MODE == 3 ? 6144u : 12288u);
+    if (MODE == 0) atomicAdd(s + k, 1.0f);
+    if (MODE == 1) atomicAdd((int*)s + k, 1);
+    if (MODE == 2) s[k] += 1.0f;
+    if (MODE == 3) atomicAdd((unsigned long long*)s + k, 1ull);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) sink[blockIdx.x] = s[blockIdx.x % 12288];
+}
+
 }  // namespace
 
 extern "C" {
+
+__attribute__((visibility("default")))
+// Returns shared-memory updates per second over the whole device.
+double gtomrln_probe_smem_update(int mode, int blocks, int threads, int iters) {
+  float* sink = nullptr;
+  if (cudaMalloc(&sink, (size_t)blocks * sizeof(float)) != cudaSuccess) return -1;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  auto launch = [&]() {
+    if (mode == 0) smem_probe_kernel<0><<<blocks, threads>>>(sink, iters);
+    else if (mode == 1) smem_probe_kernel<1><<<blocks, threads>>>(sink, iters);
+    else if (mode == 2) smem_probe_kernel<2><<<blocks, threads>>>(sink, iters);
+    else smem_probe_kernel<3><<<blocks, threads>>>(sink, iters);
+  };
+  launch();
+  cudaEventRecord(a);
+  launch();
+  cudaEventRecord(b);
+  cudaEventSynchronize(b);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaError_t e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(sink);
+  if (e != cudaSuccess) return -(double)e;
+  return (double)blocks * threads * iters / (ms * 1e-3);
+}
 
 __attribute__((visibility("default")))
 // Returns FP32 additions per second (vec * reductions), or a negative CUDA error.
