@@ -51,6 +51,7 @@ SIGNATURES: dict[str, list] = {
     "gtomrln_matrices_from_angles": [_p, _f, _u, _p],
     "gtomrln_project": [_p, _i, _i, _i, _p, _i, _i, _i, _u, _p, _u, _p],
     "gtomrln_project_angles": [_p, _i, _i, _i, _p, _i, _i, _i, _p, _f, _u, _p],
+    "gtomrln_project_angles_noalloc": [_p, _i, _i, _i, _p, _i, _i, _i, _p, _f, _u, _p],
     "gtomrln_project_tex": [_ull, _ull, _i, _i, _i, _p, _i, _i, _i, _u, _p, _u, _p],
     "gtomrln_project_tex_angles": [_ull, _ull, _i, _i, _i, _p, _i, _i, _i, _p, _f, _u, _p],
     "gtomrln_backproject": [_p, _p, _i, _i, _i, _p, _p, _i, _i, _i, _u, _p, _p,

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <mutex>
 
 #include "brick.cuh"
 #include "common.cuh"
@@ -315,11 +316,80 @@ static int launch_project(Fetch f, int ndp, float* d_proj, const float* d_mats, 
   return GTOMRLN_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Projection from host angles without any device allocation.
+//
+// The h_angles overload has to place the slices' rotation matrices in device
+// memory; gtomrln_project_angles takes that scratch from the library's
+// memory pool.  gtomrln_project_angles_noalloc keeps it instead in the
+// fixed array below, which is part of the library image: every device that
+// loads the library holds these kNoAllocMaxBatch * 36 bytes until the
+// process exits, and no call allocates anything.
+// ---------------------------------------------------------------------------
+constexpr unsigned kNoAllocMaxBatch = 4096;
+static __device__ __align__(256) float g_noalloc_matrices[kNoAllocMaxBatch * 9];
+
+// In host code g_noalloc_matrices is only a host-side stand-in; the device
+// address comes from cudaGetSymbolAddress, looked up once per device with
+// that device current.
+static std::mutex g_noalloc_mutex;
+static float* g_noalloc_ptr[64] = {};
+
+static int noalloc_matrices(float** out) {
+  int dev = 0;
+  GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return set_error(GTOMRLN_ERR_INVALID, "device index %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_matrices);
+    if (e != cudaSuccess)
+      return set_error(GTOMRLN_ERR_CUDA, "cudaGetSymbolAddress of the fixed matrix array failed: %s",
+                       cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = (float*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return GTOMRLN_OK;
+}
+
 }  // namespace gtomrln
 
 using namespace gtomrln;
 
 extern "C" {
+
+int gtomrln_project_angles_noalloc(const float* d_volumeft, int vx, int vy, int vz, float* d_proj,
+                                   int px, int py, int pz, const float* h_angles, float supersample,
+                                   unsigned batch, void* stream) {
+  clear_error();
+  if (batch > kNoAllocMaxBatch)
+    return set_error(GTOMRLN_ERR_INVALID,
+                     "project_angles_noalloc: batch %u exceeds the fixed capacity of %u slices; "
+                     "split the batch",
+                     batch, kNoAllocMaxBatch);
+  ProjArgs a;
+  int ndp;
+  int st = project_setup(vx, vy, vz, px, py, pz, (unsigned)(px / 2), batch, &a, &ndp);
+  if (st) return st;
+  if (batch == 0) return GTOMRLN_OK;
+  if (!d_volumeft || !d_proj || !h_angles)
+    return set_error(GTOMRLN_ERR_INVALID, "project_angles_noalloc: NULL pointer");
+  float* d_mats = nullptr;
+  st = noalloc_matrices(&d_mats);
+  if (st) return st;
+  // Host staging without allocation: a fixed per-thread buffer.
+  static thread_local float h_mats[kNoAllocMaxBatch * 9];
+  matrices_from_angles(h_angles, supersample, batch, h_mats);
+  cudaStream_t s = (cudaStream_t)stream;
+  // Every matrix the kernel reads is rewritten here, so nothing left from an
+  // earlier call needs clearing.  The copy is ordered on `s` after earlier
+  // work on `s`; calls on different streams that overlap on the GPU race for
+  // the shared array.
+  GTOMRLN_CUDA_TRY(cudaMemcpyAsync(d_mats, h_mats, sizeof(float) * 9 * (size_t)batch,
+                                   cudaMemcpyHostToDevice, s));
+  ArrayFetch f{(const float2*)d_volumeft, a.P, a.P / 2 + 1, a.nvox - 1};
+  return launch_project(f, ndp, d_proj, d_mats, a, batch, s);
+}
 
 int gtomrln_project(const float* d_volumeft, int vx, int vy, int vz, float* d_proj, int px, int py,
                     int pz, unsigned rmax, const float* d_matrices, unsigned batch, void* stream) {

@@ -121,6 +121,24 @@ GTOMRLN_API int gtomrln_project_tex(unsigned long long t_volumeRe, unsigned long
                         int vy, int vz, float* d_proj, int px, int py, int pz, unsigned rmax,
                         const float* d_matrices, unsigned batch, void* stream);
 
+/* Extension with no counterpart in the reference: gtomrln_project_angles
+ * for callers that cannot allocate device memory — code whose device memory
+ * is owned by another allocator (a host application's memory pool or a
+ * fixed budget), or that must not let an allocation synchronise the device
+ * in the middle of a pipeline.  The reference's h_angles overload, and
+ * gtomrln_project_angles, place the rotation matrices in freshly allocated
+ * device memory; this entry point uses a fixed array inside the library
+ * instead and allocates nothing.  Limit: batch <= 4096 slices per call
+ * (larger batches return GTOMRLN_ERR_INVALID; split them).  The array costs
+ * every device that loads the library 147,456 bytes until the process exits.
+ * The first call on a device looks up the array's device address; make it
+ * before any stream capture.  All calls share the one array: calls ordered
+ * on one stream are safe, calls on different streams that overlap on the
+ * GPU race.  Results equal gtomrln_project_angles's. */
+GTOMRLN_API int gtomrln_project_angles_noalloc(const float* d_volumeft, int vx, int vy, int vz,
+                                   float* d_proj, int px, int py, int pz, const float* h_angles,
+                                   float supersample, unsigned batch, void* stream);
+
 /* gtom::d_rlnProject(cudaTex t_volumeRe, cudaTex t_volumeIm, int3 dimsvolume,
  *     tcomplex* d_proj, int3 dimsproj, tfloat3* h_angles, float supersample, uint batch)
  * include/Relion.cuh:36, src/Relion/Project.cu:45-56 */
