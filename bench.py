@@ -83,7 +83,7 @@ def measured_peaks():
 class ClockSampler:
     """Samples SM clock and throttle reasons during the timed region."""
 
-    def __init__(self, index: int, period: float = 0.2):
+    def __init__(self, index: int, period: float = 0.02):
         self.index, self.period = index, period
         self.samples, self.reasons, self.max_mhz = [], set(), None
         self._stop = threading.Event()
@@ -181,6 +181,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
     import gtom_b200 as G
+    from gtom_b200.shard import Accumulators
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -197,8 +198,8 @@ def run_ours(args):
     ws = make_workload(args, dev, SEED + 17 * rank)
     n, P, D, rmax, e = ws["n"], ws["P"], ws["D"], ws["rmax"], ws["e"]
     nvol = (D // 2 + 1) * D * D
-    acc_ft = torch.zeros(nvol, dtype=torch.complex64, device=dev)
-    acc_w = torch.zeros(nvol, dtype=torch.float32, device=dev)
+    acc = Accumulators(nvol, dev)  # data and weights in one buffer: one all-reduce
+    acc_ft, acc_w = acc.data, acc.weights
     proj = torch.empty(B * e, dtype=torch.complex64, device=dev)
     stream = torch.cuda.current_stream()
     ev = []
@@ -221,8 +222,7 @@ def run_ours(args):
 
     for i in range(args.warmup):
         step(i, False)
-    acc_ft.zero_()
-    acc_w.zero_()
+    acc.zero_()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -232,9 +232,7 @@ def run_ours(args):
         start.record(stream)
         for k in range(args.steps):
             step(args.warmup + k, True)
-        if world > 1:  # the one exchange: sum the partial volumes of all ranks
-            dist.all_reduce(torch.view_as_real(acc_ft))
-            dist.all_reduce(acc_w)
+        acc.all_reduce()  # the one exchange: sum the partial volumes of all ranks
         end.record(stream)
         torch.cuda.synchronize()
     if world > 1:
