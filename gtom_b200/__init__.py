@@ -8,9 +8,12 @@ from .relion import (  # noqa: F401
     d_rlnBackproject,
     d_rlnProject,
     elements_fft,
+    gridding_weights,
     kaiser_bessel_table,
     matrices_from_angles,
+    mlp_param_count,
     reconstruct_gridding_tol,
+    reconstruct_gridding_warm,
     set_brick_tuning,
     set_path,
 )

@@ -62,7 +62,17 @@ SIGNATURES: dict[str, list] = {
                                      _d, _i, _d, _p],
     "gtomrln_reconstruct_gridding_tol": [_p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i, _d,
                                          _d, _i, _d, _ip, _dp, _p],
+    "gtomrln_reconstruct_gridding_warm": [_p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i, _d, _f, _p,
+                                          _f, _d, _i, _d, _ip, _dp, _ip, _p],
+    "gtomrln_gridding_weights": [_p, _i, _i, _i, _i, _i, _i, _d, _f, _p, _f, _d, _i, _d, _p, _p,
+                                 _ip, _dp, _ip, _p],
     "gtomrln_kaiser_bessel_table": [_d, _d, _i, _i, _p],
+    "gtomrln_mlp_param_count": [],
+    "gtomrln_mlp_forward": [_p, _p, _i, _p, _p],
+    "gtomrln_mlp_volume_features": [_p, _i, _p, _p, _i, _p, _p],
+    "gtomrln_mlp_gradients": [_p, _p, _p, _p, _i, _f, _p, _p, _p],
+    "gtomrln_mlp_train_batch": [_p, _p, _p, _p, _p, _i, _p, _i, _f, _p, _p, _p],
+    "gtomrln_mlp_adam": [_p, _p, _p, _p, _i, _f, _f, _f, _f, _p],
 }
 _RESTYPES = {"gtomrln_last_error": C.c_char_p}
 

@@ -25,6 +25,7 @@
 #include <tuple>
 
 #include "common.cuh"
+#include "mlp.cuh"
 
 namespace gtomrln {
 
@@ -109,6 +110,63 @@ __global__ void grid_update_kernel(float2* __restrict__ convft, const float* __r
     float fw = Fw[i];
     Fnw[i] = nw;
     if (write_conv) convft[i] = make_float2(fw * nw, 0.f);
+    if (change) {
+      double d = (double)fw * ((double)nw - (double)old);
+      double o = (double)fw * (double)old;
+      d2 = d * d;
+      o2 = o * o;
+    }
+  }
+  if (change) {
+    for (int off = 16; off > 0; off >>= 1) {
+      d2 += __shfl_down_sync(0xffffffffu, d2, off);
+      o2 += __shfl_down_sync(0xffffffffu, o2, off);
+    }
+    __shared__ double s[2][32];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { s[0][warp] = d2; s[1][warp] = o2; }
+    __syncthreads();
+    if (warp == 0) {
+      int nw = blockDim.x >> 5;
+      d2 = lane < nw ? s[0][lane] : 0;
+      o2 = lane < nw ? s[1][lane] : 0;
+      for (int off = 16; off > 0; off >>= 1) {
+        d2 += __shfl_down_sync(0xffffffffu, d2, off);
+        o2 += __shfl_down_sync(0xffffffffu, o2, off);
+      }
+      if (lane == 0) {
+        atomicAdd(change, d2);
+        atomicAdd(change + 1, o2);
+      }
+    }
+  }
+}
+
+// The update of grid_update_kernel applied at an extrapolated point V
+// (Nesterov-style momentum on the logarithm of the weights):
+//   F' = min(1e20, V / max(1e-4, c)),   V' = min(1e20, F' (F' / F)^beta),
+// where c is the real part of the spectrum computed from Fw * V.  Its fixed
+// points are the plain iteration's (c = 1 wherever Fw * F is non-zero); it
+// reaches them in far fewer iterations because the slowest modes of the
+// plain iteration contract by 1 - blob(r) per step, with blob(r) down to
+// ~0.007 at the edge of the box.  The change measure is the plain one,
+// Fw * (F' - F) against Fw * F.
+__global__ void grid_update_momentum_kernel(float2* __restrict__ convft, const float* __restrict__ Fw,
+                                            float* __restrict__ Fnw, float* __restrict__ V, GridGeom g,
+                                            float beta, int write_conv, double* __restrict__ change) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double d2 = 0, o2 = 0;
+  if (i < g.nc) {
+    float c = convft[i].x;
+    float w = fmaxf(1e-4f, c);
+    float old = Fnw[i];
+    float nw = fminf(1e20f, V[i] / w);
+    float ext = nw;
+    if (old > 0.f && nw > 0.f) ext = fminf(1e20f, nw * powf(nw / old, beta));
+    float fw = Fw[i];
+    Fnw[i] = nw;
+    V[i] = ext;
+    if (write_conv) convft[i] = make_float2(fw * ext, 0.f);
     if (change) {
       double d = (double)fw * ((double)nw - (double)old);
       double o = (double)fw * (double)old;
@@ -305,13 +363,33 @@ static int launch_check(const char* what) {
   return GTOMRLN_OK;
 }
 
+// Options beyond the reference's fixed iteration count.
+struct GridOptions {
+  double tolerance = 0;         // stop when the change measure is <= this (0: fixed count)
+  float momentum = 0;           // beta of grid_update_momentum_kernel (0: the plain update)
+  const float* mlp = nullptr;   // MLP parameters: predicted start instead of the sphere mask
+  float residual_limit = 0.5f;  // the predicted start is kept only if its first change is <= this
+  bool weights_only = false;    // stop after the weights (no map)
+  float* out_fw = nullptr;      // copies of the final Fweight / Fnewweight on the P grid
+  float* out_fnw = nullptr;
+};
+
+struct GridResult {
+  int iterations = 0;  // iterations run, including one from a rejected predicted start
+  double change = 0;   // the last change measure
+  int warm_used = 0;   // 1 if the predicted start was kept
+};
+
 static int reconstruct(const float* d_dataft, const float* d_weight, float* d_out, int ori,
                        int oldx, int oldy, int oldz, int pad, cufftHandle planf, cufftHandle planb,
-                       int iterations, double tolerance, double radius, int order, double alpha,
-                       int* iterations_done, double* final_change, cudaStream_t stream) {
+                       int iterations, double radius, int order, double alpha, const GridOptions& opt,
+                       GridResult* res, cudaStream_t stream) {
   if (ori <= 0 || pad <= 0) return set_error(GTOMRLN_ERR_INVALID, "gridding: non-positive size");
   if (iterations < 0) return set_error(GTOMRLN_ERR_INVALID, "gridding: negative iteration count");
-  if (!d_dataft || !d_weight || !d_out) return set_error(GTOMRLN_ERR_INVALID, "gridding: NULL pointer");
+  if (!d_weight || (!opt.weights_only && (!d_dataft || !d_out)))
+    return set_error(GTOMRLN_ERR_INVALID, "gridding: NULL pointer");
+  if (!(opt.momentum >= 0.f && opt.momentum < 1.f))
+    return set_error(GTOMRLN_ERR_INVALID, "gridding: momentum %g outside [0, 1)", (double)opt.momentum);
   const int P = ori * pad;
   GridGeom g;
   g.P = P;
@@ -332,13 +410,17 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   if (planf) plans.r2c = planf;
   if (planb) plans.c2r = planb;
 
+  const bool warm = opt.mlp != nullptr && iterations > 0;
+  const bool momentum = opt.momentum > 0.f;
   float2* convft = nullptr;
   float* conv = nullptr;
-  float *Fw = nullptr, *Fnw = nullptr;
+  float *Fw = nullptr, *Fnw = nullptr, *V = nullptr;
   double* change = nullptr;
+  double* sums = nullptr;
   double h_change[2] = {0, 0};
-  int done_iters = 0;
+  int total_iters = 0;
   double last_change = 0;
+  bool warm_live = warm;
   const int T = 256;
   unsigned bc = (unsigned)((g.nc + T - 1) / T), br = (unsigned)((g.nr + T - 1) / T);
 
@@ -346,14 +428,22 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   GTOMRLN_STEP(pool_alloc((void**)&conv, g.nr * sizeof(float), stream));
   GTOMRLN_STEP(pool_alloc((void**)&Fw, g.nc * sizeof(float), stream));
   GTOMRLN_STEP(pool_alloc((void**)&Fnw, g.nc * sizeof(float), stream));
-  if (tolerance > 0) GTOMRLN_STEP(pool_alloc((void**)&change, 2 * sizeof(double), stream));
+  if (momentum) GTOMRLN_STEP(pool_alloc((void**)&V, g.nc * sizeof(float), stream));
+  if (opt.tolerance > 0 || warm) GTOMRLN_STEP(pool_alloc((void**)&change, 2 * sizeof(double), stream));
+  if (warm) GTOMRLN_STEP(pool_alloc((void**)&sums, 2 * sizeof(double), stream));
 
   GTOMRLN_CUFFT_TRY(cufftSetStream(plans.r2c, stream));
   GTOMRLN_CUFFT_TRY(cufftSetStream(plans.c2r, stream));
 
   grid_init_kernel<<<bc, T, 0, stream>>>(d_weight, oldx, oldy, oldz, Fw, Fnw, convft, g, maskr2,
-                                         iterations > 0);
+                                         iterations > 0 && !warm);
   GTOMRLN_STEP(launch_check("grid_init_kernel"));
+  if (warm) {
+    GTOMRLN_CUDA_TRY(cudaMemsetAsync(sums, 0, 2 * sizeof(double), stream));
+    GTOMRLN_STEP(mlp_weight_scale(Fw, P, maskr2, sums, stream));
+    GTOMRLN_STEP(mlp_predict_start(opt.mlp, Fw, P, maskr2, sums, Fnw, convft, stream));
+  }
+  if (momentum) GTOMRLN_CUDA_TRY(cudaMemcpyAsync(V, Fnw, g.nc * sizeof(float), cudaMemcpyDeviceToDevice, stream));
 
   for (int it = 0; it < iterations; it++) {
     GTOMRLN_CUFFT_TRY(cufftExecC2R(plans.c2r, (cufftComplex*)convft, conv));
@@ -361,38 +451,67 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
                                            (float)(0.5 / kBlobSamples));
     GTOMRLN_STEP(launch_check("grid_blob_kernel"));
     GTOMRLN_CUFFT_TRY(cufftExecR2C(plans.r2c, conv, (cufftComplex*)convft));
-    if (change) GTOMRLN_CUDA_TRY(cudaMemsetAsync(change, 0, 2 * sizeof(double), stream));
-    grid_update_kernel<<<bc, T, 0, stream>>>(convft, Fw, Fnw, g, it + 1 < iterations, change);
+    // the residual check of a predicted start needs the first change
+    double* ch = (opt.tolerance > 0 || (warm_live && it == 0)) ? change : nullptr;
+    if (ch) GTOMRLN_CUDA_TRY(cudaMemsetAsync(ch, 0, 2 * sizeof(double), stream));
+    if (momentum)
+      grid_update_momentum_kernel<<<bc, T, 0, stream>>>(convft, Fw, Fnw, V, g, opt.momentum,
+                                                        it + 1 < iterations, ch);
+    else
+      grid_update_kernel<<<bc, T, 0, stream>>>(convft, Fw, Fnw, g, it + 1 < iterations, ch);
     GTOMRLN_STEP(launch_check("grid_update_kernel"));
-    done_iters = it + 1;
-    if (change) {
-      GTOMRLN_CUDA_TRY(cudaMemcpyAsync(h_change, change, sizeof(h_change), cudaMemcpyDeviceToHost, stream));
+    total_iters++;
+    if (ch) {
+      GTOMRLN_CUDA_TRY(cudaMemcpyAsync(h_change, ch, sizeof(h_change), cudaMemcpyDeviceToHost, stream));
       GTOMRLN_CUDA_TRY(cudaStreamSynchronize(stream));
       last_change = h_change[1] > 0 ? std::sqrt(h_change[0] / h_change[1]) : 0.0;
-      if (last_change <= tolerance) break;
+      if (warm_live && it == 0) {
+        warm_live = false;
+        if (!(last_change <= (double)opt.residual_limit)) {
+          // Rejected predicted start: the cold start (sphere mask) from scratch.
+          grid_init_kernel<<<bc, T, 0, stream>>>(d_weight, oldx, oldy, oldz, Fw, Fnw, convft, g,
+                                                 maskr2, 1);
+          GTOMRLN_STEP(launch_check("grid_init_kernel"));
+          if (momentum)
+            GTOMRLN_CUDA_TRY(cudaMemcpyAsync(V, Fnw, g.nc * sizeof(float), cudaMemcpyDeviceToDevice, stream));
+          if (res) res->warm_used = 0;
+          it = -1;  // restart the count
+          continue;
+        }
+        if (res) res->warm_used = 1;
+      }
+      if (opt.tolerance > 0 && last_change <= opt.tolerance) break;
       if (it + 1 == iterations) break;
     }
   }
 
-  grid_final_kernel<<<bc, T, 0, stream>>>((const float2*)d_dataft, oldx, oldy, oldz, Fw, Fnw,
-                                          convft, g, iterations == 0);
-  GTOMRLN_STEP(launch_check("grid_final_kernel"));
-  GTOMRLN_CUFFT_TRY(cufftExecC2R(plans.c2r, (cufftComplex*)convft, conv));
-  {
+  if (opt.out_fw)
+    GTOMRLN_CUDA_TRY(cudaMemcpyAsync(opt.out_fw, Fw, g.nc * sizeof(float), cudaMemcpyDeviceToDevice, stream));
+  if (opt.out_fnw)
+    GTOMRLN_CUDA_TRY(cudaMemcpyAsync(opt.out_fnw, Fnw, g.nc * sizeof(float), cudaMemcpyDeviceToDevice, stream));
+  if (!opt.weights_only) {
+    grid_final_kernel<<<bc, T, 0, stream>>>((const float2*)d_dataft, oldx, oldy, oldz, Fw, Fnw,
+                                            convft, g, iterations == 0);
+    GTOMRLN_STEP(launch_check("grid_final_kernel"));
+    GTOMRLN_CUFFT_TRY(cufftExecC2R(plans.c2r, (cufftComplex*)convft, conv));
     int64_t total = (int64_t)ori * ori * ori;
     grid_crop_kernel<<<(unsigned)((total + T - 1) / T), T, 0, stream>>>(
         conv, d_out, P, ori, P / 2 - ori / 2, 1.0f / (float)(pad * pad * pad * ori));
     GTOMRLN_STEP(launch_check("grid_crop_kernel"));
   }
-  if (iterations_done) *iterations_done = done_iters;
-  if (final_change) *final_change = last_change;
+  if (res) {
+    res->iterations = total_iters;
+    res->change = last_change;
+  }
 
 done:
   pool_free(convft, stream);
   pool_free(conv, stream);
   pool_free(Fw, stream);
   pool_free(Fnw, stream);
+  pool_free(V, stream);
   pool_free(change, stream);
+  pool_free(sums, stream);
   return st;
 }
 
@@ -461,9 +580,10 @@ int gtomrln_reconstruct_gridding(const float* d_dataft, const float* d_weight,
   clear_error();
   (void)oy;
   (void)oz;
+  GridOptions opt;
   return reconstruct(d_dataft, d_weight, d_reconstructed, ox, padx, pady, padz, paddingfactor,
-                     (cufftHandle)pre_planforw, (cufftHandle)pre_planback, iterations, 0.0,
-                     blobradius, bloborder, blobalpha, nullptr, nullptr, (cudaStream_t)stream);
+                     (cufftHandle)pre_planforw, (cufftHandle)pre_planback, iterations, blobradius,
+                     bloborder, blobalpha, opt, nullptr, (cudaStream_t)stream);
 }
 
 int gtomrln_reconstruct_gridding_tol(const float* d_dataft, const float* d_weight,
@@ -475,9 +595,63 @@ int gtomrln_reconstruct_gridding_tol(const float* d_dataft, const float* d_weigh
   clear_error();
   (void)oy;
   (void)oz;
-  return reconstruct(d_dataft, d_weight, d_reconstructed, ox, padx, pady, padz, paddingfactor, 0,
-                     0, max_iterations, tolerance, blobradius, bloborder, blobalpha,
-                     iterations_done, final_change, (cudaStream_t)stream);
+  GridOptions opt;
+  opt.tolerance = tolerance;
+  GridResult res;
+  int st = reconstruct(d_dataft, d_weight, d_reconstructed, ox, padx, pady, padz, paddingfactor, 0, 0,
+                       max_iterations, blobradius, bloborder, blobalpha, opt, &res, (cudaStream_t)stream);
+  if (iterations_done) *iterations_done = res.iterations;
+  if (final_change) *final_change = res.change;
+  return st;
+}
+
+int gtomrln_reconstruct_gridding_warm(const float* d_dataft, const float* d_weight,
+                                      float* d_reconstructed, int ox, int oy, int oz, int padx,
+                                      int pady, int padz, int paddingfactor, int max_iterations,
+                                      double tolerance, float momentum, const float* d_mlp_params,
+                                      float residual_limit, double blobradius, int bloborder,
+                                      double blobalpha, int* iterations_done, double* final_change,
+                                      int* warm_used, void* stream) {
+  clear_error();
+  (void)oy;
+  (void)oz;
+  GridOptions opt;
+  opt.tolerance = tolerance;
+  opt.momentum = momentum;
+  opt.mlp = d_mlp_params;
+  opt.residual_limit = residual_limit;
+  GridResult res;
+  int st = reconstruct(d_dataft, d_weight, d_reconstructed, ox, padx, pady, padz, paddingfactor, 0, 0,
+                       max_iterations, blobradius, bloborder, blobalpha, opt, &res, (cudaStream_t)stream);
+  if (iterations_done) *iterations_done = res.iterations;
+  if (final_change) *final_change = res.change;
+  if (warm_used) *warm_used = res.warm_used;
+  return st;
+}
+
+int gtomrln_gridding_weights(const float* d_weight, int ox, int oy, int oz, int ori,
+                             int paddingfactor, int max_iterations, double tolerance, float momentum,
+                             const float* d_mlp_params, float residual_limit, double blobradius,
+                             int bloborder, double blobalpha, float* d_fw, float* d_fnw,
+                             int* iterations_done, double* final_change, int* warm_used,
+                             void* stream) {
+  clear_error();
+  if (!d_fnw) return set_error(GTOMRLN_ERR_INVALID, "gridding_weights: NULL output");
+  GridOptions opt;
+  opt.tolerance = tolerance;
+  opt.momentum = momentum;
+  opt.mlp = d_mlp_params;
+  opt.residual_limit = residual_limit;
+  opt.weights_only = true;
+  opt.out_fw = d_fw;
+  opt.out_fnw = d_fnw;
+  GridResult res;
+  int st = reconstruct(nullptr, d_weight, nullptr, ori, ox, oy, oz, paddingfactor, 0, 0, max_iterations,
+                       blobradius, bloborder, blobalpha, opt, &res, (cudaStream_t)stream);
+  if (iterations_done) *iterations_done = res.iterations;
+  if (final_change) *final_change = res.change;
+  if (warm_used) *warm_used = res.warm_used;
+  return st;
 }
 
 int gtomrln_kaiser_bessel_table(double radius, double alpha, int order, int nsamples,

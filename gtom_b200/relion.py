@@ -208,6 +208,64 @@ def reconstruct_gridding_tol(dataft, weight, reconstructed, dimsori: Dims, dimsp
     return it.value, ch.value
 
 
+def reconstruct_gridding_warm(dataft, weight, reconstructed, dimsori: Dims, dimspadded: Dims,
+                              mlp_params=None, paddingfactor: int = 2, max_iterations: int = 1000,
+                              tolerance: float = 1e-4, momentum: float = 0.0,
+                              residual_limit: float = 0.5, blobradius: float = 1.9,
+                              bloborder: int = 0, blobalpha: float = 15.0,
+                              stream=None) -> tuple[int, float, bool]:
+    """Gridding reconstruction from the MLP's predicted start (mlp_params, a
+    CUDA float32 tensor of mlp_param_count() values; None for the
+    sphere-mask start) and/or with momentum (gtomrln_reconstruct_gridding_warm).
+    Returns (iterations run, last relative change, predicted start kept)."""
+    ox, oy, oz = (int(v) for v in dimsori)
+    qx, qy, qz = (int(v) for v in dimspadded)
+    npad = elements_fft((qx, qy, qz))
+    it, ch, used = C.c_int(0), C.c_double(0), C.c_int(0)
+    _lib.call("gtomrln_reconstruct_gridding_warm",
+              _dev_ptr(dataft, "d_dataft", torch.complex64, npad),
+              _dev_ptr(weight, "d_weight", torch.float32, npad),
+              _dev_ptr(reconstructed, "d_reconstructed", torch.float32, ox * oy * oz),
+              ox, oy, oz, qx, qy, qz, int(paddingfactor), int(max_iterations), float(tolerance),
+              C.c_float(float(momentum)),
+              _dev_ptr(mlp_params, "d_mlp_params", torch.float32, mlp_param_count(), optional=True),
+              C.c_float(float(residual_limit)), float(blobradius), int(bloborder), float(blobalpha),
+              C.byref(it), C.byref(ch), C.byref(used), _stream(stream))
+    return it.value, ch.value, bool(used.value)
+
+
+def gridding_weights(weight, dimspadded: Dims, ori: int, paddingfactor: int = 2,
+                     max_iterations: int = 1000, tolerance: float = 1e-4, momentum: float = 0.0,
+                     mlp_params=None, residual_limit: float = 0.5, blobradius: float = 1.9,
+                     bloborder: int = 0, blobalpha: float = 15.0, fw_out=None, fnw_out=None,
+                     stream=None):
+    """The gridding weights only (gtomrln_gridding_weights).  Returns
+    (Fnewweight, Fweight, iterations, last change, predicted start kept);
+    the weights are flat float32 CUDA tensors on the decentred
+    (P/2+1) x P x P grid, P = ori * paddingfactor."""
+    qx, qy, qz = (int(v) for v in dimspadded)
+    P = int(ori) * int(paddingfactor)
+    nc = (P // 2 + 1) * P * P
+    dev = weight.device
+    fnw = fnw_out if fnw_out is not None else torch.empty(nc, dtype=torch.float32, device=dev)
+    fw = fw_out if fw_out is not None else torch.empty(nc, dtype=torch.float32, device=dev)
+    it, ch, used = C.c_int(0), C.c_double(0), C.c_int(0)
+    _lib.call("gtomrln_gridding_weights",
+              _dev_ptr(weight, "d_weight", torch.float32, elements_fft((qx, qy, qz))),
+              qx, qy, qz, int(ori), int(paddingfactor), int(max_iterations), float(tolerance),
+              C.c_float(float(momentum)),
+              _dev_ptr(mlp_params, "d_mlp_params", torch.float32, mlp_param_count(), optional=True),
+              C.c_float(float(residual_limit)), float(blobradius), int(bloborder), float(blobalpha),
+              _dev_ptr(fw, "d_fw", torch.float32, nc), _dev_ptr(fnw, "d_fnw", torch.float32, nc),
+              C.byref(it), C.byref(ch), C.byref(used), _stream(stream))
+    return fnw, fw, it.value, ch.value, bool(used.value)
+
+
+def mlp_param_count() -> int:
+    """Floats in the warm-start MLP's parameter block."""
+    return int(_lib.load().gtomrln_mlp_param_count())
+
+
 _OPS = {"project": 0, "backproject": 1}
 _PATHS = {"auto": 0, "direct": 1, "brick": 2}
 

@@ -227,6 +227,85 @@ GTOMRLN_API int gtomrln_reconstruct_gridding_tol(const float* d_dataft, const fl
                                      double blobalpha, int* iterations_done,
                                      double* final_change, void* stream);
 
+/* Extension (no reference counterpart): the gridding reconstruction with a
+ * learned warm start and/or momentum.
+ *   d_mlp_params: NULL for the reference's sphere-mask start, else the
+ *     parameter block of the per-voxel MLP (gtomrln_mlp_param_count()
+ *     floats, device memory; layout in gtom_b200/csrc/mlp.cuh), which
+ *     predicts the converged Fnewweight from the 27 log-weights around each
+ *     voxel and its radius.  The first iteration from the predicted start is
+ *     its residual check: if its relative change exceeds residual_limit (or
+ *     is not finite) the prediction is discarded and the iteration restarts
+ *     from the sphere mask (*warm_used = 0; the rejected iteration still
+ *     counts in *iterations_done).
+ *   momentum: 0 for the reference's update Fnw <- Fnw / max(1e-4, c); in
+ *     (0, 1) the update is applied at the extrapolated point
+ *     V = Fnw' (Fnw' / Fnw)^momentum (same fixed points, far fewer
+ *     iterations to a given distance from them).
+ * max_iterations / tolerance / *iterations_done / *final_change as in
+ * gtomrln_reconstruct_gridding_tol; any output pointer may be NULL. */
+GTOMRLN_API int gtomrln_reconstruct_gridding_warm(const float* d_dataft, const float* d_weight,
+                                      float* d_reconstructed, int ox, int oy, int oz, int padx,
+                                      int pady, int padz, int paddingfactor, int max_iterations,
+                                      double tolerance, float momentum,
+                                      const float* d_mlp_params, float residual_limit,
+                                      double blobradius, int bloborder, double blobalpha,
+                                      int* iterations_done, double* final_change, int* warm_used,
+                                      void* stream);
+
+/* Extension (no reference counterpart): only the gridding weights of
+ * gtomrln_reconstruct_gridding_warm for the weights d_weight (centred half
+ * volume of dims ox x oy x oz, at least P + 1 with P = ori * paddingfactor):
+ * d_fnw receives Fnewweight and d_fw (may be NULL) the decentred, masked
+ * Fweight, both on the decentred (P/2+1) x P x P grid.  Used to make the
+ * MLP's training pairs and to compare starts. */
+GTOMRLN_API int gtomrln_gridding_weights(const float* d_weight, int ox, int oy, int oz, int ori,
+                             int paddingfactor, int max_iterations, double tolerance,
+                             float momentum, const float* d_mlp_params, float residual_limit,
+                             double blobradius, int bloborder, double blobalpha, float* d_fw,
+                             float* d_fnw, int* iterations_done, double* final_change,
+                             int* warm_used, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * The warm-start MLP (no reference counterpart).  28 inputs -> 64 -> 64 -> 1,
+ * ReLU, FP32; parameters, gradients and Adam moments are arrays of
+ * gtomrln_mlp_param_count() floats with the layout of
+ * gtom_b200/csrc/mlp.cuh (the first 56 entries, the input standardisation,
+ * are not trained).  Features are the raw 28 inputs of a voxel (27
+ * log-weights, radius); targets are log(Fnewweight * s).
+ * ------------------------------------------------------------------------- */
+GTOMRLN_API int gtomrln_mlp_param_count(void);
+
+/* d_out[i] = network output for the raw features d_features[i*28 .. +28). */
+GTOMRLN_API int gtomrln_mlp_forward(const float* d_params, const float* d_features, int n,
+                        float* d_out, void* stream);
+
+/* Raw features of n voxels of a stack of decentred half grids of P (each
+ * (P/2+1) x P x P floats of Fweight): voxel i is element d_index[i] of the
+ * stack, whose volume v = d_index[i] / ((P/2+1) P P) has weight scale
+ * 1 / d_inv_scale[v]. */
+GTOMRLN_API int gtomrln_mlp_volume_features(const float* d_fw, int P, const float* d_inv_scale,
+                                const long long* d_index, int n, float* d_features,
+                                void* stream);
+
+/* Loss L = loss_scale * sum_i w_i (out_i - t_i)^2 over n samples given as
+ * raw features, added to *d_loss; dL/dparams added to d_grad. */
+GTOMRLN_API int gtomrln_mlp_gradients(const float* d_params, const float* d_features,
+                          const float* d_targets, const float* d_weights, int n,
+                          float loss_scale, float* d_grad, float* d_loss, void* stream);
+
+/* The same for samples gathered from a stack of half grids (as in
+ * gtomrln_mlp_volume_features); d_target / d_weight are stacks of the same
+ * shape holding each voxel's target and loss weight. */
+GTOMRLN_API int gtomrln_mlp_train_batch(const float* d_params, const float* d_fw,
+                            const float* d_target, const float* d_weight,
+                            const float* d_inv_scale, int P, const long long* d_index, int n,
+                            float loss_scale, float* d_grad, float* d_loss, void* stream);
+
+/* One Adam step (step counts from 1) on the trained entries; zeroes d_grad. */
+GTOMRLN_API int gtomrln_mlp_adam(float* d_params, float* d_grad, float* d_m, float* d_v, int step,
+                     float lr, float beta1, float beta2, float eps, void* stream);
+
 /* The normalised Kaiser-Bessel table the gridding uses: nsamples values of
  * kaiser_Fourier_value(i * 0.5 / nsamples, radius, alpha, order) divided by
  * the value at 0 (src/Helpers/KaiserBessel.cpp:357-376,
