@@ -34,7 +34,7 @@ __device__ __forceinline__ void voxel_xyz(int64_t i, int P, int* x, int* y, int*
 __device__ __forceinline__ int signed_coord(int v, int P) { return v < P / 2 + 1 ? v : v - P; }
 
 // ------------------------------------------------------------- inference --
-__global__ void __launch_bounds__(kInferThreads) mlp_start_kernel(
+__global__ void __launch_bounds__(kInferThreads, 2) mlp_start_kernel(
     const float* __restrict__ params, const float* __restrict__ Fw, int P, int maskr2,
     const double* __restrict__ scale_sums, float* __restrict__ Fnw, float2* __restrict__ convft) {
   __shared__ __align__(16) float sp[kParamsPadded];

@@ -76,31 +76,49 @@ def random_distribution(rng, views_range=(5000, 200000), lobes_range=(1, 5),
                         seed=int(rng.integers(1 << 31)))
 
 
-def sampling_weights(box: int, dist: Distribution, pad: int = 2, device="cuda",
-                     chunk: int = 8192) -> torch.Tensor:
-    """Centred weight half volume of P + 1 (P = box * pad) accumulated from
-    the CTF^2 weights of dist.views particles (300 kV, Cs 2.7 mm, 1 A/px,
-    defocus U(0.5, 3) um, astigmatism U(0, 0.1) um) at the distribution's
-    orientations."""
+def insert_distribution(box: int, dist: Distribution, pad: int = 2, device="cuda",
+                        chunk: int = 8192, volft: torch.Tensor | None = None):
+    """Centred half volumes of P + 1 (P = box * pad) accumulated from
+    dist.views particles at the distribution's orientations, each with a CTF
+    (300 kV, Cs 2.7 mm, 1 A/px, defocus U(0.5, 3) um, astigmatism
+    U(0, 0.1) um): the CTF^2 weights, and, when volft (the decentred padded
+    half transform of a box^3 volume) is given, the CTF-weighted central
+    slices of it.  Returns (data or None, weights)."""
+    from .relion import d_rlnProject
     rng = np.random.default_rng(dist.seed)
     n = box
-    D = box * pad + 1
+    P = box * pad
+    D = P + 1
     nvol = (D // 2 + 1) * D * D
     acc = torch.zeros(nvol, dtype=torch.float32, device=device)
+    data = None if volft is None else torch.zeros(nvol, dtype=torch.complex64, device=device)
     ang = synth.vmf_mixture_angles(rng, dist.views, lobes=dist.lobes, kappa_range=dist.kappa_range,
                                    uniform_frac=dist.uniform_frac)
     mats = torch.from_numpy(matrices_from_angles(ang, float(pad))).to(device)
     e = (n // 2 + 1) * n
+    proj = None if volft is None else torch.empty(min(chunk, dist.views) * e, dtype=torch.complex64,
+                                                  device=device)
     for c0 in range(0, dist.views, chunk):
         c = min(chunk, dist.views - c0)
+        m = mats[c0:c0 + c].reshape(-1)
         df = torch.from_numpy(rng.uniform(0.5, 3.0, c).astype(np.float32)).to(device)
         da = torch.from_numpy(rng.uniform(0.0, 0.1, c).astype(np.float32)).to(device)
         aa = torch.from_numpy(rng.uniform(0.0, np.pi, c).astype(np.float32)).to(device)
         ctf = synth.ctf_half(n, df, da, aa).reshape(c, e)
         w = (ctf * ctf).contiguous()
-        d_rlnBackproject(None, acc, (D, D, D), None, w.reshape(-1), (n, n, 1), n // 2,
-                         mats[c0:c0 + c].reshape(-1), None, (1, 0, 0, 1), 0.0, False, False, c)
-    return acc
+        slices = None
+        if volft is not None:
+            d_rlnProject(volft, (P, P, P), proj, (n, n, 1), n // 2, m, c)
+            slices = (proj[:c * e].reshape(c, e) * ctf).contiguous().reshape(-1)
+        d_rlnBackproject(data, acc, (D, D, D), slices, w.reshape(-1), (n, n, 1), n // 2, m, None,
+                         (1, 0, 0, 1), 0.0, False, False, c)
+    return data, acc
+
+
+def sampling_weights(box: int, dist: Distribution, pad: int = 2, device="cuda",
+                     chunk: int = 8192) -> torch.Tensor:
+    """The CTF^2 weight volume of insert_distribution."""
+    return insert_distribution(box, dist, pad, device, chunk)[1]
 
 
 def sphere_mask(P: int, device) -> torch.Tensor:
@@ -134,16 +152,18 @@ class TrainingSet:
     converged: list = field(default_factory=list)  # (iterations, change) per distribution
 
 
-def make_training_set(weights: list, ori: int, pad: int = 2, tolerance: float = 1e-6,
-                      max_iterations: int = 5000, momentum: float = 0.9) -> TrainingSet:
+def make_training_set(weights, ori: int, pad: int = 2, tolerance: float = 1e-6,
+                      max_iterations: int = 5000, momentum: float = 0.9, count: int | None = None,
+                      device="cuda", max_voxels: int | None = None) -> TrainingSet:
     """Converged gridding weights of each centred weight volume (dims P+1)
-    and the tensors the training kernel reads."""
+    and the tensors the training kernel reads.  weights: a list of volumes,
+    or any iterable of `count` volumes (made one at a time)."""
     P = ori * pad
     D = P + 1
     nc = (P // 2 + 1) * P * P
-    dev = weights[0].device
+    nd = len(weights) if count is None else int(count)
+    dev = torch.device(device)
     mask = sphere_mask(P, dev)
-    nd = len(weights)
     fw_all = torch.empty(nd * nc, dtype=torch.float32, device=dev)
     tg_all = torch.empty(nd * nc, dtype=torch.float32, device=dev)
     lw_all = torch.zeros(nd * nc, dtype=torch.float32, device=dev)
@@ -163,7 +183,12 @@ def make_training_set(weights: list, ori: int, pad: int = 2, tolerance: float = 
         m = lw[sel].double().mean() if bool(sel.any()) else 0.0
         if m > 0:
             lw_all[d * nc:(d + 1) * nc] = (lw / m).float()
-        elig.append(torch.nonzero(sel).squeeze(1) + d * nc)
+        idx = torch.nonzero(sel).squeeze(1)
+        if max_voxels and idx.numel() > max_voxels:  # a random subset keeps the index list small
+            g = torch.Generator(device=dev)
+            g.manual_seed(d)
+            idx = idx[torch.randperm(idx.numel(), generator=g, device=dev)[:max_voxels]]
+        elig.append(idx + d * nc)
     return TrainingSet(P=P, fw=fw_all, target=tg_all, weight=lw_all, inv_scale=inv,
                        eligible=torch.cat(elig), converged=conv)
 
@@ -232,3 +257,162 @@ def train(ts: TrainingSet, params: torch.Tensor, steps: int = 2000, batch: int =
         if (log_every and step % log_every == 0) or step == steps:
             losses.append(float(loss.item()))
     return losses
+
+
+# ------------------------------------------------------------ evaluation --
+# (name, momentum, use the network)
+MODES = (("plain", 0.0, False), ("plain+mlp", 0.0, True), ("momentum", 0.9, False),
+         ("momentum+mlp", 0.9, True))
+
+
+def fsc_min(a: torch.Tensor, b: torch.Tensor, box: int) -> float:
+    """Minimum over Fourier shells 1 .. box/2 of the correlation of two
+    box^3 maps."""
+    fa = torch.fft.rfftn(a.reshape(box, box, box).double())
+    fb = torch.fft.rfftn(b.reshape(box, box, box).double())
+    k = torch.fft.fftfreq(box, device=a.device) * box
+    kx = torch.fft.rfftfreq(box, device=a.device) * box
+    r = torch.sqrt(k[:, None, None] ** 2 + k[None, :, None] ** 2 + kx[None, None, :] ** 2).round().long()
+    num = torch.zeros(box, dtype=torch.float64, device=a.device)
+    da = torch.zeros_like(num)
+    db = torch.zeros_like(num)
+    keep = r < box
+    rr = r[keep]
+    num.index_add_(0, rr, (fa * fb.conj()).real[keep])
+    da.index_add_(0, rr, (fa.abs() ** 2)[keep])
+    db.index_add_(0, rr, (fb.abs() ** 2)[keep])
+    f = num[1:box // 2 + 1] / torch.sqrt(da[1:box // 2 + 1] * db[1:box // 2 + 1]).clamp_min(1e-300)
+    return float(f.min())
+
+
+def evaluate(params: torch.Tensor | None, box: int, dists: list, pad: int = 2,
+             tolerance: float = 1e-4, max_iterations: int = 5000, volft=None) -> list:
+    """For each distribution: the converged weights (momentum, relative
+    change 1e-6, about the float32 floor of the change measure), then for each of MODES the iterations to `tolerance`, the
+    weighted distance of the stopped weights from the converged ones, the
+    wall time of the whole reconstruction through reconstruct_gridding_warm
+    (CUDA events around the call, which synchronises once per iteration),
+    and the map's minimum FSC to the plain map and to the map made with the
+    converged weights."""
+    from .relion import reconstruct_gridding_warm
+    P = box * pad
+    D = P + 1
+    rows = []
+    for dist in dists:
+        data, w = insert_distribution(box, dist, pad, volft=volft)
+        if data is None:
+            data = torch.complex(w, torch.zeros_like(w)).contiguous()
+        ref, fw, it_ref, ch_ref, _ = gridding_weights(w, (D, D, D), box, pad, 5000, 1e-6, 0.9)
+        row = {"views": dist.views, "lobes": dist.lobes, "uniform_frac": round(dist.uniform_frac, 3),
+               "reference": {"iterations": it_ref, "change": ch_ref}}
+        out = torch.empty(box ** 3, dtype=torch.float32, device=w.device)
+        reconstruct_gridding_warm(data, w, out, (box,) * 3, (D,) * 3, None, pad, 2, 0.0)  # plans
+        converged_map = torch.empty_like(out)
+        reconstruct_gridding_warm(data, w, converged_map, (box,) * 3, (D,) * 3, None, pad, 5000, 1e-6, 0.9)
+        maps = {}
+        for name, mom, use in MODES:
+            p = params if use else None
+            if use and p is None:
+                continue
+            fnw, _, it, ch, used = gridding_weights(w, (D, D, D), box, pad, max_iterations, tolerance, mom,
+                                                    mlp_params=p)
+            res = {"iterations": it, "change": ch, "warm_used": used,
+                   "distance_to_converged": weighted_distance(fw, fnw, ref)}
+            m = torch.empty_like(out)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record()
+            reconstruct_gridding_warm(data, w, m, (box,) * 3, (D,) * 3, p, pad, max_iterations, tolerance,
+                                      mom)
+            b.record()
+            torch.cuda.synchronize()
+            res["ms"] = a.elapsed_time(b)
+            maps[name] = m
+            row[name] = res
+        for name, m in maps.items():
+            row[name]["fsc_min_to_plain"] = fsc_min(m, maps["plain"], box)
+            row[name]["fsc_min_to_converged"] = fsc_min(m, converged_map, box)
+        rows.append(row)
+    return rows
+
+
+def summarise(rows: list) -> dict:
+    """Medians over distributions per mode, and the wall-time and iteration
+    ratios of each mode against the plain cold start."""
+    out = {}
+    for name, _, _ in MODES:
+        have = [r[name] for r in rows if name in r]
+        if not have:
+            continue
+        med = lambda k: float(np.median([h[k] for h in have]))
+        out[name] = {"iterations": med("iterations"), "ms": med("ms"),
+                     "distance_to_converged": med("distance_to_converged"),
+                     "fsc_min_to_plain": float(min(h["fsc_min_to_plain"] for h in have)),
+                     "fsc_min_to_converged": float(min(h["fsc_min_to_converged"] for h in have)),
+                     "warm_rejected": int(sum(1 for h in have if not h["warm_used"]))
+                     if name.endswith("+mlp") else 0,
+                     "speedup_vs_plain": float(np.median([r["plain"]["ms"] / r[name]["ms"] for r in rows
+                                                          if name in r]))}
+    return out
+
+
+def main(argv=None) -> None:
+    """Make the training set, train, save the parameters for the box size,
+    evaluate on held-out distributions and write a JSON report.
+
+        python -m gtom_b200.warmstart --box 128 --train 400 --held-out 100 \\
+            --eval 16 --steps 3000 --save --report out.json
+    """
+    import argparse
+    import json
+    import time
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--box", type=int, default=128)
+    ap.add_argument("--pad", type=int, default=2)
+    ap.add_argument("--train", type=int, default=400, help="training distributions")
+    ap.add_argument("--held-out", type=int, default=100, help="held-out distributions")
+    ap.add_argument("--eval", type=int, default=16, help="held-out distributions evaluated")
+    ap.add_argument("--views", type=int, nargs=2, default=(5000, 200000))
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--batch", type=int, default=32768)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--max-voxels", type=int, default=400000, help="trained voxels kept per distribution")
+    ap.add_argument("--seed", type=int, default=1004)
+    ap.add_argument("--save", action="store_true", help="store the parameters under gtom_b200/data/")
+    ap.add_argument("--report", default=None)
+    a = ap.parse_args(argv)
+    rng = np.random.default_rng(a.seed)
+    dists = [random_distribution(rng, views_range=tuple(a.views)) for _ in range(a.train + a.held_out)]
+    train_d, held = dists[:a.train], dists[a.train:]
+    rep = {"box": a.box, "pad": a.pad, "train": a.train, "held_out": a.held_out, "seed": a.seed,
+           "views_range": list(a.views)}
+    t0 = time.perf_counter()
+    ts = make_training_set((sampling_weights(a.box, d, a.pad) for d in train_d), a.box, a.pad,
+                           count=len(train_d), max_voxels=a.max_voxels)
+    torch.cuda.synchronize()
+    rep["make_training_set_s"] = round(time.perf_counter() - t0, 1)
+    rep["reference_iterations_median"] = float(np.median([c[0] for c in ts.converged]))
+    params = init_params(ts, seed=a.seed)
+    t0 = time.perf_counter()
+    losses = train(ts, params, steps=a.steps, batch=a.batch, lr=a.lr, log_every=max(1, a.steps // 20))
+    torch.cuda.synchronize()
+    rep["train_s"] = round(time.perf_counter() - t0, 1)
+    rep["losses"] = [round(x, 5) for x in losses]
+    del ts
+    torch.cuda.empty_cache()
+    if a.save:
+        rep["saved"] = str(save_params(params, a.box).name)
+    from .synth import blob_volume, padded_half_ft
+    volft = padded_half_ft(blob_volume(a.box, 2000 if a.box >= 128 else 200, a.seed, "cuda"), a.pad).reshape(-1)
+    rows = evaluate(params, a.box, held[:a.eval], a.pad, volft=volft)
+    rep["summary"] = summarise(rows)
+    rep["rows"] = rows
+    text = json.dumps(rep, indent=1)
+    if a.report:
+        Path(a.report).write_text(text)
+    print(json.dumps({"summary": rep["summary"], "train_s": rep["train_s"],
+                      "make_training_set_s": rep["make_training_set_s"]}))
+
+
+if __name__ == "__main__":
+    main()
