@@ -34,50 +34,215 @@ __device__ __forceinline__ void voxel_xyz(int64_t i, int P, int* x, int* y, int*
 __device__ __forceinline__ int signed_coord(int v, int P) { return v < P / 2 + 1 ? v : v - P; }
 
 // ------------------------------------------------------------- inference --
-__global__ void __launch_bounds__(kInferThreads, 2) mlp_start_kernel(
+// Predicted start over a half grid.  A block scans chunks of kChunk
+// consecutive voxels: voxels outside the sphere or without weight get the
+// cold value at once; the others are compacted into a list and evaluated
+// in tiles of kTileV voxels as two small matrix products in shared memory,
+//   H1 = relu(X W1^T + b1)   (kTileV x 28) . (28 x 64)
+//   out = b3 + relu(H1 W2^T + b2) . W3
+// each thread holding an 8-voxel x 4-unit register tile, so that three
+// shared-memory loads feed 32 FMAs.  Inputs and activations are stored
+// transposed (feature-major) for float4 loads along the voxels.
+constexpr int kTileV = 128;
+constexpr int kChunk = 1024;
+constexpr int kStartThreads = 256;  // two threads per tile voxel for the features
+constexpr int kH1Row = kTileV + 4;  // padded: the 16 rows a warp stores hit distinct banks
+
+struct StartShared {
+  float xt[kMlpIn][kTileV];
+  float h1t[kMlpHidden][kH1Row];
+  float w1t[kMlpIn][kMlpHidden];
+  float w2t[kMlpHidden][kMlpHidden];
+  float b1[kMlpHidden], b2[kMlpHidden], w3[kMlpHidden];
+  float shift[kMlpIn], scale[kMlpIn];
+  unsigned short list[kChunk];
+  int count;
+};
+
+// Feature k (0..26) of voxel (x, y, z), standardised.
+__device__ __forceinline__ float start_feature(const StartShared& S, const float* __restrict__ Fw,
+                                               int P, float inv_s, int x, int y, int z, int k) {
+  int dz = k / 9 - 1, dy = (k / 3) % 3 - 1, dx = k % 3 - 1;
+  float w = __ldg(Fw + mlp_neighbour_index(P, x, y, z, dx, dy, dz));
+  return (logf(w * inv_s + kMlpWeightFloor) - S.shift[k]) * S.scale[k];
+}
+
+__global__ void __launch_bounds__(kStartThreads) mlp_start_kernel(
     const float* __restrict__ params, const float* __restrict__ Fw, int P, int maskr2,
     const double* __restrict__ scale_sums, float* __restrict__ Fnw, float2* __restrict__ convft) {
-  __shared__ __align__(16) float sp[kParamsPadded];
-  load_params(params, sp);
-  __syncthreads();
-  const int64_t nc = (int64_t)(P / 2 + 1) * P * P;
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nc) return;
-  int x, y, z;
-  voxel_xyz(i, P, &x, &y, &z);
-  int yp = signed_coord(y, P), zp = signed_coord(z, P);
-  float nw = 0.f;
-  float fw = Fw[i];
-  if (x * x + yp * yp + zp * zp < maskr2) {
-    nw = 1.f;
-    if (fw > 0.f) {
-      double sum = scale_sums[0], cnt = scale_sums[1];
-      float inv_s = sum > 0 ? (float)(cnt / sum) : 1.f;
-      float f[kMlpIn];
-      float out;
-      if (x == 0 && (yp != 0 || zp != 0)) {
-        // Hermitian mates on x = 0 are one Fourier component: both get the
-        // mean of the two outputs, evaluated in the same order (canonical
-        // mate first) on both threads, so the two starts are bit-identical.
-        bool canonical = (zp > 0) || (zp == 0 && yp > 0);
-        int my = y == 0 ? 0 : P - y, mz = z == 0 ? 0 : P - z;
-        float o[2];
+  extern __shared__ __align__(16) unsigned char start_raw[];
+  StartShared& S = *reinterpret_cast<StartShared*>(start_raw);
+  const int t = threadIdx.x;
+  for (int i = t; i < kMlpIn * kMlpHidden; i += kStartThreads)
+    S.w1t[i / kMlpHidden][i % kMlpHidden] = __ldg(params + kMlpOffW1 + (i % kMlpHidden) * kMlpIn + i / kMlpHidden);
+  for (int i = t; i < kMlpHidden * kMlpHidden; i += kStartThreads)
+    S.w2t[i / kMlpHidden][i % kMlpHidden] =
+        __ldg(params + kMlpOffW2 + (i % kMlpHidden) * kMlpHidden + i / kMlpHidden);
+  if (t < kMlpHidden) {
+    S.b1[t] = __ldg(params + kMlpOffB1 + t);
+    S.b2[t] = __ldg(params + kMlpOffB2 + t);
+    S.w3[t] = __ldg(params + kMlpOffW3 + t);
+  }
+  if (t < kMlpIn) {
+    S.shift[t] = __ldg(params + kMlpOffShift + t);
+    S.scale[t] = __ldg(params + kMlpOffScale + t);
+  }
+  const float b3 = __ldg(params + kMlpOffB3);
+  const double sum = scale_sums[0], cnt = scale_sums[1];
+  const float inv_s = sum > 0 ? (float)(cnt / sum) : 1.f;
+  const int rowlen = P / 2 + 1;
+  const int64_t nc = (int64_t)rowlen * P * P;
+  const int64_t nchunks = (nc + kChunk - 1) / kChunk;
+  const int lane = t & 31;
+  const int tj = t & 15, tv = t >> 4;  // register tile: units 4 tj .. +3, voxels 8 tv .. +7
+  const int j0 = tj * 4, v0 = tv * 8;
+
+  for (int64_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+    const int64_t base = chunk * kChunk;
+    if (t == 0) S.count = 0;
+    __syncthreads();
 #pragma unroll 1
-        for (int q = 0; q < 2; q++) {
-          bool own = (q == 0) == canonical;
-          mlp_voxel_features(Fw, P, inv_s, 0, own ? y : my, own ? z : mz, f);
-          o[q] = mlp_forward(sp, f);
+    for (int q = 0; q < kChunk / kStartThreads; q++) {
+      const int local = q * kStartThreads + t;
+      const int64_t i = base + local;
+      bool elig = false;
+      if (i < nc) {
+        int x = (int)(i % rowlen);
+        int64_t r = i / rowlen;
+        int y = (int)(r % P), z = (int)(r / P);
+        int yp = y < P / 2 + 1 ? y : y - P, zp = z < P / 2 + 1 ? z : z - P;
+        bool inside = x * x + yp * yp + zp * zp < maskr2;
+        float fw = Fw[i];
+        elig = inside && fw > 0.f;
+        if (!elig) {
+          float nw = inside ? 1.f : 0.f;
+          Fnw[i] = nw;
+          if (convft) convft[i] = make_float2(fw * nw, 0.f);
         }
-        out = 0.5f * (o[0] + o[1]);
-      } else {
-        mlp_voxel_features(Fw, P, inv_s, x, y, z, f);
-        out = mlp_forward(sp, f);
       }
-      nw = fminf(1e20f, expf(out) * inv_s);
+      unsigned m = __ballot_sync(0xffffffffu, elig);
+      if (m) {
+        int leader = __ffs(m) - 1, first = 0;
+        if (lane == leader) first = atomicAdd(&S.count, __popc(m));
+        first = __shfl_sync(0xffffffffu, first, leader);
+        if (elig) S.list[first + __popc(m & ((1u << lane) - 1))] = (unsigned short)local;
+      }
+    }
+    __syncthreads();
+    const int n = S.count;
+#pragma unroll 1
+    for (int t0 = 0; t0 < n; t0 += kTileV) {
+      {  // features: thread pairs split the 27 neighbours (+ radius)
+        const int v = t & (kTileV - 1), half = t >> 7;
+        const int k0 = half ? 14 : 0, k1 = half ? 27 : 14;
+        if (t0 + v < n) {
+          int64_t i = base + S.list[t0 + v];
+          int x = (int)(i % rowlen);
+          int64_t r = i / rowlen;
+          int y = (int)(r % P), z = (int)(r / P);
+          for (int k = k0; k < k1; k++) S.xt[k][v] = start_feature(S, Fw, P, inv_s, x, y, z, k);
+          if (half) {
+            int yp = y < P / 2 + 1 ? y : y - P, zp = z < P / 2 + 1 ? z : z - P;
+            float rad = sqrtf((float)(x * x + yp * yp + zp * zp)) / (float)(P / 2);
+            S.xt[27][v] = (rad - S.shift[27]) * S.scale[27];
+          }
+        } else {
+          for (int k = k0; k < k1; k++) S.xt[k][v] = 0.f;
+          if (half) S.xt[27][v] = 0.f;
+        }
+      }
+      __syncthreads();
+      float acc[4][8];
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 8; b++) acc[a][b] = S.b1[j0 + a];
+#pragma unroll 4
+      for (int k = 0; k < kMlpIn; k++) {
+        float4 xa = *reinterpret_cast<const float4*>(&S.xt[k][v0]);
+        float4 xb = *reinterpret_cast<const float4*>(&S.xt[k][v0 + 4]);
+        float4 w = *reinterpret_cast<const float4*>(&S.w1t[k][j0]);
+        float xv[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+        float wv[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int b = 0; b < 8; b++) acc[a][b] = fmaf(wv[a], xv[b], acc[a][b]);
+      }
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        *reinterpret_cast<float4*>(&S.h1t[j0 + a][v0]) =
+            make_float4(fmaxf(acc[a][0], 0.f), fmaxf(acc[a][1], 0.f), fmaxf(acc[a][2], 0.f), fmaxf(acc[a][3], 0.f));
+        *reinterpret_cast<float4*>(&S.h1t[j0 + a][v0 + 4]) =
+            make_float4(fmaxf(acc[a][4], 0.f), fmaxf(acc[a][5], 0.f), fmaxf(acc[a][6], 0.f), fmaxf(acc[a][7], 0.f));
+      }
+      __syncthreads();
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 8; b++) acc[a][b] = S.b2[j0 + a];
+#pragma unroll 4
+      for (int k = 0; k < kMlpHidden; k++) {
+        float4 ha = *reinterpret_cast<const float4*>(&S.h1t[k][v0]);
+        float4 hb = *reinterpret_cast<const float4*>(&S.h1t[k][v0 + 4]);
+        float4 w = *reinterpret_cast<const float4*>(&S.w2t[k][j0]);
+        float hv[8] = {ha.x, ha.y, ha.z, ha.w, hb.x, hb.y, hb.z, hb.w};
+        float wv[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int b = 0; b < 8; b++) acc[a][b] = fmaf(wv[a], hv[b], acc[a][b]);
+      }
+      float o[8];
+#pragma unroll
+      for (int b = 0; b < 8; b++) {
+        o[b] = 0.f;
+#pragma unroll
+        for (int a = 0; a < 4; a++) o[b] = fmaf(S.w3[j0 + a], fmaxf(acc[a][b], 0.f), o[b]);
+#pragma unroll
+        for (int off = 1; off < 16; off <<= 1) o[b] += __shfl_xor_sync(0xffffffffu, o[b], off);
+      }
+      if (tj == 0) {
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+          int e = t0 + v0 + b;
+          if (e < n) {
+            int64_t i = base + S.list[e];
+            float nw = fminf(1e20f, expf(o[b] + b3) * inv_s);
+            Fnw[i] = nw;
+            if (convft) convft[i] = make_float2(Fw[i] * nw, 0.f);
+          }
+        }
+      }
+      __syncthreads();
     }
   }
-  Fnw[i] = nw;
-  if (convft) convft[i] = make_float2(fw * nw, 0.f);
+}
+
+// The two Hermitian mates (0, y, z) and (0, -y, -z) of the x = 0 plane are
+// one Fourier component: both get the geometric mean of their starts, i.e.
+// exp(mean of the two outputs) / s.  One thread per canonical mate.
+__global__ void mlp_start_mates_kernel(const float* __restrict__ Fw, int P, int maskr2,
+                                       float* __restrict__ Fnw, float2* __restrict__ convft) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= P * P) return;
+  int y = idx % P, z = idx / P;
+  int yp = y < P / 2 + 1 ? y : y - P, zp = z < P / 2 + 1 ? z : z - P;
+  if (!(zp > 0 || (zp == 0 && yp > 0))) return;
+  if (yp * yp + zp * zp >= maskr2) return;
+  const int rowlen = P / 2 + 1;
+  int my = y == 0 ? 0 : P - y, mz = z == 0 ? 0 : P - z;
+  int64_t a = ((int64_t)z * P + y) * rowlen, b = ((int64_t)mz * P + my) * rowlen;
+  if (a == b) return;
+  float fa = Fw[a], fb = Fw[b];
+  if (!(fa > 0.f && fb > 0.f)) return;
+  float m = sqrtf(Fnw[a]) * sqrtf(Fnw[b]);
+  Fnw[a] = m;
+  Fnw[b] = m;
+  if (convft) {
+    convft[a] = make_float2(fa * m, 0.f);
+    convft[b] = make_float2(fb * m, 0.f);
+  }
 }
 
 __global__ void mlp_scale_kernel(const float* __restrict__ Fw, int P, int maskr2,
@@ -392,10 +557,20 @@ int launch_train(const float* params, const Src& src, int n, float loss_scale, f
 int mlp_predict_start(const float* d_params, const float* Fw, int P, int maskr2,
                       const double* scale_sums, float* Fnw, float2* convft, cudaStream_t stream) {
   const int64_t nc = (int64_t)(P / 2 + 1) * P * P;
-  unsigned blocks = (unsigned)((nc + kInferThreads - 1) / kInferThreads);
-  mlp_start_kernel<<<blocks, kInferThreads, 0, stream>>>(d_params, Fw, P, maskr2, scale_sums, Fnw,
-                                                         convft);
+  const int smem = (int)sizeof(StartShared);
+  GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(mlp_start_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int dev = 0, sms = 0, per_sm = 0;
+  GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  GTOMRLN_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  GTOMRLN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mlp_start_kernel, kStartThreads, smem));
+  int64_t nchunks = (nc + kChunk - 1) / kChunk;
+  int64_t blocks = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
+  if (blocks > nchunks) blocks = nchunks;
+  mlp_start_kernel<<<(unsigned)blocks, kStartThreads, smem, stream>>>(d_params, Fw, P, maskr2, scale_sums,
+                                                                      Fnw, convft);
   GTOMRLN_LAUNCH_CHECK("mlp_start_kernel");
+  mlp_start_mates_kernel<<<(P * P + 255) / 256, 256, 0, stream>>>(Fw, P, maskr2, Fnw, convft);
+  GTOMRLN_LAUNCH_CHECK("mlp_start_mates_kernel");
   return GTOMRLN_OK;
 }
 

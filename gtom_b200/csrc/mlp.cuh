@@ -142,10 +142,11 @@ __device__ __forceinline__ float mlp_forward(const float* __restrict__ p, const 
 // Host launcher (mlp.cu): writes the predicted gridding start for every
 // voxel of the decentred half grid of P: 0 outside the sphere r^2 < maskr2,
 // 1 where Fw = 0 inside it (the cold value), exp(out) / s elsewhere, with
-// the x = 0 plane made Hermitian-symmetric (the mean of the two mates'
-// outputs).  s is read on the device from scale_sums = {sum of Fw, count}
-// over the sphere's non-zero weights (mlp_weight_scale).  Also writes
-// convft = Fw * start as the first iteration's input spectrum.
+// the x = 0 plane made Hermitian-symmetric (both mates get the geometric
+// mean of their two starts, exp(mean of the outputs) / s).  s is read on
+// the device from scale_sums = {sum of Fw, count} over the sphere's
+// non-zero weights (mlp_weight_scale).  Also writes convft = Fw * start as
+// the first iteration's input spectrum.
 int mlp_predict_start(const float* d_params, const float* Fw, int P, int maskr2,
                       const double* scale_sums, float* Fnw, float2* convft, cudaStream_t stream);
 

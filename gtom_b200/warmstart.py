@@ -379,6 +379,7 @@ def main(argv=None) -> None:
     ap.add_argument("--max-voxels", type=int, default=400000, help="trained voxels kept per distribution")
     ap.add_argument("--seed", type=int, default=1004)
     ap.add_argument("--save", action="store_true", help="store the parameters under gtom_b200/data/")
+    ap.add_argument("--load", action="store_true", help="evaluate the stored parameters (no training)")
     ap.add_argument("--report", default=None)
     a = ap.parse_args(argv)
     rng = np.random.default_rng(a.seed)
@@ -386,6 +387,11 @@ def main(argv=None) -> None:
     train_d, held = dists[:a.train], dists[a.train:]
     rep = {"box": a.box, "pad": a.pad, "train": a.train, "held_out": a.held_out, "seed": a.seed,
            "views_range": list(a.views)}
+    if a.load:
+        params = load_params(a.box)
+        if params is None:
+            raise SystemExit(f"no stored parameters for box {a.box}")
+        return _evaluate_and_report(a, params, held, rep)
     t0 = time.perf_counter()
     ts = make_training_set((sampling_weights(a.box, d, a.pad) for d in train_d), a.box, a.pad,
                            count=len(train_d), max_voxels=a.max_voxels)
@@ -402,6 +408,11 @@ def main(argv=None) -> None:
     torch.cuda.empty_cache()
     if a.save:
         rep["saved"] = str(save_params(params, a.box).name)
+    _evaluate_and_report(a, params, held, rep)
+
+
+def _evaluate_and_report(a, params, held, rep) -> None:
+    import json
     from .synth import blob_volume, padded_half_ft
     volft = padded_half_ft(blob_volume(a.box, 2000 if a.box >= 128 else 200, a.seed, "cuda"), a.pad).reshape(-1)
     rows = evaluate(params, a.box, held[:a.eval], a.pad, volft=volft)
@@ -410,8 +421,8 @@ def main(argv=None) -> None:
     text = json.dumps(rep, indent=1)
     if a.report:
         Path(a.report).write_text(text)
-    print(json.dumps({"summary": rep["summary"], "train_s": rep["train_s"],
-                      "make_training_set_s": rep["make_training_set_s"]}))
+    print(json.dumps({"summary": rep["summary"], "train_s": rep.get("train_s"),
+                      "make_training_set_s": rep.get("make_training_set_s")}))
 
 
 if __name__ == "__main__":
