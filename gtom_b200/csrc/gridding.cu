@@ -25,6 +25,7 @@
 #include <tuple>
 
 #include "common.cuh"
+#include "batch.cuh"
 #include "mlp.cuh"
 
 namespace gtomrln {
@@ -47,7 +48,12 @@ struct GridGeom {
 __global__ void grid_init_kernel(const float* __restrict__ weight, int oldx, int oldy, int oldz,
                                  float* __restrict__ Fw, float* __restrict__ Fnw,
                                  float2* __restrict__ convft, GridGeom g, int maskr2,
-                                 int write_conv) {
+                                 int write_conv, int64_t wstride) {
+  const int64_t b = blockIdx.y;  // volume of a batch (stacks of equal volumes)
+  weight += b * wstride;
+  Fw += b * g.nc;
+  Fnw += b * g.nc;
+  convft += b * g.nc;
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.nc) return;
   int x = (int)(i % g.rowlen);
@@ -76,6 +82,7 @@ __global__ void grid_init_kernel(const float* __restrict__ weight, int oldx, int
 // lookup (RecFourier.cu:243-262), the radius evaluated as the reference does.
 __global__ void grid_blob_kernel(float* __restrict__ conv, const float* __restrict__ table,
                                  GridGeom g, float inv_n, float funcsampling) {
+  conv += (int64_t)blockIdx.y * g.nr;
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.nr) return;
   int x = (int)(i % g.P);
@@ -100,6 +107,10 @@ __global__ void grid_blob_kernel(float* __restrict__ conv, const float* __restri
 __global__ void grid_update_kernel(float2* __restrict__ convft, const float* __restrict__ Fw,
                                    float* __restrict__ Fnw, GridGeom g, int write_conv,
                                    double* __restrict__ change) {
+  const int64_t b = blockIdx.y;  // change is only requested for a single volume
+  convft += b * g.nc;
+  Fw += b * g.nc;
+  Fnw += b * g.nc;
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double d2 = 0, o2 = 0;
   if (i < g.nc) {
@@ -154,6 +165,11 @@ __global__ void grid_update_kernel(float2* __restrict__ convft, const float* __r
 __global__ void grid_update_momentum_kernel(float2* __restrict__ convft, const float* __restrict__ Fw,
                                             float* __restrict__ Fnw, float* __restrict__ V, GridGeom g,
                                             float beta, int write_conv, double* __restrict__ change) {
+  const int64_t b = blockIdx.y;
+  convft += b * g.nc;
+  Fw += b * g.nc;
+  Fnw += b * g.nc;
+  V += b * g.nc;
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double d2 = 0, o2 = 0;
   if (i < g.nc) {
@@ -205,7 +221,13 @@ __global__ void grid_update_momentum_kernel(float2* __restrict__ convft, const f
 // (RecFourier.cu:213-214), which is the factor (-1)^(x+y+z).
 __global__ void grid_final_kernel(const float2* __restrict__ data, int oldx, int oldy, int oldz,
                                   const float* __restrict__ Fw, const float* __restrict__ Fnw,
-                                  float2* __restrict__ convft, GridGeom g, int divide) {
+                                  float2* __restrict__ convft, GridGeom g, int divide,
+                                  int64_t wstride) {
+  const int64_t b = blockIdx.y;
+  data += b * wstride;
+  Fw += b * g.nc;
+  Fnw += b * g.nc;
+  convft += b * g.nc;
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.nc) return;
   int x = (int)(i % g.rowlen);
@@ -244,7 +266,9 @@ __global__ void grid_final_kernel(const float2* __restrict__ data, int oldx, int
 // CorrectGriddingKernel (RecFourier.cu:310-332) and the final scale
 // (RecFourier.cu:237).
 __global__ void grid_crop_kernel(const float* __restrict__ conv, float* __restrict__ out, int P,
-                                 int ori, int off, float scale) {
+                                 int ori, int off, float scale, float* const* __restrict__ outs) {
+  conv += (int64_t)blockIdx.y * P * P * P;
+  if (outs) out = outs[blockIdx.y];
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int64_t total = (int64_t)ori * ori * ori;
   if (i >= total) return;
@@ -436,7 +460,7 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   GTOMRLN_CUFFT_TRY(cufftSetStream(plans.c2r, stream));
 
   grid_init_kernel<<<bc, T, 0, stream>>>(d_weight, oldx, oldy, oldz, Fw, Fnw, convft, g, maskr2,
-                                         iterations > 0 && !warm);
+                                         iterations > 0 && !warm, 0);
   GTOMRLN_STEP(launch_check("grid_init_kernel"));
   if (warm) {
     GTOMRLN_CUDA_TRY(cudaMemsetAsync(sums, 0, 2 * sizeof(double), stream));
@@ -470,7 +494,7 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
         if (!(last_change <= (double)opt.residual_limit)) {
           // Rejected predicted start: the cold start (sphere mask) from scratch.
           grid_init_kernel<<<bc, T, 0, stream>>>(d_weight, oldx, oldy, oldz, Fw, Fnw, convft, g,
-                                                 maskr2, 1);
+                                                 maskr2, 1, 0);
           GTOMRLN_STEP(launch_check("grid_init_kernel"));
           if (momentum)
             GTOMRLN_CUDA_TRY(cudaMemcpyAsync(V, Fnw, g.nc * sizeof(float), cudaMemcpyDeviceToDevice, stream));
@@ -491,12 +515,12 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
     GTOMRLN_CUDA_TRY(cudaMemcpyAsync(opt.out_fnw, Fnw, g.nc * sizeof(float), cudaMemcpyDeviceToDevice, stream));
   if (!opt.weights_only) {
     grid_final_kernel<<<bc, T, 0, stream>>>((const float2*)d_dataft, oldx, oldy, oldz, Fw, Fnw,
-                                            convft, g, iterations == 0);
+                                            convft, g, iterations == 0, 0);
     GTOMRLN_STEP(launch_check("grid_final_kernel"));
     GTOMRLN_CUFFT_TRY(cufftExecC2R(plans.c2r, (cufftComplex*)convft, conv));
     int64_t total = (int64_t)ori * ori * ori;
     grid_crop_kernel<<<(unsigned)((total + T - 1) / T), T, 0, stream>>>(
-        conv, d_out, P, ori, P / 2 - ori / 2, 1.0f / (float)(pad * pad * pad * ori));
+        conv, d_out, P, ori, P / 2 - ori / 2, 1.0f / (float)(pad * pad * pad * ori), nullptr);
     GTOMRLN_STEP(launch_check("grid_crop_kernel"));
   }
   if (res) {
@@ -512,6 +536,94 @@ done:
   pool_free(V, stream);
   pool_free(change, stream);
   pool_free(sums, stream);
+  return st;
+}
+
+// ----------------------------------------------------------- batches --
+int gridding_batch_prepare(GridBatch* gb, int count, int ori, int pad, double blobradius,
+                           int bloborder, double blobalpha) {
+  if (count <= 0 || ori <= 0 || pad <= 0 || (ori * pad) % 2)
+    return set_error(GTOMRLN_ERR_INVALID, "gridding batch: bad sizes");
+  GridBatch b;
+  b.count = count;
+  b.ori = ori;
+  b.pad = pad;
+  b.P = ori * pad;
+  b.D = b.P + 1;
+  b.wstride = (int64_t)(b.D / 2 + 1) * b.D * b.D;
+  const int64_t nc = (int64_t)(b.P / 2 + 1) * b.P * b.P, nr = (int64_t)b.P * b.P * b.P;
+  int st = get_table(blobradius * pad, blobalpha, bloborder, &b.table);
+  if (st) return st;
+  *gb = b;  // so that gridding_batch_free releases what was made on failure
+  GTOMRLN_CUDA_TRY(cudaMalloc(&gb->convft, count * nc * sizeof(float2)));
+  GTOMRLN_CUDA_TRY(cudaMalloc(&gb->conv, count * nr * sizeof(float)));
+  GTOMRLN_CUDA_TRY(cudaMalloc(&gb->Fw, count * nc * sizeof(float)));
+  GTOMRLN_CUDA_TRY(cudaMalloc(&gb->Fnw, count * nc * sizeof(float)));
+  int n[3] = {b.P, b.P, b.P};
+  cufftResult r = cufftPlanMany(&gb->r2c, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, count);
+  if (r != CUFFT_SUCCESS) {
+    gb->r2c = 0;
+    return set_error(GTOMRLN_ERR_CUFFT, "cufftPlanMany R2C %d^3 x %d failed (%d)", b.P, count, (int)r);
+  }
+  r = cufftPlanMany(&gb->c2r, 3, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, count);
+  if (r != CUFFT_SUCCESS) {
+    gb->c2r = 0;
+    return set_error(GTOMRLN_ERR_CUFFT, "cufftPlanMany C2R %d^3 x %d failed (%d)", b.P, count, (int)r);
+  }
+  return GTOMRLN_OK;
+}
+
+void gridding_batch_free(GridBatch* gb) {
+  cudaFree(gb->convft);
+  cudaFree(gb->conv);
+  cudaFree(gb->Fw);
+  cudaFree(gb->Fnw);
+  if (gb->r2c) cufftDestroy(gb->r2c);
+  if (gb->c2r) cufftDestroy(gb->c2r);
+  *gb = GridBatch();
+}
+
+// The steps of reconstruct() with a fixed iteration count, each launched once
+// over the stack (blockIdx.y = volume) and the transforms as batched plans;
+// nothing synchronises the host, so the whole sequence can be captured.
+int gridding_batch_run(const GridBatch& b, const float2* data, const float* weight,
+                       float* const* outs, int iterations, cudaStream_t stream) {
+  GridGeom g;
+  g.P = b.P;
+  g.rowlen = b.P / 2 + 1;
+  g.nc = (int64_t)g.rowlen * b.P * b.P;
+  g.nr = (int64_t)b.P * b.P * b.P;
+  const int r_max = b.ori / 2;
+  const int maskr2 = (r_max * b.pad) * (r_max * b.pad);
+  const int T = 256;
+  dim3 gc((unsigned)((g.nc + T - 1) / T), (unsigned)b.count);
+  dim3 gr((unsigned)((g.nr + T - 1) / T), (unsigned)b.count);
+  int st = GTOMRLN_OK;
+  GTOMRLN_CUFFT_TRY(cufftSetStream(b.r2c, stream));
+  GTOMRLN_CUFFT_TRY(cufftSetStream(b.c2r, stream));
+  grid_init_kernel<<<gc, T, 0, stream>>>(weight, b.D, b.D, b.D, b.Fw, b.Fnw, b.convft, g, maskr2,
+                                         iterations > 0, b.wstride);
+  GTOMRLN_STEP(launch_check("grid_init_kernel"));
+  for (int it = 0; it < iterations; it++) {
+    GTOMRLN_CUFFT_TRY(cufftExecC2R(b.c2r, (cufftComplex*)b.convft, b.conv));
+    grid_blob_kernel<<<gr, T, 0, stream>>>(b.conv, b.table, g, 1.0f / (float)g.nr, (float)(0.5 / kBlobSamples));
+    GTOMRLN_STEP(launch_check("grid_blob_kernel"));
+    GTOMRLN_CUFFT_TRY(cufftExecR2C(b.r2c, b.conv, (cufftComplex*)b.convft));
+    grid_update_kernel<<<gc, T, 0, stream>>>(b.convft, b.Fw, b.Fnw, g, it + 1 < iterations, nullptr);
+    GTOMRLN_STEP(launch_check("grid_update_kernel"));
+  }
+  grid_final_kernel<<<gc, T, 0, stream>>>(data, b.D, b.D, b.D, b.Fw, b.Fnw, b.convft, g, iterations == 0,
+                                          b.wstride);
+  GTOMRLN_STEP(launch_check("grid_final_kernel"));
+  GTOMRLN_CUFFT_TRY(cufftExecC2R(b.c2r, (cufftComplex*)b.convft, b.conv));
+  {
+    int64_t total = (int64_t)b.ori * b.ori * b.ori;
+    dim3 go((unsigned)((total + T - 1) / T), (unsigned)b.count);
+    grid_crop_kernel<<<go, T, 0, stream>>>(b.conv, nullptr, b.P, b.ori, b.P / 2 - b.ori / 2,
+                                           1.0f / (float)(b.pad * b.pad * b.pad * b.ori), outs);
+    GTOMRLN_STEP(launch_check("grid_crop_kernel"));
+  }
+done:
   return st;
 }
 

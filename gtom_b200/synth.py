@@ -127,3 +127,70 @@ def in_disk_mask(n: int, rmax: int, device) -> torch.Tensor:
     y = torch.arange(n, device=device)
     y = torch.where(y <= n // 2, y, y - n)
     return (x[None, :] ** 2 + y[:, None] ** 2) <= rmax * rmax
+
+
+def tilt_matrices(euler: np.ndarray, tilts_deg: np.ndarray, supersample: float) -> np.ndarray:
+    """(ntilts, 9) float32 matrices (the library's layout, glm column-major)
+    of a tilt series: the subvolume's rotation E (ZYZ Euler, radians), then a
+    rotation by each tilt angle about y; M = s (T E)^T."""
+    from .relion import matrices_from_angles
+    Es_t = matrices_from_angles(np.asarray(euler, np.float32)[None], 1.0)[0].reshape(3, 3).T  # E^T
+    out = np.empty((len(tilts_deg), 9), np.float32)
+    for k, t in enumerate(np.deg2rad(np.asarray(tilts_deg, np.float64))):
+        c, s = math.cos(t), math.sin(t)
+        T = np.array([[c, 0, -s], [0, 1, 0], [s, 0, c]])
+        M = supersample * (Es_t.astype(np.float64) @ T.T)
+        out[k] = M.T.ravel()
+    return out
+
+
+def tilt_series_batch(count: int, seed: int, device, boxes=(32, 48, 64, 96, 128), pad: int = 2,
+                      tilt_range: float = 60.0, tilt_step: float = 3.0, max_dose: float = 120.0,
+                      snr: float = 0.1, pixel_a: float = 1.0):
+    """Synthetic sub-tomogram batch: per subvolume a box from `boxes`
+    (uniform), a volume of Gaussian blobs, a random rotation and a tilt
+    series over +-tilt_range in tilt_step steps (41 tilts by default); per
+    tilt a CTF (300 kV, Cs 2.7 mm, defocus U(2, 5) um) and the dose filter
+    exp(-N k^2 / 4), N the dose accumulated in dose-symmetric order up to
+    max_dose e/A^2, and white noise at `snr`.  Returns a list of dicts with
+    box, projft (CTF- and dose-weighted noisy slices), projweights (their
+    squared weights), matrices and an output map buffer."""
+    from .relion import d_rlnProject
+    rng = np.random.default_rng(seed)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    tilts = np.arange(-tilt_range, tilt_range + 1e-6, tilt_step)
+    nt = len(tilts)
+    order = np.argsort(np.abs(tilts), kind="stable")  # dose-symmetric acquisition
+    dose = np.empty(nt)
+    dose[order] = (np.arange(nt) + 1) * max_dose / nt
+    out = []
+    for i in range(count):
+        n = int(rng.choice(boxes))
+        P = n * pad
+        e = (n // 2 + 1) * n
+        vol = blob_volume(n, max(20, n // 2), int(rng.integers(1 << 31)), device)
+        volft = padded_half_ft(vol, pad).reshape(-1)
+        euler = _euler_from_view(rng.normal(size=(1, 3)), rng.uniform(-np.pi, np.pi, 1))[0]
+        mats = torch.from_numpy(tilt_matrices(euler, tilts, float(pad))).to(device)
+        proj = torch.empty(nt * e, dtype=torch.complex64, device=device)
+        d_rlnProject(volft, (P, P, P), proj, (n, n, 1), n // 2, mats.reshape(-1), nt)
+        df = torch.from_numpy(rng.uniform(2.0, 5.0, nt).astype(np.float32)).to(device)
+        zero = torch.zeros(nt, dtype=torch.float32, device=device)
+        ctf = ctf_half(n, df, zero, zero, pixel_a=pixel_a).reshape(nt, e)
+        x = torch.arange(n // 2 + 1, device=device, dtype=torch.float32)
+        y = torch.arange(n, device=device, dtype=torch.float32)
+        y = torch.where(y <= n // 2, y, y - n)
+        k2 = ((x[None, :] ** 2 + y[:, None] ** 2) / (n * pixel_a) ** 2).reshape(-1)
+        filt = ctf * torch.exp(-torch.from_numpy(dose.astype(np.float32)).to(device)[:, None] * k2[None] / 4)
+        sig = proj.reshape(nt, e) * filt
+        disk = in_disk_mask(n, n // 2, device).reshape(-1)
+        pw = (sig.abs() ** 2 * disk).sum(1, keepdim=True) / disk.sum()
+        sd = torch.sqrt(pw / snr / 2)
+        noise = torch.complex(torch.randn((nt, e), device=device, generator=gen),
+                              torch.randn((nt, e), device=device, generator=gen)) * sd
+        out.append(dict(box=n, projft=((sig + noise) * filt).contiguous().reshape(-1),
+                        projweights=(filt * filt).contiguous().reshape(-1), matrices=mats.reshape(-1),
+                        out=torch.empty(n ** 3, dtype=torch.float32, device=device)))
+        del vol, volft, proj
+    return out

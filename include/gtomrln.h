@@ -306,6 +306,49 @@ GTOMRLN_API int gtomrln_mlp_train_batch(const float* d_params, const float* d_fw
 GTOMRLN_API int gtomrln_mlp_adam(float* d_params, float* d_grad, float* d_m, float* d_v, int step,
                      float lr, float beta1, float beta2, float eps, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Batched reconstruction of many volumes of uneven box size (no reference
+ * counterpart; the reference batches equal boxes only, through d_ivolume of
+ * d_rlnBackproject, src/Relion/Backproject.cu:48-124).  Per subvolume the
+ * result equals gtomrln_backproject (matrix overload, rmax = box / 2,
+ * identity magnification, flat Ewald sphere, centred accumulators of
+ * dims P + 1, P = box * paddingfactor, zeroed first) followed by
+ * gtomrln_reconstruct_gridding (ori = box, dimspadded = P + 1, the given
+ * iteration count, blob radius 1.9, order 0, alpha 15): up to the order of
+ * the floating-point additions of the insertion.
+ * ------------------------------------------------------------------------- */
+typedef struct gtomrln_subvolume {
+  int box;                     /* even, >= 4 */
+  int nslices;                 /* 2D slices of box x box, half-complex */
+  const float* d_projft;       /* nslices x (box/2+1) x box complex64, or NULL (value 1) */
+  const float* d_projweights;  /* nslices x (box/2+1) x box float, or NULL (weight 1) */
+  const float* d_matrices;     /* nslices x 9 floats, as gtomrln_backproject's */
+  float* d_out;                /* box^3 floats: the reconstructed map */
+} gtomrln_subvolume_t;
+
+/* Plans a batch: groups the subvolumes by box size, allocates the
+ * accumulators and the gridding buffers of every size class (device memory
+ * held until gtomrln_batch_destroy) and makes the batched FFT plans.  The
+ * device pointers in items must stay valid for the handle's life; their
+ * contents are read at each run. */
+GTOMRLN_API int gtomrln_batch_create(const gtomrln_subvolume_t* items, int count, int paddingfactor,
+                         int iterations, void** handle);
+
+/* Launch shape of the persistent insertion kernel: threads per CTA
+ * (multiple of 32, <= 1024), slices per work item, CTAs per SM; 0 keeps a
+ * field.  Discards a captured graph. */
+GTOMRLN_API int gtomrln_batch_set_tuning(void* handle, int threads, int slices_per_item,
+                             int blocks_per_sm);
+
+/* Runs the batch on stream: zeroes the accumulators, inserts every slice of
+ * every subvolume in one persistent launch, then grids each size class.
+ * use_graph != 0: the first call captures the sequence into a CUDA graph
+ * (on a stream of the handle's own) and every call launches that graph on
+ * `stream`; use_graph = 0 enqueues the steps directly.  Asynchronous. */
+GTOMRLN_API int gtomrln_batch_run(void* handle, int use_graph, void* stream);
+
+GTOMRLN_API int gtomrln_batch_destroy(void* handle);
+
 /* The normalised Kaiser-Bessel table the gridding uses: nsamples values of
  * kaiser_Fourier_value(i * 0.5 / nsamples, radius, alpha, order) divided by
  * the value at 0 (src/Helpers/KaiserBessel.cpp:357-376,
