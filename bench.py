@@ -59,6 +59,8 @@ def parse_args():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip gridding, e2e, CPU baseline and L2 probes (profiling runs)")
     ap.add_argument("--cpu-sample", type=int, default=256, help="slices timed on the host cores")
+    ap.add_argument("--subtomos", type=int, default=512,
+                    help="sub-tomograms of the batched uneven-box workload (0 skips it)")
     return ap.parse_args()
 
 
@@ -305,6 +307,8 @@ def run_ours(args):
 
     if not (args.no_gridding or args.no_extras) and rank == 0:
         out["gridding"] = time_gridding(G, torch, acc_ft, acc_w, n, D, dev)
+    if rank == 0 and not args.no_extras and args.subtomos > 0:
+        out["batched_uneven"] = time_batched(args, torch, dev)
     if rank == 0 and not args.no_extras:
         out["e2e"] = run_e2e(args, G, torch, ws, dev)
         out["cpu_baseline"] = cpu_baseline(args, ws)
@@ -355,6 +359,86 @@ def time_gridding(G, torch, acc_ft, acc_w, n, D, dev):
         volft = synth_volft(128, dev)
         res["warm_start_128"] = WS.summarise(WS.evaluate(p128, 128, dists, PAD, volft=volft))
     return res
+
+
+def time_batched(args, torch, dev):
+    """The batched uneven-box workload: sub-tomograms of box 32-128 with 41
+    tilts each (synth.tilt_series_batch), reconstructed (insertion + 10
+    gridding iterations) as one graph-captured batch after the autotuner has
+    chosen the insertion launch shape, against one d_rlnBackproject +
+    d_ReconstructGridding pair per sub-tomogram through this library and,
+    on a sample, through the reference's CUDA code."""
+    from gtom_b200 import synth
+    from gtom_b200.batch import BatchReconstructor, Subvolume, autotune, reconstruct_separately
+    t0 = time.perf_counter()
+    raw = synth.tilt_series_batch(args.subtomos, 1003, dev)
+    subs = [Subvolume(r["box"], r["projft"], r["projweights"], r["matrices"], r["out"]) for r in raw]
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    ref = [Subvolume(x.box, x.projft, x.projweights, x.matrices, torch.empty_like(x.out)) for x in subs]
+    scratch = {}
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.median(ts)
+
+    sep_ms = timed(lambda: reconstruct_separately(ref, PAD, 10, scratch))
+    rec = BatchReconstructor(subs, PAD, 10)
+    tune = autotune(rec, threads=(128, 256, 512), slices=(1, 4), blocks=(4, 8), reps=2)
+    graph_ms = timed(lambda: rec.run(use_graph=True), reps=5)
+    direct_ms = timed(lambda: rec.run(use_graph=False), reps=3)
+    worst = max(float(torch.linalg.norm(a.out - b.out) / torch.linalg.norm(b.out)) for a, b in zip(subs, ref))
+    res = {"subtomograms": len(subs), "boxes": sorted({x.box for x in subs}), "tilts": 41,
+           "slices": int(sum(x.nslices for x in subs)), "generate_s": round(gen_s, 1),
+           "separate_calls_ms": round(sep_ms, 2), "batched_graph_ms": round(graph_ms, 2),
+           "batched_no_graph_ms": round(direct_ms, 2), "speedup_vs_separate": round(sep_ms / graph_ms, 2),
+           "autotune_best": {"threads": tune["best"][0], "slices_per_item": tune["best"][1],
+                             "ctas_per_sm": tune["best"][2], "ms": round(tune["ms"], 2)},
+           "max_rel_l2_vs_separate": worst}
+    res["reference_separate"] = reference_separate(subs[:64], dev, len(subs))
+    rec.close()
+    return res
+
+
+def reference_separate(subs, dev, total):
+    """The reference's d_rlnBackproject + d_ReconstructGridding (rebuilt from
+    its sources into oracle/_ref/, each call synchronising as the reference
+    does) per sub-tomogram on a sample, scaled to the whole batch."""
+    import ctypes as C
+    import torch
+    from oracle import oracle as O
+    if not O.REF_PATH.exists():
+        return None
+    ref = C.CDLL(str(O.REF_PATH))
+    p, i, f, d = C.c_void_p, C.c_int, C.c_float, C.c_double
+    ref.ref_backproject.argtypes = [p, p, i, p, p, i, i, i, p, p, f, f, f, f, f, i, i, i]
+    ref.ref_reconstruct_gridding.argtypes = [p, p, p, i, i, i, i, d, i, d]
+    out = torch.empty(128 ** 3, dtype=torch.float32, device=dev)
+    t0 = time.perf_counter()
+    for s in subs:
+        D = s.box * PAD + 1
+        nvol = (D // 2 + 1) * D * D
+        acc_ft = torch.zeros(nvol + 64, dtype=torch.complex64, device=dev)
+        acc_w = torch.zeros(nvol + 64, dtype=torch.float32, device=dev)
+        rc = ref.ref_backproject(acc_ft.data_ptr(), acc_w.data_ptr(), D, s.projft.data_ptr(),
+                                 s.projweights.data_ptr(), s.box, 2, s.box // 2, s.matrices.data_ptr(), None,
+                                 1, 0, 0, 1, 0.0, 0, 0, s.nslices)
+        rc = rc or ref.ref_reconstruct_gridding(acc_ft.data_ptr(), acc_w.data_ptr(), out.data_ptr(), s.box, D,
+                                                PAD, 10, 1.9, 0, 15.0)
+        if rc:
+            return {"error": f"reference CUDA returned {rc}"}
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3
+    return {"sample": len(subs), "sample_ms": round(ms, 1), "ms_scaled_to_batch": round(ms * total / len(subs), 1)}
 
 
 def synth_volft(box, dev):
