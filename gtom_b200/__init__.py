@@ -6,7 +6,9 @@ from ._lib import GtomError, GtomLibraryMissing  # noqa: F401
 from .relion import (  # noqa: F401
     d_ReconstructGridding,
     d_rlnBackproject,
+    d_rlnBackprojectShifted,
     d_rlnProject,
+    d_rlnProjectShifted,
     elements_fft,
     gridding_weights,
     kaiser_bessel_table,

@@ -351,6 +351,85 @@ static int backproject_brick(float* d_volumeft, float* d_volumeweights, const fl
   return GTOMRLN_OK;
 }
 
+// d_rlnBackprojectShifted (BackprojectShifted.cu:67-186): a different
+// insertion from Backproject3DtoNDKernel in the reference itself, kept as it
+// is: r^2 <= rmax^2 (y, z signed by comparing with rmax), the whole x = 0
+// column inserted, Friedel flip of the position only (no mirrored
+// neighbours, no second insertion on x = 0), plain FP32 trilinear weights,
+// centred output, the sample times exp(i phi), phi = -(x sx + y sy [+ z sz])
+// with the slice's 2 pi / n-scaled shift, and the value and weight times the
+// slice's global weight.  The reference writes without bounds checks; the
+// indices here are clamped like place<false> (unsigned compares).
+template <int NDIMS>
+__global__ void __launch_bounds__(kBpThreads)
+backproject_shifted_kernel(float2* __restrict__ volft, float* __restrict__ volw,
+                           const float2* __restrict__ projft, const float* __restrict__ projw,
+                           const float* __restrict__ mats, const float* __restrict__ shifts,
+                           const float* __restrict__ gweights, BpArgs a, int rmax) {
+  const int slice = blockIdx.x / a.tiles;
+  const int tile = blockIdx.x - slice * a.tiles;
+  float m[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) m[i] = __ldg(mats + 9 * (int64_t)slice + i);
+  const float sx = __ldg(shifts + 3 * (int64_t)slice), sy = __ldg(shifts + 3 * (int64_t)slice + 1);
+  const float sz = __ldg(shifts + 3 * (int64_t)slice + 2);
+  const float gw = __ldg(gweights + slice);
+  const int V = a.P;
+  for (int k = 0; k < kBpPerThread; k++) {
+    int64_t id = (int64_t)tile * kBpTile + k * kBpThreads + threadIdx.x;
+    if (id >= a.elements) break;
+    int idx = (int)(id % a.dimft);
+    int idy = (int)((NDIMS == 3 ? id % a.area : id) / a.dimft);
+    int idz = NDIMS == 3 ? (int)(id / a.area) : 0;
+    int x = idx;
+    int y = idy <= rmax ? idy : idy - a.n;
+    int z = NDIMS == 3 ? (idz <= rmax ? idz : idz - a.n) : 0;
+    int r2 = NDIMS == 3 ? z * z + y * y + x * x : y * y + x * x;
+    if (r2 > a.rmax2) continue;
+    float3 pos = mat_apply(m, (float)x, (float)y, (float)z);
+    float sign = 1.f;
+    if (pos.x + 1e-5f < 0.f) {
+      pos.x = fabsf(pos.x);
+      pos.y = -pos.y;
+      pos.z = -pos.z;
+      sign = -1.f;
+    }
+    int x0 = (int)floorf(pos.x + 1e-5f);
+    float fx = pos.x - (float)x0;
+    int y0 = (int)floorf(pos.y);
+    float fy = pos.y - (float)y0;
+    int z0 = (int)floorf(pos.z);
+    float fz = pos.z - (float)z0;
+    y0 += V / 2;
+    z0 += V / 2;
+    float c0 = 1.f - fz, c1 = fz;
+    float c00 = (1.f - fy) * c0, c10 = fy * c0, c01 = (1.f - fy) * c1, c11 = fy * c1;
+    float w[8] = {(1.f - fx) * c00, fx * c00, (1.f - fx) * c10, fx * c10,
+                  (1.f - fx) * c01, fx * c01, (1.f - fx) * c11, fx * c11};
+    float2 v = projft ? __ldg(projft + a.elements * slice + id) : make_float2(1.f, 0.f);
+    float phase = fmaf((float)x, sx, (float)y * sy);
+    if (NDIMS == 3) phase = fmaf((float)z, sz, phase);
+    phase = -phase;
+    float c = __cosf(phase), s = __sinf(phase);
+    float re = fmaf(v.x, c, -(v.y * s)), im = fmaf(v.x, s, v.y * c);
+    im *= sign;
+    re *= gw;
+    im *= gw;
+    float pw = (projw ? __ldg(projw + a.elements * slice + id) : 1.f) * gw;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      unsigned tx = (unsigned)(x0 + (i & 1)), ty = (unsigned)(y0 + ((i >> 1) & 1));
+      unsigned tz = (unsigned)(z0 + ((i >> 2) & 1));
+      tx = tx > (unsigned)(V / 2) ? (unsigned)(V / 2) : tx;
+      ty = ty > (unsigned)(V - 1) ? (unsigned)(V - 1) : ty;
+      tz = tz > (unsigned)(V - 1) ? (unsigned)(V - 1) : tz;
+      int64_t o = ((int64_t)tz * V + ty) * a.rowlen + tx;
+      if (volft) red_add2((float*)(volft + o), w[i] * re, w[i] * im);
+      if (volw) red_add(volw + o, w[i] * pw);
+    }
+  }
+}
+
 static int backproject_launch(float* d_volumeft, float* d_volumeweights, int vx, int vy, int vz,
                               const float* d_projft, const float* d_projweights, int px, int py,
                               int pz, unsigned rmax, const float* d_matrices, const int* d_ivolume,
@@ -444,6 +523,67 @@ int gtomrln_backproject_angles(float* d_volumeft, float* d_volumeweights, int vx
     int st2 = pool_free(d_iv, s);
     return st ? st : st2;
   });
+}
+
+// ---------------------------------------------------------------- shifted --
+int gtomrln_backproject_shifted(float* d_volumeft, float* d_volumeweights, int vx, int vy, int vz,
+                                const float* d_projft, const float* d_projweights, int px, int py,
+                                int pz, unsigned rmax, const float* d_matrices,
+                                const float* d_shifts, const float* d_globalweights,
+                                unsigned batch, void* stream) {
+  clear_error();
+  int ndv = dimension_count(vx, vy, vz), ndp = dimension_count(px, py, pz);
+  if (ndv < ndp || ndv != 3)
+    return set_error(GTOMRLN_ERR_INVALID,
+                     "backproject_shifted: volume must be 3D and have at least the projections' "
+                     "dimensions (reference throws)");
+  if (ndp != 2 && ndp != 3)
+    return set_error(GTOMRLN_ERR_INVALID, "backproject_shifted: projections must be 2D or 3D");
+  if (vx <= 0 || px <= 0) return set_error(GTOMRLN_ERR_INVALID, "backproject_shifted: non-positive dimension");
+  if (batch == 0) return GTOMRLN_OK;
+  if (!d_matrices || !d_shifts || !d_globalweights)
+    return set_error(GTOMRLN_ERR_INVALID, "backproject_shifted: NULL matrices, shifts or weights");
+  if (rmax > (unsigned)(px / 2)) rmax = px / 2;
+  BpArgs a;
+  a.n = px;
+  a.dimft = px / 2 + 1;
+  a.area = (int64_t)a.dimft * px;
+  a.elements = ndp == 3 ? a.area * px : a.area;
+  a.tiles = (int)((a.elements + kBpTile - 1) / kBpTile);
+  a.rmax2 = (int)(rmax * rmax);
+  a.P = vx;
+  a.rowlen = vx / 2 + 1;
+  a.nvox = (int64_t)a.rowlen * vx * vx;
+  a.mag = make_float4(1.f, 0.f, 0.f, 1.f);
+  a.ewalddiaminv = 0.f;
+  if ((int64_t)a.tiles * batch > 0x7fffffffLL)
+    return set_error(GTOMRLN_ERR_INVALID, "backproject_shifted: batch too large for one launch");
+  dim3 grid((unsigned)(a.tiles * (int64_t)batch));
+  if (ndp == 2)
+    backproject_shifted_kernel<2><<<grid, kBpThreads, 0, (cudaStream_t)stream>>>(
+        (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_matrices, d_shifts,
+        d_globalweights, a, (int)rmax);
+  else
+    backproject_shifted_kernel<3><<<grid, kBpThreads, 0, (cudaStream_t)stream>>>(
+        (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_matrices, d_shifts,
+        d_globalweights, a, (int)rmax);
+  GTOMRLN_LAUNCH_CHECK("backproject_shifted_kernel");
+  return GTOMRLN_OK;
+}
+
+int gtomrln_backproject_shifted_angles(float* d_volumeft, float* d_volumeweights, int vx, int vy,
+                                       int vz, const float* d_projft, const float* d_projweights,
+                                       int px, int py, int pz, unsigned rmax, const float* h_angles,
+                                       const float* h_shifts, const float* h_globalweights,
+                                       float supersample, unsigned batch, void* stream) {
+  clear_error();
+  return with_device_shifted(h_angles, h_shifts, h_globalweights, supersample, px, batch,
+                             (cudaStream_t)stream,
+                             [&](const float* d_m, const float* d_s, const float* d_w) {
+                               return gtomrln_backproject_shifted(d_volumeft, d_volumeweights, vx, vy, vz,
+                                                                  d_projft, d_projweights, px, py, pz, rmax,
+                                                                  d_m, d_s, d_w, batch, stream);
+                             });
 }
 
 }  // extern "C"

@@ -128,4 +128,35 @@ inline int with_device_matrices(const float* h_angles, float supersample, unsign
   return st;
 }
 
+// The h_angles overloads of the shifted projector / backprojector
+// (ProjectShifted.cu:32-56, BackprojectShifted.cu:11-35): matrices as above,
+// shifts scaled to radians per pixel, shift * 2 pi / n in float, and the
+// global weights, uploaded together; fn(d_matrices, d_shifts, d_weights).
+template <class Fn>
+inline int with_device_shifted(const float* h_angles, const float* h_shifts, const float* h_weights,
+                               float supersample, int n, unsigned batch, cudaStream_t stream, Fn fn) {
+  if (batch == 0) return fn((const float*)nullptr, (const float*)nullptr, (const float*)nullptr);
+  if (!h_angles || !h_shifts || !h_weights)
+    return set_error(GTOMRLN_ERR_INVALID, "h_angles, h_shifts or h_globalweights is NULL");
+  std::vector<float> h(13 * (size_t)batch);
+  matrices_from_angles(h_angles, supersample, batch, h.data());
+  float* sh = h.data() + 9 * (size_t)batch;
+  const float two_pi = 6.28318530717958647692f;
+  for (unsigned i = 0; i < 3 * batch; i++) sh[i] = h_shifts[i] * two_pi / (float)n;
+  for (unsigned i = 0; i < batch; i++) sh[3 * batch + i] = h_weights[i];
+  void* d = nullptr;
+  int st = pool_alloc(&d, h.size() * sizeof(float), stream);
+  if (st) return st;
+  cudaError_t e = cudaMemcpyAsync(d, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) {
+    pool_free(d, stream);
+    return set_error(GTOMRLN_ERR_CUDA, "upload of matrices and shifts failed: %s", cudaGetErrorString(e));
+  }
+  const float* dm = (const float*)d;
+  st = fn(dm, dm + 9 * (size_t)batch, dm + 12 * (size_t)batch);
+  int st2 = pool_free(d, stream);
+  if (!st) st = st2;
+  return st;
+}
+
 }  // namespace gtomrln

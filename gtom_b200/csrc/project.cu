@@ -56,10 +56,36 @@ struct TexFetch {
   }
 };
 
-template <int NDIMS, class Fetch>
+// Value of an in-disk sample as stored: unchanged for d_rlnProject.
+struct NoPost {
+  template <int NDIMS>
+  __device__ __forceinline__ float2 apply(int, int, int, int, float2 v) const { return v; }
+};
+
+// d_rlnProjectShifted (ProjectShifted.cu:214-220): the sample times
+// exp(i phi), phi = -(x sx + y sy [+ z sz]) with the 2 pi / n-scaled shift of
+// the slice, then times its global weight.  Phase and complex product with
+// the contractions and fast sine/cosine of the reference's build.
+struct ShiftPost {
+  const float* __restrict__ shifts;   // 3 per slice
+  const float* __restrict__ weights;  // 1 per slice
+  template <int NDIMS>
+  __device__ __forceinline__ float2 apply(int slice, int x, int y, int z, float2 v) const {
+    float sx = __ldg(shifts + 3 * (int64_t)slice), sy = __ldg(shifts + 3 * (int64_t)slice + 1);
+    float phase = fmaf((float)x, sx, (float)y * sy);
+    if (NDIMS == 3) phase = fmaf((float)z, __ldg(shifts + 3 * (int64_t)slice + 2), phase);
+    phase = -phase;
+    float c = __cosf(phase), s = __sinf(phase);
+    float w = __ldg(weights + slice);
+    float re = fmaf(v.x, c, -(v.y * s)), im = fmaf(v.x, s, v.y * c);
+    return make_float2(re * w, im * w);
+  }
+};
+
+template <int NDIMS, class Fetch, class Post = NoPost>
 __device__ __forceinline__ void project_direct_tile(const Fetch& fetch, float2* __restrict__ proj,
                                                     const float* __restrict__ mats, const ProjArgs& a,
-                                                    int slice, int tile) {
+                                                    int slice, int tile, const Post& post = Post()) {
   float m[9];
 #pragma unroll
   for (int i = 0; i < 9; i++) m[i] = __ldg(mats + 9 * (int64_t)slice + i);
@@ -115,16 +141,16 @@ __device__ __forceinline__ void project_direct_tile(const Fetch& fetch, float2* 
     float rxy0 = lerpf(rx00, rx01, fy), ixy0 = lerpf(ix00, ix01, fy);
     float rxy1 = lerpf(rx10, rx11, fy), ixy1 = lerpf(ix10, ix11, fy);
     float2 v = make_float2(lerpf(rxy0, rxy1, fz), lerpf(ixy0, ixy1, fz) * sign);
-    out[id] = v;
+    out[id] = post.template apply<NDIMS>(slice, x, y, z, v);
   }
 }
 
-template <int NDIMS, class Fetch>
+template <int NDIMS, class Fetch, class Post = NoPost>
 __global__ void __launch_bounds__(kProjThreads)
 project_direct_kernel(Fetch fetch, float2* __restrict__ proj, const float* __restrict__ mats,
-                      ProjArgs a) {
+                      ProjArgs a, Post post = Post()) {
   const int slice = blockIdx.x / a.tiles;
-  project_direct_tile<NDIMS>(fetch, proj, mats, a, slice, blockIdx.x - slice * a.tiles);
+  project_direct_tile<NDIMS>(fetch, proj, mats, a, slice, blockIdx.x - slice * a.tiles, post);
 }
 
 // The direct kernel over the slices listed in list[0 .. *nlist), which the
@@ -303,15 +329,15 @@ static int project_setup(int vx, int vy, int vz, int px, int py, int pz, unsigne
   return GTOMRLN_OK;
 }
 
-template <class Fetch>
+template <class Fetch, class Post = NoPost>
 static int launch_project(Fetch f, int ndp, float* d_proj, const float* d_mats, const ProjArgs& a,
-                          unsigned batch, cudaStream_t stream) {
+                          unsigned batch, cudaStream_t stream, Post post = Post()) {
   if (batch == 0) return GTOMRLN_OK;
   dim3 grid((unsigned)(a.tiles * (int64_t)batch));
   if (ndp == 2)
-    project_direct_kernel<2, Fetch><<<grid, kProjThreads, 0, stream>>>(f, (float2*)d_proj, d_mats, a);
+    project_direct_kernel<2, Fetch, Post><<<grid, kProjThreads, 0, stream>>>(f, (float2*)d_proj, d_mats, a, post);
   else
-    project_direct_kernel<3, Fetch><<<grid, kProjThreads, 0, stream>>>(f, (float2*)d_proj, d_mats, a);
+    project_direct_kernel<3, Fetch, Post><<<grid, kProjThreads, 0, stream>>>(f, (float2*)d_proj, d_mats, a, post);
   GTOMRLN_LAUNCH_CHECK("project_direct_kernel");
   return GTOMRLN_OK;
 }
@@ -443,6 +469,68 @@ int gtomrln_project_tex_angles(unsigned long long t_re, unsigned long long t_im,
                                                            pz, (unsigned)(px / 2), d_m, batch,
                                                            stream);
                               });
+}
+
+// ---------------------------------------------------------------- shifted --
+int gtomrln_project_shifted(const float* d_volumeft, int vx, int vy, int vz, float* d_proj, int px,
+                            int py, int pz, unsigned rmax, const float* d_matrices,
+                            const float* d_shifts, const float* d_globalweights, unsigned batch,
+                            void* stream) {
+  clear_error();
+  ProjArgs a;
+  int ndp;
+  int st = project_setup(vx, vy, vz, px, py, pz, rmax, batch, &a, &ndp);
+  if (st) return st;
+  if (batch && (!d_volumeft || !d_proj || !d_matrices || !d_shifts || !d_globalweights))
+    return set_error(GTOMRLN_ERR_INVALID, "project_shifted: NULL device pointer");
+  ArrayFetch f{(const float2*)d_volumeft, a.P, a.P / 2 + 1, a.nvox - 1};
+  return launch_project(f, ndp, d_proj, d_matrices, a, batch, (cudaStream_t)stream,
+                        ShiftPost{d_shifts, d_globalweights});
+}
+
+int gtomrln_project_shifted_angles(const float* d_volumeft, int vx, int vy, int vz, float* d_proj,
+                                   int px, int py, int pz, const float* h_angles,
+                                   const float* h_shifts, const float* h_globalweights,
+                                   float supersample, unsigned batch, void* stream) {
+  clear_error();
+  return with_device_shifted(h_angles, h_shifts, h_globalweights, supersample, px, batch,
+                             (cudaStream_t)stream,
+                             [&](const float* d_m, const float* d_s, const float* d_w) {
+                               return gtomrln_project_shifted(d_volumeft, vx, vy, vz, d_proj, px, py, pz,
+                                                              (unsigned)(px / 2), d_m, d_s, d_w, batch,
+                                                              stream);
+                             });
+}
+
+int gtomrln_project_shifted_tex(unsigned long long t_re, unsigned long long t_im, int vx, int vy,
+                                int vz, float* d_proj, int px, int py, int pz, unsigned rmax,
+                                const float* d_matrices, const float* d_shifts,
+                                const float* d_globalweights, unsigned batch, void* stream) {
+  clear_error();
+  ProjArgs a;
+  int ndp;
+  int st = project_setup(vx, vy, vz, px, py, pz, rmax, batch, &a, &ndp);
+  if (st) return st;
+  if (batch && (!d_proj || !d_matrices || !d_shifts || !d_globalweights))
+    return set_error(GTOMRLN_ERR_INVALID, "project_shifted_tex: NULL device pointer");
+  TexFetch f{(cudaTextureObject_t)t_re, (cudaTextureObject_t)t_im};
+  return launch_project(f, ndp, d_proj, d_matrices, a, batch, (cudaStream_t)stream,
+                        ShiftPost{d_shifts, d_globalweights});
+}
+
+int gtomrln_project_shifted_tex_angles(unsigned long long t_re, unsigned long long t_im, int vx,
+                                       int vy, int vz, float* d_proj, int px, int py, int pz,
+                                       const float* h_angles, const float* h_shifts,
+                                       const float* h_globalweights, float supersample,
+                                       unsigned batch, void* stream) {
+  clear_error();
+  return with_device_shifted(h_angles, h_shifts, h_globalweights, supersample, px, batch,
+                             (cudaStream_t)stream,
+                             [&](const float* d_m, const float* d_s, const float* d_w) {
+                               return gtomrln_project_shifted_tex(t_re, t_im, vx, vy, vz, d_proj, px, py,
+                                                                  pz, (unsigned)(px / 2), d_m, d_s, d_w,
+                                                                  batch, stream);
+                             });
 }
 
 }  // extern "C"

@@ -115,6 +115,83 @@ def d_rlnProject(volumeft, dimsvolume: Dims, proj: torch.Tensor, dimsproj: Dims,
             _lib.call("gtomrln_project", vp, vx, vy, vz, pp, px, py, pz, rmax, mp, batch, s)
 
 
+def d_rlnProjectShifted(volumeft, dimsvolume: Dims, proj: torch.Tensor, dimsproj: Dims, *args,
+                        stream=None) -> None:
+    """Central-slice gather times a per-slice phase shift and global weight
+    (include/Relion.cuh:40-43).
+
+    Overloads, after ``(volumeft, dimsvolume, d_proj, dimsproj)``:
+      ``(h_angles, h_shifts, h_globalweights, supersample, batch)`` — ProjectShifted.cu:32-56
+      ``(rmax, d_matrices, d_shifts, d_globalweights, batch)``     — ProjectShifted.cu:58-75
+    h_shifts are in pixels; d_shifts already scaled by 2 pi / dimsproj.x.
+    ``volumeft`` may be a ``(t_volumeRe, t_volumeIm)`` texture pair
+    (ProjectShifted.cu:78-122).
+    """
+    if len(args) != 5:
+        raise TypeError("d_rlnProjectShifted expects (h_angles, h_shifts, h_globalweights, supersample, "
+                        "batch) or (rmax, d_matrices, d_shifts, d_globalweights, batch)")
+    vx, vy, vz = (int(v) for v in dimsvolume)
+    px, py, pz = (int(v) for v in dimsproj)
+    batch = int(args[4])
+    pp = _dev_ptr(proj, "d_proj", torch.complex64, elements_fft((px, py, pz)) * batch)
+    tex = isinstance(volumeft, tuple)
+    vol = (int(volumeft[0]), int(volumeft[1])) if tex else \
+        (_dev_ptr(volumeft, "d_volumeft", torch.complex64, elements_fft((vx, vy, vz))),)
+    s = _stream(stream)
+    if _is_host(args[0]):
+        ang = _host_f32(args[0], "h_angles", 3 * batch)
+        sh = _host_f32(args[1], "h_shifts", 3 * batch)
+        gw = _host_f32(args[2], "h_globalweights", batch)
+        _lib.call("gtomrln_project_shifted_tex_angles" if tex else "gtomrln_project_shifted_angles",
+                  *vol, vx, vy, vz, pp, px, py, pz, ang.ctypes.data, sh.ctypes.data, gw.ctypes.data,
+                  C.c_float(args[3]), batch, s)
+    else:
+        mp = _dev_ptr(args[1], "d_matrices", torch.float32, 9 * batch)
+        sp = _dev_ptr(args[2], "d_shifts", torch.float32, 3 * batch)
+        wp = _dev_ptr(args[3], "d_globalweights", torch.float32, batch)
+        _lib.call("gtomrln_project_shifted_tex" if tex else "gtomrln_project_shifted", *vol, vx, vy, vz,
+                  pp, px, py, pz, int(args[0]), mp, sp, wp, batch, s)
+
+
+def d_rlnBackprojectShifted(volumeft, volumeweights, dimsvolume: Dims, projft, projweights,
+                            dimsproj: Dims, rmax: int, *args, stream=None) -> None:
+    """Shifted, globally weighted insertion (include/Relion.cuh:17-18), into
+    centred accumulators.
+
+    Overloads, after ``(..., dimsproj, rmax)``:
+      ``(h_angles, h_shifts, h_globalweights, supersample, batch)`` — BackprojectShifted.cu:11-35
+      ``(d_matrices, d_shifts, d_globalweights, batch)``            — BackprojectShifted.cu:37-58
+    """
+    vx, vy, vz = (int(v) for v in dimsvolume)
+    px, py, pz = (int(v) for v in dimsproj)
+    nvol = elements_fft((vx, vy, vz))
+    s = _stream(stream)
+    if len(args) == 5:
+        batch = int(args[4])
+    elif len(args) == 4:
+        batch = int(args[3])
+    else:
+        raise TypeError("d_rlnBackprojectShifted expects (h_angles, h_shifts, h_globalweights, "
+                        "supersample, batch) or (d_matrices, d_shifts, d_globalweights, batch)")
+    e = elements_fft((px, py, pz)) * batch
+    common = (_dev_ptr(volumeft, "d_volumeft", torch.complex64, nvol, optional=True),
+              _dev_ptr(volumeweights, "d_volumeweights", torch.float32, nvol, optional=True),
+              vx, vy, vz, _dev_ptr(projft, "d_projft", torch.complex64, e, optional=True),
+              _dev_ptr(projweights, "d_projweights", torch.float32, e, optional=True),
+              px, py, pz, int(rmax))
+    if len(args) == 5:
+        ang = _host_f32(args[0], "h_angles", 3 * batch)
+        sh = _host_f32(args[1], "h_shifts", 3 * batch)
+        gw = _host_f32(args[2], "h_globalweights", batch)
+        _lib.call("gtomrln_backproject_shifted_angles", *common, ang.ctypes.data, sh.ctypes.data,
+                  gw.ctypes.data, C.c_float(args[3]), batch, s)
+    else:
+        _lib.call("gtomrln_backproject_shifted", *common,
+                  _dev_ptr(args[0], "d_matrices", torch.float32, 9 * batch),
+                  _dev_ptr(args[1], "d_shifts", torch.float32, 3 * batch),
+                  _dev_ptr(args[2], "d_globalweights", torch.float32, batch), batch, s)
+
+
 def d_rlnBackproject(volumeft, volumeweights, dimsvolume: Dims, projft, projweights,
                      dimsproj: Dims, rmax: int, *args, stream=None) -> None:
     """Trilinear scatter-insert, accumulating in place (include/Relion.cuh:9-10).

@@ -186,6 +186,74 @@ GTOMRLN_API int gtomrln_backproject_angles(float* d_volumeft, float* d_volumewei
                                void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Shifted projector / backprojector: the slices are multiplied by the phase
+ * exp(-i (x sx + y sy [+ z sz])) of a per-slice shift and by a per-slice
+ * global weight.  The matrix overloads take the shifts already scaled to
+ * radians per pixel (pixels * 2 pi / dimsproj.x, float3 per slice) and the
+ * weights in device memory; the h_angles overloads take pixels and scale
+ * them.  The shifted backprojector is its own insertion in the reference
+ * (no binary16 weights, no mirrored neighbours, the whole x = 0 column,
+ * r^2 <= rmax^2, centred output) and is reproduced as such; the reference
+ * writes without bounds checks, here indices are clamped as in
+ * gtomrln_backproject.  NULL d_projft / d_projweights mean value 1 / weight 1.
+ * ------------------------------------------------------------------------- */
+
+/* gtom::d_rlnProjectShifted(tcomplex* d_volumeft, int3 dimsvolume, tcomplex* d_proj,
+ *     int3 dimsproj, uint rmax, glm::mat3* d_matrices, tfloat3* d_shifts,
+ *     float* d_globalweights, uint batch)
+ * include/Relion.cuh:41, src/Relion/ProjectShifted.cu:58-75, kernel :124-224. */
+GTOMRLN_API int gtomrln_project_shifted(const float* d_volumeft, int vx, int vy, int vz, float* d_proj,
+                            int px, int py, int pz, unsigned rmax, const float* d_matrices,
+                            const float* d_shifts, const float* d_globalweights, unsigned batch,
+                            void* stream);
+
+/* gtom::d_rlnProjectShifted(tcomplex* d_volumeft, int3 dimsvolume, tcomplex* d_proj,
+ *     int3 dimsproj, tfloat3* h_angles, tfloat3* h_shifts, float* h_globalweights,
+ *     float supersample, uint batch)
+ * include/Relion.cuh:40, src/Relion/ProjectShifted.cu:32-56 (rmax = dimsproj.x / 2). */
+GTOMRLN_API int gtomrln_project_shifted_angles(const float* d_volumeft, int vx, int vy, int vz,
+                                   float* d_proj, int px, int py, int pz, const float* h_angles,
+                                   const float* h_shifts, const float* h_globalweights,
+                                   float supersample, unsigned batch, void* stream);
+
+/* gtom::d_rlnProjectShifted(cudaTex t_volumeRe, cudaTex t_volumeIm, int3 dimsvolume, ...,
+ *     uint rmax, glm::mat3* d_matrices, tfloat3* d_shifts, float* d_globalweights, uint batch)
+ * include/Relion.cuh:43, src/Relion/ProjectShifted.cu:103-122, kernel :226-338. */
+GTOMRLN_API int gtomrln_project_shifted_tex(unsigned long long t_re, unsigned long long t_im, int vx,
+                                int vy, int vz, float* d_proj, int px, int py, int pz,
+                                unsigned rmax, const float* d_matrices, const float* d_shifts,
+                                const float* d_globalweights, unsigned batch, void* stream);
+
+/* gtom::d_rlnProjectShifted(cudaTex, cudaTex, int3, tcomplex*, int3, tfloat3* h_angles,
+ *     tfloat3* h_shifts, float* h_globalweights, float supersample, uint batch)
+ * include/Relion.cuh:42, src/Relion/ProjectShifted.cu:78-101. */
+GTOMRLN_API int gtomrln_project_shifted_tex_angles(unsigned long long t_re, unsigned long long t_im,
+                                       int vx, int vy, int vz, float* d_proj, int px, int py,
+                                       int pz, const float* h_angles, const float* h_shifts,
+                                       const float* h_globalweights, float supersample,
+                                       unsigned batch, void* stream);
+
+/* gtom::d_rlnBackprojectShifted(tcomplex* d_volumeft, tfloat* d_volumeweights,
+ *     int3 dimsvolume, tcomplex* d_projft, tfloat* d_projweights, int3 dimsproj, uint rmax,
+ *     glm::mat3* d_matrices, tfloat3* d_shifts, float* d_globalweights, uint batch)
+ * include/Relion.cuh:18, src/Relion/BackprojectShifted.cu:37-58, kernel :60-186. */
+GTOMRLN_API int gtomrln_backproject_shifted(float* d_volumeft, float* d_volumeweights, int vx, int vy,
+                                int vz, const float* d_projft, const float* d_projweights,
+                                int px, int py, int pz, unsigned rmax, const float* d_matrices,
+                                const float* d_shifts, const float* d_globalweights,
+                                unsigned batch, void* stream);
+
+/* gtom::d_rlnBackprojectShifted(..., uint rmax, tfloat3* h_angles, tfloat3* h_shifts,
+ *     float* h_globalweights, float supersample, uint batch)
+ * include/Relion.cuh:17, src/Relion/BackprojectShifted.cu:11-35. */
+GTOMRLN_API int gtomrln_backproject_shifted_angles(float* d_volumeft, float* d_volumeweights, int vx,
+                                       int vy, int vz, const float* d_projft,
+                                       const float* d_projweights, int px, int py, int pz,
+                                       unsigned rmax, const float* h_angles,
+                                       const float* h_shifts, const float* h_globalweights,
+                                       float supersample, unsigned batch, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Gridding reconstructor: RELION-style iterative gridding-weight correction
  * with a Kaiser-Bessel blob, then the inverse FFT, crop and sinc^2 correction.
  * d_dataft / d_weight are CENTRED half-complex volumes of dimspadded (the

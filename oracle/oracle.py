@@ -46,6 +46,8 @@ def lib() -> C.CDLL:
             bp = [p, p, i, p, p, i, i, i, p, p, p, f, i, i, i, i]
             L.orc_backproject_f64.argtypes = bp
             L.orc_backproject_f32.argtypes = bp
+            L.orc_project_shifted_f64.argtypes = [p, i, p, i, i, i, p, p, p, i]
+            L.orc_backproject_shifted_f64.argtypes = [p, p, i, p, p, i, i, i, p, p, p, i]
             L.orc_kaiser_fourier_value.argtypes = [d, d, d, i]
             L.orc_kaiser_fourier_value.restype = d
             L.orc_kb_table.argtypes = [d, d, i, i, p]
@@ -116,6 +118,48 @@ def backproject(volft: np.ndarray | None, volw: np.ndarray | None, P: int, projf
             raise ValueError(f"accumulator must be contiguous {dt}")
     fn(_ptr(volft), _ptr(volw), P, _ptr(pf), _ptr(pw), n, ndims, rmax, m.ctypes.data, _ptr(iv),
        mag.ctypes.data, C.c_float(ewinv), int(decentered), int(square), int(half_weights), batch)
+
+
+def scaled_shifts(h_shifts, n: int) -> np.ndarray:
+    """The matrix overloads' shifts: pixels * 2 pi / n in float32, as the
+    h_angles overloads compute them (ProjectShifted.cu:40-44)."""
+    h = np.asarray(h_shifts, np.float32).reshape(-1, 3)
+    return (h * np.float32(6.283185307179586) / np.float32(n)).astype(np.float32)
+
+
+def project_shifted(volume: np.ndarray, P: int, n: int, rmax: int, mats: np.ndarray, shifts,
+                    globalweights, ndims: int = 2) -> np.ndarray:
+    """ProjectShifted3DArraytoNDKernel (ProjectShifted.cu:124-224) in
+    float64: the projection times exp(-i (x sx + y sy [+ z sz])) times the
+    slice's global weight.  shifts: (batch, 3) already scaled by 2 pi / n."""
+    vol = _c(volume, np.complex64)
+    m = _c(mats, np.float32).reshape(-1, 9)
+    batch = m.shape[0]
+    sh = _c(shifts, np.float32).reshape(batch, 3)
+    gw = _c(globalweights, np.float32).reshape(batch)
+    out = np.zeros((batch, elements_fft(n, ndims)), np.complex128)
+    lib().orc_project_shifted_f64(vol.ctypes.data, P, out.ctypes.data, n, ndims, min(int(rmax), n // 2),
+                                  m.ctypes.data, sh.ctypes.data, gw.ctypes.data, batch)
+    return out
+
+
+def backproject_shifted(volft, volw, V: int, projft, projw, n: int, rmax: int, mats, shifts,
+                        globalweights, ndims: int = 2) -> None:
+    """BackprojectShifted3DtoNDKernel (BackprojectShifted.cu:67-186) in
+    float64, accumulating into volft (complex128) / volw (float64), centred
+    volumes of V; indices clamped as in the unshifted backprojector."""
+    m = _c(mats, np.float32).reshape(-1, 9)
+    batch = m.shape[0]
+    pf = None if projft is None else _c(projft, np.complex64)
+    pw = None if projw is None else _c(projw, np.float32)
+    sh = _c(shifts, np.float32).reshape(batch, 3)
+    gw = _c(globalweights, np.float32).reshape(batch)
+    for a, dt in ((volft, np.complex128), (volw, np.float64)):
+        if a is not None and (a.dtype != dt or not a.flags.c_contiguous):
+            raise ValueError(f"accumulator must be contiguous {dt}")
+    lib().orc_backproject_shifted_f64(_ptr(volft), _ptr(volw), V, _ptr(pf), _ptr(pw), n, ndims,
+                                      min(int(rmax), n // 2), m.ctypes.data, sh.ctypes.data, gw.ctypes.data,
+                                      batch)
 
 
 def kb_table(radius: float, alpha: float, order: int = 0, nsamples: int = 10000) -> np.ndarray:

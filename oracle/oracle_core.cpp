@@ -284,6 +284,104 @@ void backproject_slice(R* volft, R* volw, const float* projft, const float* proj
 // ---------------------------------------------------------------------------
 const double kPi = 3.14159265358979323846;
 
+// ---------------------------------------------------------------------------
+// Shifted variants (src/Relion/ProjectShifted.cu:124-224,
+// src/Relion/BackprojectShifted.cu:67-186), in float64.  shifts are the
+// per-slice 2*pi/n-scaled shifts the matrix overloads take; the phase is
+// exp(i phi), phi = -(x sx + y sy [+ z sz]), and the global weight scales
+// the value (and, for insertion, the weight).
+// ---------------------------------------------------------------------------
+void project_shifted_f64(const float* vol, int P, double* out, int n, int ndims, int rmax,
+                         const float* mats, const float* shifts, const float* gw, int batch) {
+  project_impl<double, double>(vol, P, out, n, ndims, rmax, mats, batch);
+  const int dimft = n / 2 + 1;
+  const int64_t slice = (int64_t)dimft * n;
+  const int64_t elements = ndims == 3 ? slice * n : slice;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int b = 0; b < batch; b++) {
+    double* o = out + 2 * elements * (int64_t)b;
+    double sx = shifts[3 * b], sy = shifts[3 * b + 1], sz = shifts[3 * b + 2], w = gw[b];
+    for (int64_t id = 0; id < elements; id++) {
+      int x = (int)(id % dimft);
+      int idy = (int)((ndims == 3 ? id % slice : id) / dimft);
+      int idz = ndims == 3 ? (int)(id / slice) : 0;
+      int y = idy <= n / 2 ? idy : idy - n;
+      int z = idz <= n / 2 ? idz : idz - n;
+      if ((ndims == 3 ? z * z : 0) + y * y + x * x > rmax * rmax) continue;  // stays 0
+      double phase = -(x * sx + y * sy + (ndims == 3 ? z * sz : 0.0));
+      double c = std::cos(phase), sn = std::sin(phase);
+      double re = o[2 * id], im = o[2 * id + 1];
+      o[2 * id] = (re * c - im * sn) * w;
+      o[2 * id + 1] = (re * sn + im * c) * w;
+    }
+  }
+}
+
+// BackprojectShifted3DtoNDKernel: plain (not binary16-rounded) trilinear
+// weights, no mirroring of neighbours and no second insertion on x = 0 (the
+// whole x = 0 column is inserted), r^2 <= rmax^2, centred output.  The
+// reference writes without bounds checks; here every index is clamped as
+// in the unshifted backprojector (x <= V/2, y, z <= V-1, compared unsigned).
+void backproject_shifted_f64(double* volft, double* volw, int V, const float* projft,
+                             const float* projw, int n, int ndims, int rmax, const float* mats,
+                             const float* shifts, const float* gw, int batch) {
+  const int dimft = n / 2 + 1;
+  const int64_t slice = (int64_t)dimft * n;
+  const int64_t elements = ndims == 3 ? slice * n : slice;
+  const int rowlen = V / 2 + 1;
+  for (int b = 0; b < batch; b++) {
+    Mat3<double> M(mats + 9 * (int64_t)b);
+    double sx = shifts[3 * b], sy = shifts[3 * b + 1], sz = shifts[3 * b + 2], w = gw[b];
+    for (int64_t id = 0; id < elements; id++) {
+      int x = (int)(id % dimft);
+      int idy = (int)((ndims == 3 ? id % slice : id) / dimft);
+      int idz = ndims == 3 ? (int)(id / slice) : 0;
+      int y = idy <= rmax ? idy : idy - n;
+      int z = ndims == 3 ? (idz <= rmax ? idz : idz - n) : 0;
+      int r2 = ndims == 3 ? z * z + y * y + x * x : y * y + x * x;
+      if (r2 > rmax * rmax) continue;
+      double px, py, pz;
+      M.apply(x, y, z, px, py, pz);
+      double sign = 1;
+      if (px + kEps < 0) {
+        px = std::fabs(px);
+        py = -py;
+        pz = -pz;
+        sign = -1;
+      }
+      int x0 = (int)std::floor(px + kEps);
+      double fx = px - x0;
+      int y0 = (int)std::floor(py);
+      double fy = py - y0;
+      int z0 = (int)std::floor(pz);
+      double fz = pz - z0;
+      y0 += V / 2;
+      z0 += V / 2;
+      double re = projft ? projft[2 * (elements * b + id)] : 1.0;
+      double im = projft ? projft[2 * (elements * b + id) + 1] : 0.0;
+      double phase = -(x * sx + y * sy + (ndims == 3 ? z * sz : 0.0));
+      double c = std::cos(phase), sn = std::sin(phase);
+      double vr = (re * c - im * sn) * w;
+      double vi = (re * sn + im * c) * w * sign;
+      double wt = (projw ? projw[elements * b + id] : 1.0) * w;
+      for (int i = 0; i < 8; i++) {
+        int dx = i & 1, dy = (i >> 1) & 1, dz = (i >> 2) & 1;
+        double cw = (dx ? fx : 1 - fx) * (dy ? fy : 1 - fy) * (dz ? fz : 1 - fz);
+        unsigned tx = (unsigned)(x0 + dx), ty = (unsigned)(y0 + dy), tz = (unsigned)(z0 + dz);
+        if (tx > (unsigned)(V / 2)) tx = V / 2;
+        if (ty > (unsigned)(V - 1)) ty = V - 1;
+        if (tz > (unsigned)(V - 1)) tz = V - 1;
+        int64_t o = ((int64_t)tz * V + ty) * rowlen + tx;
+        if (volft) {
+          volft[2 * o] += cw * vr;
+          volft[2 * o + 1] += cw * vi;
+        }
+        if (volw) volw[o] += cw * wt;
+      }
+    }
+  }
+}
+
 double bessel_i0(double x) {
   double t = x * x / 4, term = 1, sum = 1;
   for (int k = 1; k < 500; k++) {
@@ -410,6 +508,18 @@ void orc_backproject_f32(float* volft, float* volw, int P, const float* projft,
 }
 
 // kaiser_Fourier_value(w, a, alpha, m) for m in {0, 2}; returns NaN otherwise.
+// ProjectShifted.cu:124-224 / BackprojectShifted.cu:67-186 (float64).
+void orc_project_shifted_f64(const float* vol, int P, double* out, int n, int ndims, int rmax,
+                             const float* mats, const float* shifts, const float* gw, int batch) {
+  project_shifted_f64(vol, P, out, n, ndims, rmax, mats, shifts, gw, batch);
+}
+
+void orc_backproject_shifted_f64(double* volft, double* volw, int V, const float* projft,
+                                 const float* projw, int n, int ndims, int rmax, const float* mats,
+                                 const float* shifts, const float* gw, int batch) {
+  backproject_shifted_f64(volft, volw, V, projft, projw, n, ndims, rmax, mats, shifts, gw, batch);
+}
+
 double orc_kaiser_fourier_value(double w, double a, double alpha, int m) {
   double t = 2 * kPi * a * w;
   double sigma = std::sqrt(std::fabs(alpha * alpha - t * t));

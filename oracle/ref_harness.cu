@@ -71,6 +71,27 @@ int ref_backproject_angles(float* d_volumeft, float* d_volumeweights, int P, flo
   return (int)cudaGetLastError();
 }
 
+// include/Relion.cuh:41 -> src/Relion/ProjectShifted.cu:58-75
+int ref_project_shifted(float* d_volumeft, int P, float* d_proj, int n, int ndims, int rmax,
+                        float* d_matrices, float* d_shifts, float* d_globalweights, int batch) {
+  d_rlnProjectShifted((tcomplex*)d_volumeft, toInt3(P, P, P), (tcomplex*)d_proj,
+                      toInt3(n, n, ndims == 3 ? n : 1), (uint)rmax, (glm::mat3*)d_matrices,
+                      (tfloat3*)d_shifts, d_globalweights, (uint)batch);
+  cudaDeviceSynchronize();
+  return (int)cudaGetLastError();
+}
+
+// include/Relion.cuh:18 -> src/Relion/BackprojectShifted.cu:37-58
+int ref_backproject_shifted(float* d_volumeft, float* d_volumeweights, int V, float* d_projft,
+                            float* d_projweights, int n, int ndims, int rmax, float* d_matrices,
+                            float* d_shifts, float* d_globalweights, int batch) {
+  d_rlnBackprojectShifted((tcomplex*)d_volumeft, d_volumeweights, toInt3(V, V, V), (tcomplex*)d_projft,
+                          d_projweights, toInt3(n, n, ndims == 3 ? n : 1), (uint)rmax,
+                          (glm::mat3*)d_matrices, (tfloat3*)d_shifts, d_globalweights, (uint)batch);
+  cudaDeviceSynchronize();
+  return (int)cudaGetLastError();
+}
+
 // include/Reconstruction.cuh:16 -> src/Reconstruction/RecFourier.cu:98-241
 int ref_reconstruct_gridding(float* d_dataft, float* d_weight, float* d_reconstructed, int ori,
                              int padded, int paddingfactor, int iterations, double blobradius,

@@ -36,6 +36,8 @@ REF.ref_backproject.argtypes = [_p, _p, _i, _p, _p, _i, _i, _i, _p, _p, _f, _f, 
 REF.ref_backproject_angles.argtypes = [_p, _p, _i, _p, _p, _i, _i, _i, _p, _p, _f, _f, _f, _f, _f,
                                        _f, _i, _i, _i]
 REF.ref_reconstruct_gridding.argtypes = [_p, _p, _p, _i, _i, _i, _i, _d, _i, _d]
+REF.ref_project_shifted.argtypes = [_p, _i, _p, _i, _i, _i, _p, _p, _p, _i]
+REF.ref_backproject_shifted.argtypes = [_p, _p, _i, _p, _p, _i, _i, _i, _p, _p, _p, _i]
 
 
 def _ok(rc: int, what: str) -> None:
@@ -138,13 +140,63 @@ def gen_gridding(out: Path, rng) -> None:
         print(name, np.abs(rec).max())
 
 
+def gen_shifted(out: Path, rng) -> None:
+    """d_rlnProjectShifted / d_rlnBackprojectShifted (matrix overloads).  The
+    backprojection cases keep rmax * supersample below the centred box's
+    half-width: the reference writes without bounds checks."""
+    for name, n, ndims, batch, rmax in (("project_shifted_2d", 16, 2, 12, 8), ("project_shifted_3d", 8, 3, 3, 4)):
+        P = 2 * n
+        vol = blob_volume_ft(rng, n, P, 12)
+        ang = random_angles(rng, batch)
+        mats = O.matrices_f64(ang, 2.0).astype(np.float32)
+        shifts_px = rng.uniform(-3, 3, (batch, 3)).astype(np.float32)
+        shifts = O.scaled_shifts(shifts_px, n)
+        gw = rng.uniform(0.5, 1.5, batch).astype(np.float32)
+        e = O.elements_fft(n, ndims)
+        dv, dm, ds, dw = dev(vol, extra=64), dev(mats), dev(shifts), dev(gw)
+        dp = torch.zeros(e * batch * 8, dtype=torch.uint8, device="cuda")
+        _ok(REF.ref_project_shifted(dv.data_ptr(), P, dp.data_ptr(), n, ndims, rmax, dm.data_ptr(), ds.data_ptr(),
+                                    dw.data_ptr(), batch), name)
+        proj = host(dp, np.complex64, e * batch).reshape(batch, e)
+        np.savez_compressed(out / f"{name}.npz", volume=vol, P=P, n=n, ndims=ndims, rmax=rmax, angles=ang,
+                            matrices=mats, shifts_px=shifts_px, shifts=shifts, globalweights=gw, proj=proj)
+        print(name, np.abs(proj).max())
+    for name, n, ndims, V, batch, rmax in (("bp_shifted_2d", 16, 2, 33, 30, 7), ("bp_shifted_3d", 8, 3, 17, 3, 3)):
+        ang = random_angles(rng, batch)
+        mats = O.matrices_f64(ang, 2.0).astype(np.float32)
+        shifts_px = rng.uniform(-3, 3, (batch, 3)).astype(np.float32)
+        shifts = O.scaled_shifts(shifts_px, n)
+        gw = rng.uniform(0.5, 1.5, batch).astype(np.float32)
+        e = O.elements_fft(n, ndims)
+        projft = (rng.normal(size=(batch, e)) + 1j * rng.normal(size=(batch, e))).astype(np.complex64)
+        projw = rng.uniform(0.1, 1.0, size=(batch, e)).astype(np.float32)
+        nv = (V // 2 + 1) * V * V
+        dvf = torch.zeros(nv * 8, dtype=torch.uint8, device="cuda")
+        dvw = torch.zeros(nv * 4, dtype=torch.uint8, device="cuda")
+        dpf, dpw, dm, ds, dw = dev(projft), dev(projw), dev(mats), dev(shifts), dev(gw)
+        _ok(REF.ref_backproject_shifted(dvf.data_ptr(), dvw.data_ptr(), V, dpf.data_ptr(), dpw.data_ptr(), n, ndims,
+                                        rmax, dm.data_ptr(), ds.data_ptr(), dw.data_ptr(), batch), name)
+        volft = host(dvf, np.complex64, nv)
+        volw = host(dvw, np.float32, nv)
+        np.savez_compressed(out / f"{name}.npz", V=V, n=n, ndims=ndims, rmax=rmax, angles=ang, matrices=mats,
+                            shifts_px=shifts_px, shifts=shifts, globalweights=gw, projft=projft, projw=projw,
+                            volft=volft, volw=volw)
+        print(name, np.abs(volft).max(), volw.max())
+
+
 def main() -> None:
-    out = Path(sys.argv[1]) if len(sys.argv) > 1 else Path(__file__).resolve().parent
+    """make_golden.py [outdir] [--only project|backproject|gridding|shifted ...]"""
+    args = sys.argv[1:]
+    only = set(args[args.index("--only") + 1:]) if "--only" in args else None
+    args = args[:args.index("--only")] if "--only" in args else args
+    out = Path(args[0]) if args else Path(__file__).resolve().parent
     out.mkdir(parents=True, exist_ok=True)
     rng = np.random.default_rng(20261203)
-    gen_project(out, rng)
-    gen_backproject(out, rng)
-    gen_gridding(out, rng)
+    for key, fn in (("project", gen_project), ("backproject", gen_backproject), ("gridding", gen_gridding)):
+        if only is None or key in only:
+            fn(out, rng)
+    if only is None or "shifted" in only:
+        gen_shifted(out, np.random.default_rng(20261204))
 
 
 if __name__ == "__main__":

@@ -51,3 +51,27 @@ def test_oracle_gridding_matches_reference(name):
                                  ori, (dp,) * 3, pad, iterations=it)
     assert rel_l2(rec, g["reconstructed"]) <= 1e-5
     assert fsc(rec, g["reconstructed"]).min() >= 0.9999
+
+
+@pytest.mark.parametrize("name", ["project_shifted_2d", "project_shifted_3d"])
+def test_oracle_project_shifted_matches_reference(name):
+    """The reference multiplies by the phase with the fast hardware sine and
+    cosine (ProjectShifted.cu:217); the float64 oracle with exact ones."""
+    g = load_golden(name)
+    out = O.project_shifted(g["volume"], int(g["P"]), int(g["n"]), int(g["rmax"]), g["matrices"], g["shifts"],
+                            g["globalweights"], ndims=int(g["ndims"]))
+    assert rel_l2(out, g["proj"]) <= 1e-5
+    np.testing.assert_array_equal(O.scaled_shifts(g["shifts_px"], int(g["n"])), g["shifts"])
+
+
+@pytest.mark.parametrize("name", ["bp_shifted_2d", "bp_shifted_3d"])
+def test_oracle_backproject_shifted_matches_reference(name):
+    g = load_golden(name)
+    V = int(g["V"])
+    nv = (V // 2 + 1) * V * V
+    vf = np.zeros(nv, np.complex128)
+    vw = np.zeros(nv, np.float64)
+    O.backproject_shifted(vf, vw, V, g["projft"], g["projw"], int(g["n"]), int(g["rmax"]), g["matrices"],
+                          g["shifts"], g["globalweights"], ndims=int(g["ndims"]))
+    assert rel_l2(vf, g["volft"]) <= 1e-5
+    assert rel_l2(vw, g["volw"]) <= 1e-5
