@@ -92,6 +92,7 @@ int pool_free(void* ptr, cudaStream_t stream) {
 }
 
 int release_gridding_plans();  // gridding.cu
+int release_ctf_plans();       // ctf.cu
 
 static std::atomic<int> g_path[2] = {{GTOMRLN_PATH_AUTO}, {GTOMRLN_PATH_AUTO}};
 
@@ -120,6 +121,8 @@ const char* gtomrln_last_error(void) { return g_last_error.c_str(); }
 
 int gtomrln_release_caches(void) {
   int st = release_gridding_plans();
+  if (st) return st;
+  st = release_ctf_plans();
   if (st) return st;
   int dev = 0;
   GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));

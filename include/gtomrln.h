@@ -375,6 +375,41 @@ GTOMRLN_API int gtomrln_mlp_adam(float* d_params, float* d_grad, float* d_m, flo
                      float lr, float beta1, float beta2, float eps, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * CTF and particle preprocessing (the step before insertion).
+ * ------------------------------------------------------------------------- */
+
+/* gtom::CTFParams (include/CTF.cuh:11-42): lengths in metres, angles in
+ * radians; the reference's defaults are pixelsize 1e-10, Cs 2e-3, voltage
+ * 300e3, defocus -3e-6, amplitude 0.07, scale 1, all else 0. */
+typedef struct gtomrln_ctf_params {
+  float pixelsize, pixeldelta, pixelangle, Cs, voltage, defocus, astigmatismangle, defocusdelta,
+      amplitude, Bfactor, Bfactordelta, Bfactorangle, scale, phaseshift;
+} gtomrln_ctf_params_t;
+
+/* gtom::d_CTFSimulate(CTFParams* h_params, float2* d_addresses, float* d_gammacorrection,
+ *     tfloat* d_output, uint n, bool amplitudesquared = false, bool ignorefirstpeak = false,
+ *     int batch = 1)
+ * include/CTF.cuh:317, src/CTF/Simulate.cu:22-47, kernel :117-139, d_GetCTF
+ * include/CTF.cuh:195-223.  d_addresses: n float2 (spatial frequency in
+ * 1/pixel, azimuth); d_gammacorrection may be NULL; d_output: batch x n. */
+GTOMRLN_API int gtomrln_ctf_simulate(const gtomrln_ctf_params_t* h_params, const float* d_addresses,
+                         const float* d_gammacorrection, float* d_output, unsigned n,
+                         int amplitudesquared, int ignorefirstpeak, int batch, void* stream);
+
+/* Extension (no single reference function; the steps a caller of
+ * d_rlnBackproject makes before it): batch real-space particles of n x n
+ * (row-major, centred at (n/2, n/2)) to d_projft = CTF * FT and
+ * d_projweights = CTF^2 (may be NULL), both half-complex (n/2+1) x n per
+ * particle, ready for gtomrln_backproject.  FT is cuFFT's unnormalised R2C
+ * of the particle moved to the origin (a factor (-1)^(x+y)); the CTF at
+ * each element is gtomrln_ctf_simulate's for the address
+ * (sqrt(x^2 + y^2) / n, atan2(y, x)).  h_params NULL: no CTF (weights 1).
+ * batch <= 65535. */
+GTOMRLN_API int gtomrln_preprocess_particles(const float* d_images, int n, unsigned batch,
+                                 const gtomrln_ctf_params_t* h_params, float* d_projft,
+                                 float* d_projweights, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Batched reconstruction of many volumes of uneven box size (no reference
  * counterpart; the reference batches equal boxes only, through d_ivolume of
  * d_rlnBackproject, src/Relion/Backproject.cu:48-124).  Per subvolume the

@@ -12,6 +12,7 @@
 #include "Helper.cuh"
 #include "Relion.cuh"
 #include "Reconstruction.cuh"
+#include "CTF.cuh"
 
 using namespace gtom;
 
@@ -88,6 +89,16 @@ int ref_backproject_shifted(float* d_volumeft, float* d_volumeweights, int V, fl
   d_rlnBackprojectShifted((tcomplex*)d_volumeft, d_volumeweights, toInt3(V, V, V), (tcomplex*)d_projft,
                           d_projweights, toInt3(n, n, ndims == 3 ? n : 1), (uint)rmax,
                           (glm::mat3*)d_matrices, (tfloat3*)d_shifts, d_globalweights, (uint)batch);
+  cudaDeviceSynchronize();
+  return (int)cudaGetLastError();
+}
+
+// include/CTF.cuh:317 -> src/CTF/Simulate.cu:22-47 (h_params: 14 floats per
+// CTFParams, in the struct's order)
+int ref_ctf_simulate(float* h_params, float* d_addresses, float* d_gammacorrection, float* d_output,
+                     int n, int amplitudesquared, int ignorefirstpeak, int batch) {
+  d_CTFSimulate((CTFParams*)h_params, (float2*)d_addresses, d_gammacorrection, d_output, (uint)n,
+                amplitudesquared != 0, ignorefirstpeak != 0, batch);
   cudaDeviceSynchronize();
   return (int)cudaGetLastError();
 }

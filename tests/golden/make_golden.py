@@ -38,6 +38,7 @@ REF.ref_backproject_angles.argtypes = [_p, _p, _i, _p, _p, _i, _i, _i, _p, _p, _
 REF.ref_reconstruct_gridding.argtypes = [_p, _p, _p, _i, _i, _i, _i, _d, _i, _d]
 REF.ref_project_shifted.argtypes = [_p, _i, _p, _i, _i, _i, _p, _p, _p, _i]
 REF.ref_backproject_shifted.argtypes = [_p, _p, _i, _p, _p, _i, _i, _i, _p, _p, _p, _i]
+REF.ref_ctf_simulate.argtypes = [_p, _p, _p, _p, _i, _i, _i, _i]
 
 
 def _ok(rc: int, what: str) -> None:
@@ -184,8 +185,42 @@ def gen_shifted(out: Path, rng) -> None:
         print(name, np.abs(volft).max(), volw.max())
 
 
+def gen_ctf(out: Path, rng) -> None:
+    """d_CTFSimulate on the half-complex grid of 32 (frequencies up to
+    0.25/pixel at 1-1.5 A/pixel keep the phase below ~60 rad) and on random
+    points, with and without amplitude squaring / first-peak flattening,
+    astigmatism, anisotropic pixels, B-factors, phase shift and a gamma
+    correction."""
+    from oracle import ctf_oracle as CO
+    batch = 6
+    params = CO.params_array([dict(pixelsize=rng.uniform(1.0, 1.5) * 1e-10, pixeldelta=rng.uniform(0, 0.02) * 1e-10,
+                                   pixelangle=rng.uniform(0, np.pi), defocus=-rng.uniform(0.3, 1.5) * 1e-6,
+                                   defocusdelta=rng.uniform(0, 0.1) * 1e-6, astigmatismangle=rng.uniform(0, np.pi),
+                                   Bfactor=-rng.uniform(0, 60) * 1e-20 if i % 2 else 0.0,
+                                   Bfactordelta=rng.uniform(0, 10) * 1e-20 if i % 3 == 0 else 0.0,
+                                   Bfactorangle=rng.uniform(0, np.pi), phaseshift=rng.uniform(0, 0.5),
+                                   scale=rng.uniform(0.8, 1.2)) for i in range(batch)])
+    grid = CO.half_grid_addresses(32)
+    grid = grid[grid[:, 0] <= 0.25]
+    pts = np.stack([rng.uniform(0, 0.25, 300), rng.uniform(-np.pi, np.pi, 300)], -1)
+    addresses = np.concatenate([grid, pts]).astype(np.float32)
+    n = len(addresses)
+    gcorr = rng.uniform(-0.2, 0.2, n).astype(np.float32)
+    da, dg = dev(addresses), dev(gcorr)
+    res = {}
+    for sq in (0, 1):
+        for ign in (0, 1):
+            for gc in (0, 1):
+                do = torch.zeros(n * batch * 4, dtype=torch.uint8, device="cuda")
+                _ok(REF.ref_ctf_simulate(params.ctypes.data, da.data_ptr(), dg.data_ptr() if gc else None,
+                                         do.data_ptr(), n, sq, ign, batch), "ctf")
+                res[f"out_sq{sq}_ign{ign}_gc{gc}"] = host(do, np.float32, n * batch).reshape(batch, n)
+    np.savez_compressed(out / "ctf_simulate.npz", params=params, addresses=addresses, gammacorrection=gcorr, **res)
+    print("ctf_simulate", {k: float(np.abs(v).max()) for k, v in res.items()})
+
+
 def main() -> None:
-    """make_golden.py [outdir] [--only project|backproject|gridding|shifted ...]"""
+    """make_golden.py [outdir] [--only project|backproject|gridding|shifted|ctf ...]"""
     args = sys.argv[1:]
     only = set(args[args.index("--only") + 1:]) if "--only" in args else None
     args = args[:args.index("--only")] if "--only" in args else args
@@ -197,6 +232,8 @@ def main() -> None:
             fn(out, rng)
     if only is None or "shifted" in only:
         gen_shifted(out, np.random.default_rng(20261204))
+    if only is None or "ctf" in only:
+        gen_ctf(out, np.random.default_rng(20261205))
 
 
 if __name__ == "__main__":
