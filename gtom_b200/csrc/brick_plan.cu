@@ -138,9 +138,15 @@ __global__ void __launch_bounds__(kBinThreads)
 bin_slices_kernel(const float* __restrict__ mats, BrickGrid g, PixelSet px, float limit,
                   int* __restrict__ entries, int64_t entries_cap, PixelBin* __restrict__ bins,
                   int64_t bins_cap, unsigned long long* __restrict__ counters,
-                  int* __restrict__ brick_pairs, int* __restrict__ fallback, int* __restrict__ nfallback) {
+                  int* __restrict__ brick_pairs, int* __restrict__ fallback, int* __restrict__ nfallback,
+                  int use_codes) {
   extern __shared__ int hist[];  // interior counts [nbricks], then boundary counts [nbricks]
   int* hist_b = hist + g.nbricks;
+  // With use_codes, one 16-bit code per pixel id after the histograms: the
+  // pixel's brick + 1 when it has exactly one brick and lies inside it
+  // (every projector pixel, most backprojector pixels), else 0; the placing
+  // pass then skips the sample evaluation for coded pixels.
+  unsigned short* codes = reinterpret_cast<unsigned short*>(hist + 2 * g.nbricks);
   __shared__ int s_bad, s_sum[kBinThreads / 32], s_nz[kBinThreads / 32];
   __shared__ long long s_base_e, s_base_b;
   const int slice = blockIdx.x;
@@ -155,9 +161,18 @@ bin_slices_kernel(const float* __restrict__ mats, BrickGrid g, PixelSet px, floa
   for (int b = tid; b < 2 * g.nbricks; b += kBinThreads) hist[b] = 0;
   if (tid == 0) s_bad = 0;
   __syncthreads();
-  for_each_set_pixel(px, [&](int, int u, int v) {
-    bool ok = pixel_bricks<OP>(m, u, v, g, [&](int b, bool in) { atomicAdd(in ? &hist[b] : &hist_b[b], 1); });
+  for_each_set_pixel(px, [&](int id, int u, int v) {
+    int nb = 0, first = 0;
+    bool first_in = false;
+    bool ok = pixel_bricks<OP>(m, u, v, g, [&](int b, bool in) {
+      atomicAdd(in ? &hist[b] : &hist_b[b], 1);
+      if (nb++ == 0) {
+        first = b;
+        first_in = in;
+      }
+    });
     if (!ok) s_bad = 1;
+    if (use_codes) codes[id] = (ok && nb == 1 && first_in) ? (unsigned short)(first + 1) : (unsigned short)0;
   });
   __syncthreads();
   if (s_bad) {
@@ -222,6 +237,11 @@ bin_slices_kernel(const float* __restrict__ mats, BrickGrid g, PixelSet px, floa
   }
   __syncthreads();
   for_each_set_pixel(px, [&](int id, int u, int v) {
+    const unsigned c = use_codes ? codes[id] : 0u;
+    if (c) {
+      entries[s_base_e + atomicAdd(&hist[c - 1], 1)] = id;
+      return;
+    }
     pixel_bricks<OP>(m, u, v, g, [&](int b, bool in) {
       entries[s_base_e + atomicAdd(in ? &hist[b] : &hist_b[b], 1)] = id;
     });
@@ -334,6 +354,11 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
   size_t hist_bytes = 2 * sizeof(int) * (size_t)g.nbricks;
   if (hist_bytes > 200 * 1024)
     return set_error(GTOMRLN_ERR_INVALID, "brick grid of %d bricks too fine for the binning plan", g.nbricks);
+  // The per-pixel brick codes join the histograms when they fit (2 bytes per
+  // pixel id of a slice: 66 KB at n = 256).
+  const size_t code_bytes = ((size_t)px.elements * 2 + 3) & ~(size_t)3;
+  const int use_codes = g.nbricks < 65535 && hist_bytes + code_bytes <= 200 * 1024 ? 1 : 0;
+  const size_t smem_bytes = hist_bytes + (use_codes ? code_bytes : 0);
   const int* d_order = nullptr;
   int st = brick_order(g, &d_order);
   if (st) return st;
@@ -390,16 +415,16 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
   if (e == cudaSuccess && batch > 0) {
     if (op == GTOMRLN_OP_PROJECT) {
       cudaFuncSetAttribute(bin_slices_kernel<GTOMRLN_OP_PROJECT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)hist_bytes);
-      bin_slices_kernel<GTOMRLN_OP_PROJECT><<<batch, kBinThreads, hist_bytes, stream>>>(
+                           (int)smem_bytes);
+      bin_slices_kernel<GTOMRLN_OP_PROJECT><<<batch, kBinThreads, smem_bytes, stream>>>(
           d_mats, g, px, limit, plan->entries, entries_cap, plan->bins, bins_cap, counters, counts,
-          plan->fallback, plan->nfallback);
+          plan->fallback, plan->nfallback, use_codes);
     } else {
       cudaFuncSetAttribute(bin_slices_kernel<GTOMRLN_OP_BACKPROJECT>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_bytes);
-      bin_slices_kernel<GTOMRLN_OP_BACKPROJECT><<<batch, kBinThreads, hist_bytes, stream>>>(
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+      bin_slices_kernel<GTOMRLN_OP_BACKPROJECT><<<batch, kBinThreads, smem_bytes, stream>>>(
           d_mats, g, px, limit, plan->entries, entries_cap, plan->bins, bins_cap, counters, counts,
-          plan->fallback, plan->nfallback);
+          plan->fallback, plan->nfallback, use_codes);
     }
     pairs_scan_kernel<<<1, kScanThreads, 0, stream>>>(counts, d_order, g.nbricks, chunk, offsets, item_off,
                                                       cursor, plan->nitems);
