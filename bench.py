@@ -307,6 +307,8 @@ def run_ours(args):
 
     if not (args.no_gridding or args.no_extras) and rank == 0:
         out["gridding"] = time_gridding(G, torch, acc_ft, acc_w, n, D, dev)
+    if rank == 0 and not args.no_extras:
+        out["extensions"] = time_extensions(args, G, torch, ws, acc_ft, acc_w, dev, hbm_peak, probe)
     if rank == 0 and not args.no_extras and args.subtomos > 0:
         out["batched_uneven"] = time_batched(args, torch, dev)
     if rank == 0 and not args.no_extras:
@@ -358,6 +360,56 @@ def time_gridding(G, torch, acc_ft, acc_w, n, D, dev):
         dists = [WS.random_distribution(rng) for _ in range(360)][300:302]
         volft = synth_volft(128, dev)
         res["warm_start_128"] = WS.summarise(WS.evaluate(p128, 128, dists, PAD, volft=volft))
+    return res
+
+
+def time_extensions(args, G, torch, ws, acc_ft, acc_w, dev, hbm_peak, probe):
+    """The next operators on the same workload, CUDA events around one call
+    after one untimed call: the shifted projector and backprojector (a
+    per-slice phase shift and global weight; direct kernels) and the
+    particle preprocessing (batched R2C + centring phase + CTF and CTF^2)."""
+    from gtom_b200.ctf import preprocess_particles
+    n, P, D, rmax, e = ws["n"], ws["P"], ws["D"], ws["rmax"], ws["e"]
+    B = min(args.batch, ws["N"])
+    rng = np.random.default_rng(7)
+    m = ws["mats"][:B].reshape(-1)
+    shifts = torch.from_numpy((rng.uniform(-5, 5, (B, 3)) * 2 * np.pi / n).astype(np.float32)).to(dev).reshape(-1)
+    gw = torch.from_numpy(rng.uniform(0.5, 1.5, B).astype(np.float32)).to(dev)
+    proj = torch.empty(B * e, dtype=torch.complex64, device=dev)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    res = {}
+    ms = timed(lambda: G.d_rlnProjectShifted(ws["volft"], (P, P, P), proj, (n, n, 1), rmax, m, shifts, gw, B))
+    byt = B * (ws["sp"] * 72 + (e - ws["sp"]) * 8)
+    res["project_shifted"] = {"slices_per_s": round(B / (ms * 1e-3), 1), "ms": round(ms, 3),
+                              "algorithmic_gbs": round(byt / (ms * 1e-3) / 1e9, 1),
+                              "frac_of_hbm": round(byt / (ms * 1e-3) / 1e9 / hbm_peak, 4)}
+    ms = timed(lambda: G.d_rlnBackprojectShifted(acc_ft, acc_w, (D, D, D), ws["data"][:B].reshape(-1),
+                                                 ws["wts"][:B].reshape(-1), (n, n, 1), rmax, m, shifts, gw, B))
+    reds = B * ws["sp"] * 24
+    l2 = probe.get("l2_red_v2_gadds")
+    res["backproject_shifted"] = {"slices_per_s": round(B / (ms * 1e-3), 1), "ms": round(ms, 3),
+                                  "g_reductions_per_s": round(reds / (ms * 1e-3) / 1e9, 1),
+                                  "frac_of_l2_red_v2": None if not l2 else round(reds / (ms * 1e-3) / 1e9 / l2, 4)}
+    imgs = torch.randn((B, n, n), device=dev)
+    params = [dict(defocus=-float(d) * 1e-6) for d in rng.uniform(0.5, 3.0, B)]
+    from gtom_b200.ctf import ctf_params
+    arr = ctf_params(params)
+    ms = timed(lambda: preprocess_particles(imgs, arr))
+    byt = B * (n * n * 4 + e * 12)
+    res["preprocess_particles"] = {"particles_per_s": round(B / (ms * 1e-3), 1), "ms": round(ms, 3),
+                                   "compulsory_gbs": round(byt / (ms * 1e-3) / 1e9, 1),
+                                   "frac_of_hbm": round(byt / (ms * 1e-3) / 1e9 / hbm_peak, 4)}
+    del imgs, proj
     return res
 
 
