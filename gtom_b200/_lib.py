@@ -77,6 +77,16 @@ SIGNATURES: dict[str, list] = {
     "gtomrln_kaiser_bessel_table": [_d, _d, _i, _i, _p],
     "gtomrln_ctf_simulate": [_p, _p, _p, _p, _u, _i, _i, _i, _p],
     "gtomrln_preprocess_particles": [_p, _i, _u, _p, _p, _p, _p],
+    "gtomrln_squared_differences_sparse": [_p, _p, _p, _i, _i, _i, _p, _p, _p, _p, _u, _u, _i, _p],
+    "gtomrln_squared_differences": [_p, _p, _p, _i, _i, _i, _u, _p, _u, _p, _u, _u, _p, _i, _p],
+    "gtomrln_convert_weights_dense": [_p, _u, _u, _u, _u, _p, _p, _p, _p],
+    "gtomrln_convert_weights_sparse": [_p, _p, _p, _u, _u, _u, _p, _p, _p, _p],
+    "gtomrln_convert_weights_sort": [_p, _u, _p],
+    "gtomrln_convert_weights_compact": [_p, _p, C.POINTER(C.c_uint), _p],
+    "gtomrln_diff_remap_dense": [_p, _p, _p, _u, _u, _u, _u, _u, _u, _u, _p, _p, _i, _p],
+    "gtomrln_diff_remap_sparse": [_p, _p, _p, _p, _p, _u, _u, _u, _u, _p, _p, _i, _p],
+    "gtomrln_create_minvsigma2s": [_p, _p, _u, _p, _f, _p],
+    "gtomrln_store_weights_add": [_p, _p, _p, _p, _p, _u, _u, _p, _f, _f, _p, _p, _p, _p, _p, _p, _p, _i, _p],
     "gtomrln_batch_create": [_p, _i, _i, _i, _p],
     "gtomrln_batch_set_tuning": [_p, _i, _i, _i],
     "gtomrln_batch_run": [_p, _i, _p],

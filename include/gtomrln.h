@@ -410,6 +410,88 @@ GTOMRLN_API int gtomrln_preprocess_particles(const float* d_images, int n, unsig
                                  float* d_projweights, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * RELION E-step consumers of the projections.  Complex arrays are
+ * interleaved float pairs; uint3 / uint4 arrays are 3 / 4 unsigned per item.
+ * ------------------------------------------------------------------------- */
+
+/* gtom::d_rlnSquaredDifferencesSparse(tcomplex* d_particleft, tfloat* d_minvsigma2,
+ *     tfloat* d_ctf, int3 dimsparticle, tcomplex* d_precalcshifts, tcomplex* d_refft,
+ *     tfloat* d_diff2, uint3* d_combination, uint ncombinations, uint groupsize,
+ *     bool dofirstitercc)
+ * include/Relion.cuh:48; the reference declares it but src/Relion/SquaredDifferences.cu
+ * is empty: defined here from GTOMTest/RelionSquaredDiff.cpp:55-69.  Combination k
+ * = (first shift, particle, first reference) covers groupsize x groupsize outputs
+ * d_diff2[k g^2 + r g + s] = 0.5 sum_i minvsigma2_i |ctf_i ref_{z+r,i} - part_i shift_{x+s,i}|^2
+ * (ctf of the particle y, elements per particle; NULL minvsigma2 / ctf = 1), or
+ * with dofirstitercc the negative cross-correlation normalised by the
+ * reference power.  ncombinations counts outputs; groupsize 1, 2, 4 or 8. */
+GTOMRLN_API int gtomrln_squared_differences_sparse(const float* d_particleft, const float* d_minvsigma2,
+                                       const float* d_ctf, int dx, int dy, int dz,
+                                       const float* d_precalcshifts, const float* d_refft,
+                                       float* d_diff2, const unsigned* d_combination,
+                                       unsigned ncombinations, unsigned groupsize,
+                                       int dofirstitercc, void* stream);
+
+/* gtom::d_rlnSquaredDifferences (include/Relion.cuh:46; no reference source,
+ * see above): every particle against every reference and shift,
+ * d_diff2[(particle * nrefs + ref) * nshifts + shift], tile 1, 2, 4 or 8. */
+GTOMRLN_API int gtomrln_squared_differences(const float* d_particleft, const float* d_minvsigma2,
+                                const float* d_ctf, int dx, int dy, int dz, unsigned nparticles,
+                                const float* d_precalcshifts, unsigned nshifts,
+                                const float* d_refft, unsigned nrefs, unsigned tile,
+                                float* d_diff2, int dofirstitercc, void* stream);
+
+/* gtom::d_rlnConvertWeightsDense — include/Relion.cuh:21, src/Relion/ConvertWeights.cu:12-44. */
+GTOMRLN_API int gtomrln_convert_weights_dense(float* d_weights, unsigned nparticles, unsigned nclasses,
+                                  unsigned nrot, unsigned ntrans, const float* d_pdfrot,
+                                  const float* d_pdftrans, const float* d_mindiff2, void* stream);
+
+/* gtom::d_rlnConvertWeightsSparse — include/Relion.cuh:22, ConvertWeights.cu:46-73. */
+GTOMRLN_API int gtomrln_convert_weights_sparse(float* d_weightsdense, float* d_weightssparse,
+                                   const unsigned* d_combinations, unsigned nsparse, unsigned nrot,
+                                   unsigned ntrans, const float* d_pdfrot, const float* d_pdftrans,
+                                   const float* d_mindiff2, void* stream);
+
+/* gtom::d_rlnConvertWeightsSort (ascending, in place) — include/Relion.cuh:23,
+ * ConvertWeights.cu:75-78. */
+GTOMRLN_API int gtomrln_convert_weights_sort(float* d_input, unsigned n, void* stream);
+
+/* gtom::d_rlnConvertWeightsCompact (the positive values, in order; *n in:
+ * input length, out: kept count; synchronises the stream) —
+ * include/Relion.cuh:24, ConvertWeights.cu:80-91. */
+GTOMRLN_API int gtomrln_convert_weights_compact(const float* d_input, float* d_output, unsigned* n,
+                                    void* stream);
+
+/* gtom::d_rlnDiffRemapDense — include/Relion.cuh:27, src/Relion/DiffRemap.cu:9-18, :30-51. */
+GTOMRLN_API int gtomrln_diff_remap_dense(const float* d_input, float* d_output,
+                             const unsigned* d_orientationindices, unsigned norientations,
+                             unsigned iclass, unsigned nparticles, unsigned nclasses, unsigned nrot,
+                             unsigned ntrans, unsigned ntranspadded, const float* d_xi2imgs,
+                             const float* d_sqrtxi2, int docc, void* stream);
+
+/* gtom::d_rlnDiffRemapSparse — include/Relion.cuh:28, DiffRemap.cu:20-28, :65-88
+ * (d_mindiff2 receives the per-particle minimum, min-combined with its contents;
+ * no limit on the particle count). */
+GTOMRLN_API int gtomrln_diff_remap_sparse(const float* d_input, float* d_output, float* d_mindiff2,
+                              const unsigned* d_combinations, const unsigned* d_hiddenover,
+                              unsigned elements, unsigned tileelements, unsigned weightsperpart,
+                              unsigned nparticles, const float* d_xi2imgs, const float* d_sqrtxi2,
+                              int docc, void* stream);
+
+/* gtom::d_rlnCreateMinvsigma2s — include/Relion.cuh:31, src/Relion/Misc.cu:12-29. */
+GTOMRLN_API int gtomrln_create_minvsigma2s(float* d_output, const int* d_mresol, unsigned elements,
+                               const float* d_sigma2noise, float sigma2fudge, void* stream);
+
+/* gtom::d_rlnStoreWeightsAdd — include/Relion.cuh:51-57, src/Relion/StoreWeights.cu:9-63. */
+GTOMRLN_API int gtomrln_store_weights_add(const float* d_input, const float* d_ctf, const float* d_ref,
+                              const float* d_minvsigma2, const int* d_mresol, unsigned elements,
+                              unsigned ntrans, const float* d_weights, float sigweight,
+                              float sumweight, float* d_output, float* d_outputweights,
+                              float* d_sigma2noise, float* d_normcorrection,
+                              const float* d_priorclass, float* d_correctionxa,
+                              float* d_correctionaa, int doscale, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Batched reconstruction of many volumes of uneven box size (no reference
  * counterpart; the reference batches equal boxes only, through d_ivolume of
  * d_rlnBackproject, src/Relion/Backproject.cu:48-124).  Per subvolume the

@@ -103,6 +103,60 @@ int ref_ctf_simulate(float* h_params, float* d_addresses, float* d_gammacorrecti
   return (int)cudaGetLastError();
 }
 
+// include/Relion.cuh:21-24 -> src/Relion/ConvertWeights.cu
+int ref_convert_weights_dense(float* d_weights, int nparticles, int nclasses, int nrot, int ntrans,
+                              float* d_pdfrot, float* d_pdftrans, float* d_mindiff2) {
+  d_rlnConvertWeightsDense(d_weights, nparticles, nclasses, nrot, ntrans, d_pdfrot, d_pdftrans, d_mindiff2);
+  cudaDeviceSynchronize();
+  return (int)cudaGetLastError();
+}
+
+int ref_convert_weights_sparse(float* d_dense, float* d_sparse, unsigned* d_combinations, int nsparse, int nrot,
+                               int ntrans, float* d_pdfrot, float* d_pdftrans, float* d_mindiff2) {
+  d_rlnConvertWeightsSparse(d_dense, d_sparse, (uint4*)d_combinations, nsparse, nrot, ntrans, d_pdfrot, d_pdftrans,
+                            d_mindiff2);
+  cudaDeviceSynchronize();
+  return (int)cudaGetLastError();
+}
+
+// include/Relion.cuh:27-28 -> src/Relion/DiffRemap.cu
+int ref_diff_remap_dense(float* d_input, float* d_output, unsigned* d_orient, int norient, int iclass,
+                         int nparticles, int nclasses, int nrot, int ntrans, int ntranspadded, float* d_xi2,
+                         float* d_sqrtxi2, int docc) {
+  d_rlnDiffRemapDense(d_input, d_output, (uint3*)d_orient, norient, iclass, nparticles, nclasses, nrot, ntrans,
+                      ntranspadded, d_xi2, d_sqrtxi2, docc != 0);
+  cudaDeviceSynchronize();
+  return (int)cudaGetLastError();
+}
+
+int ref_diff_remap_sparse(float* d_input, float* d_output, float* d_mindiff2, unsigned* d_combinations,
+                          unsigned* d_hiddenover, int elements, int tileelements, int weightsperpart,
+                          int nparticles, float* d_xi2, float* d_sqrtxi2, int docc) {
+  d_rlnDiffRemapSparse(d_input, d_output, d_mindiff2, (uint3*)d_combinations, d_hiddenover, elements, tileelements,
+                       weightsperpart, nparticles, d_xi2, d_sqrtxi2, docc != 0);
+  cudaDeviceSynchronize();
+  return (int)cudaGetLastError();
+}
+
+// include/Relion.cuh:31 -> src/Relion/Misc.cu:12-17
+int ref_create_minvsigma2s(float* d_output, int* d_mresol, int elements, float* d_sigma2noise, float fudge) {
+  d_rlnCreateMinvsigma2s(d_output, d_mresol, elements, d_sigma2noise, fudge);
+  cudaDeviceSynchronize();
+  return (int)cudaGetLastError();
+}
+
+// include/Relion.cuh:51-57 -> src/Relion/StoreWeights.cu:9-18
+int ref_store_weights_add(float* d_input, float* d_ctf, float* d_ref, float* d_minvsigma2, int* d_mresol,
+                          int elements, int ntrans, float* d_weights, float sigweight, float sumweight,
+                          float* d_output, float* d_outputweights, float* d_sigma2noise, float* d_normcorrection,
+                          float* d_priorclass, float* d_correctionxa, float* d_correctionaa, int doscale) {
+  d_rlnStoreWeightsAdd((tcomplex*)d_input, d_ctf, (tcomplex*)d_ref, d_minvsigma2, d_mresol, elements, ntrans,
+                       d_weights, sigweight, sumweight, (tcomplex*)d_output, d_outputweights, d_sigma2noise,
+                       d_normcorrection, d_priorclass, d_correctionxa, d_correctionaa, doscale != 0);
+  cudaDeviceSynchronize();
+  return (int)cudaGetLastError();
+}
+
 // include/Reconstruction.cuh:16 -> src/Reconstruction/RecFourier.cu:98-241
 int ref_reconstruct_gridding(float* d_dataft, float* d_weight, float* d_reconstructed, int ori,
                              int padded, int paddingfactor, int iterations, double blobradius,

@@ -39,6 +39,12 @@ REF.ref_reconstruct_gridding.argtypes = [_p, _p, _p, _i, _i, _i, _i, _d, _i, _d]
 REF.ref_project_shifted.argtypes = [_p, _i, _p, _i, _i, _i, _p, _p, _p, _i]
 REF.ref_backproject_shifted.argtypes = [_p, _p, _i, _p, _p, _i, _i, _i, _p, _p, _p, _i]
 REF.ref_ctf_simulate.argtypes = [_p, _p, _p, _p, _i, _i, _i, _i]
+REF.ref_convert_weights_dense.argtypes = [_p, _i, _i, _i, _i, _p, _p, _p]
+REF.ref_convert_weights_sparse.argtypes = [_p, _p, _p, _i, _i, _i, _p, _p, _p]
+REF.ref_diff_remap_dense.argtypes = [_p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _p, _p, _i]
+REF.ref_diff_remap_sparse.argtypes = [_p, _p, _p, _p, _p, _i, _i, _i, _i, _p, _p, _i]
+REF.ref_create_minvsigma2s.argtypes = [_p, _p, _i, _p, _f]
+REF.ref_store_weights_add.argtypes = [_p, _p, _p, _p, _p, _i, _i, _p, _f, _f, _p, _p, _p, _p, _p, _p, _p, _i]
 
 
 def _ok(rc: int, what: str) -> None:
@@ -219,8 +225,114 @@ def gen_ctf(out: Path, rng) -> None:
     print("ctf_simulate", {k: float(np.abs(v).max()) for k, v in res.items()})
 
 
+def gen_estep(out: Path, rng) -> None:
+    """The reference's E-step consumers on random inputs.  Every device
+    buffer handed to the reference is held in `keep` until the calls are
+    done (a temporary's memory would go back to torch's allocator and be
+    reused by the next argument)."""
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    keep = []
+
+    def D(a) -> int:
+        t = dev(a)
+        keep.append(t)
+        return t.data_ptr()
+
+    res = {}
+    # ConvertWeightsDense
+    npart, ncls, nrot, ntr = 3, 2, 20, 7
+    w = f32(rng.uniform(0, 5, npart * ncls * nrot * ntr))
+    pr, pt, md = f32(rng.uniform(0, 1, ncls * nrot)), f32(rng.uniform(0, 1, npart * ncls * ntr)), f32(rng.uniform(0, 1, npart))
+    dw = dev(w)
+    _ok(REF.ref_convert_weights_dense(dw.data_ptr(), npart, ncls, nrot, ntr, D(pr), D(pt),
+                                      D(md)), "convert dense")
+    res.update(cd_in=w, cd_pdfrot=pr, cd_pdftrans=pt, cd_mindiff2=md, cd_out=host(dw, np.float32, w.size),
+               cd_shape=np.array([npart, ncls, nrot, ntr]))
+    # ConvertWeightsSparse
+    nsp, ndense = 100, 500
+    comb = np.stack([rng.integers(0, ncls, nsp), rng.integers(0, nrot, nsp), rng.integers(0, ntr, nsp),
+                     rng.permutation(ndense)[:nsp]], 1).astype(np.uint32)
+    dense = f32(rng.uniform(0, 5, ndense))
+    pt2 = f32(rng.uniform(0, 1, ncls * ntr))
+    md1 = f32([0.5])
+    dd, dsp = dev(dense), torch.zeros(nsp * 4, dtype=torch.uint8, device="cuda")
+    _ok(REF.ref_convert_weights_sparse(dd.data_ptr(), dsp.data_ptr(), D(comb), nsp, nrot, ntr,
+                                       D(pr), D(pt2), D(md1)), "convert sparse")
+    res.update(cs_dense=dense, cs_comb=comb, cs_pdftrans=pt2, cs_mindiff2=md1, cs_out_dense=host(dd, np.float32, ndense),
+               cs_out_sparse=host(dsp, np.float32, nsp))
+    # DiffRemapDense, both modes
+    norient, iclass, nrot2, ntr2, ntp = 10, 1, 12, 5, 8
+    orient = np.stack([np.zeros(norient), rng.permutation(nrot2)[:norient], np.zeros(norient)], 1).astype(np.uint32)
+    inp = f32(rng.uniform(0, 5, norient * npart * ntp))
+    xi2, sq = f32(rng.uniform(1, 2, npart)), f32(rng.uniform(0.5, 1, npart))
+    for cc in (0, 1):
+        o0 = f32(rng.uniform(0, 1, npart * ncls * nrot2 * ntr2))
+        do = dev(o0)
+        _ok(REF.ref_diff_remap_dense(D(inp), do.data_ptr(), D(orient), norient, iclass, npart,
+                                     ncls, nrot2, ntr2, ntp, D(xi2), D(sq), cc), "remap dense")
+        res[f"rd_out0_cc{cc}"] = o0
+        res[f"rd_out_cc{cc}"] = host(do, np.float32, o0.size)
+    res.update(rd_in=inp, rd_orient=orient, rd_xi2=xi2, rd_sqrtxi2=sq,
+               rd_shape=np.array([norient, iclass, npart, ncls, nrot2, ntr2, ntp]))
+    # DiffRemapSparse, both modes
+    nel, tile, wpp = 208, 16, 256
+    combs = np.stack([np.zeros(nel // tile), rng.integers(0, npart, nel // tile), np.zeros(nel // tile)], 1).astype(np.uint32)
+    # hidden indices unique within each particle (the reference writes them without ordering)
+    perms, used = [rng.permutation(wpp) for _ in range(npart)], [0] * npart
+    hid = []
+    for c in combs:
+        p_ = int(c[1])
+        hid.append(perms[p_][used[p_]:used[p_] + tile])
+        used[p_] += tile
+    hid = np.concatenate(hid).astype(np.uint32)
+    inp2 = f32(rng.uniform(-1, 5, nel))
+    for cc in (0, 1):
+        o0 = f32(np.zeros(npart * wpp))
+        m0 = f32(np.full(npart, 1e30))
+        do, dm = dev(o0), dev(m0)
+        _ok(REF.ref_diff_remap_sparse(D(inp2), do.data_ptr(), dm.data_ptr(), D(combs),
+                                      D(hid), nel, tile, wpp, npart, D(xi2), D(sq),
+                                      cc), "remap sparse")
+        res[f"rs_out_cc{cc}"] = host(do, np.float32, o0.size)
+        res[f"rs_min_cc{cc}"] = host(dm, np.float32, npart)
+    res.update(rs_in=inp2, rs_comb=combs, rs_hidden=hid, rs_shape=np.array([nel, tile, wpp, npart]))
+    # CreateMinvsigma2s
+    nm = 500
+    mres = rng.integers(-1, 21, nm).astype(np.int32)
+    s2 = f32(rng.uniform(0.5, 2, 21))
+    dmo = torch.zeros(nm * 4, dtype=torch.uint8, device="cuda")
+    _ok(REF.ref_create_minvsigma2s(dmo.data_ptr(), D(mres), nm, D(s2), 1.3), "minvsigma2s")
+    res.update(mv_mresol=mres, mv_sigma2=s2, mv_out=host(dmo, np.float32, nm))
+    # StoreWeightsAdd, both modes
+    ne, nt = 300, 4
+    inp3 = (rng.normal(size=(nt, ne)) + 1j * rng.normal(size=(nt, ne))).astype(np.complex64)
+    ctf = f32(rng.uniform(-1, 1, ne))
+    ref = (rng.normal(size=ne) + 1j * rng.normal(size=ne)).astype(np.complex64)
+    mv = f32(rng.uniform(0.1, 1, ne))
+    mr = rng.integers(-1, 16, ne).astype(np.int32)
+    wts = f32([0.3, 0.0001, 0.5, 0.2])
+    prior = f32(rng.uniform(0, 6, 16))
+    res.update(sw_in=inp3, sw_ctf=ctf, sw_ref=ref, sw_minvsigma2=mv, sw_mresol=mr, sw_weights=wts, sw_prior=prior)
+    for sc in (0, 1):
+        o0 = (rng.normal(size=(nt, ne)) + 1j * rng.normal(size=(nt, ne))).astype(np.complex64)
+        ow0 = f32(rng.uniform(0, 1, (nt, ne)))
+        s20, nc0, xa0, aa0 = f32(rng.uniform(0, 1, 16)), f32([0.25]), f32(rng.uniform(0, 1, 16)), f32(rng.uniform(0, 1, 16))
+        do, dow, ds2, dnc, dxa, daa = dev(o0), dev(ow0), dev(s20), dev(nc0), dev(xa0), dev(aa0)
+        _ok(REF.ref_store_weights_add(D(inp3), D(ctf), D(ref), D(mv),
+                                      D(mr), ne, nt, D(wts), 0.001, 1.7, do.data_ptr(),
+                                      dow.data_ptr(), ds2.data_ptr(), dnc.data_ptr(), D(prior),
+                                      dxa.data_ptr(), daa.data_ptr(), sc), "store weights")
+        res.update({f"sw{sc}_out0": o0, f"sw{sc}_ow0": ow0, f"sw{sc}_s20": s20, f"sw{sc}_nc0": nc0,
+                    f"sw{sc}_xa0": xa0, f"sw{sc}_aa0": aa0,
+                    f"sw{sc}_out": host(do, np.complex64, nt * ne), f"sw{sc}_ow": host(dow, np.float32, nt * ne),
+                    f"sw{sc}_s2": host(ds2, np.float32, 16), f"sw{sc}_nc": host(dnc, np.float32, 1),
+                    f"sw{sc}_xa": host(dxa, np.float32, 16), f"sw{sc}_aa": host(daa, np.float32, 16)})
+    np.savez_compressed(out / "estep.npz", **res)
+    print("estep", len(res), "arrays")
+
+
 def main() -> None:
-    """make_golden.py [outdir] [--only project|backproject|gridding|shifted|ctf ...]"""
+    """make_golden.py [outdir] [--only project|backproject|gridding|shifted|ctf|estep ...]"""
     args = sys.argv[1:]
     only = set(args[args.index("--only") + 1:]) if "--only" in args else None
     args = args[:args.index("--only")] if "--only" in args else args
@@ -234,6 +346,8 @@ def main() -> None:
         gen_shifted(out, np.random.default_rng(20261204))
     if only is None or "ctf" in only:
         gen_ctf(out, np.random.default_rng(20261205))
+    if only is None or "estep" in only:
+        gen_estep(out, np.random.default_rng(20261206))
 
 
 if __name__ == "__main__":
