@@ -4,6 +4,7 @@ d_ReconstructGridding.  The compute lives in libgtomrln.so (CUDA, sm_100a);
 this package binds its C ABI."""
 from ._lib import GtomError, GtomLibraryMissing  # noqa: F401
 from .relion import (  # noqa: F401
+    d_BackprojectTomo,
     d_ReconstructGridding,
     d_rlnBackproject,
     d_rlnBackprojectShifted,

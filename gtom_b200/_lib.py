@@ -58,6 +58,8 @@ SIGNATURES: dict[str, list] = {
                             _f, _f, _f, _f, _f, _i, _i, _u, _p],
     "gtomrln_backproject_angles": [_p, _p, _i, _i, _i, _p, _p, _i, _i, _i, _u, _p, _p,
                                    _f, _f, _f, _f, _f, _f, _i, _i, _u, _p],
+    "gtomrln_backproject_tomo": [_p, _i, _i, _i, _p, _p, _i, _i, _i, _u, _p, _u, _p],
+    "gtomrln_backproject_tomo_angles": [_p, _i, _i, _i, _p, _p, _i, _i, _i, _u, _p, _u, _p],
     "gtomrln_project_shifted": [_p, _i, _i, _i, _p, _i, _i, _i, _u, _p, _p, _p, _u, _p],
     "gtomrln_project_shifted_angles": [_p, _i, _i, _i, _p, _i, _i, _i, _p, _p, _p, _f, _u, _p],
     "gtomrln_project_shifted_tex": [_ull, _ull, _i, _i, _i, _p, _i, _i, _i, _u, _p, _p, _p, _u, _p],

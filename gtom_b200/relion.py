@@ -192,6 +192,26 @@ def d_rlnBackprojectShifted(volumeft, volumeweights, dimsvolume: Dims, projft, p
                   _dev_ptr(args[2], "d_globalweights", torch.float32, batch), batch, s)
 
 
+def d_BackprojectTomo(volumeft, dimsvolume: Dims, projft, projweights, dimsproj: Dims, rmax: int, angles_or_matrices,
+                      batch: int, stream=None) -> None:
+    """Lanczos-5 gather insertion for tomograms (include/Relion.cuh:13-14):
+    host Euler angles (BackprojectTomo.cu:11-28) or device matrices
+    (:30-46)."""
+    vx, vy, vz = (int(v) for v in dimsvolume)
+    px, py, pz = (int(v) for v in dimsproj)
+    batch = int(batch)
+    e = elements_fft((px, py, pz)) * batch
+    common = (_dev_ptr(volumeft, "d_volumeft", torch.complex64, elements_fft((vx, vy, vz))), vx, vy, vz,
+              _dev_ptr(projft, "d_projft", torch.complex64, e), _dev_ptr(projweights, "d_projweights", torch.float32, e),
+              px, py, pz, int(rmax))
+    if _is_host(angles_or_matrices):
+        ang = _host_f32(angles_or_matrices, "h_angles", 3 * batch)
+        _lib.call("gtomrln_backproject_tomo_angles", *common, ang.ctypes.data, batch, _stream(stream))
+    else:
+        _lib.call("gtomrln_backproject_tomo", *common,
+                  _dev_ptr(angles_or_matrices, "d_matrices", torch.float32, 9 * batch), batch, _stream(stream))
+
+
 def d_rlnBackproject(volumeft, volumeweights, dimsvolume: Dims, projft, projweights,
                      dimsproj: Dims, rmax: int, *args, stream=None) -> None:
     """Trilinear scatter-insert, accumulating in place (include/Relion.cuh:9-10).

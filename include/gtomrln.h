@@ -185,6 +185,25 @@ GTOMRLN_API int gtomrln_backproject_angles(float* d_volumeft, float* d_volumewei
                                int outputdecentered, int squareinterpweights, unsigned batch,
                                void* stream);
 
+/* gtom::d_BackprojectTomo(tcomplex* d_volumeft, int3 dimsvolume, tcomplex* d_projft,
+ *     tfloat* d_projweights, int3 dimsproj, uint rmax, glm::mat3* d_matrices, uint batch)
+ * include/Relion.cuh:14, src/Relion/BackprojectTomo.cu:30-46, kernel :48-153: a gather
+ * with a Lanczos-5 kernel instead of a scatter; every voxel of the decentred
+ * half volume inside rmax with kernel weight sum above 1e-3 is overwritten
+ * with sum(w v) / sum(w weight) times the clamped weight sum.  The volume
+ * must be cubic; d_projweights is required (the reference reads it). */
+GTOMRLN_API int gtomrln_backproject_tomo(float* d_volumeft, int vx, int vy, int vz, const float* d_projft,
+                             const float* d_projweights, int px, int py, int pz, unsigned rmax,
+                             const float* d_matrices, unsigned batch, void* stream);
+
+/* gtom::d_BackprojectTomo(..., uint rmax, tfloat3* h_angles, uint batch)
+ * include/Relion.cuh:13, src/Relion/BackprojectTomo.cu:11-28 (matrices
+ * transpose(Euler), no supersampling). */
+GTOMRLN_API int gtomrln_backproject_tomo_angles(float* d_volumeft, int vx, int vy, int vz,
+                                    const float* d_projft, const float* d_projweights, int px,
+                                    int py, int pz, unsigned rmax, const float* h_angles,
+                                    unsigned batch, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Shifted projector / backprojector: the slices are multiplied by the phase
  * exp(-i (x sx + y sy [+ z sz])) of a per-slice shift and by a per-slice

@@ -103,6 +103,15 @@ int ref_ctf_simulate(float* h_params, float* d_addresses, float* d_gammacorrecti
   return (int)cudaGetLastError();
 }
 
+// include/Relion.cuh:14 -> src/Relion/BackprojectTomo.cu:30-46
+int ref_backproject_tomo(float* d_volumeft, int V, float* d_projft, float* d_projweights, int n, int rmax,
+                         float* d_matrices, int batch) {
+  d_BackprojectTomo((tcomplex*)d_volumeft, toInt3(V, V, V), (tcomplex*)d_projft, d_projweights, toInt3(n, n, 1),
+                    (uint)rmax, (glm::mat3*)d_matrices, (uint)batch);
+  cudaDeviceSynchronize();
+  return (int)cudaGetLastError();
+}
+
 // include/Relion.cuh:21-24 -> src/Relion/ConvertWeights.cu
 int ref_convert_weights_dense(float* d_weights, int nparticles, int nclasses, int nrot, int ntrans,
                               float* d_pdfrot, float* d_pdftrans, float* d_mindiff2) {

@@ -40,6 +40,7 @@ REF.ref_project_shifted.argtypes = [_p, _i, _p, _i, _i, _i, _p, _p, _p, _i]
 REF.ref_backproject_shifted.argtypes = [_p, _p, _i, _p, _p, _i, _i, _i, _p, _p, _p, _i]
 REF.ref_ctf_simulate.argtypes = [_p, _p, _p, _p, _i, _i, _i, _i]
 REF.ref_convert_weights_dense.argtypes = [_p, _i, _i, _i, _i, _p, _p, _p]
+REF.ref_backproject_tomo.argtypes = [_p, _i, _p, _p, _i, _i, _p, _i]
 REF.ref_convert_weights_sparse.argtypes = [_p, _p, _p, _i, _i, _i, _p, _p, _p]
 REF.ref_diff_remap_dense.argtypes = [_p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _p, _p, _i]
 REF.ref_diff_remap_sparse.argtypes = [_p, _p, _p, _p, _p, _i, _i, _i, _i, _p, _p, _i]
@@ -331,8 +332,30 @@ def gen_estep(out: Path, rng) -> None:
     print("estep", len(res), "arrays")
 
 
+def gen_tomo(out: Path, rng) -> None:
+    """d_BackprojectTomo: a 16^3 half volume from 7 tilted 16^2 slices (a
+    tilt series about y under a random rotation), volume pre-filled so that
+    the voxels it leaves alone are visible."""
+    from tests.synthdata import random_angles
+    V, n, batch, rmax = 16, 16, 7, 7
+    base = random_angles(rng, 1)[0]
+    ang = np.array([[base[0], base[1] + t, base[2]] for t in np.deg2rad(np.linspace(-45, 45, batch))], np.float32)
+    mats = O.matrices_f64(ang, 1.0).astype(np.float32)
+    e = O.elements_fft(n)
+    projft = (rng.normal(size=(batch, e)) + 1j * rng.normal(size=(batch, e))).astype(np.complex64)
+    projw = rng.uniform(0.5, 1.0, size=(batch, e)).astype(np.float32)
+    nv = (V // 2 + 1) * V * V
+    vol0 = np.full(nv, 7 + 7j, np.complex64)
+    dv, dpf, dpw, dm = dev(vol0), dev(projft), dev(projw), dev(mats)
+    _ok(REF.ref_backproject_tomo(dv.data_ptr(), V, dpf.data_ptr(), dpw.data_ptr(), n, rmax, dm.data_ptr(), batch),
+        "tomo")
+    np.savez_compressed(out / "bp_tomo.npz", V=V, n=n, rmax=rmax, angles=ang, matrices=mats, projft=projft,
+                        projw=projw, volume0=vol0, volume=host(dv, np.complex64, nv))
+    print("bp_tomo", np.abs(host(dv, np.complex64, nv)).max())
+
+
 def main() -> None:
-    """make_golden.py [outdir] [--only project|backproject|gridding|shifted|ctf|estep ...]"""
+    """make_golden.py [outdir] [--only project|backproject|gridding|shifted|ctf|estep|tomo ...]"""
     args = sys.argv[1:]
     only = set(args[args.index("--only") + 1:]) if "--only" in args else None
     args = args[:args.index("--only")] if "--only" in args else args
@@ -348,6 +371,8 @@ def main() -> None:
         gen_ctf(out, np.random.default_rng(20261205))
     if only is None or "estep" in only:
         gen_estep(out, np.random.default_rng(20261206))
+    if only is None or "tomo" in only:
+        gen_tomo(out, np.random.default_rng(20261207))
 
 
 if __name__ == "__main__":
