@@ -55,6 +55,8 @@ def parse_args():
     ap.add_argument("--batch", type=int, default=10000, help="particles per step")
     ap.add_argument("--pool", type=int, default=40000, help="distinct particles resident on the GPU")
     ap.add_argument("--e2e-batch", type=int, default=2000)
+    ap.add_argument("--path", default="auto", choices=["auto", "direct", "brick", "segment"],
+                    help="implementation of the projector and backprojector (gtomrln_set_path)")
     ap.add_argument("--no-gridding", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip gridding, e2e, CPU baseline and L2 probes (profiling runs)")
@@ -86,19 +88,36 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def nvml_init() -> bool:
+    """Initialises NVML once, before any timed work (its start-up must not
+    fall into a timed region)."""
+    try:
+        import pynvml
+        pynvml.nvmlInit()
+        return True
+    except Exception:
+        return False
+
+
 class ClockSampler:
-    """Samples SM clock and throttle reasons during the timed region."""
+    """Samples SM clock and throttle reasons during the timed region.
+
+    The sampling thread starts before the warm-up (start()) so that NVML's
+    first queries, which can stall the GPU for milliseconds to hundreds of
+    milliseconds, fall outside the timed region; samples are kept only
+    while recording (between begin() and end(), around the timed steps)."""
 
     def __init__(self, index: int, period: float = 0.02):
         self.index, self.period = index, period
         self.samples, self.reasons, self.max_mhz = [], set(), None
         self._stop = threading.Event()
+        self._recording = threading.Event()
         self._t = None
 
-    def __enter__(self):
+    def start(self) -> "ClockSampler":
         try:
             import pynvml
-            pynvml.nvmlInit()
+            nvml_init()
             h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
             self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
             names = {
@@ -112,11 +131,13 @@ class ClockSampler:
             def run():
                 while not self._stop.is_set():
                     try:
-                        self.samples.append(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                        mhz = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
                         r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
-                        for k, bit in names.items():
-                            if r & bit:
-                                self.reasons.add(k)
+                        if self._recording.is_set():
+                            self.samples.append(mhz)
+                            for k, bit in names.items():
+                                if r & bit:
+                                    self.reasons.add(k)
                     except Exception:
                         pass
                     self._stop.wait(self.period)
@@ -127,7 +148,14 @@ class ClockSampler:
             self._t = None
         return self
 
-    def __exit__(self, *a):
+    def begin(self) -> None:
+        self._recording.set()
+
+    def end(self) -> None:
+        self._recording.clear()
+
+    def stop(self) -> None:
+        self._recording.clear()
         self._stop.set()
         if self._t:
             self._t.join(timeout=2)
@@ -198,6 +226,8 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
 
+    G.set_path("project", args.path)
+    G.set_path("backproject", args.path)
     B = args.batch
     if args.pool % B:
         args.pool = (args.pool // B + 1) * B
@@ -226,6 +256,7 @@ def run_ours(args):
             c.record(stream)
             ev.append((a, b, c))
 
+    clocks = ClockSampler(local).start()
     for i in range(args.warmup):
         step(i, False)
     acc.zero_()
@@ -233,14 +264,15 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        torch.cuda.synchronize()
-        start.record(stream)
-        for k in range(args.steps):
-            step(args.warmup + k, True)
-        acc.all_reduce()  # the one exchange: sum the partial volumes of all ranks
-        end.record(stream)
-        torch.cuda.synchronize()
+    clocks.begin()
+    torch.cuda.synchronize()
+    start.record(stream)
+    for k in range(args.steps):
+        step(args.warmup + k, True)
+    acc.all_reduce()  # the one exchange: sum the partial volumes of all ranks
+    end.record(stream)
+    torch.cuda.synchronize()
+    clocks.stop()
     if world > 1:
         dist.barrier()
     ms = start.elapsed_time(end)

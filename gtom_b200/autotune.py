@@ -58,7 +58,7 @@ def tune(op: str, run: Callable[[], None], cands=None, reps: int = 3) -> dict:
     """Times `run` (one call of the op) under every candidate launch shape and
     installs the fastest.  Returns {"best": (edge, threads, chunk), "ms": ...,
     "table": [(edge, threads, chunk, ms), ...]}."""
-    set_path(op, "brick")
+    set_path(op, "segment")  # the default brick-major variant
     table = []
     try:
         for e, t, c in (cands or candidates(op)):

@@ -91,6 +91,102 @@ int pool_free(void* ptr, cudaStream_t stream) {
   return GTOMRLN_OK;
 }
 
+// Per-(device, stream) scratch that outlives a call: the brick plans take it
+// instead of a pool allocation, so that repeated calls allocate nothing.  A
+// pool allocation that has to map new memory blocks the host for
+// milliseconds (observed 5-45 ms for ~700 MB after a device synchronisation
+// had regrouped the pool's free blocks), while the device drains the queue
+// and idles.  A slot grows (by 1/8 plus rounding to 64 MB) and never shrinks
+// until gtomrln_release_caches().  Calls on the same stream reuse it in
+// stream order; an event recorded at release and waited for at the next
+// acquisition covers a stream handle that was destroyed and handed out
+// again.  Under stream capture, or while the slot is held by another host
+// thread, a plain pool allocation is used.
+namespace {
+struct ScratchSlot {
+  int dev;
+  cudaStream_t stream;
+  void* ptr;
+  size_t bytes;
+  bool busy;
+  cudaEvent_t done;
+};
+std::mutex g_scratch_mutex;
+std::vector<ScratchSlot> g_scratch;
+}  // namespace
+
+int scratch_alloc(void** ptr, size_t bytes, cudaStream_t stream) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    cs = cudaStreamCaptureStatusActive;
+  }
+  if (cs != cudaStreamCaptureStatusNone) return pool_alloc(ptr, bytes, stream);
+  int dev = 0;
+  GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  ScratchSlot* slot = nullptr;
+  for (auto& s : g_scratch)
+    if (s.dev == dev && s.stream == stream) slot = &s;
+  if (!slot) {
+    cudaEvent_t ev;
+    GTOMRLN_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    g_scratch.push_back({dev, stream, nullptr, 0, false, ev});
+    slot = &g_scratch.back();
+  }
+  if (slot->busy) return pool_alloc(ptr, bytes, stream);
+  GTOMRLN_CUDA_TRY(cudaStreamWaitEvent(stream, slot->done, 0));
+  if (slot->bytes < bytes) {
+    if (slot->ptr) {
+      int st = pool_free(slot->ptr, stream);
+      slot->ptr = nullptr;
+      slot->bytes = 0;
+      if (st) return st;
+    }
+    const size_t grain = (size_t)64 << 20;
+    const size_t want = (bytes + bytes / 8 + grain - 1) / grain * grain;
+    int st = pool_alloc(&slot->ptr, want, stream);
+    if (st) return st;
+    slot->bytes = want;
+  }
+  slot->busy = true;
+  *ptr = slot->ptr;
+  return GTOMRLN_OK;
+}
+
+int scratch_free(void* ptr, cudaStream_t stream) {
+  if (!ptr) return GTOMRLN_OK;
+  {
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    for (auto& s : g_scratch)
+      if (s.busy && s.ptr == ptr) {
+        s.busy = false;
+        GTOMRLN_CUDA_TRY(cudaEventRecord(s.done, stream));
+        return GTOMRLN_OK;
+      }
+  }
+  return pool_free(ptr, stream);
+}
+
+// Frees the idle scratch slots of device dev (after a device synchronisation).
+static int release_scratch(int dev) {
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  std::vector<ScratchSlot> keep;
+  for (auto& s : g_scratch) {
+    if (s.dev != dev || s.busy) {
+      keep.push_back(s);
+      continue;
+    }
+    if (s.ptr) {
+      GTOMRLN_CUDA_TRY(cudaFreeAsync(s.ptr, 0));
+      GTOMRLN_CUDA_TRY(cudaStreamSynchronize(0));
+    }
+    GTOMRLN_CUDA_TRY(cudaEventDestroy(s.done));
+  }
+  g_scratch.swap(keep);
+  return GTOMRLN_OK;
+}
+
 int release_gridding_plans();  // gridding.cu
 int release_ctf_plans();       // ctf.cu
 
@@ -126,18 +222,18 @@ int gtomrln_release_caches(void) {
   if (st) return st;
   int dev = 0;
   GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  GTOMRLN_CUDA_TRY(cudaDeviceSynchronize());
+  st = release_scratch(dev);
+  if (st) return st;
   std::lock_guard<std::mutex> lock(g_pool_mutex);
-  if ((int)g_pools.size() > dev && g_pools[dev]) {
-    GTOMRLN_CUDA_TRY(cudaDeviceSynchronize());
-    GTOMRLN_CUDA_TRY(cudaMemPoolTrimTo(g_pools[dev], 0));
-  }
+  if ((int)g_pools.size() > dev && g_pools[dev]) GTOMRLN_CUDA_TRY(cudaMemPoolTrimTo(g_pools[dev], 0));
   return GTOMRLN_OK;
 }
 
 int gtomrln_set_path(int op, int path) {
   clear_error();
   if ((op != GTOMRLN_OP_PROJECT && op != GTOMRLN_OP_BACKPROJECT) || path < GTOMRLN_PATH_AUTO ||
-      path > GTOMRLN_PATH_BRICK)
+      path > GTOMRLN_PATH_SEGMENT)
     return set_error(GTOMRLN_ERR_INVALID, "set_path: unknown op %d or path %d", op, path);
   g_path[op].store(path);
   return GTOMRLN_OK;

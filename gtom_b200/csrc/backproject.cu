@@ -14,6 +14,7 @@
 #include "brick.cuh"
 #include "common.cuh"
 #include "sample.cuh"
+#include "segment.cuh"
 
 namespace gtomrln {
 
@@ -158,6 +159,47 @@ backproject_direct_kernel(float2* __restrict__ volft_base, float* __restrict__ v
 // ---------------------------------------------------------------------------
 constexpr unsigned kBrickMinBatch = 32;
 
+// Adds a brick's shared-memory accumulators to the volume: plain
+// read-add-write when the work item is the brick's only one and the voxel has
+// no alias (decentred y or z = +-V/2 share storage), else vector L2
+// reductions.  Voxels that received nothing are skipped.
+template <bool DECENTERED>
+__device__ __forceinline__ void bp_flush_brick(float2* __restrict__ volft, float* __restrict__ volw,
+                                               const float* are, const float* aim, const float* aw, int B,
+                                               int RS, int PS, int3 o, int V, int rowlen, bool exclusive) {
+  for (int e = threadIdx.x; e < B * B * B; e += blockDim.x) {
+    int lx = e % B, t = e / B, ly = t % B, lz = t / B;
+    int k = lz * PS + ly * RS + lx;
+    float r = are[k], im = aim[k], ww = aw[k];
+    if (r == 0.f && im == 0.f && ww == 0.f) continue;
+    int x = o.x + lx, y = o.y + ly, z = o.z + lz;
+    int ys, zs;
+    bool alias;
+    if (DECENTERED) {
+      ys = y < 0 ? y + V : y;
+      zs = z < 0 ? z + V : z;
+      alias = (y == V / 2 || y == -(V / 2) || z == V / 2 || z == -(V / 2));
+    } else {
+      ys = y + V / 2;
+      zs = z + V / 2;
+      alias = false;
+    }
+    if ((unsigned)x > (unsigned)(V / 2) || (unsigned)ys >= (unsigned)V || (unsigned)zs >= (unsigned)V)
+      continue;  // outside the volume: nothing can have been added here
+    int64_t idx = ((int64_t)zs * V + ys) * rowlen + x;
+    if (exclusive && !alias) {
+      if (volft) {
+        float2 c = volft[idx];
+        volft[idx] = make_float2(c.x + r, c.y + im);
+      }
+      if (volw) volw[idx] += ww;
+    } else {
+      if (volft) red_add2((float*)(volft + idx), r, im);
+      if (volw) red_add(volw + idx, ww);
+    }
+  }
+}
+
 template <bool DECENTERED, bool SQUARE>
 __global__ void __launch_bounds__(1024)
 backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
@@ -249,38 +291,130 @@ backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
     __syncthreads();
 
     // flush the brick into the volume
-    const int rowlen = a.rowlen;
-    for (int e = threadIdx.x; e < B * B * B; e += blockDim.x) {
-      int lx = e % B, t = e / B, ly = t % B, lz = t / B;
-      int k = lz * PS + ly * RS + lx;
-      float r = are[k], im = aim[k], ww = aw[k];
-      if (r == 0.f && im == 0.f && ww == 0.f) continue;
-      int x = o.x + lx, y = o.y + ly, z = o.z + lz;
-      int ys, zs;
-      bool alias;
-      if (DECENTERED) {
-        ys = y < 0 ? y + V : y;
-        zs = z < 0 ? z + V : z;
-        alias = (y == V / 2 || y == -(V / 2) || z == V / 2 || z == -(V / 2));
-      } else {
-        ys = y + V / 2;
-        zs = z + V / 2;
-        alias = false;
-      }
-      if ((unsigned)x > (unsigned)(V / 2) || (unsigned)ys >= (unsigned)V || (unsigned)zs >= (unsigned)V)
-        continue;  // outside the volume: nothing can have been added here
-      int64_t idx = ((int64_t)zs * V + ys) * rowlen + x;
-      if (it.exclusive && !alias) {
-        if (volft) {
-          float2 c = volft[idx];
-          volft[idx] = make_float2(c.x + r, c.y + im);
-        }
-        if (volw) volw[idx] += ww;
-      } else {
-        if (volft) red_add2((float*)(volft + idx), r, im);
-        if (volw) red_add(volw + idx, ww);
+    bp_flush_brick<DECENTERED>(volft, volw, are, aim, aw, B, RS, PS, o, V, a.rowlen, it.exclusive != 0);
+  }
+}
+
+// Segment variant of the brick backprojector: the same accumulators and
+// flush, but a warp takes a (slice, brick) pair of the segment plan and finds
+// the pixels itself, by row segments (segment.cuh).  Side 0 walks the pixels
+// whose position lies in the brick widened by one voxel below (where their
+// neighbours can reach it) and adds their unconjugated targets, the
+// neighbours with x >= 0; side 1 walks the pixels whose mirrored position
+// does and adds their conjugated targets, the mirrored neighbours (x < 0)
+// and the second insertions on the x = 0 plane.  Each target of each pixel
+// is added once, by the pair of its brick on the side of its conjugation,
+// with the weights and values of the binned variant.
+template <bool DECENTERED, bool SQUARE>
+__global__ void __launch_bounds__(1024)
+backproject_segment_kernel(float2* __restrict__ volft, float* __restrict__ volw,
+                           const float2* __restrict__ projft, const float* __restrict__ projw,
+                           const float* __restrict__ mats, BpArgs a, BrickGrid g, PixelSet px,
+                           const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
+                           const int* __restrict__ pairs, const PixelBin* __restrict__ bins,
+                           int* __restrict__ counter) {
+  extern __shared__ float acc[];
+  __shared__ int item_s, next_s;
+  const int nitems = *nitems_ptr;
+  // Accumulator layout as in backproject_brick_kernel (rows padded to B+1,
+  // planes to (B+1)^2 floats).
+  const int B = g.B, RS = g.B + 1, PS = (g.B + 1) * (g.B + 1), NA = g.B * PS;
+  float* are = acc;
+  float* aim = acc + NA;
+  float* aw = acc + 2 * NA;
+  const int lane = threadIdx.x & 31;
+  const int V = a.P;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      item_s = atomicAdd(counter, 1);
+      next_s = 0;
+    }
+    for (int k = threadIdx.x; k < 3 * NA; k += blockDim.x) acc[k] = 0.f;
+    __syncthreads();
+    const int w = item_s;
+    if (w >= nitems) break;
+    const BrickItem it = items[w];
+    const int3 o = brick_origin(g, it.brick);
+
+    for (;;) {  // warps take the item's pairs one at a time
+      int j = 0;
+      if (lane == 0) j = atomicAdd(&next_s, 1);
+      j = __shfl_sync(0xffffffffu, j, 0);
+      if (j >= it.count) break;
+      const int slice = bins[__ldg(pairs + it.offset + j)].slice;
+      float m[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
+      const int64_t sbase = a.elements * slice;
+#pragma unroll 1
+      for (int side = 0; side < 2; side++) {
+        const SegBox box = seg_box(m, side, o, B, 1.f);
+        const bool plane0 = side == 1 && o.x == 0;  // second insertions can land in this brick
+        seg_for_each_pixel(box, px, [&](int u, int v, bool valid) {
+          if (!valid) return;
+          const int idy = v < 0 ? v + a.n : v;
+          const int64_t id = sbase + (int64_t)idy * a.dimft + u;
+          BpSample s = backproject_sample(m, (float)u, (float)v, 0.f);
+          const float2 val = projft ? __ldg(projft + id) : make_float2(1.f, 0.f);
+          const float pw = projw ? __ldg(projw + id) : 1.f;
+          if (side == 0) {
+            const int lx0 = s.x0 - o.x, ly0 = s.y0 - o.y, lz0 = s.z0 - o.z;
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+              const int dx = i & 1, dy = (i >> 1) & 1, dz = (i >> 2) & 1;
+              const int lx = lx0 + dx, ly = ly0 + dy, lz = lz0 + dz;
+              if (s.x0 + dx >= 0 && (unsigned)lx < (unsigned)B && (unsigned)ly < (unsigned)B &&
+                  (unsigned)lz < (unsigned)B) {
+                const float wt = SQUARE ? s.w[i] * s.w[i] : s.w[i];
+                const int k = lz * PS + ly * RS + lx;
+                atomicAdd(are + k, wt * val.x);
+                atomicAdd(aim + k, wt * val.y);
+                atomicAdd(aw + k, wt * pw);
+              }
+            }
+          } else {
+            // mirrored neighbour -n of n = base + (dx, dy, dz), local coordinates
+            const int lx0 = -s.x0 - o.x, ly0 = -s.y0 - o.y, lz0 = -s.z0 - o.z;
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+              const int dx = i & 1, dy = (i >> 1) & 1, dz = (i >> 2) & 1;
+              const int lx = lx0 - dx, ly = ly0 - dy, lz = lz0 - dz;
+              if (s.x0 + dx < 0 && (unsigned)lx < (unsigned)B && (unsigned)ly < (unsigned)B &&
+                  (unsigned)lz < (unsigned)B) {
+                const float wt = SQUARE ? s.w[i] * s.w[i] : s.w[i];
+                const int k = lz * PS + ly * RS + lx;
+                atomicAdd(are + k, wt * val.x);
+                atomicAdd(aim + k, -(wt * val.y));
+                atomicAdd(aw + k, wt * pw);
+              }
+            }
+            if (plane0) {
+              // second insertion at (0, -ny, -nz) of each neighbour with
+              // nx == 0 and (ny, nz) != 0; here o.x == 0, so local x is 0
+#pragma unroll
+              for (int i = 0; i < 8; i++) {
+                const int dx = i & 1, dy = (i >> 1) & 1, dz = (i >> 2) & 1;
+                const int ny = s.y0 + dy, nz = s.z0 + dz;
+                const int ly = -ny - o.y, lz = -nz - o.z;
+                if (s.x0 + dx == 0 && (ny != 0 || nz != 0) && (unsigned)ly < (unsigned)B &&
+                    (unsigned)lz < (unsigned)B) {
+                  const float wt = SQUARE ? s.w[i] * s.w[i] : s.w[i];
+                  const int k = lz * PS + ly * RS;
+                  atomicAdd(are + k, wt * val.x);
+                  atomicAdd(aim + k, -(wt * val.y));
+                  atomicAdd(aw + k, wt * pw);
+                }
+              }
+            }
+          }
+        });
       }
     }
+    __syncthreads();
+
+    // flush the brick into the volume
+    bp_flush_brick<DECENTERED>(volft, volw, are, aim, aw, B, RS, PS, o, V, a.rowlen, it.exclusive != 0);
   }
 }
 
@@ -310,7 +444,8 @@ static void launch_bp_direct_any(dim3 grid, cudaStream_t stream, float2* vf, flo
 // plan could not take.  Nothing synchronises.
 static int backproject_brick(float* d_volumeft, float* d_volumeweights, const float* d_projft,
                              const float* d_projweights, const float* d_mats, const BpArgs& a,
-                             int rmax, int decentered, int square, unsigned batch, cudaStream_t stream) {
+                             int rmax, int decentered, int square, unsigned batch, cudaStream_t stream,
+                             int segments) {
   const int V = a.P;
   // Neighbours stay inside x [0, V/2] and y, z [-V/2, yhi] (no clamp, no
   // wrap beyond the reference's) while every sample radius is below limit.
@@ -321,14 +456,21 @@ static int backproject_brick(float* d_volumeft, float* d_volumeweights, const fl
   size_t smem = sizeof(float) * 3 * (size_t)tune.edge * (tune.edge + 1) * (tune.edge + 1);
   auto kern = decentered ? (square ? backproject_brick_kernel<true, true> : backproject_brick_kernel<true, false>)
                          : (square ? backproject_brick_kernel<false, true> : backproject_brick_kernel<false, false>);
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  auto skern = decentered
+                   ? (square ? backproject_segment_kernel<true, true> : backproject_segment_kernel<true, false>)
+                   : (square ? backproject_segment_kernel<false, true> : backproject_segment_kernel<false, false>);
+  cudaError_t e = segments ? cudaFuncSetAttribute(skern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                           : cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess)
     return set_error(GTOMRLN_ERR_CUDA, "brick backprojector: %zu B of shared memory refused: %s", smem,
                      cudaGetErrorString(e));
   int dev = 0, sms = 148, occ = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, tune.threads, smem);
+  if (segments)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, skern, tune.threads, smem);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, tune.threads, smem);
   PixelSet px;
   px.n = a.n;
   px.dimft = a.dimft;
@@ -337,11 +479,17 @@ static int backproject_brick(float* d_volumeft, float* d_volumeweights, const fl
   px.strict = 1;
   px.pmax = std::sqrt((float)std::max(0, rmax * rmax - 1));
   BrickPlan plan;
-  int st = build_brick_plan(GTOMRLN_OP_BACKPROJECT, d_mats, (int)batch, g, px, limit, tune.chunk, stream, &plan);
+  int st = build_brick_plan(GTOMRLN_OP_BACKPROJECT, d_mats, (int)batch, g, px, limit, tune.chunk, stream, &plan,
+                            segments);
   if (st) return st;
-  kern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
-      (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, a, g, plan.items,
-      plan.nitems, plan.pairs, plan.bins, plan.entries, plan.counter);
+  if (segments)
+    skern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
+        (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, a, g, px,
+        plan.items, plan.nitems, plan.pairs, plan.bins, plan.counter);
+  else
+    kern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
+        (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, a, g, plan.items,
+        plan.nitems, plan.pairs, plan.bins, plan.entries, plan.counter);
   launch_bp_direct_any(dim3(sms * 4), stream, (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft,
                        d_projweights, d_mats, nullptr, a, plan.fallback, plan.nfallback, 2, decentered, square);
   e = cudaGetLastError();
@@ -466,9 +614,10 @@ static int backproject_launch(float* d_volumeft, float* d_volumeweights, int vx,
   const int choice = path_choice(GTOMRLN_OP_BACKPROJECT);
   if (ndp == 2 && vx == vy && vx == vz && vx >= 4 && !d_ivolume && mag.x == 1.f && mag.y == 0.f &&
       mag.z == 0.f && mag.w == 1.f && a.ewalddiaminv == 0.f && (d_volumeft || d_volumeweights) &&
-      (choice == GTOMRLN_PATH_BRICK || (choice == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch)))
+      (choice == GTOMRLN_PATH_BRICK || choice == GTOMRLN_PATH_SEGMENT ||
+       (choice == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch)))
     return backproject_brick(d_volumeft, d_volumeweights, d_projft, d_projweights, d_matrices, a, (int)rmax,
-                             decentered, square, batch, stream);
+                             decentered, square, batch, stream, choice == GTOMRLN_PATH_BRICK ? 0 : 1);
 
   launch_bp_direct_any(dim3((unsigned)(a.tiles * (int64_t)batch)), stream, (float2*)d_volumeft, d_volumeweights,
                        (const float2*)d_projft, d_projweights, d_matrices, d_ivolume, a, nullptr, nullptr, ndp,

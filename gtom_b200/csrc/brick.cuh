@@ -125,9 +125,11 @@ struct BrickPlan {
 // voxel).  A slice whose samples could reach radius `limit` (beyond which
 // the brick kernels would need the reference's clamps) is not planned but
 // listed in plan->fallback for the direct kernels.  chunk caps the bins per
-// work item.
+// work item.  segments = 1 builds the segment plan instead: bins without
+// entries, one per (slice, brick) pair whose brick the slice's plane
+// crosses, and the kernels enumerate the pixels themselves (segment.cuh).
 int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g, const PixelSet& px,
-                     float limit, int chunk, cudaStream_t stream, BrickPlan* plan);
+                     float limit, int chunk, cudaStream_t stream, BrickPlan* plan, int segments = 0);
 int free_brick_plan(BrickPlan* plan, cudaStream_t stream);
 
 // Pixel id -> signed slice coordinates (FFT order in y).

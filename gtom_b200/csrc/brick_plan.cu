@@ -4,6 +4,9 @@
 //   bin_slices_kernel   one CTA per slice: brick(s) of every pixel, a
 //                       shared-memory histogram over bricks, the slice's bins
 //                       and its pixel ids sorted by brick;
+//   segment_pairs_kernel  (segment plan, instead of the above) one CTA per
+//                       slice: the bricks its plane crosses, as bins
+//                       without pixel lists;
 //   pairs_scan_kernel   one CTA: per-brick bin offsets and work items, bricks
 //                       in order of increasing distance from the origin so
 //                       that the heaviest items start first;
@@ -18,6 +21,7 @@
 
 #include "brick.cuh"
 #include "sample.cuh"
+#include "segment.cuh"
 
 namespace gtomrln {
 
@@ -248,6 +252,76 @@ bin_slices_kernel(const float* __restrict__ mats, BrickGrid g, PixelSet px, floa
   });
 }
 
+// Segment plan: one CTA per slice lists the bricks whose box, widened by
+// `below` voxels on the low side and by the segment margin, meets the
+// slice's plane within the radius its samples reach.  Each becomes a bin
+// without entries; the brick kernel finds the pixels by row segments
+// (segment.cuh).  Positions of a slice lie on the plane through the origin
+// spanned by the first two matrix columns and within plane_scale * pmax of
+// the origin, mirrored positions too, so the list covers every brick a
+// pixel of the slice (or its mirror) can reach.
+constexpr int kPairThreads = 256;
+__global__ void __launch_bounds__(kPairThreads)
+segment_pairs_kernel(const float* __restrict__ mats, BrickGrid g, float pmax, float limit, float below,
+                     PixelBin* __restrict__ bins, int64_t bins_cap, unsigned long long* __restrict__ counters,
+                     int* __restrict__ brick_pairs, int* __restrict__ fallback, int* __restrict__ nfallback) {
+  extern __shared__ int hits[];  // brick ids of this slice
+  __shared__ int s_n;
+  __shared__ long long s_base;
+  const int slice = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
+  float m[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
+  const float scale = plane_scale(m);
+  if (!(scale * pmax < limit)) {  // uniform over the block
+    if (tid == 0) fallback[atomicAdd(nfallback, 1)] = slice;
+    return;
+  }
+  if (tid == 0) s_n = 0;
+  __syncthreads();
+  const float n0 = m[1] * m[5] - m[2] * m[4], n1 = m[2] * m[3] - m[0] * m[5], n2 = m[0] * m[4] - m[1] * m[3];
+  const float R = scale * pmax;
+  const float R2 = R * R * (1.f + 1e-5f) + 1e-3f;
+  const float lo_pad = below + kSegMargin, hi_pad = (float)g.B + kSegMargin;
+  for (int base = 0; base < g.nbricks; base += kPairThreads) {
+    const int b = base + tid;
+    bool hit = false;
+    if (b < g.nbricks) {
+      const int3 o = brick_origin(g, b);
+      const float lo0 = o.x - lo_pad, lo1 = o.y - lo_pad, lo2 = o.z - lo_pad;
+      const float hi0 = o.x + hi_pad, hi1 = o.y + hi_pad, hi2 = o.z + hi_pad;
+      const float c0 = 0.5f * (lo0 + hi0), c1 = 0.5f * (lo1 + hi1), c2 = 0.5f * (lo2 + hi2);
+      const float h0 = 0.5f * (hi0 - lo0), h1 = 0.5f * (hi1 - lo1), h2 = 0.5f * (hi2 - lo2);
+      const float dist = fabsf(n0 * c0 + n1 * c1 + n2 * c2);
+      const float reach = fabsf(n0) * h0 + fabsf(n1) * h1 + fabsf(n2) * h2;
+      const float eps = 1e-5f * (fabsf(n0) * (fabsf(c0) + h0) + fabsf(n1) * (fabsf(c1) + h1) +
+                                 fabsf(n2) * (fabsf(c2) + h2));
+      const float d0 = fmaxf(0.f, fmaxf(lo0, -hi0)), d1 = fmaxf(0.f, fmaxf(lo1, -hi1)),
+                  d2 = fmaxf(0.f, fmaxf(lo2, -hi2));
+      hit = dist <= reach + eps && d0 * d0 + d1 * d1 + d2 * d2 <= R2;
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, hit);
+    int wbase = 0;
+    if (lane == 0 && mask) wbase = atomicAdd(&s_n, __popc(mask));
+    wbase = __shfl_sync(0xffffffffu, wbase, 0);
+    if (hit) hits[wbase + __popc(mask & ((1u << lane) - 1u))] = b;
+  }
+  __syncthreads();
+  const int nh = s_n;
+  if (tid == 0) s_base = (long long)atomicAdd(counters + 1, (unsigned long long)nh);
+  __syncthreads();
+  if (s_base + nh > bins_cap) {  // out of room: direct path
+    for (long long k = s_base + tid; k < s_base + nh && k < bins_cap; k += kPairThreads) bins[k].brick = -1;
+    if (tid == 0) fallback[atomicAdd(nfallback, 1)] = slice;
+    return;
+  }
+  for (int k = tid; k < nh; k += kPairThreads) {
+    const int b = hits[k];
+    bins[s_base + k] = {slice, 0, 0, b, 0, 0, 0, 0};
+    atomicAdd(brick_pairs + b, 1);
+  }
+}
+
 // Single block.  Bricks are visited in `order` (increasing distance from the
 // origin); writes bin-list offsets, per-brick item offsets and the item count.
 constexpr int kScanThreads = 1024;
@@ -348,7 +422,7 @@ static int brick_order(const BrickGrid& g, const int** out) {
 }
 
 int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g, const PixelSet& px,
-                     float limit, int chunk, cudaStream_t stream, BrickPlan* plan) {
+                     float limit, int chunk, cudaStream_t stream, BrickPlan* plan, int segments) {
   plan->g = g;
   plan->batch = batch;
   size_t hist_bytes = 2 * sizeof(int) * (size_t)g.nbricks;
@@ -358,7 +432,8 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
   // pixel id of a slice: 66 KB at n = 256).
   const size_t code_bytes = ((size_t)px.elements * 2 + 3) & ~(size_t)3;
   const int use_codes = g.nbricks < 65535 && hist_bytes + code_bytes <= 200 * 1024 ? 1 : 0;
-  const size_t smem_bytes = hist_bytes + (use_codes ? code_bytes : 0);
+  const size_t smem_bytes = segments ? sizeof(int) * (size_t)g.nbricks
+                                     : hist_bytes + (use_codes ? code_bytes : 0);
   const int* d_order = nullptr;
   int st = brick_order(g, &d_order);
   if (st) return st;
@@ -373,8 +448,20 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
       npix += px.strict ? (r2 < px.rmax2 && !(u == 0 && v < 0)) : (r2 <= px.rmax2);
     }
   }
-  int64_t entries_cap = std::max<int64_t>(1, (int64_t)batch * npix * (op == GTOMRLN_OP_PROJECT ? 1 : 2));
-  int64_t bins_cap = std::max<int64_t>(1, (int64_t)batch * std::min(g.nbricks, kMaxBinsPerSlice));
+  int64_t entries_cap =
+      segments ? 1 : std::max<int64_t>(1, (int64_t)batch * npix * (op == GTOMRLN_OP_PROJECT ? 1 : 2));
+  int per_slice = std::min(g.nbricks, kMaxBinsPerSlice);
+  if (segments) {
+    // A crossed brick's centre lies within h = sqrt(3)/2 * B' (B' the widened
+    // edge) of the plane and within limit + h of the origin: about
+    // pi (limit + h)^2 * 2h / B^3 lattice points per slice; half as much
+    // again is reserved (the cap is an average over the batch).
+    const double Bw = g.B + (op == GTOMRLN_OP_PROJECT ? 0.0 : 1.0) + 2.0 * kSegMargin;
+    const double h = 0.8660254037844386 * Bw, R = (double)limit + h;
+    const double est = 3.141592653589793 * R * R * 2.0 * h / ((double)g.B * g.B * g.B);
+    per_slice = (int)std::min<double>(g.nbricks, 1.5 * est + 64.0);
+  }
+  int64_t bins_cap = std::max<int64_t>(1, (int64_t)batch * per_slice);
   if (entries_cap > 0x7fffffffLL || bins_cap > 0x7fffffffLL)
     return set_error(GTOMRLN_ERR_INVALID, "brick plan too large for one call; split the batch");
   int64_t cap_items = (int64_t)g.nbricks + bins_cap / chunk + 1;
@@ -392,7 +479,7 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
   size_t o_entries = o_pairs + al((size_t)bins_cap * 4);
   size_t bytes = o_entries + al((size_t)entries_cap * 4);
   char* base = nullptr;
-  st = pool_alloc((void**)&base, bytes, stream);
+  st = scratch_alloc((void**)&base, bytes, stream);
   if (st) return st;
   plan->scratch = base;
   int* counts = (int*)(base + o_counts);
@@ -413,7 +500,15 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
   cudaError_t e = cudaMemsetAsync(counts, 0, nb * 4, stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(base + o_misc, 0, 256, stream);
   if (e == cudaSuccess && batch > 0) {
-    if (op == GTOMRLN_OP_PROJECT) {
+    if (segments) {
+      // The projector's samples reach the brick of their base voxel, the
+      // backprojector's also the bricks of the voxel above it on each axis.
+      const float below = op == GTOMRLN_OP_PROJECT ? 0.f : 1.f;
+      cudaFuncSetAttribute(segment_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+      segment_pairs_kernel<<<batch, kPairThreads, smem_bytes, stream>>>(
+          d_mats, g, px.pmax, limit, below, plan->bins, bins_cap, counters, counts, plan->fallback,
+          plan->nfallback);
+    } else if (op == GTOMRLN_OP_PROJECT) {
       cudaFuncSetAttribute(bin_slices_kernel<GTOMRLN_OP_PROJECT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem_bytes);
       bin_slices_kernel<GTOMRLN_OP_PROJECT><<<batch, kBinThreads, smem_bytes, stream>>>(
@@ -445,7 +540,7 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
 }
 
 int free_brick_plan(BrickPlan* plan, cudaStream_t stream) {
-  int st = pool_free(plan->scratch, stream);
+  int st = scratch_free(plan->scratch, stream);
   *plan = BrickPlan();
   return st;
 }

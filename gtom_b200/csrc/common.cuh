@@ -57,6 +57,10 @@ BrickTuning brick_tuning(int op);
 // Stream-ordered device scratch from the library's memory pool.
 int pool_alloc(void** ptr, size_t bytes, cudaStream_t stream);
 int pool_free(void* ptr, cudaStream_t stream);
+// Scratch cached per (device, stream) across calls (abi.cu); the pointer is
+// valid until the matching scratch_free, in stream order.
+int scratch_alloc(void** ptr, size_t bytes, cudaStream_t stream);
+int scratch_free(void* ptr, cudaStream_t stream);
 
 // ---------------------------------------------------------------- device --
 struct Mat3 {

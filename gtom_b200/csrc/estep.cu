@@ -17,7 +17,6 @@ namespace gtomrln {
 namespace {
 
 constexpr int kDiffThreads = 256;
-constexpr int kMaxGroup = 8;  // groupsize (tile) limit of the squared differences
 
 // diff2 for a group of refs x shifts of one particle over n elements:
 //   plain: 0.5 sum_i w_i |c_i ref_i - p_i shift_i|^2

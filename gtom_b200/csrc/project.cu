@@ -15,6 +15,7 @@
 #include "brick.cuh"
 #include "common.cuh"
 #include "sample.cuh"
+#include "segment.cuh"
 
 namespace gtomrln {
 
@@ -232,6 +233,74 @@ project_brick_kernel(const float2* __restrict__ vol, float2* __restrict__ proj,
   }
 }
 
+// Segment variant of the brick projector: the same staging and arithmetic,
+// but a warp takes a (slice, brick) pair of the segment plan and finds the
+// pixels itself, by row segments (segment.cuh), among those whose position
+// (side 0) or mirrored position (side 1) falls in the brick.  A pixel is
+// written by the pair whose brick holds its base voxel, on the side of its
+// Friedel flip: exactly one pair, as in the binned variant.
+__global__ void __launch_bounds__(1024)
+project_segment_kernel(const float2* __restrict__ vol, float2* __restrict__ proj,
+                       const float* __restrict__ mats, ProjArgs a, BrickGrid g, PixelSet px,
+                       const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
+                       const int* __restrict__ pairs, const PixelBin* __restrict__ bins,
+                       int* __restrict__ counter) {
+  extern __shared__ float2 tile[];
+  __shared__ int item_s, next_s;
+  const int nitems = *nitems_ptr;
+  const int B = g.B, T = g.B + 1;
+  const int rowlen = a.P / 2 + 1;
+  const int64_t last = a.nvox - 1;
+  for (;;) {
+    __syncthreads();  // previous item done with the tile
+    if (threadIdx.x == 0) {
+      item_s = atomicAdd(counter, 1);
+      next_s = 0;
+    }
+    __syncthreads();
+    const int w = item_s;
+    if (w >= nitems) break;
+    const BrickItem it = items[w];
+    const int3 o = brick_origin(g, it.brick);
+    for (int k = threadIdx.x; k < T * T * T; k += blockDim.x) {
+      int tx = k % T, t2 = k / T, ty = t2 % T, tz = t2 / T;
+      int x = o.x + tx, y = o.y + ty, z = o.z + tz;
+      int ys = y < 0 ? y + a.P : y, zs = z < 0 ? z + a.P : z;
+      int64_t i = ((int64_t)zs * a.P + ys) * rowlen + x;
+      i = i < 0 ? 0 : (i > last ? last : i);
+      tile[k] = __ldg(vol + i);
+    }
+    __syncthreads();
+    for (;;) {  // warps take the item's pairs one at a time
+      int j = 0;
+      if ((threadIdx.x & 31) == 0) j = atomicAdd(&next_s, 1);
+      j = __shfl_sync(0xffffffffu, j, 0);
+      if (j >= it.count) break;
+      const int slice = bins[__ldg(pairs + it.offset + j)].slice;
+      float m[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
+      float2* out = proj + a.elements * slice;
+#pragma unroll 1
+      for (int side = 0; side < 2; side++) {
+        const SegBox box = seg_box(m, side, o, B, 0.f);
+        seg_for_each_pixel(box, px, [&](int u, int v, bool valid) {
+          if (!valid) return;
+          ProjSample s = project_sample(m, u, v, 0);
+          if ((s.sign < 0.f) != (side == 1)) return;  // the other side's pixel
+          int lx = s.x0 - o.x, ly = s.y0 - o.y, lz = s.z0 - o.z;
+          if ((unsigned)lx >= (unsigned)B || (unsigned)ly >= (unsigned)B || (unsigned)lz >= (unsigned)B)
+            return;  // another brick's pixel
+          const float2* c = tile + (lz * T + ly) * T + lx;
+          const int idy = v < 0 ? v + a.n : v;
+          out[(int64_t)idy * a.dimft + u] = trilerp(s, c[0], c[1], c[T], c[T + 1], c[T * T], c[T * T + 1],
+                                                    c[T * T + T], c[T * T + T + 1]);
+        });
+      }
+    }
+  }
+}
+
 // Zeroes the elements outside rmax (Project.cu:111-115) for the brick path.
 // In each row they form the tail x > sqrt(rmax^2 - y^2); one warp writes
 // one row's tail, coalesced.
@@ -259,22 +328,28 @@ constexpr unsigned kBrickMinBatch = 32;
 // The brick path: plan, zero fill outside rmax, brick kernel, and the direct
 // kernel for any slice the plan could not take.  Nothing synchronises.
 static int project_brick(const float* d_volumeft, float* d_proj, const float* d_mats, const ProjArgs& a,
-                         unsigned batch, cudaStream_t stream) {
+                         unsigned batch, cudaStream_t stream, int segments) {
   const int P = a.P;
   const BrickTuning tune = brick_tuning(GTOMRLN_OP_PROJECT);
   // While every sample radius stays below P/2 + 0.99, the base voxels lie in
   // x [0, P/2] and y, z [-P/2 - 1, P/2].
   BrickGrid g = make_brick_grid(P, tune.edge, P / 2, -(P / 2) - 1, P / 2);
   size_t smem = sizeof(float2) * (size_t)(tune.edge + 1) * (tune.edge + 1) * (tune.edge + 1);
-  cudaError_t e = cudaFuncSetAttribute(project_brick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  auto kern = segments ? project_segment_kernel : nullptr;
+  cudaError_t e = segments ? cudaFuncSetAttribute(project_segment_kernel,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                           : cudaFuncSetAttribute(project_brick_kernel,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess)
     return set_error(GTOMRLN_ERR_CUDA, "brick projector: %zu B of shared memory refused: %s", smem,
                      cudaGetErrorString(e));
   int dev = 0, sms = 148, occ = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, project_brick_kernel, tune.threads, smem);
+  if (segments)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, project_segment_kernel, tune.threads, smem);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, project_brick_kernel, tune.threads, smem);
   PixelSet px;
   px.n = a.n;
   px.dimft = a.dimft;
@@ -284,13 +359,18 @@ static int project_brick(const float* d_volumeft, float* d_proj, const float* d_
   px.pmax = (float)a.rmax;
   BrickPlan plan;
   int st = build_brick_plan(GTOMRLN_OP_PROJECT, d_mats, (int)batch, g, px, (float)(P / 2) + 0.99f, tune.chunk,
-                            stream, &plan);
+                            stream, &plan, segments);
   if (st) return st;
   int64_t rows = (int64_t)a.n * batch;  // 2D slices: n rows of dimft elements each
   project_zero_kernel<<<sms * 8, 256, 0, stream>>>((float2*)d_proj, a, rows);
-  project_brick_kernel<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
-      (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, plan.items, plan.nitems, plan.pairs, plan.bins,
-      plan.entries, plan.counter);
+  if (segments)
+    kern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
+        (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, px, plan.items, plan.nitems, plan.pairs,
+        plan.bins, plan.counter);
+  else
+    project_brick_kernel<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
+        (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, plan.items, plan.nitems, plan.pairs, plan.bins,
+        plan.entries, plan.counter);
   ArrayFetch f{(const float2*)d_volumeft, a.P, a.P / 2 + 1, a.nvox - 1};
   project_listed_kernel<<<sms * 4, kProjThreads, 0, stream>>>(f, (float2*)d_proj, d_mats, a, plan.fallback,
                                                                plan.nfallback);
@@ -426,9 +506,12 @@ int gtomrln_project(const float* d_volumeft, int vx, int vy, int vz, float* d_pr
   if (st) return st;
   if (batch && (!d_volumeft || !d_proj || !d_matrices))
     return set_error(GTOMRLN_ERR_INVALID, "project: NULL device pointer");
+  const int choice = path_choice(GTOMRLN_OP_PROJECT);
   if (ndp == 2 && vx == vy && vx == vz && vx >= 4 &&
-      (path_choice(0) == GTOMRLN_PATH_BRICK || (path_choice(0) == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch)))
-    return project_brick(d_volumeft, d_proj, d_matrices, a, batch, (cudaStream_t)stream);
+      (choice == GTOMRLN_PATH_BRICK || choice == GTOMRLN_PATH_SEGMENT ||
+       (choice == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch)))
+    return project_brick(d_volumeft, d_proj, d_matrices, a, batch, (cudaStream_t)stream,
+                         choice == GTOMRLN_PATH_BRICK ? 0 : 1);
   ArrayFetch f{(const float2*)d_volumeft, a.P, a.P / 2 + 1, a.nvox - 1};
   return launch_project(f, ndp, d_proj, d_matrices, a, batch, (cudaStream_t)stream);
 }

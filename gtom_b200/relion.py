@@ -364,12 +364,13 @@ def mlp_param_count() -> int:
 
 
 _OPS = {"project": 0, "backproject": 1}
-_PATHS = {"auto": 0, "direct": 1, "brick": 2}
+_PATHS = {"auto": 0, "direct": 1, "brick": 2, "segment": 3}
 
 
 def set_path(op: str, path: str) -> None:
     """Selects the implementation of "project" or "backproject" for this
-    process: "auto" (default), "direct" or "brick" (gtomrln_set_path)."""
+    process: "auto" (default), "direct", "brick" (pixels binned per brick) or
+    "segment" (pixels found per brick by row segments) (gtomrln_set_path)."""
     _lib.call("gtomrln_set_path", _OPS[op], _PATHS[path])
 
 

@@ -64,17 +64,21 @@ GTOMRLN_API int gtomrln_release_caches(void);
 
 /* Extension (no reference counterpart): choose the implementation of an
  * operation for the calling process.  op: GTOMRLN_OP_PROJECT or
- * GTOMRLN_OP_BACKPROJECT; path: GTOMRLN_PATH_AUTO (default: brick-major for
- * batches of 32 or more 2D slices whose geometry allows it, else direct),
+ * GTOMRLN_OP_BACKPROJECT; path: GTOMRLN_PATH_AUTO (default: brick-major with
+ * row segments for batches of 32 or more 2D slices whose geometry allows
+ * it, else direct),
  * GTOMRLN_PATH_DIRECT (one thread per slice element, global gathers /
- * reductions) or GTOMRLN_PATH_BRICK (brick-major, shared-memory staging;
- * falls back to direct where the geometry does not allow it).  Both paths
- * compute the same per-sample arithmetic. */
+ * reductions), GTOMRLN_PATH_BRICK (brick-major, shared-memory staging, pixels
+ * binned per brick by a planning pass; falls back to direct where the
+ * geometry does not allow it) or GTOMRLN_PATH_SEGMENT (brick-major, pixels
+ * found per brick by row segments instead of binning).  All paths compute
+ * the same per-sample arithmetic. */
 #define GTOMRLN_OP_PROJECT 0
 #define GTOMRLN_OP_BACKPROJECT 1
 #define GTOMRLN_PATH_AUTO 0
 #define GTOMRLN_PATH_DIRECT 1
 #define GTOMRLN_PATH_BRICK 2
+#define GTOMRLN_PATH_SEGMENT 3
 GTOMRLN_API int gtomrln_set_path(int op, int path);
 
 /* Extension (no reference counterpart): launch shape of the brick-major

@@ -51,14 +51,15 @@ def test_brick_projector_is_bit_identical(cuda, n, scale, batch, kind):
     e = (n // 2 + 1) * n
     dv = torch.from_numpy(vol).cuda().reshape(-1)
     outs = {}
-    for p in ("direct", "brick"):
+    for p in ("direct", "brick", "segment"):
         _paths(p, "auto")
         out = torch.full((batch * e,), complex(np.nan, np.nan), dtype=torch.complex64, device="cuda")
         d_rlnProject(dv, (P, P, P), out, (n, n, 1), n // 2, mats, batch)
         torch.cuda.synchronize()
         outs[p] = out
-    assert torch.isfinite(torch.view_as_real(outs["brick"])).all()
-    assert torch.equal(outs["direct"], outs["brick"])
+    for p in ("brick", "segment"):
+        assert torch.isfinite(torch.view_as_real(outs[p])).all(), p
+        assert torch.equal(outs["direct"], outs[p]), p
 
 
 @pytest.mark.parametrize("n,V,batch,kind,dec,sq", [(64, 129, 300, "uniform", False, False),
@@ -81,7 +82,7 @@ def test_brick_backprojector_matches_direct(cuda, n, V, batch, kind, dec, sq):
     dpw = torch.from_numpy(projw).cuda().reshape(-1)
     nv = (V // 2 + 1) * V * V
     res = {}
-    for b in ("direct", "brick"):
+    for b in ("direct", "brick", "segment"):
         _paths("auto", b)
         vf = torch.zeros(nv, dtype=torch.complex64, device="cuda")
         vw = torch.zeros(nv, dtype=torch.float32, device="cuda")
@@ -89,13 +90,14 @@ def test_brick_backprojector_matches_direct(cuda, n, V, batch, kind, dec, sq):
                          batch)
         torch.cuda.synchronize()
         res[b] = (vf.cpu().numpy(), vw.cpu().numpy())
-    assert rel_l2(res["brick"][0], res["direct"][0]) <= 1e-6
-    assert rel_l2(res["brick"][1], res["direct"][1]) <= 1e-6
     of, ow = np.zeros(nv, np.complex64), np.zeros(nv, np.float32)
     O.backproject(of, ow, V, projft, projw, n, n // 2, m_host, decentered=dec, square=sq, fp32=True)
-    assert rel_l2(res["brick"][0], of) <= 1e-5 and rel_l2(res["brick"][1], ow) <= 1e-5
-    # the voxels that received nothing are exactly the same ones
-    assert np.array_equal(res["brick"][1] == 0, res["direct"][1] == 0)
+    for p in ("brick", "segment"):
+        assert rel_l2(res[p][0], res["direct"][0]) <= 1e-6, p
+        assert rel_l2(res[p][1], res["direct"][1]) <= 1e-6, p
+        assert rel_l2(res[p][0], of) <= 1e-5 and rel_l2(res[p][1], ow) <= 1e-5, p
+        # the voxels that received nothing are exactly the same ones
+        assert np.array_equal(res[p][1] == 0, res["direct"][1] == 0), p
 
 
 def test_brick_backprojector_accumulates_across_calls(cuda):
@@ -121,3 +123,61 @@ def test_brick_backprojector_accumulates_across_calls(cuda):
     torch.cuda.synchronize()
     assert rel_l2(a_f.cpu().numpy(), b_f.cpu().numpy()) <= 1e-6
     assert rel_l2(a_w.cpu().numpy(), b_w.cpu().numpy()) <= 1e-6
+
+
+@pytest.mark.parametrize("kind,edge", [("unit_scale", 0), ("unit_scale", 12), ("sheared", 0), ("sheared", 9),
+                                       ("odd_size", 0)])
+def test_segment_paths_on_general_geometry(cuda, kind, edge):
+    """The segment variants against the direct kernels where the row
+    segments are least regular: a pixel spacing of one voxel (a brick spans
+    more than 32 slice rows, so the rows come in several batches), sheared
+    non-orthogonal slice matrices (the row range uses the full inverse of
+    the columns' Gram matrix), an odd slice size (rows -n/2 .. n/2) and small
+    bricks (many pairs per slice)."""
+    from gtom_b200 import d_rlnBackproject, d_rlnProject, matrices_from_angles, set_brick_tuning
+    rng = np.random.default_rng(91 + edge + len(kind))
+    n = 63 if kind == "odd_size" else 64
+    scale = 1.0 if kind == "unit_scale" else 2.0
+    batch = 96
+    m_host = matrices_from_angles(random_angles(rng, batch), scale).reshape(batch, 9)
+    if kind == "sheared":
+        m_host = (m_host + rng.normal(scale=0.15, size=m_host.shape) * scale).astype(np.float32)
+        m_host *= 0.8  # keep every sample inside the brick grids
+    mats = torch.from_numpy(np.ascontiguousarray(m_host)).cuda().reshape(-1)
+    try:
+        if edge:
+            set_brick_tuning("project", edge=edge)
+            set_brick_tuning("backproject", edge=edge)
+        P = int(scale * n)
+        vol = blob_volume_ft(rng, n, P, 12)
+        dv = torch.from_numpy(vol.astype(np.complex64)).cuda().reshape(-1)
+        e = (n // 2 + 1) * n
+        outs = {}
+        for p in ("direct", "segment"):
+            _paths(p, "auto")
+            out = torch.full((batch * e,), complex(np.nan, np.nan), dtype=torch.complex64, device="cuda")
+            d_rlnProject(dv, (P, P, P), out, (n, n, 1), n // 2, mats, batch)
+            torch.cuda.synchronize()
+            outs[p] = out
+        assert torch.equal(outs["direct"], outs["segment"])
+        V = P + 1
+        projft = (rng.normal(size=(batch, e)) + 1j * rng.normal(size=(batch, e))).astype(np.complex64)
+        projw = rng.uniform(0.1, 1, size=(batch, e)).astype(np.float32)
+        dpf = torch.from_numpy(projft).cuda().reshape(-1)
+        dpw = torch.from_numpy(projw).cuda().reshape(-1)
+        nv = (V // 2 + 1) * V * V
+        res = {}
+        for b in ("direct", "segment"):
+            _paths("auto", b)
+            vf = torch.zeros(nv, dtype=torch.complex64, device="cuda")
+            vw = torch.zeros(nv, dtype=torch.float32, device="cuda")
+            d_rlnBackproject(vf, vw, (V, V, V), dpf, dpw, (n, n, 1), n // 2, mats, None, (1, 0, 0, 1), 0.0, False,
+                             False, batch)
+            torch.cuda.synchronize()
+            res[b] = (vf.cpu().numpy(), vw.cpu().numpy())
+        assert rel_l2(res["segment"][0], res["direct"][0]) <= 1e-6
+        assert rel_l2(res["segment"][1], res["direct"][1]) <= 1e-6
+        assert np.array_equal(res["segment"][1] == 0, res["direct"][1] == 0)
+    finally:
+        set_brick_tuning("project")
+        set_brick_tuning("backproject")

@@ -24,7 +24,7 @@ from tests.synthdata import blob_volume_ft, random_angles
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(params=["direct", "brick"])
+@pytest.fixture(params=["direct", "brick", "segment"])
 def impl(request, gtom_lib):
     """Runs a test once per implementation of the projector / backprojector."""
     from gtom_b200 import set_path
