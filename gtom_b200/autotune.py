@@ -26,7 +26,7 @@ import torch
 from . import _lib
 from .relion import set_brick_tuning, set_path
 
-EDGES = (12, 16, 20, 24, 28)
+EDGES = (16, 20, 24, 26, 28, 29)
 THREADS = (256, 512, 1024)
 CHUNKS = (512, 2048, 8192)
 

@@ -195,8 +195,9 @@ static std::atomic<int> g_path[2] = {{GTOMRLN_PATH_AUTO}, {GTOMRLN_PATH_AUTO}};
 int path_choice(int op) { return (op == 0 || op == 1) ? g_path[op].load() : GTOMRLN_PATH_AUTO; }
 
 // Defaults measured on the B200 at 256^3 (padding 2) with 10,000-slice
-// batches; the autotuner (gtom_b200/autotune.py) can replace them.
-static const BrickTuning kDefaultTuning[2] = {{28, 1024, 4096}, {24, 1024, 4096}};
+// batches (row-segment variants; the largest bricks whose shared memory fits
+// a CTA win); the autotuner (gtom_b200/autotune.py) can replace them.
+static const BrickTuning kDefaultTuning[2] = {{29, 1024, 4096}, {26, 1024, 4096}};
 static std::mutex g_tuning_mutex;
 static BrickTuning g_tuning[2] = {kDefaultTuning[0], kDefaultTuning[1]};
 

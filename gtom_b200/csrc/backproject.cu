@@ -167,35 +167,38 @@ template <bool DECENTERED>
 __device__ __forceinline__ void bp_flush_brick(float2* __restrict__ volft, float* __restrict__ volw,
                                                const float* are, const float* aim, const float* aw, int B,
                                                int RS, int PS, int3 o, int V, int rowlen, bool exclusive) {
-  for (int e = threadIdx.x; e < B * B * B; e += blockDim.x) {
-    int lx = e % B, t = e / B, ly = t % B, lz = t / B;
-    int k = lz * PS + ly * RS + lx;
-    float r = are[k], im = aim[k], ww = aw[k];
-    if (r == 0.f && im == 0.f && ww == 0.f) continue;
-    int x = o.x + lx, y = o.y + ly, z = o.z + lz;
-    int ys, zs;
-    bool alias;
-    if (DECENTERED) {
-      ys = y < 0 ? y + V : y;
-      zs = z < 0 ? z + V : z;
-      alias = (y == V / 2 || y == -(V / 2) || z == V / 2 || z == -(V / 2));
-    } else {
-      ys = y + V / 2;
-      zs = z + V / 2;
-      alias = false;
-    }
-    if ((unsigned)x > (unsigned)(V / 2) || (unsigned)ys >= (unsigned)V || (unsigned)zs >= (unsigned)V)
-      continue;  // outside the volume: nothing can have been added here
-    int64_t idx = ((int64_t)zs * V + ys) * rowlen + x;
-    if (exclusive && !alias) {
-      if (volft) {
-        float2 c = volft[idx];
-        volft[idx] = make_float2(c.x + r, c.y + im);
+  const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  for (int row = threadIdx.x >> 5; row < B * B; row += nwarps) {  // one warp per (y, z) row
+    const int ly = row % B, lz = row / B;
+    for (int lx = lane; lx < B; lx += 32) {
+      int k = lz * PS + ly * RS + lx;
+      float r = are[k], im = aim[k], ww = aw[k];
+      if (r == 0.f && im == 0.f && ww == 0.f) continue;
+      int x = o.x + lx, y = o.y + ly, z = o.z + lz;
+      int ys, zs;
+      bool alias;
+      if (DECENTERED) {
+        ys = y < 0 ? y + V : y;
+        zs = z < 0 ? z + V : z;
+        alias = (y == V / 2 || y == -(V / 2) || z == V / 2 || z == -(V / 2));
+      } else {
+        ys = y + V / 2;
+        zs = z + V / 2;
+        alias = false;
       }
-      if (volw) volw[idx] += ww;
-    } else {
-      if (volft) red_add2((float*)(volft + idx), r, im);
-      if (volw) red_add(volw + idx, ww);
+      if ((unsigned)x > (unsigned)(V / 2) || (unsigned)ys >= (unsigned)V || (unsigned)zs >= (unsigned)V)
+        continue;  // outside the volume: nothing can have been added here
+      int64_t idx = ((int64_t)zs * V + ys) * rowlen + x;
+      if (exclusive && !alias) {
+        if (volft) {
+          float2 c = volft[idx];
+          volft[idx] = make_float2(c.x + r, c.y + im);
+        }
+        if (volw) volw[idx] += ww;
+      } else {
+        if (volft) red_add2((float*)(volft + idx), r, im);
+        if (volw) red_add(volw + idx, ww);
+      }
     }
   }
 }
@@ -311,8 +314,7 @@ backproject_segment_kernel(float2* __restrict__ volft, float* __restrict__ volw,
                            const float2* __restrict__ projft, const float* __restrict__ projw,
                            const float* __restrict__ mats, BpArgs a, BrickGrid g, PixelSet px,
                            const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
-                           const int* __restrict__ pairs, const PixelBin* __restrict__ bins,
-                           int* __restrict__ counter) {
+                           const int* __restrict__ slices, int* __restrict__ counter) {
   extern __shared__ float acc[];
   __shared__ int item_s, next_s;
   const int nitems = *nitems_ptr;
@@ -337,12 +339,18 @@ backproject_segment_kernel(float2* __restrict__ volft, float* __restrict__ volw,
     const BrickItem it = items[w];
     const int3 o = brick_origin(g, it.brick);
 
-    for (;;) {  // warps take the item's pairs one at a time
+    // warps take the item's pairs one at a time, the next one's slice
+    // fetched before the current one is processed
+    auto take = [&]() {
       int j = 0;
       if (lane == 0) j = atomicAdd(&next_s, 1);
-      j = __shfl_sync(0xffffffffu, j, 0);
-      if (j >= it.count) break;
-      const int slice = bins[__ldg(pairs + it.offset + j)].slice;
+      return __shfl_sync(0xffffffffu, j, 0);
+    };
+    int j = take();
+    int slice = j < it.count ? __ldg(slices + it.offset + j) : 0;
+    while (j < it.count) {
+      const int jn = take();
+      const int next = jn < it.count ? __ldg(slices + it.offset + jn) : 0;
       float m[9];
 #pragma unroll
       for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
@@ -410,6 +418,8 @@ backproject_segment_kernel(float2* __restrict__ volft, float* __restrict__ volw,
           }
         });
       }
+      j = jn;
+      slice = next;
     }
     __syncthreads();
 
@@ -485,7 +495,7 @@ static int backproject_brick(float* d_volumeft, float* d_volumeweights, const fl
   if (segments)
     skern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
         (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, a, g, px,
-        plan.items, plan.nitems, plan.pairs, plan.bins, plan.counter);
+        plan.items, plan.nitems, plan.pairs, plan.counter);
   else
     kern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
         (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, a, g, plan.items,

@@ -110,7 +110,7 @@ struct BrickPlan {
   int max_items = 0;
   BrickItem* items = nullptr;
   int* nitems = nullptr;      // number of valid items
-  int* pairs = nullptr;       // per brick: indices into bins
+  int* pairs = nullptr;       // per brick: indices into bins (segment plan: slices)
   PixelBin* bins = nullptr;
   int* entries = nullptr;     // pixel ids, grouped by bin
   int* counter = nullptr;     // work counter of the persistent kernel (starts at 0)

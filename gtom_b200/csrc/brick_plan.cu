@@ -364,17 +364,20 @@ pairs_scan_kernel(const int* __restrict__ counts, const int* __restrict__ order,
   if (threadIdx.x == 0) *nitems = carry_i;
 }
 
+// Groups the bins by brick: pairs[offsets[b] ..] lists brick b's bins (the
+// binning plan) or directly their slices (the segment plan, whose bins carry
+// nothing else), so that a kernel reaches the slice in one load.
 __global__ void pairs_fill_kernel(const PixelBin* __restrict__ bins,
                                   const unsigned long long* __restrict__ counters, int64_t bins_cap,
                                   const int* __restrict__ counts, const int* __restrict__ offsets,
-                                  int* __restrict__ cursor, int* __restrict__ pairs) {
+                                  int* __restrict__ cursor, int* __restrict__ pairs, int store_slice) {
   int64_t nb = (int64_t)min(counters[1], (unsigned long long)bins_cap);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb;
        i += (int64_t)gridDim.x * blockDim.x) {
     int b = bins[i].brick;
     if (b < 0) continue;  // reserved by a slice that fell back
     int s = atomicAdd(cursor + b, 1);
-    if (s < counts[b]) pairs[offsets[b] + s] = (int)i;
+    if (s < counts[b]) pairs[offsets[b] + s] = store_slice ? bins[i].slice : (int)i;
   }
 }
 
@@ -527,7 +530,7 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     pairs_fill_kernel<<<sms * 4, 256, 0, stream>>>(plan->bins, counters, bins_cap, counts, offsets, cursor,
-                                                   plan->pairs);
+                                                   plan->pairs, segments);
     plan_items_kernel<<<(g.nbricks + 255) / 256, 256, 0, stream>>>(counts, offsets, item_off, g.nbricks, chunk,
                                                                    plan->items);
     e = cudaGetLastError();

@@ -243,14 +243,14 @@ __global__ void __launch_bounds__(1024)
 project_segment_kernel(const float2* __restrict__ vol, float2* __restrict__ proj,
                        const float* __restrict__ mats, ProjArgs a, BrickGrid g, PixelSet px,
                        const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
-                       const int* __restrict__ pairs, const PixelBin* __restrict__ bins,
-                       int* __restrict__ counter) {
+                       const int* __restrict__ slices, int* __restrict__ counter) {
   extern __shared__ float2 tile[];
   __shared__ int item_s, next_s;
   const int nitems = *nitems_ptr;
   const int B = g.B, T = g.B + 1;
   const int rowlen = a.P / 2 + 1;
   const int64_t last = a.nvox - 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (;;) {
     __syncthreads();  // previous item done with the tile
     if (threadIdx.x == 0) {
@@ -262,21 +262,31 @@ project_segment_kernel(const float2* __restrict__ vol, float2* __restrict__ proj
     if (w >= nitems) break;
     const BrickItem it = items[w];
     const int3 o = brick_origin(g, it.brick);
-    for (int k = threadIdx.x; k < T * T * T; k += blockDim.x) {
-      int tx = k % T, t2 = k / T, ty = t2 % T, tz = t2 / T;
-      int x = o.x + tx, y = o.y + ty, z = o.z + tz;
-      int ys = y < 0 ? y + a.P : y, zs = z < 0 ? z + a.P : z;
-      int64_t i = ((int64_t)zs * a.P + ys) * rowlen + x;
-      i = i < 0 ? 0 : (i > last ? last : i);
-      tile[k] = __ldg(vol + i);
+    // stage the brick and its halo, one warp per (y, z) row, lanes along x
+    for (int r = warp; r < T * T; r += nwarps) {
+      const int ty = r % T, tz = r / T;
+      const int y = o.y + ty, z = o.z + tz;
+      const int ys = y < 0 ? y + a.P : y, zs = z < 0 ? z + a.P : z;
+      const int64_t row = ((int64_t)zs * a.P + ys) * rowlen + o.x;
+      for (int tx = lane; tx < T; tx += 32) {
+        int64_t i = row + tx;
+        i = i < 0 ? 0 : (i > last ? last : i);
+        tile[r * T + tx] = __ldg(vol + i);
+      }
     }
     __syncthreads();
-    for (;;) {  // warps take the item's pairs one at a time
+    // warps take the item's pairs one at a time, the next one's slice
+    // fetched before the current one is processed
+    auto take = [&]() {
       int j = 0;
-      if ((threadIdx.x & 31) == 0) j = atomicAdd(&next_s, 1);
-      j = __shfl_sync(0xffffffffu, j, 0);
-      if (j >= it.count) break;
-      const int slice = bins[__ldg(pairs + it.offset + j)].slice;
+      if (lane == 0) j = atomicAdd(&next_s, 1);
+      return __shfl_sync(0xffffffffu, j, 0);
+    };
+    int j = take();
+    int slice = j < it.count ? __ldg(slices + it.offset + j) : 0;
+    while (j < it.count) {
+      const int jn = take();
+      const int next = jn < it.count ? __ldg(slices + it.offset + jn) : 0;
       float m[9];
 #pragma unroll
       for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
@@ -297,6 +307,8 @@ project_segment_kernel(const float2* __restrict__ vol, float2* __restrict__ proj
                                                     c[T * T + T], c[T * T + T + 1]);
         });
       }
+      j = jn;
+      slice = next;
     }
   }
 }
@@ -366,7 +378,7 @@ static int project_brick(const float* d_volumeft, float* d_proj, const float* d_
   if (segments)
     kern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
         (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, px, plan.items, plan.nitems, plan.pairs,
-        plan.bins, plan.counter);
+        plan.counter);
   else
     project_brick_kernel<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
         (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, plan.items, plan.nitems, plan.pairs, plan.bins,

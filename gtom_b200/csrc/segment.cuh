@@ -61,17 +61,25 @@ __device__ __forceinline__ bool seg_rows(const SegBox& b, const PixelSet& px, in
   const float g11 = b.c1(0) * b.c1(0) + b.c1(1) * b.c1(1) + b.c1(2) * b.c1(2);
   const float g01 = b.c0(0) * b.c1(0) + b.c0(1) * b.c1(1) + b.c0(2) * b.c1(2);
   const float det = g00 * g11 - g01 * g01;
-  // v(p) = w . p on the plane, w = (g00 c1 - g01 c0) / det.  Near-parallel
-  // columns (det small against g00 g11) keep the full row range.
+  // v(p) = w . p and u(p) = w' . p on the plane, w = (g00 c1 - g01 c0) / det,
+  // w' = (g11 c0 - g01 c1) / det: their extremes over the box bound the rows
+  // and reject a box that lies wholly at u < 0 (the other side's pixels).
+  // Near-parallel columns (det small against g00 g11) keep the full range.
   if (det > 1e-3f * g00 * g11 && g00 > 0.f) {
     const float inv = 1.f / det;
-    float vc = 0.f, vh = 0.f;
+    float vc = 0.f, vh = 0.f, uc = 0.f, uh = 0.f;
 #pragma unroll
     for (int r = 0; r < 3; r++) {
       const float w = (g00 * b.c1(r) - g01 * b.c0(r)) * inv;
-      vc = fmaf(w, 0.5f * (b.lo(r) + b.hi(r)), vc);
-      vh = fmaf(fabsf(w), 0.5f * (b.hi(r) - b.lo(r)), vh);
+      const float wu = (g11 * b.c0(r) - g01 * b.c1(r)) * inv;
+      const float c = 0.5f * (b.lo(r) + b.hi(r)), h = 0.5f * (b.hi(r) - b.lo(r));
+      vc = fmaf(w, c, vc);
+      vh = fmaf(fabsf(w), h, vh);
+      uc = fmaf(wu, c, uc);
+      uh = fmaf(fabsf(wu), h, uh);
     }
+    const float upad = 0.5f + 1e-3f * (fabsf(uc) + uh);
+    if (uc + uh + upad < 0.f || uc - uh - upad > (float)(px.dimft - 1)) return false;
     const float pad = 0.5f + 1e-3f * (fabsf(vc) + vh);
     const float flo = fmaxf(vc - vh - pad, -1e6f), fhi = fminf(vc + vh + pad, 1e6f);
     vlo = max(vlo, (int)floorf(flo));
@@ -81,19 +89,21 @@ __device__ __forceinline__ bool seg_rows(const SegBox& b, const PixelSet& px, in
 }
 
 // Pixel interval [ua, ub] of row v holding the box, clipped to the pixel set
-// (ub < ua when empty).
+// (ub < ua when empty).  The bounds multiply by the correctly rounded
+// reciprocal of the column entry: one more rounding, far inside the margin.
 __device__ __forceinline__ void seg_row(const SegBox& b, const PixelSet& px, int v, int& ua, int& ub) {
   float umin = -1.f, umax = (float)px.dimft;
 #pragma unroll
   for (int r = 0; r < 3; r++) {
     const float a = b.c0(r), t = (float)v * b.c1(r);
     const float l = b.lo(r) - t, h = b.hi(r) - t;
-    if (a > 0.f) {
-      umin = fmaxf(umin, l / a);
-      umax = fminf(umax, h / a);
-    } else if (a < 0.f) {
-      umin = fmaxf(umin, h / a);
-      umax = fminf(umax, l / a);
+    // |a| <= 1e-20 moves a * u by < 1e-16 over the row: a u-free test, which
+    // the margin keeps conservative (and 1 / a stays finite otherwise)
+    if (fabsf(a) > 1e-20f) {
+      const float ra = __frcp_rn(a);
+      const float e0 = l * ra, e1 = h * ra;
+      umin = fmaxf(umin, fminf(e0, e1));
+      umax = fminf(umax, fmaxf(e0, e1));
     } else if (l > 0.f || h < 0.f) {
       umin = 1.f;
       umax = 0.f;
