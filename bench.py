@@ -57,6 +57,9 @@ def parse_args():
     ap.add_argument("--e2e-batch", type=int, default=2000)
     ap.add_argument("--path", default="auto", choices=["auto", "direct", "brick", "segment"],
                     help="implementation of the projector and backprojector (gtomrln_set_path)")
+    ap.add_argument("--sweep", action="store_true",
+                    help="instead of the bench: run the autotuner over brick edge x threads x pairs per "
+                         "item for both operators on one step's workload and print the tables")
     ap.add_argument("--no-gridding", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip gridding, e2e, CPU baseline and L2 probes (profiling runs)")
@@ -398,8 +401,9 @@ def time_gridding(G, torch, acc_ft, acc_w, n, D, dev):
 def time_extensions(args, G, torch, ws, acc_ft, acc_w, dev, hbm_peak, probe):
     """The next operators on the same workload, CUDA events around one call
     after one untimed call: the shifted projector and backprojector (a
-    per-slice phase shift and global weight; direct kernels) and the
-    particle preprocessing (batched R2C + centring phase + CTF and CTF^2)."""
+    per-slice phase shift and global weight; row-segment brick kernels, like
+    the main pair) and the particle preprocessing (batched R2C + centring
+    phase + CTF and CTF^2)."""
     from gtom_b200.ctf import preprocess_particles
     n, P, D, rmax, e = ws["n"], ws["P"], ws["D"], ws["rmax"], ws["e"]
     B = min(args.batch, ws["N"])
@@ -429,8 +433,10 @@ def time_extensions(args, G, torch, ws, acc_ft, acc_w, dev, hbm_peak, probe):
                                                  ws["wts"][:B].reshape(-1), (n, n, 1), rmax, m, shifts, gw, B))
     reds = B * ws["sp"] * 24
     l2 = probe.get("l2_red_v2_gadds")
+    sm = probe.get("smem_f32_atomic_gadds")
     res["backproject_shifted"] = {"slices_per_s": round(B / (ms * 1e-3), 1), "ms": round(ms, 3),
                                   "g_reductions_per_s": round(reds / (ms * 1e-3) / 1e9, 1),
+                                  "frac_of_smem_atomic": None if not sm else round(reds / (ms * 1e-3) / 1e9 / sm, 4),
                                   "frac_of_l2_red_v2": None if not l2 else round(reds / (ms * 1e-3) / 1e9 / l2, 4)}
     imgs = torch.randn((B, n, n), device=dev)
     params = [dict(defocus=-float(d) * 1e-6) for d in rng.uniform(0.5, 3.0, B)]
@@ -751,8 +757,48 @@ def ncu_traffic():
     return {}
 
 
+def run_sweep(args):
+    """The autotuner's tables for both operators on one step of the bench's
+    workload (gtom_b200.autotune.tune: median of 3 timed calls per shape)."""
+    import torch
+    import gtom_b200 as G
+    from gtom_b200 import autotune
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    G.set_path("project", args.path)
+    G.set_path("backproject", args.path)
+    a2 = argparse.Namespace(**vars(args))
+    a2.pool = args.batch
+    ws = make_workload(a2, dev, SEED)
+    n, P, D, rmax, e, B = ws["n"], ws["P"], ws["D"], ws["rmax"], ws["e"], args.batch
+    nvol = (D // 2 + 1) * D * D
+    acc_ft = torch.zeros(nvol, dtype=torch.complex64, device=dev)
+    acc_w = torch.zeros(nvol, dtype=torch.float32, device=dev)
+    proj = torch.empty(B * e, dtype=torch.complex64, device=dev)
+    m = ws["mats"][:B].reshape(-1)
+
+    def run_p():
+        G.d_rlnProject(ws["volft"], (P, P, P), proj, (n, n, 1), rmax, m, B)
+
+    def run_b():
+        G.d_rlnBackproject(acc_ft, acc_w, (D, D, D), ws["data"][:B].reshape(-1), ws["wts"][:B].reshape(-1),
+                           (n, n, 1), rmax, m, None, (1, 0, 0, 1), 0.0, False, False, B)
+
+    out = {}
+    for op, fn in (("project", run_p), ("backproject", run_b)):
+        cands = autotune.candidates(op, threads=(512, 768, 1024), chunks=(1024, 4096, 16384))
+        res = autotune.tune(op, fn, cands, reps=3, path="brick" if args.path == "brick" else "segment")
+        out[op] = {"best": res["best"], "ms": round(res["ms"], 3),
+                   "table": [(e_, t_, c_, round(ms, 3)) for e_, t_, c_, ms in sorted(res["table"], key=lambda r: r[3])]}
+        G.set_brick_tuning(op)  # back to the compiled-in default for the next operator's timing
+    print(json.dumps({"sweep": out, "path": args.path, "batch": B, "box": n, "padding": PAD}), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.sweep:
+        run_sweep(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

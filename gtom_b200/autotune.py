@@ -54,11 +54,12 @@ def _time(fn: Callable[[], None], reps: int) -> float:
     return statistics.median(ts)
 
 
-def tune(op: str, run: Callable[[], None], cands=None, reps: int = 3) -> dict:
-    """Times `run` (one call of the op) under every candidate launch shape and
+def tune(op: str, run: Callable[[], None], cands=None, reps: int = 3, path: str = "segment") -> dict:
+    """Times `run` (one call of the op) under every candidate launch shape of
+    the brick-major `path` ("segment", the default variant, or "brick") and
     installs the fastest.  Returns {"best": (edge, threads, chunk), "ms": ...,
     "table": [(edge, threads, chunk, ms), ...]}."""
-    set_path(op, "segment")  # the default brick-major variant
+    set_path(op, path)
     table = []
     try:
         for e, t, c in (cands or candidates(op)):

@@ -162,8 +162,11 @@ constexpr unsigned kBrickMinBatch = 32;
 // Adds a brick's shared-memory accumulators to the volume: plain
 // read-add-write when the work item is the brick's only one and the voxel has
 // no alias (decentred y or z = +-V/2 share storage), else vector L2
-// reductions.  Voxels that received nothing are skipped.
-template <bool DECENTERED>
+// reductions.  Voxels that received nothing are skipped.  CLAMP (centred
+// only): voxels beyond the volume are folded onto its edge with the clamps
+// of place<false> (unsigned compares) instead of being skipped, and every
+// voxel of the faces they fold onto counts as an alias.
+template <bool DECENTERED, bool CLAMP = false>
 __device__ __forceinline__ void bp_flush_brick(float2* __restrict__ volft, float* __restrict__ volw,
                                                const float* are, const float* aim, const float* aw, int B,
                                                int RS, int PS, int3 o, int V, int rowlen, bool exclusive) {
@@ -186,8 +189,18 @@ __device__ __forceinline__ void bp_flush_brick(float2* __restrict__ volft, float
         zs = z + V / 2;
         alias = false;
       }
-      if ((unsigned)x > (unsigned)(V / 2) || (unsigned)ys >= (unsigned)V || (unsigned)zs >= (unsigned)V)
+      if (CLAMP && !DECENTERED) {
+        const unsigned cx = min((unsigned)x, (unsigned)(V / 2)), cy = min((unsigned)ys, (unsigned)(V - 1)),
+                       cz = min((unsigned)zs, (unsigned)(V - 1));
+        // every voxel on a face the clamps fold onto, not only the folded
+        // ones: a plain read-add-write there would race with their reductions
+        alias = cx == (unsigned)(V / 2) || cy == (unsigned)(V - 1) || cz == (unsigned)(V - 1);
+        x = (int)cx;
+        ys = (int)cy;
+        zs = (int)cz;
+      } else if ((unsigned)x > (unsigned)(V / 2) || (unsigned)ys >= (unsigned)V || (unsigned)zs >= (unsigned)V) {
         continue;  // outside the volume: nothing can have been added here
+      }
       int64_t idx = ((int64_t)zs * V + ys) * rowlen + x;
       if (exclusive && !alias) {
         if (volft) {
@@ -523,9 +536,15 @@ __global__ void __launch_bounds__(kBpThreads)
 backproject_shifted_kernel(float2* __restrict__ volft, float* __restrict__ volw,
                            const float2* __restrict__ projft, const float* __restrict__ projw,
                            const float* __restrict__ mats, const float* __restrict__ shifts,
-                           const float* __restrict__ gweights, BpArgs a, int rmax) {
-  const int slice = blockIdx.x / a.tiles;
-  const int tile = blockIdx.x - slice * a.tiles;
+                           const float* __restrict__ gweights, BpArgs a, int rmax,
+                           const int* __restrict__ list = nullptr, const int* __restrict__ nlist = nullptr) {
+  // Without a list the grid covers every (slice, tile) once; with one (the
+  // slices a brick plan left over) a persistent grid strides over them.
+  const int64_t total = list ? (int64_t)(*nlist) * a.tiles : (int64_t)gridDim.x;
+  for (int64_t work = blockIdx.x; work < total; work += gridDim.x) {
+  const int entry = (int)(work / a.tiles);
+  const int tile = (int)(work - (int64_t)entry * a.tiles);
+  const int slice = list ? __ldg(list + entry) : entry;
   float m[9];
 #pragma unroll
   for (int i = 0; i < 9; i++) m[i] = __ldg(mats + 9 * (int64_t)slice + i);
@@ -586,6 +605,168 @@ backproject_shifted_kernel(float2* __restrict__ volft, float* __restrict__ volw,
       if (volw) red_add(volw + o, w[i] * pw);
     }
   }
+  }  // work loop
+}
+
+// Segment variant of the shifted insertion for 2D slices: per sample the
+// arithmetic of backproject_shifted_kernel (Friedel flip of the position when
+// pos.x + 1e-5 < 0, plain trilinear weights on the 2x2x2 cube at the flipped
+// position's base voxel, the sample times exp(i phi) and the slice's weight),
+// with the targets accumulated per shared-memory brick as in
+// backproject_segment_kernel.  Side 0 walks the unflipped samples, side 1
+// the flipped ones (negated positions), each over the brick widened by one
+// voxel below; a sample's eight targets are added by the pairs of their
+// bricks on the side of its flip.  Centred output.  The brick grid reaches one
+// voxel past the volume (the insertion takes the whole rmax disk, so at
+// padding 2 the rim's cubes reach x = V/2 + 1), and the flush folds those
+// voxels onto the edge with the direct kernel's clamps.
+__global__ void __launch_bounds__(1024)
+backproject_shifted_segment_kernel(float2* __restrict__ volft, float* __restrict__ volw,
+                                   const float2* __restrict__ projft, const float* __restrict__ projw,
+                                   const float* __restrict__ mats, const float* __restrict__ shifts,
+                                   const float* __restrict__ gweights, BpArgs a, BrickGrid g, PixelSet px,
+                                   const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
+                                   const int* __restrict__ slices, int* __restrict__ counter) {
+  extern __shared__ float acc[];
+  __shared__ int item_s, next_s;
+  const int nitems = *nitems_ptr;
+  const int B = g.B, RS = g.B + 1, PS = (g.B + 1) * (g.B + 1), NA = g.B * PS;
+  float* are = acc;
+  float* aim = acc + NA;
+  float* aw = acc + 2 * NA;
+  const int lane = threadIdx.x & 31;
+  const int V = a.P;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      item_s = atomicAdd(counter, 1);
+      next_s = 0;
+    }
+    for (int k = threadIdx.x; k < 3 * NA; k += blockDim.x) acc[k] = 0.f;
+    __syncthreads();
+    const int w = item_s;
+    if (w >= nitems) break;
+    const BrickItem it = items[w];
+    const int3 o = brick_origin(g, it.brick);
+    auto take = [&]() {
+      int j = 0;
+      if (lane == 0) j = atomicAdd(&next_s, 1);
+      return __shfl_sync(0xffffffffu, j, 0);
+    };
+    int j = take();
+    int slice = j < it.count ? __ldg(slices + it.offset + j) : 0;
+    while (j < it.count) {
+      const int jn = take();
+      const int next = jn < it.count ? __ldg(slices + it.offset + jn) : 0;
+      float m[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
+      const float sx = __ldg(shifts + 3 * (int64_t)slice), sy = __ldg(shifts + 3 * (int64_t)slice + 1);
+      const float gw = __ldg(gweights + slice);
+      const int64_t sbase = a.elements * slice;
+#pragma unroll 1
+      for (int side = 0; side < 2; side++) {
+        const SegBox box = seg_box(m, side, o, B, 1.f);
+        seg_for_each_pixel(box, px, [&](int u, int v, bool valid) {
+          if (!valid) return;
+          float3 pos = mat_apply(m, (float)u, (float)v, 0.f);
+          const bool flip = pos.x + 1e-5f < 0.f;
+          if (flip != (side == 1)) return;  // the other side's sample
+          float sign = 1.f;
+          if (flip) {
+            pos.x = fabsf(pos.x);
+            pos.y = -pos.y;
+            pos.z = -pos.z;
+            sign = -1.f;
+          }
+          const int x0 = (int)floorf(pos.x + 1e-5f);
+          const float fx = pos.x - (float)x0;
+          const int y0 = (int)floorf(pos.y);
+          const float fy = pos.y - (float)y0;
+          const int z0 = (int)floorf(pos.z);
+          const float fz = pos.z - (float)z0;
+          const int lx0 = x0 - o.x, ly0 = y0 - o.y, lz0 = z0 - o.z;
+          if (lx0 < -1 || lx0 >= B || ly0 < -1 || ly0 >= B || lz0 < -1 || lz0 >= B) return;
+          const float c0 = 1.f - fz, c1 = fz;
+          const float c00 = (1.f - fy) * c0, c10 = fy * c0, c01 = (1.f - fy) * c1, c11 = fy * c1;
+          const float wt[8] = {(1.f - fx) * c00, fx * c00, (1.f - fx) * c10, fx * c10,
+                               (1.f - fx) * c01, fx * c01, (1.f - fx) * c11, fx * c11};
+          const int idy = v < 0 ? v + a.n : v;
+          const int64_t id = sbase + (int64_t)idy * a.dimft + u;
+          const float2 val = projft ? __ldg(projft + id) : make_float2(1.f, 0.f);
+          float phase = fmaf((float)u, sx, (float)v * sy);
+          phase = -phase;
+          const float c = __cosf(phase), sn = __sinf(phase);
+          float re = fmaf(val.x, c, -(val.y * sn)), im = fmaf(val.x, sn, val.y * c);
+          im *= sign;
+          re *= gw;
+          im *= gw;
+          const float pw = (projw ? __ldg(projw + id) : 1.f) * gw;
+#pragma unroll
+          for (int i = 0; i < 8; i++) {
+            const int lx = lx0 + (i & 1), ly = ly0 + ((i >> 1) & 1), lz = lz0 + ((i >> 2) & 1);
+            if ((unsigned)lx < (unsigned)B && (unsigned)ly < (unsigned)B && (unsigned)lz < (unsigned)B) {
+              const int k = lz * PS + ly * RS + lx;
+              atomicAdd(are + k, wt[i] * re);
+              atomicAdd(aim + k, wt[i] * im);
+              atomicAdd(aw + k, wt[i] * pw);
+            }
+          }
+        });
+      }
+      j = jn;
+      slice = next;
+    }
+    __syncthreads();
+    bp_flush_brick<false, true>(volft, volw, are, aim, aw, B, RS, PS, o, V, a.rowlen, it.exclusive != 0);
+  }
+}
+
+// The segment path of the shifted insertion: plan, segment kernel, and the
+// direct kernel for any slice the plan could not take.  Nothing synchronises.
+static int backproject_shifted_brick(float* d_volumeft, float* d_volumeweights, const float* d_projft,
+                                     const float* d_projweights, const float* d_mats, const float* d_shifts,
+                                     const float* d_gweights, const BpArgs& a, int rmax, unsigned batch,
+                                     cudaStream_t stream) {
+  const int V = a.P;
+  // While every sample radius stays below V/2 + 0.99, the cubes' voxels lie
+  // in x [0, V/2 + 1] and y, z [-V/2 - 1, V/2 + 1] (centred, before clamps).
+  const float limit = (float)(V / 2) + 0.99f;
+  const BrickTuning tune = brick_tuning(GTOMRLN_OP_BACKPROJECT);
+  BrickGrid g = make_brick_grid(V, tune.edge, V / 2 + 1, -(V / 2) - 1, V / 2 + 1);
+  size_t smem = sizeof(float) * 3 * (size_t)tune.edge * (tune.edge + 1) * (tune.edge + 1);
+  cudaError_t e = cudaFuncSetAttribute(backproject_shifted_segment_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess)
+    return set_error(GTOMRLN_ERR_CUDA, "shifted brick backprojector: %zu B of shared memory refused: %s", smem,
+                     cudaGetErrorString(e));
+  int dev = 0, sms = 148, occ = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, backproject_shifted_segment_kernel, tune.threads, smem);
+  PixelSet px;
+  px.n = a.n;
+  px.dimft = a.dimft;
+  px.elements = a.elements;
+  px.rmax2 = a.rmax2;
+  px.strict = 0;  // r^2 <= rmax^2, the whole x = 0 column
+  px.pmax = (float)rmax;
+  BrickPlan plan;
+  int st = build_brick_plan(GTOMRLN_OP_BACKPROJECT, d_mats, (int)batch, g, px, limit, tune.chunk, stream, &plan,
+                            1);
+  if (st) return st;
+  backproject_shifted_segment_kernel<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
+      (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, d_shifts, d_gweights,
+      a, g, px, plan.items, plan.nitems, plan.pairs, plan.counter);
+  backproject_shifted_kernel<2><<<sms * 4, kBpThreads, 0, stream>>>(
+      (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, d_shifts, d_gweights,
+      a, rmax, plan.fallback, plan.nfallback);
+  e = cudaGetLastError();
+  free_brick_plan(&plan, stream);
+  if (e != cudaSuccess)
+    return set_error(GTOMRLN_ERR_CUDA, "launch of the shifted brick backprojector failed: %s",
+                     cudaGetErrorString(e));
+  return GTOMRLN_OK;
 }
 
 static int backproject_launch(float* d_volumeft, float* d_volumeweights, int vx, int vy, int vz,
@@ -717,6 +898,12 @@ int gtomrln_backproject_shifted(float* d_volumeft, float* d_volumeweights, int v
   a.ewalddiaminv = 0.f;
   if ((int64_t)a.tiles * batch > 0x7fffffffLL)
     return set_error(GTOMRLN_ERR_INVALID, "backproject_shifted: batch too large for one launch");
+  const int choice = path_choice(GTOMRLN_OP_BACKPROJECT);
+  if (ndp == 2 && vx == vy && vx == vz && vx >= 4 && (d_volumeft || d_volumeweights) &&
+      (choice == GTOMRLN_PATH_BRICK || choice == GTOMRLN_PATH_SEGMENT ||
+       (choice == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch)))
+    return backproject_shifted_brick(d_volumeft, d_volumeweights, d_projft, d_projweights, d_matrices, d_shifts,
+                                     d_globalweights, a, (int)rmax, batch, (cudaStream_t)stream);
   dim3 grid((unsigned)(a.tiles * (int64_t)batch));
   if (ndp == 2)
     backproject_shifted_kernel<2><<<grid, kBpThreads, 0, (cudaStream_t)stream>>>(

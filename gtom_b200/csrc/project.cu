@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <mutex>
+#include <type_traits>
 
 #include "brick.cuh"
 #include "common.cuh"
@@ -156,12 +157,14 @@ project_direct_kernel(Fetch fetch, float2* __restrict__ proj, const float* __res
 
 // The direct kernel over the slices listed in list[0 .. *nlist), which the
 // brick plan left to it; a persistent grid strides over (slice, tile).
+template <class Post = NoPost>
 __global__ void __launch_bounds__(kProjThreads)
 project_listed_kernel(ArrayFetch fetch, float2* __restrict__ proj, const float* __restrict__ mats,
-                      ProjArgs a, const int* __restrict__ list, const int* __restrict__ nlist) {
+                      ProjArgs a, const int* __restrict__ list, const int* __restrict__ nlist,
+                      Post post = Post()) {
   const int64_t total = (int64_t)(*nlist) * a.tiles;
   for (int64_t w = blockIdx.x; w < total; w += gridDim.x)
-    project_direct_tile<2>(fetch, proj, mats, a, __ldg(list + w / a.tiles), (int)(w % a.tiles));
+    project_direct_tile<2>(fetch, proj, mats, a, __ldg(list + w / a.tiles), (int)(w % a.tiles), post);
 }
 
 // ---------------------------------------------------------------------------
@@ -238,12 +241,15 @@ project_brick_kernel(const float2* __restrict__ vol, float2* __restrict__ proj,
 // pixels itself, by row segments (segment.cuh), among those whose position
 // (side 0) or mirrored position (side 1) falls in the brick.  A pixel is
 // written by the pair whose brick holds its base voxel, on the side of its
-// Friedel flip: exactly one pair, as in the binned variant.
+// Friedel flip: exactly one pair, as in the binned variant.  Post turns the
+// interpolated value into the stored one (identity, or the phase shift and
+// weight of d_rlnProjectShifted), as in the direct kernel.
+template <class Post = NoPost>
 __global__ void __launch_bounds__(1024)
 project_segment_kernel(const float2* __restrict__ vol, float2* __restrict__ proj,
                        const float* __restrict__ mats, ProjArgs a, BrickGrid g, PixelSet px,
                        const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
-                       const int* __restrict__ slices, int* __restrict__ counter) {
+                       const int* __restrict__ slices, int* __restrict__ counter, Post post = Post()) {
   extern __shared__ float2 tile[];
   __shared__ int item_s, next_s;
   const int nitems = *nitems_ptr;
@@ -303,8 +309,9 @@ project_segment_kernel(const float2* __restrict__ vol, float2* __restrict__ proj
             return;  // another brick's pixel
           const float2* c = tile + (lz * T + ly) * T + lx;
           const int idy = v < 0 ? v + a.n : v;
-          out[(int64_t)idy * a.dimft + u] = trilerp(s, c[0], c[1], c[T], c[T + 1], c[T * T], c[T * T + 1],
-                                                    c[T * T + T], c[T * T + T + 1]);
+          const float2 val = trilerp(s, c[0], c[1], c[T], c[T + 1], c[T * T], c[T * T + 1], c[T * T + T],
+                                     c[T * T + T + 1]);
+          out[(int64_t)idy * a.dimft + u] = post.template apply<2>(slice, u, v, 0, val);
         });
       }
       j = jn;
@@ -338,18 +345,20 @@ __global__ void project_zero_kernel(float2* __restrict__ proj, ProjArgs a, int64
 constexpr unsigned kBrickMinBatch = 32;
 
 // The brick path: plan, zero fill outside rmax, brick kernel, and the direct
-// kernel for any slice the plan could not take.  Nothing synchronises.
+// kernel for any slice the plan could not take.  Nothing synchronises.  A
+// Post other than NoPost (the shifted projector) takes the segment variant.
+template <class Post = NoPost>
 static int project_brick(const float* d_volumeft, float* d_proj, const float* d_mats, const ProjArgs& a,
-                         unsigned batch, cudaStream_t stream, int segments) {
+                         unsigned batch, cudaStream_t stream, int segments, Post post = Post()) {
+  if (!std::is_same<Post, NoPost>::value) segments = 1;
   const int P = a.P;
   const BrickTuning tune = brick_tuning(GTOMRLN_OP_PROJECT);
   // While every sample radius stays below P/2 + 0.99, the base voxels lie in
   // x [0, P/2] and y, z [-P/2 - 1, P/2].
   BrickGrid g = make_brick_grid(P, tune.edge, P / 2, -(P / 2) - 1, P / 2);
   size_t smem = sizeof(float2) * (size_t)(tune.edge + 1) * (tune.edge + 1) * (tune.edge + 1);
-  auto kern = segments ? project_segment_kernel : nullptr;
-  cudaError_t e = segments ? cudaFuncSetAttribute(project_segment_kernel,
-                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+  auto kern = project_segment_kernel<Post>;
+  cudaError_t e = segments ? cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
                            : cudaFuncSetAttribute(project_brick_kernel,
                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess)
@@ -359,7 +368,7 @@ static int project_brick(const float* d_volumeft, float* d_proj, const float* d_
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (segments)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, project_segment_kernel, tune.threads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, tune.threads, smem);
   else
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, project_brick_kernel, tune.threads, smem);
   PixelSet px;
@@ -378,14 +387,14 @@ static int project_brick(const float* d_volumeft, float* d_proj, const float* d_
   if (segments)
     kern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
         (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, px, plan.items, plan.nitems, plan.pairs,
-        plan.counter);
+        plan.counter, post);
   else
     project_brick_kernel<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
         (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, plan.items, plan.nitems, plan.pairs, plan.bins,
         plan.entries, plan.counter);
   ArrayFetch f{(const float2*)d_volumeft, a.P, a.P / 2 + 1, a.nvox - 1};
-  project_listed_kernel<<<sms * 4, kProjThreads, 0, stream>>>(f, (float2*)d_proj, d_mats, a, plan.fallback,
-                                                               plan.nfallback);
+  project_listed_kernel<Post><<<sms * 4, kProjThreads, 0, stream>>>(f, (float2*)d_proj, d_mats, a, plan.fallback,
+                                                                     plan.nfallback, post);
   e = cudaGetLastError();
   free_brick_plan(&plan, stream);
   if (e != cudaSuccess)
@@ -578,6 +587,12 @@ int gtomrln_project_shifted(const float* d_volumeft, int vx, int vy, int vz, flo
   if (st) return st;
   if (batch && (!d_volumeft || !d_proj || !d_matrices || !d_shifts || !d_globalweights))
     return set_error(GTOMRLN_ERR_INVALID, "project_shifted: NULL device pointer");
+  const int choice = path_choice(GTOMRLN_OP_PROJECT);
+  if (ndp == 2 && vx == vy && vx == vz && vx >= 4 &&
+      (choice == GTOMRLN_PATH_BRICK || choice == GTOMRLN_PATH_SEGMENT ||
+       (choice == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch)))
+    return project_brick(d_volumeft, d_proj, d_matrices, a, batch, (cudaStream_t)stream, 1,
+                         ShiftPost{d_shifts, d_globalweights});
   ArrayFetch f{(const float2*)d_volumeft, a.P, a.P / 2 + 1, a.nvox - 1};
   return launch_project(f, ndp, d_proj, d_matrices, a, batch, (cudaStream_t)stream,
                         ShiftPost{d_shifts, d_globalweights});

@@ -17,8 +17,19 @@ def cu(a, dtype=None):
     return (t if dtype is None else t.to(dtype)).cuda()
 
 
+@pytest.fixture(params=["auto", "segment"])
+def path(request, gtom_lib):
+    """The small golden batches take the direct kernels under "auto"; forcing
+    "segment" runs the same cases through the brick-major segment kernels."""
+    G.set_path("project", request.param)
+    G.set_path("backproject", request.param)
+    yield request.param
+    G.set_path("project", "auto")
+    G.set_path("backproject", "auto")
+
+
 @pytest.mark.parametrize("name", ["project_shifted_2d", "project_shifted_3d"])
-def test_project_shifted_matches_reference(gtom_lib, cuda, name):
+def test_project_shifted_matches_reference(gtom_lib, cuda, name, path):
     g = load_golden(name)
     P, n, nd, rmax = int(g["P"]), int(g["n"]), int(g["ndims"]), int(g["rmax"])
     batch = g["matrices"].shape[0]
@@ -86,7 +97,7 @@ def test_project_shifted_texture_overload(gtom_lib, cuda):
 
 
 @pytest.mark.parametrize("name", ["bp_shifted_2d", "bp_shifted_3d"])
-def test_backproject_shifted_matches_reference(gtom_lib, cuda, name):
+def test_backproject_shifted_matches_reference(gtom_lib, cuda, name, path):
     g = load_golden(name)
     V, n, nd, rmax = int(g["V"]), int(g["n"]), int(g["ndims"]), int(g["rmax"])
     batch = g["matrices"].shape[0]
@@ -119,3 +130,50 @@ def test_shifted_rejects_bad_dims(gtom_lib, cuda):
     m = torch.zeros(9, dtype=torch.float32, device="cuda")
     with pytest.raises(G.GtomError):  # a 2D volume: the reference throws
         G.d_rlnBackprojectShifted(v, w, (4, 4, 1), None, None, (4, 4, 1), 2, m, m[:3], m[:1], 1)
+
+
+@pytest.mark.parametrize("V,sheared", [(129, False), (128, False), (129, True)])
+def test_shifted_segment_paths_match_direct(gtom_lib, cuda, V, sheared):
+    """The segment kernels of both shifted operators against their direct
+    kernels on a batch above the brick threshold: the projector bit for bit
+    (same arithmetic, same fast sine and cosine), the insertion to FP32
+    rounding of the sums (odd and even centred volumes, sheared matrices)."""
+    from tests.synthdata import blob_volume_ft, random_angles
+    rng = np.random.default_rng(V + 7 * sheared)
+    n, batch = 64, 160
+    e = (n // 2 + 1) * n
+    m = G.matrices_from_angles(random_angles(rng, batch), 2.0).reshape(batch, 9)
+    if sheared:
+        m = ((m + rng.normal(scale=0.3, size=m.shape)) * 0.8).astype(np.float32)
+    shifts = rng.normal(scale=0.2, size=(batch, 3)).astype(np.float32)
+    gws = rng.uniform(0.5, 1.5, batch).astype(np.float32)
+    P = 2 * n
+    vol = cu(blob_volume_ft(rng, n, P, 12).astype(np.complex64)).reshape(-1)
+    outs = {}
+    try:
+        for p in ("direct", "segment"):
+            G.set_path("project", p)
+            out = torch.full((batch * e,), complex(np.nan, np.nan), dtype=torch.complex64, device="cuda")
+            G.d_rlnProjectShifted(vol, (P, P, P), out, (n, n, 1), n // 2, cu(m).reshape(-1), cu(shifts).reshape(-1),
+                                  cu(gws), batch)
+            torch.cuda.synchronize()
+            outs[p] = out
+        assert torch.equal(outs["direct"], outs["segment"])
+        pf = (rng.normal(size=(batch, e)) + 1j * rng.normal(size=(batch, e))).astype(np.complex64)
+        pw = rng.uniform(0.1, 1, size=(batch, e)).astype(np.float32)
+        nv = (V // 2 + 1) * V * V
+        res = {}
+        for p in ("direct", "segment"):
+            G.set_path("backproject", p)
+            vf = torch.zeros(nv, dtype=torch.complex64, device="cuda")
+            vw = torch.zeros(nv, dtype=torch.float32, device="cuda")
+            G.d_rlnBackprojectShifted(vf, vw, (V, V, V), cu(pf).reshape(-1), cu(pw).reshape(-1), (n, n, 1), n // 2,
+                                      cu(m).reshape(-1), cu(shifts).reshape(-1), cu(gws), batch)
+            torch.cuda.synchronize()
+            res[p] = (vf.cpu().numpy(), vw.cpu().numpy())
+        assert rel_l2(res["segment"][0], res["direct"][0]) <= 1e-6
+        assert rel_l2(res["segment"][1], res["direct"][1]) <= 1e-6
+        assert np.array_equal(res["segment"][1] == 0, res["direct"][1] == 0)
+    finally:
+        G.set_path("project", "auto")
+        G.set_path("backproject", "auto")
