@@ -448,7 +448,76 @@ def time_extensions(args, G, torch, ws, acc_ft, acc_w, dev, hbm_peak, probe):
                                    "compulsory_gbs": round(byt / (ms * 1e-3) / 1e9, 1),
                                    "frac_of_hbm": round(byt / (ms * 1e-3) / 1e9 / hbm_peak, 4)}
     del imgs, proj
+    res.update(time_next_rows(G, torch, ws, dev, hbm_peak, probe))
     return res
+
+
+def time_next_rows(G, torch, ws, dev, hbm_peak, probe):
+    """The remaining operators beside the path, one timed call each after one
+    untimed call: the 3D->3D projector (64 rotations of a 128^3 box from the
+    bench's 512^3 padded volume), the dense squared differences of the
+    E-step (64 particles x 256 references x 128 shifts at 128^2, groups of
+    8 x 8) and the tomographic gather insertion (41 tilts of 128^2 into a
+    128^3 volume)."""
+    from gtom_b200.estep import d_rlnSquaredDifferences
+    from gtom_b200 import synth
+    rng = np.random.default_rng(11)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    out = {}
+    # 3D -> 3D projection: rotated copies of the volume's 128^3 central region
+    P, n3, nb = ws["P"], 128, 64
+    r3 = n3 // 2
+    e3 = (n3 // 2 + 1) * n3 * n3
+    x = np.arange(n3 // 2 + 1)[None, None, :]
+    yz = np.where(np.arange(n3) <= n3 // 2, np.arange(n3), np.arange(n3) - n3)
+    samples = int(((x ** 2 + yz[None, :, None] ** 2 + yz[:, None, None] ** 2) <= r3 * r3).sum())
+    mats = torch.from_numpy(G.matrices_from_angles(synth.vmf_mixture_angles(rng, nb), float(P // n3))).to(dev)
+    proj3 = torch.empty(nb * e3, dtype=torch.complex64, device=dev)
+    ms = timed(lambda: G.d_rlnProject(ws["volft"], (P, P, P), proj3, (n3, n3, n3), r3, mats.reshape(-1), nb))
+    byt = nb * (samples * 72 + (e3 - samples) * 8)
+    out["project_3d"] = {"volumes_per_s": round(nb / (ms * 1e-3), 1), "ms": round(ms, 3), "box": n3,
+                         "algorithmic_gbs": round(byt / (ms * 1e-3) / 1e9, 1),
+                         "frac_of_hbm": round(byt / (ms * 1e-3) / 1e9 / hbm_peak, 4)}
+    del proj3
+    # E-step squared differences, dense layout [particle][reference][shift]
+    n2, npart, nref, nsh, tile = 128, 64, 256, 128, 8
+    e2 = (n2 // 2 + 1) * n2
+    cplx = lambda *sh: torch.complex(torch.randn(sh, device=dev), torch.randn(sh, device=dev))
+    part, shf, refs = cplx(npart, e2), cplx(nsh, e2), cplx(nref, e2)
+    wv = torch.rand(e2, device=dev) + 0.1
+    ctf = torch.rand(npart, e2, device=dev) * 2 - 1
+    d2 = torch.empty(npart * nref * nsh, device=dev)
+    ms = timed(lambda: d_rlnSquaredDifferences(part, wv, ctf, (n2, n2, 1), npart, shf, nsh, refs, nref, tile, d2))
+    flops = 8.0 * npart * nref * nsh * e2  # per (particle, reference, shift, element)
+    fp32 = probe.get("fp32_fma_tflops")
+    out["squared_differences"] = {"comparisons_per_s": round(npart * nref * nsh / (ms * 1e-3), 1),
+                                  "ms": round(ms, 3), "tflops": round(flops / (ms * 1e-3) / 1e12, 2),
+                                  "flops_per_element": 8,
+                                  "frac_of_fp32": None if not fp32 else round(flops / (ms * 1e-3) / 1e12 / fp32, 4)}
+    del part, shf, refs, ctf, d2
+    # tomographic gather insertion
+    nt, nv = 41, 128
+    et = (nv // 2 + 1) * nv
+    tm = torch.from_numpy(synth.tilt_matrices(np.zeros(3, np.float32), np.linspace(-60, 60, nt), 1.0)).to(dev)
+    tp = cplx(nt, et)
+    tw = torch.rand(nt, et, device=dev)
+    tv = torch.zeros((nv // 2 + 1) * nv * nv, dtype=torch.complex64, device=dev)
+    ms = timed(lambda: G.d_BackprojectTomo(tv, (nv, nv, nv), tp.reshape(-1), tw.reshape(-1), (nv, nv, 1), nv // 2,
+                                           tm.reshape(-1), nt))
+    vox = int(((x ** 2 + yz[None, :, None] ** 2 + yz[:, None, None] ** 2) < (nv // 2) ** 2).sum())  # nv == n3
+    out["backproject_tomo"] = {"tilt_series_per_s": round(1 / (ms * 1e-3), 2), "ms": round(ms, 3), "box": nv,
+                               "tilts": nt, "voxel_slice_pairs_per_s": round(vox * nt / (ms * 1e-3), 1)}
+    return out
 
 
 def time_batched(args, torch, dev):
@@ -742,8 +811,13 @@ def l2_probe():
     for mode, key in ((0, "smem_f32_atomic_gadds"), (1, "smem_i32_atomic_gadds")):
         v = L.gtomrln_probe_smem_update(mode, 148 * 4, 256, 4096)
         out[key] = round(v / 1e9, 1) if v > 0 else None
+    L.gtomrln_probe_fp32_fma.restype = C.c_double
+    L.gtomrln_probe_fp32_fma.argtypes = [C.c_int] * 3
+    v = L.gtomrln_probe_fp32_fma(148 * 8, 256, 8192)
+    out["fp32_fma_tflops"] = round(v / 1e12, 2) if v > 0 else None
     out["how"] = ("L2: random addresses in a 64 MiB L2-resident buffer, 148*8 blocks x 256 threads; "
-                  "shared memory: random words of a 48 KB array, 148*4 blocks x 256 threads")
+                  "shared memory: random words of a 48 KB array, 148*4 blocks x 256 threads; "
+                  "FP32: 8 independent FMA chains per thread, 148*8 blocks x 256 threads")
     return out
 
 

@@ -3,7 +3,9 @@
 //   * L2 FP32 reduction rate: fire-and-forget red.global.add to random
 //     addresses of an L2-resident buffer (scalar, .v2 and .v4 forms),
 //   * L2 -> SM gather bandwidth: random 8-byte loads from an L2-resident
-//     buffer, the access pattern of the projector's corner fetches.
+//     buffer, the access pattern of the projector's corner fetches,
+//   * shared-memory update rates (FP32 / int32 / int64 atomics, plain
+//     read-add-write) and the CUDA cores' FP32 FMA rate.
 // Built into a separate library (gtom_b200/lib/libgtomrln_probe.so); the
 // product library does not contain it.
 #include <cuda_runtime.h>
@@ -78,9 +80,48 @@ __global__ void smem_probe_kernel(float* __restrict__ sink, int iters) {
   if (threadIdx.x == 0) sink[blockIdx.x] = s[blockIdx.x % 12288];
 }
 
+// FP32 FMA rate of the CUDA cores: eight independent chains per thread
+// (enough to cover the FMA latency at full occupancy).
+__global__ void fma_probe_kernel(float* __restrict__ sink, int iters, float a, float b) {
+  float x[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) x[k] = (float)(threadIdx.x + k) * 1e-3f;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = fmaf(x[k], a, b);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; k++) s += x[k];
+  if (s == 123.456f) sink[blockIdx.x] = s;  // keeps the chains alive
+}
+
 }  // namespace
 
 extern "C" {
+
+__attribute__((visibility("default")))
+// Returns FP32 FLOP/s of fused multiply-adds (2 per FMA) over the whole device.
+double gtomrln_probe_fp32_fma(int blocks, int threads, int iters) {
+  float* sink = nullptr;
+  if (cudaMalloc(&sink, (size_t)blocks * sizeof(float)) != cudaSuccess) return -1;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  fma_probe_kernel<<<blocks, threads>>>(sink, iters, 0.999f, 1e-3f);
+  cudaEventRecord(a);
+  fma_probe_kernel<<<blocks, threads>>>(sink, iters, 0.999f, 1e-3f);
+  cudaEventRecord(b);
+  cudaEventSynchronize(b);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaError_t e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(sink);
+  if (e != cudaSuccess) return -(double)e;
+  return 2.0 * 8.0 * (double)blocks * threads * iters / (ms * 1e-3);
+}
 
 __attribute__((visibility("default")))
 // Returns shared-memory updates per second over the whole device.
