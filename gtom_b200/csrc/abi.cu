@@ -1,8 +1,10 @@
 // Library-wide pieces of the C ABI: error state, version, the device memory
 // pool for per-call scratch, and the host matrix builder.
+#include <algorithm>
 #include <cmath>
 #include <atomic>
 #include <cstdarg>
+#include <deque>
 #include <mutex>
 #include <vector>
 
@@ -168,6 +170,130 @@ int scratch_free(void* ptr, cudaStream_t stream) {
   return pool_free(ptr, stream);
 }
 
+// Pinned host staging for the uploads of the h_angles overloads.  A
+// cudaMemcpyAsync from pageable memory is staged by the driver before it
+// returns, behind every transfer already queued on the copy engine, so a
+// caller that overlaps its own gigabyte copies with compute would stall in
+// each call.  From a pinned slot the copy is truly asynchronous; a slot is
+// reused once the event recorded after its copy has completed (eight slots
+// per device in turn, so the wait is normally over before it starts).  When
+// every slot is held by another host thread the caller falls back to its
+// pageable copy.
+namespace {
+constexpr int kStageSlots = 8;
+struct StageSlot {
+  int dev;
+  void* ptr;
+  size_t cap;
+  cudaEvent_t done;
+  bool busy;
+};
+std::mutex g_stage_mutex;
+std::deque<StageSlot> g_stage;  // stable references under push_back
+unsigned g_stage_turn = 0;
+}  // namespace
+
+int stage_acquire(size_t bytes, void** ptr, int* slot) {
+  int dev = 0;
+  GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  StageSlot* s = nullptr;
+  int idx = -1;
+  {
+    std::lock_guard<std::mutex> lock(g_stage_mutex);
+    std::vector<int> mine;
+    for (int i = 0; i < (int)g_stage.size(); i++)
+      if (g_stage[i].dev == dev) mine.push_back(i);
+    if (mine.empty()) {
+      for (int k = 0; k < kStageSlots; k++) {
+        cudaEvent_t ev;
+        GTOMRLN_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        g_stage.push_back({dev, nullptr, 0, ev, false});
+        mine.push_back((int)g_stage.size() - 1);
+      }
+    }
+    for (int t = 0; t < (int)mine.size() && !s; t++) {
+      const int i = mine[(g_stage_turn + t) % mine.size()];
+      if (!g_stage[i].busy) {
+        s = &g_stage[i];
+        idx = i;
+      }
+    }
+    if (!s) return GTOMRLN_ERR_ALLOC;  // all held: the caller copies from pageable memory
+    g_stage_turn++;
+    s->busy = true;
+  }
+  cudaError_t e = cudaEventSynchronize(s->done);  // this slot's previous copy has read it
+  if (e == cudaSuccess && s->cap < bytes) {
+    if (s->ptr) cudaFreeHost(s->ptr);
+    s->ptr = nullptr;
+    s->cap = 0;
+    const size_t want = std::max<size_t>(bytes, (size_t)64 << 10);
+    e = cudaHostAlloc(&s->ptr, want, cudaHostAllocDefault);
+    if (e == cudaSuccess) s->cap = want;
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    std::lock_guard<std::mutex> lock(g_stage_mutex);
+    s->busy = false;
+    return GTOMRLN_ERR_ALLOC;
+  }
+  *ptr = s->ptr;
+  *slot = idx;
+  return GTOMRLN_OK;
+}
+
+int stage_release(int slot, cudaStream_t stream) {
+  std::lock_guard<std::mutex> lock(g_stage_mutex);
+  StageSlot& s = g_stage[slot];
+  cudaError_t e = cudaEventRecord(s.done, stream);
+  s.busy = false;
+  if (e != cudaSuccess) return set_error(GTOMRLN_ERR_CUDA, "staging event: %s", cudaGetErrorString(e));
+  return GTOMRLN_OK;
+}
+
+// Host floats to device memory through kernel parameters: each launch carries
+// up to kParamFloats floats by value (30 KB of the 32 764-byte parameter
+// space), so the upload never enters a copy engine's queue.  A stream-ordered
+// cudaMemcpyAsync of the same few kilobytes waits behind every transfer the
+// caller has queued in that direction (measured: 3 ms per call behind an
+// 800 MB copy of the next batch), stalling the compute that needs it.
+namespace {
+constexpr int kParamFloats = 7680;
+struct ParamChunk {
+  float v[kParamFloats];
+};
+__global__ void param_copy_kernel(const ParamChunk c, float* __restrict__ dst, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = c.v[i];
+}
+}  // namespace
+
+size_t param_upload_limit() { return (size_t)64 * kParamFloats; }
+
+int upload_via_params(float* dst, const float* src, size_t count, cudaStream_t stream) {
+  ParamChunk c;
+  for (size_t off = 0; off < count; off += kParamFloats) {
+    const int n = (int)std::min<size_t>(kParamFloats, count - off);
+    std::copy(src + off, src + off + n, c.v);
+    param_copy_kernel<<<(n + 255) / 256, 256, 0, stream>>>(c, dst + off, n);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(GTOMRLN_ERR_CUDA, "parameter upload failed: %s", cudaGetErrorString(e));
+  return GTOMRLN_OK;
+}
+
+// Frees the idle staging slots' pinned memory on device dev (after a device
+// synchronisation); the slots and their events stay.
+static void release_stage(int dev) {
+  std::lock_guard<std::mutex> lock(g_stage_mutex);
+  for (auto& s : g_stage)
+    if (s.dev == dev && !s.busy && s.ptr) {
+      cudaFreeHost(s.ptr);
+      s.ptr = nullptr;
+      s.cap = 0;
+    }
+}
+
 // Frees the idle scratch slots of device dev (after a device synchronisation).
 static int release_scratch(int dev) {
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
@@ -226,6 +352,7 @@ int gtomrln_release_caches(void) {
   GTOMRLN_CUDA_TRY(cudaDeviceSynchronize());
   st = release_scratch(dev);
   if (st) return st;
+  release_stage(dev);
   std::lock_guard<std::mutex> lock(g_pool_mutex);
   if ((int)g_pools.size() > dev && g_pools[dev]) GTOMRLN_CUDA_TRY(cudaMemPoolTrimTo(g_pools[dev], 0));
   return GTOMRLN_OK;

@@ -61,6 +61,38 @@ int pool_free(void* ptr, cudaStream_t stream);
 // valid until the matching scratch_free, in stream order.
 int scratch_alloc(void** ptr, size_t bytes, cudaStream_t stream);
 int scratch_free(void* ptr, cudaStream_t stream);
+// Pinned host staging slot for an upload (abi.cu): write the data into *ptr,
+// issue the cudaMemcpyAsync, then stage_release(slot, stream).  A non-zero
+// return means no slot is free: copy from pageable memory instead.
+int stage_acquire(size_t bytes, void** ptr, int* slot);
+int stage_release(int slot, cudaStream_t stream);
+// Copies count host floats to dst in stream order through kernel parameters
+// (no copy engine; abi.cu); for count <= param_upload_limit().
+int upload_via_params(float* dst, const float* src, size_t count, cudaStream_t stream);
+size_t param_upload_limit();
+
+// Uploads count host floats built by fill(float* host) to dst on stream: by
+// kernel parameters when small enough, else from a pinned staging slot,
+// else from pageable memory.
+template <class Fill>
+inline cudaError_t upload_host_floats(float* dst, size_t count, cudaStream_t stream, Fill fill) {
+  if (count <= param_upload_limit()) {
+    std::vector<float> h(count);
+    fill(h.data());
+    return upload_via_params(dst, h.data(), count, stream) == GTOMRLN_OK ? cudaSuccess : cudaErrorUnknown;
+  }
+  void* hp = nullptr;
+  int slot = -1;
+  if (stage_acquire(count * sizeof(float), &hp, &slot) == GTOMRLN_OK) {
+    fill((float*)hp);
+    cudaError_t e = cudaMemcpyAsync(dst, hp, count * sizeof(float), cudaMemcpyHostToDevice, stream);
+    if (stage_release(slot, stream) && e == cudaSuccess) e = cudaErrorUnknown;
+    return e;
+  }
+  std::vector<float> h(count);  // cudaMemcpyAsync stages pageable memory before returning
+  fill(h.data());
+  return cudaMemcpyAsync(dst, h.data(), count * sizeof(float), cudaMemcpyHostToDevice, stream);
+}
 
 // ---------------------------------------------------------------- device --
 struct Mat3 {
@@ -114,12 +146,12 @@ inline int with_device_matrices(const float* h_angles, float supersample, unsign
                                 cudaStream_t stream, Fn fn) {
   if (batch == 0) return fn((const float*)nullptr);
   if (!h_angles) return set_error(GTOMRLN_ERR_INVALID, "h_angles is NULL");
-  std::vector<float> h(9 * (size_t)batch);
-  matrices_from_angles(h_angles, supersample, batch, h.data());
+  const size_t count = 9 * (size_t)batch;
   void* d = nullptr;
-  int st = pool_alloc(&d, h.size() * sizeof(float), stream);
+  int st = pool_alloc(&d, count * sizeof(float), stream);
   if (st) return st;
-  cudaError_t e = cudaMemcpyAsync(d, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, stream);
+  cudaError_t e = upload_host_floats((float*)d, count, stream,
+                                     [&](float* h) { matrices_from_angles(h_angles, supersample, batch, h); });
   if (e != cudaSuccess) {
     pool_free(d, stream);
     return set_error(GTOMRLN_ERR_CUDA, "matrix upload failed: %s", cudaGetErrorString(e));
@@ -127,8 +159,6 @@ inline int with_device_matrices(const float* h_angles, float supersample, unsign
   st = fn((const float*)d);
   int st2 = pool_free(d, stream);
   if (!st) st = st2;
-  // The pageable source buffer h dies here; cudaMemcpyAsync from pageable
-  // memory has already staged it before returning.
   return st;
 }
 
@@ -142,16 +172,17 @@ inline int with_device_shifted(const float* h_angles, const float* h_shifts, con
   if (batch == 0) return fn((const float*)nullptr, (const float*)nullptr, (const float*)nullptr);
   if (!h_angles || !h_shifts || !h_weights)
     return set_error(GTOMRLN_ERR_INVALID, "h_angles, h_shifts or h_globalweights is NULL");
-  std::vector<float> h(13 * (size_t)batch);
-  matrices_from_angles(h_angles, supersample, batch, h.data());
-  float* sh = h.data() + 9 * (size_t)batch;
-  const float two_pi = 6.28318530717958647692f;
-  for (unsigned i = 0; i < 3 * batch; i++) sh[i] = h_shifts[i] * two_pi / (float)n;
-  for (unsigned i = 0; i < batch; i++) sh[3 * batch + i] = h_weights[i];
+  const size_t count = 13 * (size_t)batch;
   void* d = nullptr;
-  int st = pool_alloc(&d, h.size() * sizeof(float), stream);
+  int st = pool_alloc(&d, count * sizeof(float), stream);
   if (st) return st;
-  cudaError_t e = cudaMemcpyAsync(d, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, stream);
+  cudaError_t e = upload_host_floats((float*)d, count, stream, [&](float* hm) {
+    matrices_from_angles(h_angles, supersample, batch, hm);
+    float* sh = hm + 9 * (size_t)batch;
+    const float two_pi = 6.28318530717958647692f;
+    for (unsigned i = 0; i < 3 * batch; i++) sh[i] = h_shifts[i] * two_pi / (float)n;
+    for (unsigned i = 0; i < batch; i++) sh[3 * batch + i] = h_weights[i];
+  });
   if (e != cudaSuccess) {
     pool_free(d, stream);
     return set_error(GTOMRLN_ERR_CUDA, "upload of matrices and shifts failed: %s", cudaGetErrorString(e));
