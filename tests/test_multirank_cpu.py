@@ -13,7 +13,7 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from gtom_b200.shard import Accumulators, slice_range
+from gtom_b200.shard import Accumulators, broadcast_reference, slice_range, volumes_for_rank
 from oracle import oracle as O
 from tests.helpers import rel_l2
 from tests.synthdata import random_angles
@@ -53,6 +53,12 @@ def _rank_main(rank, world, port, outdir):
     from datetime import timedelta
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
     try:
+        # the reference volume, built on rank 0 only, reaches every rank
+        ref = torch.zeros(6, 5, 4, dtype=torch.complex64)
+        if rank == 0:
+            ref = torch.complex(torch.arange(120.).reshape(6, 5, 4), -torch.arange(120.).reshape(6, 5, 4))
+        broadcast_reference(ref)
+        np.save(os.path.join(outdir, f"ref{rank}.npy"), ref.numpy())
         data, wts, mats = _inputs()
         first, count = slice_range(N_SLICES, rank, world)
         acc = Accumulators(_nvox(), "cpu")
@@ -97,11 +103,24 @@ def test_two_rank_insertion_equals_single_process():
         mp.start_processes(_rank_main, args=(world, _free_port(), d), nprocs=world, join=True,
                            start_method="spawn")
         got = [np.load(os.path.join(d, f"acc{r}.npy")) for r in range(world)]
+        refs = [np.load(os.path.join(d, f"ref{r}.npy")) for r in range(world)]
     want = ref.buffer.numpy()
     assert np.abs(want).max() > 0
     for g in got:  # every rank holds the full sums after the all-reduce
         assert rel_l2(g, want) <= 1e-6
     np.testing.assert_array_equal(got[0], got[1])
+    expect = np.arange(120.).reshape(6, 5, 4) * (1 - 1j)
+    for r in refs:  # the broadcast reference volume
+        np.testing.assert_array_equal(r, expect.astype(np.complex64))
+
+
+def test_volumes_for_rank_partitions_the_volumes():
+    for n, world in ((0, 1), (1, 3), (8, 2), (9, 4), (512, 8)):
+        parts = [volumes_for_rank(n, r, world) for r in range(world)]
+        assert sorted(sum(parts, [])) == list(range(n))
+        assert max(map(len, parts)) - min(map(len, parts)) <= 1
+    with pytest.raises(ValueError):
+        volumes_for_rank(4, 2, 2)
 
 
 def test_sharded_projection_concatenates_to_the_full_batch():
