@@ -19,6 +19,7 @@
 // The P^3 R2C / C2R transforms are cuFFT library calls; plans are cached
 // per (device, P).
 #include <cufft.h>
+#include <algorithm>
 #include <cmath>
 #include <map>
 #include <mutex>
@@ -80,23 +81,48 @@ __global__ void grid_init_kernel(const float* __restrict__ weight, int oldx, int
 // conv <- (conv * 1/P^3) * blob(r): d_IFFTC2R's renormalisation
 // (IFFT.cu:36-46) and d_MultiplyByVector with PrecomputeBlobKernel's table
 // lookup (RecFourier.cu:243-262), the radius evaluated as the reference does.
+// Grid: x blocks along a row, blockIdx.y = a group of kBlobRows rows (y),
+// blockIdx.z = volume * P + z.  Each thread loads its kBlobRows elements
+// before using any (eight loads in flight per thread: one alone leaves too
+// few bytes in flight to cover the memory latency), and no index needs a
+// division.
+constexpr int kBlobRows = 8;
 __global__ void grid_blob_kernel(float* __restrict__ conv, const float* __restrict__ table,
                                  GridGeom g, float inv_n, float funcsampling) {
-  conv += (int64_t)blockIdx.y * g.nr;
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= g.nr) return;
-  int x = (int)(i % g.P);
-  int64_t t = i / g.P;
-  int y = (int)(t % g.P);
-  int z = (int)(t / g.P);
-  int zp = z < g.P / 2 ? z : z - g.P;
-  int yp = y < g.P / 2 ? y : y - g.P;
-  float xp = (float)(x < g.P / 2 ? x : x - g.P);
-  float r = sqrtf(xp * xp + (float)(yp * yp) + (float)(zp * zp)) / (float)g.P / funcsampling;
-  int ti = (int)r;
-  ti = ti < kBlobSamples - 1 ? ti : kBlobSamples - 1;
-  float v = conv[i] * inv_n;
-  conv[i] = v * __ldg(table + ti);
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= g.P) return;
+  const int vol = blockIdx.z / g.P, z = blockIdx.z - vol * g.P;
+  const int y0 = blockIdx.y * kBlobRows;
+  const int64_t base = (int64_t)vol * g.nr + (int64_t)z * g.P * g.P + x;
+  float v[kBlobRows];
+#pragma unroll
+  for (int r = 0; r < kBlobRows; r++)
+    if (y0 + r < g.P) v[r] = conv[base + (int64_t)(y0 + r) * g.P];
+  const int zp = z < g.P / 2 ? z : z - g.P;
+  const float xp = (float)(x < g.P / 2 ? x : x - g.P);
+#pragma unroll
+  for (int r = 0; r < kBlobRows; r++) {
+    const int y = y0 + r;
+    if (y >= g.P) break;
+    const int yp = y < g.P / 2 ? y : y - g.P;
+    float rad = sqrtf(xp * xp + (float)(yp * yp) + (float)(zp * zp)) / (float)g.P / funcsampling;
+    int ti = (int)rad;
+    ti = ti < kBlobSamples - 1 ? ti : kBlobSamples - 1;
+    conv[base + (int64_t)y * g.P] = v[r] * inv_n * __ldg(table + ti);
+  }
+}
+
+// Launches grid_blob_kernel over `count` consecutive volumes, in groups whose
+// P * count fits the grid's z extent.
+static void launch_blob(float* conv, const float* table, const GridGeom& g, int count, cudaStream_t stream) {
+  const int T = 256;
+  const int per = std::max(1, 65535 / g.P);
+  for (int v0 = 0; v0 < count; v0 += per) {
+    const int c = std::min(per, count - v0);
+    dim3 grid((unsigned)((g.P + T - 1) / T), (unsigned)((g.P + kBlobRows - 1) / kBlobRows), (unsigned)(g.P * c));
+    grid_blob_kernel<<<grid, T, 0, stream>>>(conv + (int64_t)v0 * g.nr, table, g, 1.0f / (float)g.nr,
+                                             (float)(0.5 / kBlobSamples));
+  }
 }
 
 // Iteration2Kernel (RecFourier.cu:293-308) fused with the next iteration's
@@ -446,7 +472,7 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   double last_change = 0;
   bool warm_live = warm;
   const int T = 256;
-  unsigned bc = (unsigned)((g.nc + T - 1) / T), br = (unsigned)((g.nr + T - 1) / T);
+  unsigned bc = (unsigned)((g.nc + T - 1) / T);
 
   GTOMRLN_STEP(pool_alloc((void**)&convft, g.nc * sizeof(float2), stream));
   GTOMRLN_STEP(pool_alloc((void**)&conv, g.nr * sizeof(float), stream));
@@ -471,8 +497,7 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
 
   for (int it = 0; it < iterations; it++) {
     GTOMRLN_CUFFT_TRY(cufftExecC2R(plans.c2r, (cufftComplex*)convft, conv));
-    grid_blob_kernel<<<br, T, 0, stream>>>(conv, table, g, 1.0f / (float)g.nr,
-                                           (float)(0.5 / kBlobSamples));
+    launch_blob(conv, table, g, 1, stream);
     GTOMRLN_STEP(launch_check("grid_blob_kernel"));
     GTOMRLN_CUFFT_TRY(cufftExecR2C(plans.r2c, conv, (cufftComplex*)convft));
     // the residual check of a predicted start needs the first change
@@ -597,7 +622,6 @@ int gridding_batch_run(const GridBatch& b, const float2* data, const float* weig
   const int maskr2 = (r_max * b.pad) * (r_max * b.pad);
   const int T = 256;
   dim3 gc((unsigned)((g.nc + T - 1) / T), (unsigned)b.count);
-  dim3 gr((unsigned)((g.nr + T - 1) / T), (unsigned)b.count);
   int st = GTOMRLN_OK;
   GTOMRLN_CUFFT_TRY(cufftSetStream(b.r2c, stream));
   GTOMRLN_CUFFT_TRY(cufftSetStream(b.c2r, stream));
@@ -606,7 +630,7 @@ int gridding_batch_run(const GridBatch& b, const float2* data, const float* weig
   GTOMRLN_STEP(launch_check("grid_init_kernel"));
   for (int it = 0; it < iterations; it++) {
     GTOMRLN_CUFFT_TRY(cufftExecC2R(b.c2r, (cufftComplex*)b.convft, b.conv));
-    grid_blob_kernel<<<gr, T, 0, stream>>>(b.conv, b.table, g, 1.0f / (float)g.nr, (float)(0.5 / kBlobSamples));
+    launch_blob(b.conv, b.table, g, b.count, stream);
     GTOMRLN_STEP(launch_check("grid_blob_kernel"));
     GTOMRLN_CUFFT_TRY(cufftExecR2C(b.r2c, b.conv, (cufftComplex*)b.convft));
     grid_update_kernel<<<gc, T, 0, stream>>>(b.convft, b.Fw, b.Fnw, g, it + 1 < iterations, nullptr);
