@@ -316,9 +316,9 @@ static int release_scratch(int dev) {
 int release_gridding_plans();  // gridding.cu
 int release_ctf_plans();       // ctf.cu
 
-static std::atomic<int> g_path[2] = {{GTOMRLN_PATH_AUTO}, {GTOMRLN_PATH_AUTO}};
+static std::atomic<int> g_path[3] = {{GTOMRLN_PATH_AUTO}, {GTOMRLN_PATH_AUTO}, {GTOMRLN_PATH_AUTO}};
 
-int path_choice(int op) { return (op == 0 || op == 1) ? g_path[op].load() : GTOMRLN_PATH_AUTO; }
+int path_choice(int op) { return (op >= 0 && op <= 2) ? g_path[op].load() : GTOMRLN_PATH_AUTO; }
 
 // Defaults measured on the B200 at 256^3 (padding 2) with 10,000-slice
 // batches (row-segment variants; the largest bricks whose shared memory fits
@@ -360,8 +360,10 @@ int gtomrln_release_caches(void) {
 
 int gtomrln_set_path(int op, int path) {
   clear_error();
-  if ((op != GTOMRLN_OP_PROJECT && op != GTOMRLN_OP_BACKPROJECT) || path < GTOMRLN_PATH_AUTO ||
-      path > GTOMRLN_PATH_SEGMENT)
+  const bool grid = op == GTOMRLN_OP_GRIDDING;
+  if ((op != GTOMRLN_OP_PROJECT && op != GTOMRLN_OP_BACKPROJECT && !grid) || path < GTOMRLN_PATH_AUTO ||
+      (!grid && path > GTOMRLN_PATH_SEGMENT) ||
+      (grid && path != GTOMRLN_PATH_AUTO && path != GTOMRLN_PATH_DIRECT && path != GTOMRLN_PATH_FUSED))
     return set_error(GTOMRLN_ERR_INVALID, "set_path: unknown op %d or path %d", op, path);
   g_path[op].store(path);
   return GTOMRLN_OK;

@@ -27,22 +27,14 @@
 
 #include "common.cuh"
 #include "batch.cuh"
+#include "gridfft.cuh"
 #include "mlp.cuh"
 
 namespace gtomrln {
 
 double kaiser_fourier_value(double w, double a, double alpha, int m);  // below
 
-constexpr int kBlobSamples = 10000;
-
 // ---------------------------------------------------------------- kernels --
-struct GridGeom {
-  int P;         // padded working grid
-  int rowlen;    // P/2 + 1
-  int64_t nc;    // rowlen * P * P complex elements
-  int64_t nr;    // P^3 real elements
-};
-
 // RecFourier.cu:264-285 (DecenterKernel) for the weights + SphereMask.cu:167-189
 // (Fnewweight = 1 inside r^2 < (r_max*pad)^2) + Iteration1Kernel
 // (RecFourier.cu:287-291).  old* are the centred input dims.
@@ -98,17 +90,11 @@ __global__ void grid_blob_kernel(float* __restrict__ conv, const float* __restri
 #pragma unroll
   for (int r = 0; r < kBlobRows; r++)
     if (y0 + r < g.P) v[r] = conv[base + (int64_t)(y0 + r) * g.P];
-  const int zp = z < g.P / 2 ? z : z - g.P;
-  const float xp = (float)(x < g.P / 2 ? x : x - g.P);
 #pragma unroll
   for (int r = 0; r < kBlobRows; r++) {
     const int y = y0 + r;
     if (y >= g.P) break;
-    const int yp = y < g.P / 2 ? y : y - g.P;
-    float rad = sqrtf(xp * xp + (float)(yp * yp) + (float)(zp * zp)) / (float)g.P / funcsampling;
-    int ti = (int)rad;
-    ti = ti < kBlobSamples - 1 ? ti : kBlobSamples - 1;
-    conv[base + (int64_t)y * g.P] = v[r] * inv_n * __ldg(table + ti);
+    conv[base + (int64_t)y * g.P] = v[r] * inv_n * grid_blob_at(table, g.P, x, y, z, funcsampling);
   }
 }
 
@@ -140,10 +126,8 @@ __global__ void grid_update_kernel(float2* __restrict__ convft, const float* __r
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double d2 = 0, o2 = 0;
   if (i < g.nc) {
-    float c = convft[i].x;
-    float w = fmaxf(1e-4f, c);
     float old = Fnw[i];
-    float nw = fminf(1e20f, old / w);
+    float nw = grid_update_value(convft[i].x, old);
     float fw = Fw[i];
     Fnw[i] = nw;
     if (write_conv) convft[i] = make_float2(fw * nw, 0.f);
@@ -154,29 +138,7 @@ __global__ void grid_update_kernel(float2* __restrict__ convft, const float* __r
       o2 = o * o;
     }
   }
-  if (change) {
-    for (int off = 16; off > 0; off >>= 1) {
-      d2 += __shfl_down_sync(0xffffffffu, d2, off);
-      o2 += __shfl_down_sync(0xffffffffu, o2, off);
-    }
-    __shared__ double s[2][32];
-    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) { s[0][warp] = d2; s[1][warp] = o2; }
-    __syncthreads();
-    if (warp == 0) {
-      int nw = blockDim.x >> 5;
-      d2 = lane < nw ? s[0][lane] : 0;
-      o2 = lane < nw ? s[1][lane] : 0;
-      for (int off = 16; off > 0; off >>= 1) {
-        d2 += __shfl_down_sync(0xffffffffu, d2, off);
-        o2 += __shfl_down_sync(0xffffffffu, o2, off);
-      }
-      if (lane == 0) {
-        atomicAdd(change, d2);
-        atomicAdd(change + 1, o2);
-      }
-    }
-  }
+  if (change) grid_change_reduce(d2, o2, change);
 }
 
 // The update of grid_update_kernel applied at an extrapolated point V
@@ -199,12 +161,9 @@ __global__ void grid_update_momentum_kernel(float2* __restrict__ convft, const f
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double d2 = 0, o2 = 0;
   if (i < g.nc) {
-    float c = convft[i].x;
-    float w = fmaxf(1e-4f, c);
     float old = Fnw[i];
-    float nw = fminf(1e20f, V[i] / w);
-    float ext = nw;
-    if (old > 0.f && nw > 0.f) ext = fminf(1e20f, nw * powf(nw / old, beta));
+    float nw, ext;
+    grid_update_momentum_value(convft[i].x, old, V[i], beta, nw, ext);
     float fw = Fw[i];
     Fnw[i] = nw;
     V[i] = ext;
@@ -216,29 +175,7 @@ __global__ void grid_update_momentum_kernel(float2* __restrict__ convft, const f
       o2 = o * o;
     }
   }
-  if (change) {
-    for (int off = 16; off > 0; off >>= 1) {
-      d2 += __shfl_down_sync(0xffffffffu, d2, off);
-      o2 += __shfl_down_sync(0xffffffffu, o2, off);
-    }
-    __shared__ double s[2][32];
-    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) { s[0][warp] = d2; s[1][warp] = o2; }
-    __syncthreads();
-    if (warp == 0) {
-      int nw = blockDim.x >> 5;
-      d2 = lane < nw ? s[0][lane] : 0;
-      o2 = lane < nw ? s[1][lane] : 0;
-      for (int off = 16; off > 0; off >>= 1) {
-        d2 += __shfl_down_sync(0xffffffffu, d2, off);
-        o2 += __shfl_down_sync(0xffffffffu, o2, off);
-      }
-      if (lane == 0) {
-        atomicAdd(change, d2);
-        atomicAdd(change + 1, o2);
-      }
-    }
-  }
+  if (change) grid_change_reduce(d2, o2, change);
 }
 
 // DecenterKernel<tcomplex> for the data (RecFourier.cu:175-179), then
@@ -473,6 +410,10 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   bool warm_live = warm;
   const int T = 256;
   unsigned bc = (unsigned)((g.nc + T - 1) / T);
+  // The fused FFT iteration (gridfft.cu) for power-of-two grids when the
+  // caller chose it; the final map always uses cuFFT.
+  const bool fused = path_choice(GTOMRLN_OP_GRIDDING) == GTOMRLN_PATH_FUSED && gridfft_available(P, 1);
+  bool need_first = true;  // the fused loop starts with the inverse transform along z
 
   GTOMRLN_STEP(pool_alloc((void**)&convft, g.nc * sizeof(float2), stream));
   GTOMRLN_STEP(pool_alloc((void**)&conv, g.nr * sizeof(float), stream));
@@ -496,19 +437,27 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   if (momentum) GTOMRLN_CUDA_TRY(cudaMemcpyAsync(V, Fnw, g.nc * sizeof(float), cudaMemcpyDeviceToDevice, stream));
 
   for (int it = 0; it < iterations; it++) {
-    GTOMRLN_CUFFT_TRY(cufftExecC2R(plans.c2r, (cufftComplex*)convft, conv));
-    launch_blob(conv, table, g, 1, stream);
-    GTOMRLN_STEP(launch_check("grid_blob_kernel"));
-    GTOMRLN_CUFFT_TRY(cufftExecR2C(plans.r2c, conv, (cufftComplex*)convft));
     // the residual check of a predicted start needs the first change
     double* ch = (opt.tolerance > 0 || (warm_live && it == 0)) ? change : nullptr;
-    if (ch) GTOMRLN_CUDA_TRY(cudaMemsetAsync(ch, 0, 2 * sizeof(double), stream));
-    if (momentum)
-      grid_update_momentum_kernel<<<bc, T, 0, stream>>>(convft, Fw, Fnw, V, g, opt.momentum,
-                                                        it + 1 < iterations, ch);
-    else
-      grid_update_kernel<<<bc, T, 0, stream>>>(convft, Fw, Fnw, g, it + 1 < iterations, ch);
-    GTOMRLN_STEP(launch_check("grid_update_kernel"));
+    if (fused) {
+      if (need_first) GTOMRLN_STEP(gridfft_first(convft, g, 1, stream));
+      need_first = false;
+      if (ch) GTOMRLN_CUDA_TRY(cudaMemsetAsync(ch, 0, 2 * sizeof(double), stream));
+      GTOMRLN_STEP(gridfft_iteration(convft, g, 1, table, Fw, Fnw, momentum ? V : nullptr, opt.momentum,
+                                     it + 1 < iterations, ch, stream));
+    } else {
+      GTOMRLN_CUFFT_TRY(cufftExecC2R(plans.c2r, (cufftComplex*)convft, conv));
+      launch_blob(conv, table, g, 1, stream);
+      GTOMRLN_STEP(launch_check("grid_blob_kernel"));
+      GTOMRLN_CUFFT_TRY(cufftExecR2C(plans.r2c, conv, (cufftComplex*)convft));
+      if (ch) GTOMRLN_CUDA_TRY(cudaMemsetAsync(ch, 0, 2 * sizeof(double), stream));
+      if (momentum)
+        grid_update_momentum_kernel<<<bc, T, 0, stream>>>(convft, Fw, Fnw, V, g, opt.momentum,
+                                                          it + 1 < iterations, ch);
+      else
+        grid_update_kernel<<<bc, T, 0, stream>>>(convft, Fw, Fnw, g, it + 1 < iterations, ch);
+      GTOMRLN_STEP(launch_check("grid_update_kernel"));
+    }
     total_iters++;
     if (ch) {
       GTOMRLN_CUDA_TRY(cudaMemcpyAsync(h_change, ch, sizeof(h_change), cudaMemcpyDeviceToHost, stream));
@@ -521,6 +470,7 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
           grid_init_kernel<<<bc, T, 0, stream>>>(d_weight, oldx, oldy, oldz, Fw, Fnw, convft, g,
                                                  maskr2, 1, 0);
           GTOMRLN_STEP(launch_check("grid_init_kernel"));
+          need_first = true;
           if (momentum)
             GTOMRLN_CUDA_TRY(cudaMemcpyAsync(V, Fnw, g.nc * sizeof(float), cudaMemcpyDeviceToDevice, stream));
           if (res) res->warm_used = 0;
@@ -579,6 +529,9 @@ int gridding_batch_prepare(GridBatch* gb, int count, int ori, int pad, double bl
   const int64_t nc = (int64_t)(b.P / 2 + 1) * b.P * b.P, nr = (int64_t)b.P * b.P * b.P;
   int st = get_table(blobradius * pad, blobalpha, bloborder, &b.table);
   if (st) return st;
+  // decided (and its tables and kernel attributes set up) here, outside the
+  // stream capture of gridding_batch_run
+  b.fused = gridfft_available(b.P, count);
   *gb = b;  // so that gridding_batch_free releases what was made on failure
   GTOMRLN_CUDA_TRY(cudaMalloc(&gb->convft, count * nc * sizeof(float2)));
   GTOMRLN_CUDA_TRY(cudaMalloc(&gb->conv, count * nr * sizeof(float)));
@@ -623,12 +576,19 @@ int gridding_batch_run(const GridBatch& b, const float2* data, const float* weig
   const int T = 256;
   dim3 gc((unsigned)((g.nc + T - 1) / T), (unsigned)b.count);
   int st = GTOMRLN_OK;
+  const bool fused = b.fused && path_choice(GTOMRLN_OP_GRIDDING) == GTOMRLN_PATH_FUSED;
   GTOMRLN_CUFFT_TRY(cufftSetStream(b.r2c, stream));
   GTOMRLN_CUFFT_TRY(cufftSetStream(b.c2r, stream));
   grid_init_kernel<<<gc, T, 0, stream>>>(weight, b.D, b.D, b.D, b.Fw, b.Fnw, b.convft, g, maskr2,
                                          iterations > 0, b.wstride);
   GTOMRLN_STEP(launch_check("grid_init_kernel"));
+  if (fused && iterations > 0) GTOMRLN_STEP(gridfft_first(b.convft, g, b.count, stream));
   for (int it = 0; it < iterations; it++) {
+    if (fused) {
+      GTOMRLN_STEP(gridfft_iteration(b.convft, g, b.count, b.table, b.Fw, b.Fnw, nullptr, 0.f,
+                                     it + 1 < iterations, nullptr, stream));
+      continue;
+    }
     GTOMRLN_CUFFT_TRY(cufftExecC2R(b.c2r, (cufftComplex*)b.convft, b.conv));
     launch_blob(b.conv, b.table, g, b.count, stream);
     GTOMRLN_STEP(launch_check("grid_blob_kernel"));

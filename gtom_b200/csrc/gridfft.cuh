@@ -1,0 +1,95 @@
+// Pieces of the gridding reconstructor shared by its cuFFT path
+// (gridding.cu) and its fused FFT path (gridfft.cu): the P-grid geometry,
+// the blob lookup, and the per-voxel weight updates.
+#pragma once
+
+#include "common.cuh"
+
+namespace gtomrln {
+
+constexpr int kBlobSamples = 10000;
+
+struct GridGeom {
+  int P;         // padded working grid
+  int rowlen;    // P/2 + 1
+  int64_t nc;    // rowlen * P * P complex elements
+  int64_t nr;    // P^3 real elements
+};
+
+// PrecomputeBlobKernel's table lookup (RecFourier.cu:243-262) at real-space
+// voxel (x, y, z) of the P grid, the radius evaluated as the reference does.
+__device__ __forceinline__ float grid_blob_at(const float* __restrict__ table, int P, int x, int y, int z,
+                                              float funcsampling) {
+  const int zp = z < P / 2 ? z : z - P;
+  const int yp = y < P / 2 ? y : y - P;
+  const float xp = (float)(x < P / 2 ? x : x - P);
+  const float r = sqrtf(xp * xp + (float)(yp * yp) + (float)(zp * zp)) / (float)P / funcsampling;
+  int ti = (int)r;
+  ti = ti < kBlobSamples - 1 ? ti : kBlobSamples - 1;
+  return __ldg(table + ti);
+}
+
+// Iteration2Kernel (RecFourier.cu:293-308) for one voxel: the new
+// Fnewweight from the real part c of the convolved spectrum.
+__device__ __forceinline__ float grid_update_value(float c, float old) {
+  const float w = fmaxf(1e-4f, c);
+  return fminf(1e20f, old / w);
+}
+
+// The same update applied at the extrapolated point v (momentum in the
+// logarithm of the weights): nw = min(1e20, v / max(1e-4, c)) and the next
+// extrapolation ext = min(1e20, nw (nw / old)^beta).
+__device__ __forceinline__ void grid_update_momentum_value(float c, float old, float v, float beta, float& nw,
+                                                           float& ext) {
+  const float w = fmaxf(1e-4f, c);
+  nw = fminf(1e20f, v / w);
+  ext = nw;
+  if (old > 0.f && nw > 0.f) ext = fminf(1e20f, nw * powf(nw / old, beta));
+}
+
+// Adds the block's (d2, o2) to change[0..1] (one atomic pair per block).
+__device__ __forceinline__ void grid_change_reduce(double d2, double o2, double* change) {
+  for (int off = 16; off > 0; off >>= 1) {
+    d2 += __shfl_down_sync(0xffffffffu, d2, off);
+    o2 += __shfl_down_sync(0xffffffffu, o2, off);
+  }
+  __shared__ double s[2][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    s[0][warp] = d2;
+    s[1][warp] = o2;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    d2 = lane < nw ? s[0][lane] : 0;
+    o2 = lane < nw ? s[1][lane] : 0;
+    for (int off = 16; off > 0; off >>= 1) {
+      d2 += __shfl_down_sync(0xffffffffu, d2, off);
+      o2 += __shfl_down_sync(0xffffffffu, o2, off);
+    }
+    if (lane == 0) {
+      atomicAdd(change, d2);
+      atomicAdd(change + 1, o2);
+    }
+  }
+}
+
+// ------------------------------------------------------- fused FFT path --
+// For power-of-two grids P in [64, 512] the iteration's two 3D transforms,
+// the blob multiply and the weight update run as two kernels of gridfft.cu
+// (see there).  `data` is the complex working spectrum (nc per volume).
+
+// Whether the fused path can run `count` volumes of grid P on this device.
+bool gridfft_available(int P, int count);
+// data <- inverse transform along z of data (before the first iteration).
+int gridfft_first(float2* data, const GridGeom& g, int count, cudaStream_t stream);
+// One iteration: the rest of the inverse transform, the blob multiply
+// (with the in-loop 1/P^3), the forward transform and the update of Fnw
+// (and V with momentum beta > 0; change accumulates the convergence sums
+// when non-null); with write_next, data <- the inverse transform along z of
+// Fw * Fnw (Fw * V) for the next iteration.
+int gridfft_iteration(float2* data, const GridGeom& g, int count, const float* table, const float* Fw,
+                      float* Fnw, float* V, float beta, bool write_next, double* change, cudaStream_t stream);
+
+}  // namespace gtomrln

@@ -363,14 +363,17 @@ def mlp_param_count() -> int:
     return int(_lib.load().gtomrln_mlp_param_count())
 
 
-_OPS = {"project": 0, "backproject": 1}
-_PATHS = {"auto": 0, "direct": 1, "brick": 2, "segment": 3}
+_OPS = {"project": 0, "backproject": 1, "gridding": 2}
+_PATHS = {"auto": 0, "direct": 1, "brick": 2, "segment": 3, "fused": 4}
 
 
 def set_path(op: str, path: str) -> None:
     """Selects the implementation of "project" or "backproject" for this
     process: "auto" (default), "direct", "brick" (pixels binned per brick) or
-    "segment" (pixels found per brick by row segments) (gtomrln_set_path)."""
+    "segment" (pixels found per brick by row segments); of "gridding": "auto"
+    or "direct" (cuFFT transforms) or "fused" (two fused passes per iteration
+    with the library's own transforms on power-of-two grids)
+    (gtomrln_set_path)."""
     _lib.call("gtomrln_set_path", _OPS[op], _PATHS[path])
 
 

@@ -75,10 +75,17 @@ GTOMRLN_API int gtomrln_release_caches(void);
  * the same per-sample arithmetic. */
 #define GTOMRLN_OP_PROJECT 0
 #define GTOMRLN_OP_BACKPROJECT 1
+/* op GTOMRLN_OP_GRIDDING: GTOMRLN_PATH_AUTO (default) and
+ * GTOMRLN_PATH_DIRECT run the gridding iterations' 3D transforms with cuFFT;
+ * GTOMRLN_PATH_FUSED runs each iteration as two fused passes with the
+ * library's own transforms on power-of-two grids P = 64 .. 512 (cuFFT
+ * elsewhere). */
+#define GTOMRLN_OP_GRIDDING 2
 #define GTOMRLN_PATH_AUTO 0
 #define GTOMRLN_PATH_DIRECT 1
 #define GTOMRLN_PATH_BRICK 2
 #define GTOMRLN_PATH_SEGMENT 3
+#define GTOMRLN_PATH_FUSED 4
 GTOMRLN_API int gtomrln_set_path(int op, int path);
 
 /* Extension (no reference counterpart): launch shape of the brick-major
