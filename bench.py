@@ -815,6 +815,10 @@ def l2_probe():
     L.gtomrln_probe_fp32_fma.argtypes = [C.c_int] * 3
     v = L.gtomrln_probe_fp32_fma(148 * 8, 256, 8192)
     out["fp32_fma_tflops"] = round(v / 1e12, 2) if v > 0 else None
+    L.gtomrln_probe_fp32x2_fma.restype = C.c_double
+    L.gtomrln_probe_fp32x2_fma.argtypes = [C.c_int] * 3
+    v = L.gtomrln_probe_fp32x2_fma(148 * 8, 256, 8192)
+    out["fp32x2_fma_tflops"] = round(v / 1e12, 2) if v > 0 else None
     out["how"] = ("L2: random addresses in a 64 MiB L2-resident buffer, 148*8 blocks x 256 threads; "
                   "shared memory: random words of a 48 KB array, 148*4 blocks x 256 threads; "
                   "FP32: 8 independent FMA chains per thread, 148*8 blocks x 256 threads")

@@ -118,6 +118,94 @@ diff2_group_kernel(const float2* __restrict__ particle, const float* __restrict_
   }
 }
 
+// Dense layout [particle][reference][shift] (gtomrln_squared_differences):
+// one CTA per 64 references x 64 shifts of one particle.  Chunks of 32
+// elements of c * ref and particle * shift are staged in shared memory
+// (element-major, rows padded against bank conflicts); each thread holds
+// 4 x 4 outputs (references tr + 16 k, shifts ts + 16 k), with the group
+// kernel's per-element arithmetic.
+constexpr int kDT = 64;        // references and shifts per tile
+constexpr int kDK = 32;        // elements per staged chunk
+constexpr int kDThreads = 256;
+template <bool CC>
+__global__ void __launch_bounds__(kDThreads)
+diff2_dense_tiled_kernel(const float2* __restrict__ particle, const float* __restrict__ minvsigma2,
+                         const float* __restrict__ ctf, int64_t elements, const float2* __restrict__ shifts,
+                         const float2* __restrict__ refs, float* __restrict__ diff2, unsigned nrefs,
+                         unsigned nshifts) {
+  __shared__ float2 As[kDK][kDT + 1];  // c * ref
+  __shared__ float2 Bs[kDK][kDT + 1];  // particle * shift
+  __shared__ float Ws[kDK];
+  const unsigned part = blockIdx.z, r0 = blockIdx.y * kDT, s0 = blockIdx.x * kDT;
+  const int tid = threadIdx.x, tr = tid >> 4, ts = tid & 15;
+  const int li = tid & (kDK - 1), lrow = tid / kDK;  // loader: element li, rows lrow + 8 k
+  const float2* pp = particle + elements * part;
+  const float* cp = ctf ? ctf + elements * part : nullptr;
+  float acc[4][4], nn[4];
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    nn[a] = 0.f;
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[a][b] = 0.f;
+  }
+  for (int64_t i0 = 0; i0 < elements; i0 += kDK) {
+    const int64_t gi = i0 + li;
+    const bool ok = gi < elements;
+    const float2 pv = ok ? pp[gi] : make_float2(0.f, 0.f);
+    const float c = ok ? (cp ? cp[gi] : 1.f) : 0.f;
+    float2 rv[kDT / (kDThreads / kDK)], sv[kDT / (kDThreads / kDK)];
+#pragma unroll
+    for (int k = 0; k < kDT / (kDThreads / kDK); k++) {
+      const unsigned row = lrow + k * (kDThreads / kDK);
+      rv[k] = ok && r0 + row < nrefs ? refs[elements * (r0 + row) + gi] : make_float2(0.f, 0.f);
+      sv[k] = ok && s0 + row < nshifts ? shifts[elements * (s0 + row) + gi] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int k = 0; k < kDT / (kDThreads / kDK); k++) {
+      const int row = lrow + k * (kDThreads / kDK);
+      As[li][row] = make_float2(rv[k].x * c, rv[k].y * c);
+      Bs[li][row] = make_float2(pv.x * sv[k].x - pv.y * sv[k].y, pv.x * sv[k].y + pv.y * sv[k].x);
+    }
+    if (tid < kDK) Ws[tid] = i0 + tid < elements ? (minvsigma2 ? minvsigma2[i0 + tid] : 1.f) : 0.f;
+    __syncthreads();
+#pragma unroll 4
+    for (int i = 0; i < kDK; i++) {
+      float2 a[4], b[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        a[k] = As[i][tr + 16 * k];
+        b[k] = Bs[i][ts + 16 * k];
+      }
+      const float w = Ws[i];
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        if (CC) nn[x] = fmaf(a[x].x, a[x].x, fmaf(a[x].y, a[x].y, nn[x]));
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+          if (CC) {
+            acc[x][y] = fmaf(a[x].x, b[y].x, fmaf(a[x].y, b[y].y, acc[x][y]));
+          } else {
+            const float dx = a[x].x - b[y].x, dy = a[x].y - b[y].y;
+            acc[x][y] = fmaf(w, fmaf(dx, dx, dy * dy), acc[x][y]);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int x = 0; x < 4; x++) {
+    const unsigned r = r0 + tr + 16 * x;
+    if (r >= nrefs) continue;
+#pragma unroll
+    for (int y = 0; y < 4; y++) {
+      const unsigned s2 = s0 + ts + 16 * y;
+      if (s2 < nshifts)
+        diff2[((int64_t)part * nrefs + r) * nshifts + s2] = CC ? -acc[x][y] / sqrtf(nn[x]) : 0.5f * acc[x][y];
+    }
+  }
+}
+
 template <int G>
 int launch_diff2(bool cc, unsigned blocks, cudaStream_t stream, const float2* particle, const float* w,
                  const float* ctf, int64_t elements, const float2* shifts, const float2* refs, float* diff2,
@@ -324,14 +412,22 @@ int gtomrln_squared_differences(const float* d_particleft, const float* d_minvsi
   if (!d_particleft || !d_precalcshifts || !d_refft || !d_diff2)
     return set_error(GTOMRLN_ERR_INVALID, "squared_differences: NULL pointer");
   int64_t elements = (int64_t)(dx / 2 + 1) * dy * (dz > 1 ? dz : 1);
-  uint64_t blocks = (uint64_t)nparticles * ((nrefs + tile - 1) / (tile ? tile : 1)) *
-                    ((nshifts + tile - 1) / (tile ? tile : 1));
-  if (tile == 0 || blocks > 0x7fffffffULL)
-    return set_error(GTOMRLN_ERR_INVALID, "squared_differences: bad tile or too many groups");
-  return diff2_dispatch(tile, dofirstitercc != 0, (unsigned)blocks, (cudaStream_t)stream,
-                        (const float2*)d_particleft, d_minvsigma2, d_ctf, elements,
-                        (const float2*)d_precalcshifts, (const float2*)d_refft, d_diff2, nullptr, nrefs, nshifts,
-                        nparticles);
+  if (tile != 1 && tile != 2 && tile != 4 && tile != 8)
+    return set_error(GTOMRLN_ERR_INVALID, "squared_differences: group size %u not 1, 2, 4 or 8", tile);
+  if (nparticles > 65535)
+    return set_error(GTOMRLN_ERR_INVALID, "squared_differences: more than 65535 particles per call");
+  // The dense layout does not depend on the group size: one tiled kernel.
+  dim3 grid((nshifts + kDT - 1) / kDT, (nrefs + kDT - 1) / kDT, nparticles);
+  if (dofirstitercc)
+    diff2_dense_tiled_kernel<true><<<grid, kDThreads, 0, (cudaStream_t)stream>>>(
+        (const float2*)d_particleft, d_minvsigma2, d_ctf, elements, (const float2*)d_precalcshifts,
+        (const float2*)d_refft, d_diff2, nrefs, nshifts);
+  else
+    diff2_dense_tiled_kernel<false><<<grid, kDThreads, 0, (cudaStream_t)stream>>>(
+        (const float2*)d_particleft, d_minvsigma2, d_ctf, elements, (const float2*)d_precalcshifts,
+        (const float2*)d_refft, d_diff2, nrefs, nshifts);
+  GTOMRLN_LAUNCH_CHECK("diff2_dense_tiled_kernel");
+  return GTOMRLN_OK;
 }
 
 int gtomrln_convert_weights_dense(float* d_weights, unsigned nparticles, unsigned nclasses, unsigned nrot,

@@ -96,9 +96,57 @@ __global__ void fma_probe_kernel(float* __restrict__ sink, int iters, float a, f
   if (s == 123.456f) sink[blockIdx.x] = s;  // keeps the chains alive
 }
 
+// The packed form: eight independent chains of fma.rn.f32x2 (two FMAs per
+// instruction) per thread.
+__global__ void fma2_probe_kernel(float* __restrict__ sink, int iters, float a, float b) {
+  unsigned long long x[8];
+  const float2 av = make_float2(a, a), bv = make_float2(b, b);
+  const unsigned long long A = *reinterpret_cast<const unsigned long long*>(&av);
+  const unsigned long long Bv = *reinterpret_cast<const unsigned long long*>(&bv);
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const float2 v = make_float2((float)(threadIdx.x + k) * 1e-3f, (float)k);
+    x[k] = *reinterpret_cast<const unsigned long long*>(&v);
+  }
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) asm volatile("fma.rn.f32x2 %0, %0, %1, %2;" : "+l"(x[k]) : "l"(A), "l"(Bv));
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const float2 v = *reinterpret_cast<const float2*>(&x[k]);
+    s += v.x + v.y;
+  }
+  if (s == 123.456f) sink[blockIdx.x] = s;
+}
+
 }  // namespace
 
 extern "C" {
+
+__attribute__((visibility("default")))
+// Returns FP32 FLOP/s of packed f32x2 fused multiply-adds (4 per instruction).
+double gtomrln_probe_fp32x2_fma(int blocks, int threads, int iters) {
+  float* sink = nullptr;
+  if (cudaMalloc(&sink, (size_t)blocks * sizeof(float)) != cudaSuccess) return -1;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  fma2_probe_kernel<<<blocks, threads>>>(sink, iters, 0.999f, 1e-3f);
+  cudaEventRecord(a);
+  fma2_probe_kernel<<<blocks, threads>>>(sink, iters, 0.999f, 1e-3f);
+  cudaEventRecord(b);
+  cudaEventSynchronize(b);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaError_t e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(sink);
+  if (e != cudaSuccess) return -(double)e;
+  return 4.0 * 8.0 * (double)blocks * threads * iters / (ms * 1e-3);
+}
 
 __attribute__((visibility("default")))
 // Returns FP32 FLOP/s of fused multiply-adds (2 per FMA) over the whole device.
