@@ -128,8 +128,12 @@ struct BrickPlan {
 // work item.  segments = 1 builds the segment plan instead: bins without
 // entries, one per (slice, brick) pair whose brick the slice's plane
 // crosses, and the kernels enumerate the pixels themselves (segment.cuh).
+// With a segment plan, zero_out (the projector's output, complex, elements
+// per slice as px) receives the zeros outside px's radius for every planned
+// slice, in the plan's own per-slice pass.
 int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g, const PixelSet& px,
-                     float limit, int chunk, cudaStream_t stream, BrickPlan* plan, int segments = 0);
+                     float limit, int chunk, cudaStream_t stream, BrickPlan* plan, int segments = 0,
+                     void* zero_out = nullptr);
 int free_brick_plan(BrickPlan* plan, cudaStream_t stream);
 
 // Pixel id -> signed slice coordinates (FFT order in y).

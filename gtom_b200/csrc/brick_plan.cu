@@ -264,7 +264,8 @@ constexpr int kPairThreads = 256;
 __global__ void __launch_bounds__(kPairThreads)
 segment_pairs_kernel(const float* __restrict__ mats, BrickGrid g, float pmax, float limit, float below,
                      PixelBin* __restrict__ bins, int64_t bins_cap, unsigned long long* __restrict__ counters,
-                     int* __restrict__ brick_pairs, int* __restrict__ fallback, int* __restrict__ nfallback) {
+                     int* __restrict__ brick_pairs, int* __restrict__ fallback, int* __restrict__ nfallback,
+                     float2* __restrict__ zero_out, PixelSet zpx) {
   extern __shared__ int hits[];  // brick ids of this slice
   __shared__ int s_n;
   __shared__ long long s_base;
@@ -276,6 +277,18 @@ segment_pairs_kernel(const float* __restrict__ mats, BrickGrid g, float pmax, fl
   if (!(scale * pmax < limit)) {  // uniform over the block
     if (tid == 0) fallback[atomicAdd(nfallback, 1)] = slice;
     return;
+  }
+  if (zero_out) {
+    // the projector's zeros outside rmax (Project.cu:111-115): in each row
+    // the tail x > sqrt(rmax^2 - y^2), one warp per row (slices taking the
+    // direct path write their own zeros)
+    float2* out = zero_out + zpx.elements * slice;
+    for (int idy = tid >> 5; idy < zpx.n; idy += kPairThreads / 32) {
+      const int v = idy <= zpx.n / 2 ? idy : idy - zpx.n;
+      const int rem = zpx.rmax2 - v * v;
+      const int x0 = rem >= 0 ? seg_isqrt(rem) + 1 : 0;
+      for (int x = x0 + lane; x < zpx.dimft; x += 32) out[(int64_t)idy * zpx.dimft + x] = make_float2(0.f, 0.f);
+    }
   }
   if (tid == 0) s_n = 0;
   __syncthreads();
@@ -425,7 +438,8 @@ static int brick_order(const BrickGrid& g, const int** out) {
 }
 
 int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g, const PixelSet& px,
-                     float limit, int chunk, cudaStream_t stream, BrickPlan* plan, int segments) {
+                     float limit, int chunk, cudaStream_t stream, BrickPlan* plan, int segments,
+                     void* zero_out) {
   plan->g = g;
   plan->batch = batch;
   size_t hist_bytes = 2 * sizeof(int) * (size_t)g.nbricks;
@@ -510,7 +524,7 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
       cudaFuncSetAttribute(segment_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
       segment_pairs_kernel<<<batch, kPairThreads, smem_bytes, stream>>>(
           d_mats, g, px.pmax, limit, below, plan->bins, bins_cap, counters, counts, plan->fallback,
-          plan->nfallback);
+          plan->nfallback, (float2*)zero_out, px);
     } else if (op == GTOMRLN_OP_PROJECT) {
       cudaFuncSetAttribute(bin_slices_kernel<GTOMRLN_OP_PROJECT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem_bytes);

@@ -379,11 +379,15 @@ static int project_brick(const float* d_volumeft, float* d_proj, const float* d_
   px.strict = 0;
   px.pmax = (float)a.rmax;
   BrickPlan plan;
+  // the segment plan writes the zeros outside rmax of the slices it plans
+  // (the direct kernel those of the slices it leaves over)
   int st = build_brick_plan(GTOMRLN_OP_PROJECT, d_mats, (int)batch, g, px, (float)(P / 2) + 0.99f, tune.chunk,
-                            stream, &plan, segments);
+                            stream, &plan, segments, segments ? d_proj : nullptr);
   if (st) return st;
-  int64_t rows = (int64_t)a.n * batch;  // 2D slices: n rows of dimft elements each
-  project_zero_kernel<<<sms * 8, 256, 0, stream>>>((float2*)d_proj, a, rows);
+  if (!segments) {
+    int64_t rows = (int64_t)a.n * batch;  // 2D slices: n rows of dimft elements each
+    project_zero_kernel<<<sms * 8, 256, 0, stream>>>((float2*)d_proj, a, rows);
+  }
   if (segments)
     kern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
         (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, px, plan.items, plan.nitems, plan.pairs,
