@@ -332,10 +332,13 @@ def run_ours(args):
                       "volume": f"{P // 2 + 1}x{P}x{P} c64 decentred", "accumulators": f"{D // 2 + 1}x{D}x{D} "
                       "c64 + f32 centred", "l2_flush": "inputs larger than L2 (per-step data 3.96 GB)",
                       "parallelism": f"dp{world}"},
-           # per step: the brick projector launches 7 kernels (plan: bin, scan,
-           # fill, items; zero fill, brick kernel, direct fallback) and the brick
-           # backprojector 6 (plan x4, brick kernel, direct fallback)
-           "gpu_launches": 13 * args.steps,
+           # per step with the default (row-segment) path: the projector launches
+           # 6 kernels (plan: pairs with the zero fill, scan, fill, items; the
+           # segment kernel; the direct fallback over its list) and the
+           # backprojector 6 (plan x4, segment kernel, direct fallback); the
+           # binned path adds a zero fill to the projector's; the direct path
+           # launches one kernel per operator
+           "gpu_launches": {"brick": 13, "direct": 2}.get(args.path, 12) * args.steps,
            "roofline": dominant, "rooflines": [roof_proj, roof_bp],
            "kernel_ms_per_step": {"project": round(proj_ms, 4), "backproject": round(bp_ms, 4)},
            "peaks": probe, "clocks": clocks.summary()}
