@@ -63,7 +63,8 @@ def parse_args():
     ap.add_argument("--no-gridding", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip gridding, e2e, CPU baseline and L2 probes (profiling runs)")
-    ap.add_argument("--cpu-sample", type=int, default=256, help="slices timed on the host cores")
+    ap.add_argument("--cpu-sample", type=int, default=10240,
+                    help="slices timed on the host cores (about 10 s of work on 16 threads)")
     ap.add_argument("--subtomos", type=int, default=512,
                     help="sub-tomograms of the batched uneven-box workload (0 skips it)")
     return ap.parse_args()
