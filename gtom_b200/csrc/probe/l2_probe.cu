@@ -61,7 +61,8 @@ __global__ void gather_probe_kernel(const float2* __restrict__ buf, uint32_t mas
 
 // Shared-memory update rate: every thread adds to pseudo-random words of a
 // 12K-word (48 KB) array.  mode 0: FP32 atomicAdd, 1: int32 atomicAdd,
-// 2: plain FP32 read-add-write (no atomicity), 3: int64 atomicAdd.
+// 2: plain FP32 read-add-write (no atomicity), 3: int64 atomicAdd,
+// 4: FP32 red.shared.add (no returned value).
 template <int MODE>
 __global__ void smem_probe_kernel(float* __restrict__ sink, int iters) {
   __shared__ float s[12288];
@@ -75,6 +76,10 @@ __global__ void smem_probe_kernel(float* __restrict__ sink, int iters) {
     if (MODE == 1) atomicAdd((int*)s + k, 1);
     if (MODE == 2) s[k] += 1.0f;
     if (MODE == 3) atomicAdd((unsigned long long*)s + k, 1ull);
+    if (MODE == 4) {  // explicit reduction (no returned value)
+      const unsigned a = (unsigned)__cvta_generic_to_shared(s + k);
+      asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(1.0f) : "memory");
+    }
   }
   __syncthreads();
   if (threadIdx.x == 0) sink[blockIdx.x] = s[blockIdx.x % 12288];
@@ -183,7 +188,8 @@ double gtomrln_probe_smem_update(int mode, int blocks, int threads, int iters) {
     if (mode == 0) smem_probe_kernel<0><<<blocks, threads>>>(sink, iters);
     else if (mode == 1) smem_probe_kernel<1><<<blocks, threads>>>(sink, iters);
     else if (mode == 2) smem_probe_kernel<2><<<blocks, threads>>>(sink, iters);
-    else smem_probe_kernel<3><<<blocks, threads>>>(sink, iters);
+    else if (mode == 3) smem_probe_kernel<3><<<blocks, threads>>>(sink, iters);
+    else smem_probe_kernel<4><<<blocks, threads>>>(sink, iters);
   };
   launch();
   cudaEventRecord(a);
