@@ -73,42 +73,82 @@ __global__ void grid_init_kernel(const float* __restrict__ weight, int oldx, int
 // conv <- (conv * 1/P^3) * blob(r): d_IFFTC2R's renormalisation
 // (IFFT.cu:36-46) and d_MultiplyByVector with PrecomputeBlobKernel's table
 // lookup (RecFourier.cu:243-262), the radius evaluated as the reference does.
-// Grid: x blocks along a row, blockIdx.y = a group of kBlobRows rows (y),
-// blockIdx.z = volume * P + z.  Each thread loads its kBlobRows elements
-// before using any (eight loads in flight per thread: one alone leaves too
-// few bytes in flight to cover the memory latency), and no index needs a
-// division.
+// A grid-stride kernel over units of kBlobRows rows (y) of one (volume, z)
+// plane; each CTA stages the 10 000-entry table in shared memory once (read
+// from global memory, lanes at consecutive x touch one cache line each).
+// Each thread loads its kBlobRows elements of a column before using any
+// (eight loads in flight per thread), and no index needs a 64-bit division.
 constexpr int kBlobRows = 8;
-__global__ void grid_blob_kernel(float* __restrict__ conv, const float* __restrict__ table,
-                                 GridGeom g, float inv_n, float funcsampling) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  if (x >= g.P) return;
-  const int vol = blockIdx.z / g.P, z = blockIdx.z - vol * g.P;
-  const int y0 = blockIdx.y * kBlobRows;
-  const int64_t base = (int64_t)vol * g.nr + (int64_t)z * g.P * g.P + x;
-  float v[kBlobRows];
+constexpr int kBlobThreads = 512;
+template <bool HOIST>
+__global__ void __launch_bounds__(kBlobThreads, 3)
+grid_blob_kernel(float* __restrict__ conv, const float* __restrict__ table, GridGeom g, int count, float inv_n,
+                 float funcsampling) {
+  __shared__ float stab[kBlobSamples];
+  for (int i = threadIdx.x; i < kBlobSamples; i += blockDim.x) stab[i] = __ldg(table + i);
+  __syncthreads();
+  const int P = g.P;
+  const int groups = (P + kBlobRows - 1) / kBlobRows;
+  const int64_t units = (int64_t)count * P * groups;
+  for (int64_t unit = blockIdx.x; unit < units; unit += gridDim.x) {
+    const int64_t plane = unit / groups;  // volume * P + z
+    const int y0 = (int)(unit - plane * groups) * kBlobRows;
+    const int z = (int)(plane % P);
+    const int rows = min(kBlobRows, P - y0);
+    // HOIST (P <= 4096): grid_blob_index's radius with the conversions
+    // hoisted: xp^2 + yp^2 + zp^2 is then an integer below 2^24, exact in
+    // FP32 however it is summed, so the row part yp^2 + zp^2 is formed once
+    // per row and only the square root, the division and the truncation
+    // remain per voxel
+    const int zp = z < P / 2 ? z : z - P;
+    float c[kBlobRows];
 #pragma unroll
-  for (int r = 0; r < kBlobRows; r++)
-    if (y0 + r < g.P) v[r] = conv[base + (int64_t)(y0 + r) * g.P];
+    for (int r = 0; r < kBlobRows; r++) {
+      const int y = y0 + r, yp = y < P / 2 ? y : y - P;
+      c[r] = (float)(yp * yp + zp * zp);
+    }
+    const bool pow2 = (P & (P - 1)) == 0;
+    const float inv_p = __frcp_rn((float)P);
+    for (int x = threadIdx.x; x < P; x += blockDim.x) {
+      float* col = conv + (plane * P + y0) * P + x;
+      float v[kBlobRows];
 #pragma unroll
-  for (int r = 0; r < kBlobRows; r++) {
-    const int y = y0 + r;
-    if (y >= g.P) break;
-    conv[base + (int64_t)y * g.P] = v[r] * inv_n * grid_blob_at(table, g.P, x, y, z, funcsampling);
+      for (int r = 0; r < kBlobRows; r++)
+        if (r < rows) v[r] = col[r * P];
+      const float xp = (float)(x < P / 2 ? x : x - P);
+      const float xx = xp * xp;
+#pragma unroll
+      for (int r = 0; r < kBlobRows; r++) {
+        if (r >= rows) break;
+        int ti;
+        if (HOIST) {
+          const float sq = sqrtf(xx + c[r]);
+          const float rr = (pow2 ? sq * inv_p : sq / (float)P) / funcsampling;
+          ti = (int)rr;
+          ti = ti < kBlobSamples - 1 ? ti : kBlobSamples - 1;
+        } else {
+          ti = grid_blob_index(P, x, y0 + r, z, funcsampling);
+        }
+        col[r * P] = v[r] * inv_n * stab[ti];
+      }
+    }
   }
 }
 
-// Launches grid_blob_kernel over `count` consecutive volumes, in groups whose
-// P * count fits the grid's z extent.
+// Launches grid_blob_kernel over `count` consecutive volumes: three CTAs per
+// SM (40 registers, 40 KB of table each), striding over the row units.
 static void launch_blob(float* conv, const float* table, const GridGeom& g, int count, cudaStream_t stream) {
-  const int T = 256;
-  const int per = std::max(1, 65535 / g.P);
-  for (int v0 = 0; v0 < count; v0 += per) {
-    const int c = std::min(per, count - v0);
-    dim3 grid((unsigned)((g.P + T - 1) / T), (unsigned)((g.P + kBlobRows - 1) / kBlobRows), (unsigned)(g.P * c));
-    grid_blob_kernel<<<grid, T, 0, stream>>>(conv + (int64_t)v0 * g.nr, table, g, 1.0f / (float)g.nr,
-                                             (float)(0.5 / kBlobSamples));
-  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t units = (int64_t)count * g.P * ((g.P + kBlobRows - 1) / kBlobRows);
+  const unsigned blocks = (unsigned)std::min<int64_t>(units, 3LL * sms);
+  if (g.P <= 4096)
+    grid_blob_kernel<true><<<blocks, kBlobThreads, 0, stream>>>(conv, table, g, count, 1.0f / (float)g.nr,
+                                                              (float)(0.5 / kBlobSamples));
+  else
+    grid_blob_kernel<false><<<blocks, kBlobThreads, 0, stream>>>(conv, table, g, count, 1.0f / (float)g.nr,
+                                                               (float)(0.5 / kBlobSamples));
 }
 
 // Iteration2Kernel (RecFourier.cu:293-308) fused with the next iteration's

@@ -16,17 +16,28 @@ struct GridGeom {
   int64_t nr;    // P^3 real elements
 };
 
-// PrecomputeBlobKernel's table lookup (RecFourier.cu:243-262) at real-space
-// voxel (x, y, z) of the P grid, the radius evaluated as the reference does.
-__device__ __forceinline__ float grid_blob_at(const float* __restrict__ table, int P, int x, int y, int z,
-                                              float funcsampling) {
+// PrecomputeBlobKernel's table index (RecFourier.cu:243-262) at real-space
+// voxel (x, y, z) of the P grid, the radius evaluated as the reference does:
+// sqrt(r^2) / P / funcsampling in FP32.  For a power-of-two P the division by
+// P is the multiplication by its reciprocal (exact: a power of two), which
+// leaves one division per voxel.
+__device__ __forceinline__ int grid_blob_index(int P, int x, int y, int z, float funcsampling) {
   const int zp = z < P / 2 ? z : z - P;
   const int yp = y < P / 2 ? y : y - P;
   const float xp = (float)(x < P / 2 ? x : x - P);
-  const float r = sqrtf(xp * xp + (float)(yp * yp) + (float)(zp * zp)) / (float)P / funcsampling;
-  int ti = (int)r;
-  ti = ti < kBlobSamples - 1 ? ti : kBlobSamples - 1;
-  return __ldg(table + ti);
+  const float s = sqrtf(xp * xp + (float)(yp * yp) + (float)(zp * zp));
+  const float sp = (P & (P - 1)) == 0 ? s * __frcp_rn((float)P) : s / (float)P;
+  const float r = sp / funcsampling;
+  const int ti = (int)r;
+  return ti < kBlobSamples - 1 ? ti : kBlobSamples - 1;
+}
+
+// The table value there, read from global memory.  Lanes at consecutive x
+// read entries ~20000/P apart, one cache line each: kernels that stream
+// many voxels stage the table in shared memory and use grid_blob_index.
+__device__ __forceinline__ float grid_blob_at(const float* __restrict__ table, int P, int x, int y, int z,
+                                              float funcsampling) {
+  return __ldg(table + grid_blob_index(P, x, y, z, funcsampling));
 }
 
 // Iteration2Kernel (RecFourier.cu:293-308) for one voxel: the new
