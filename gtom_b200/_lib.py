@@ -75,7 +75,7 @@ SIGNATURES: dict[str, list] = {
     "gtomrln_reconstruct_gridding_warm": [_p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i, _d, _f, _p,
                                           _f, _d, _i, _d, _ip, _dp, _ip, _p],
     "gtomrln_gridding_weights": [_p, _i, _i, _i, _i, _i, _i, _d, _f, _p, _f, _d, _i, _d, _p, _p,
-                                 _ip, _dp, _ip, _p],
+                                 _ip, _dp, _ip, _p, _d, _dp, _p],
     "gtomrln_kaiser_bessel_table": [_d, _d, _i, _i, _p],
     "gtomrln_ctf_simulate": [_p, _p, _p, _p, _u, _i, _i, _i, _p],
     "gtomrln_preprocess_particles": [_p, _i, _u, _p, _p, _p, _p],

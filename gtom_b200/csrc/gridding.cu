@@ -156,15 +156,18 @@ static void launch_blob(float* conv, const float* table, const GridGeom& g, int 
 // sum((Fw*(new-old))^2) and sum((Fw*old)^2): the change of the corrected
 // weight Fw*Fnw.  Unweighted, voxels with Fw = 0 would dominate: there
 // Fnw grows by 1e4 per iteration until the 1e20 clamp and never matters.
+// With ref (a single volume's reference weights, e.g. converged ones) it
+// also accumulates sum((Fw*(new-ref))^2) and sum((Fw*ref)^2) into
+// change[2..3]: the distance of the corrected weight from the reference's.
 __global__ void grid_update_kernel(float2* __restrict__ convft, const float* __restrict__ Fw,
                                    float* __restrict__ Fnw, GridGeom g, int write_conv,
-                                   double* __restrict__ change) {
+                                   double* __restrict__ change, const float* __restrict__ ref) {
   const int64_t b = blockIdx.y;  // change is only requested for a single volume
   convft += b * g.nc;
   Fw += b * g.nc;
   Fnw += b * g.nc;
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  double d2 = 0, o2 = 0;
+  double d2 = 0, o2 = 0, r2 = 0, q2 = 0;
   if (i < g.nc) {
     float old = Fnw[i];
     float nw = grid_update_value(convft[i].x, old);
@@ -176,9 +179,19 @@ __global__ void grid_update_kernel(float2* __restrict__ convft, const float* __r
       double o = (double)fw * (double)old;
       d2 = d * d;
       o2 = o * o;
+      if (ref) {
+        const double rf = (double)ref[i];
+        const double e = (double)fw * ((double)nw - rf), q = (double)fw * rf;
+        r2 = e * e;
+        q2 = q * q;
+      }
     }
   }
   if (change) grid_change_reduce(d2, o2, change);
+  if (change && ref) {
+    __syncthreads();  // grid_change_reduce's shared scratch is reused
+    grid_change_reduce(r2, q2, change + 2);
+  }
 }
 
 // The update of grid_update_kernel applied at an extrapolated point V
@@ -192,14 +205,15 @@ __global__ void grid_update_kernel(float2* __restrict__ convft, const float* __r
 // Fw * (F' - F) against Fw * F.
 __global__ void grid_update_momentum_kernel(float2* __restrict__ convft, const float* __restrict__ Fw,
                                             float* __restrict__ Fnw, float* __restrict__ V, GridGeom g,
-                                            float beta, int write_conv, double* __restrict__ change) {
+                                            float beta, int write_conv, double* __restrict__ change,
+                                            const float* __restrict__ ref) {
   const int64_t b = blockIdx.y;
   convft += b * g.nc;
   Fw += b * g.nc;
   Fnw += b * g.nc;
   V += b * g.nc;
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  double d2 = 0, o2 = 0;
+  double d2 = 0, o2 = 0, r2 = 0, q2 = 0;
   if (i < g.nc) {
     float old = Fnw[i];
     float nw, ext;
@@ -213,9 +227,19 @@ __global__ void grid_update_momentum_kernel(float2* __restrict__ convft, const f
       double o = (double)fw * (double)old;
       d2 = d * d;
       o2 = o * o;
+      if (ref) {
+        const double rf = (double)ref[i];
+        const double e = (double)fw * ((double)nw - rf), q = (double)fw * rf;
+        r2 = e * e;
+        q2 = q * q;
+      }
     }
   }
   if (change) grid_change_reduce(d2, o2, change);
+  if (change && ref) {
+    __syncthreads();  // grid_change_reduce's shared scratch is reused
+    grid_change_reduce(r2, q2, change + 2);
+  }
 }
 
 // DecenterKernel<tcomplex> for the data (RecFourier.cu:175-179), then
@@ -399,12 +423,15 @@ struct GridOptions {
   bool weights_only = false;    // stop after the weights (no map)
   float* out_fw = nullptr;      // copies of the final Fweight / Fnewweight on the P grid
   float* out_fnw = nullptr;
+  const float* ref_fnw = nullptr;  // reference weights on the P grid: measure the distance to them
+  double ref_tolerance = 0;        // and stop when it is <= this (cuFFT path)
 };
 
 struct GridResult {
   int iterations = 0;  // iterations run, including one from a rejected predicted start
   double change = 0;   // the last change measure
   int warm_used = 0;   // 1 if the predicted start was kept
+  double distance = 0;  // the last distance from the reference weights (when given)
 };
 
 static int reconstruct(const float* d_dataft, const float* d_weight, float* d_out, int ori,
@@ -444,7 +471,9 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   float *Fw = nullptr, *Fnw = nullptr, *V = nullptr;
   double* change = nullptr;
   double* sums = nullptr;
-  double h_change[2] = {0, 0};
+  double h_change[4] = {0, 0, 0, 0};  // change sums, then distance-to-reference sums
+  const bool measure_ref = opt.ref_fnw != nullptr;
+  double last_distance = 0;
   int total_iters = 0;
   double last_change = 0;
   bool warm_live = warm;
@@ -452,7 +481,8 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   unsigned bc = (unsigned)((g.nc + T - 1) / T);
   // The fused FFT iteration (gridfft.cu) for power-of-two grids when the
   // caller chose it; the final map always uses cuFFT.
-  const bool fused = path_choice(GTOMRLN_OP_GRIDDING) == GTOMRLN_PATH_FUSED && gridfft_available(P, 1);
+  const bool fused = path_choice(GTOMRLN_OP_GRIDDING) == GTOMRLN_PATH_FUSED && !measure_ref &&
+                     gridfft_available(P, 1);
   bool need_first = true;  // the fused loop starts with the inverse transform along z
 
   GTOMRLN_STEP(pool_alloc((void**)&convft, g.nc * sizeof(float2), stream));
@@ -460,7 +490,8 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   GTOMRLN_STEP(pool_alloc((void**)&Fw, g.nc * sizeof(float), stream));
   GTOMRLN_STEP(pool_alloc((void**)&Fnw, g.nc * sizeof(float), stream));
   if (momentum) GTOMRLN_STEP(pool_alloc((void**)&V, g.nc * sizeof(float), stream));
-  if (opt.tolerance > 0 || warm) GTOMRLN_STEP(pool_alloc((void**)&change, 2 * sizeof(double), stream));
+  if (opt.tolerance > 0 || warm || measure_ref)
+    GTOMRLN_STEP(pool_alloc((void**)&change, sizeof(h_change), stream));
   if (warm) GTOMRLN_STEP(pool_alloc((void**)&sums, 2 * sizeof(double), stream));
 
   GTOMRLN_CUFFT_TRY(cufftSetStream(plans.r2c, stream));
@@ -478,11 +509,11 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
 
   for (int it = 0; it < iterations; it++) {
     // the residual check of a predicted start needs the first change
-    double* ch = (opt.tolerance > 0 || (warm_live && it == 0)) ? change : nullptr;
+    double* ch = (opt.tolerance > 0 || measure_ref || (warm_live && it == 0)) ? change : nullptr;
     if (fused) {
       if (need_first) GTOMRLN_STEP(gridfft_first(convft, g, 1, stream));
       need_first = false;
-      if (ch) GTOMRLN_CUDA_TRY(cudaMemsetAsync(ch, 0, 2 * sizeof(double), stream));
+      if (ch) GTOMRLN_CUDA_TRY(cudaMemsetAsync(ch, 0, sizeof(h_change), stream));
       GTOMRLN_STEP(gridfft_iteration(convft, g, 1, table, Fw, Fnw, momentum ? V : nullptr, opt.momentum,
                                      it + 1 < iterations, ch, stream));
     } else {
@@ -490,12 +521,12 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
       launch_blob(conv, table, g, 1, stream);
       GTOMRLN_STEP(launch_check("grid_blob_kernel"));
       GTOMRLN_CUFFT_TRY(cufftExecR2C(plans.r2c, conv, (cufftComplex*)convft));
-      if (ch) GTOMRLN_CUDA_TRY(cudaMemsetAsync(ch, 0, 2 * sizeof(double), stream));
+      if (ch) GTOMRLN_CUDA_TRY(cudaMemsetAsync(ch, 0, sizeof(h_change), stream));
       if (momentum)
         grid_update_momentum_kernel<<<bc, T, 0, stream>>>(convft, Fw, Fnw, V, g, opt.momentum,
-                                                          it + 1 < iterations, ch);
+                                                          it + 1 < iterations, ch, opt.ref_fnw);
       else
-        grid_update_kernel<<<bc, T, 0, stream>>>(convft, Fw, Fnw, g, it + 1 < iterations, ch);
+        grid_update_kernel<<<bc, T, 0, stream>>>(convft, Fw, Fnw, g, it + 1 < iterations, ch, opt.ref_fnw);
       GTOMRLN_STEP(launch_check("grid_update_kernel"));
     }
     total_iters++;
@@ -503,6 +534,7 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
       GTOMRLN_CUDA_TRY(cudaMemcpyAsync(h_change, ch, sizeof(h_change), cudaMemcpyDeviceToHost, stream));
       GTOMRLN_CUDA_TRY(cudaStreamSynchronize(stream));
       last_change = h_change[1] > 0 ? std::sqrt(h_change[0] / h_change[1]) : 0.0;
+      if (measure_ref) last_distance = h_change[3] > 0 ? std::sqrt(h_change[2] / h_change[3]) : 0.0;
       if (warm_live && it == 0) {
         warm_live = false;
         if (!(last_change <= (double)opt.residual_limit)) {
@@ -520,6 +552,7 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
         if (res) res->warm_used = 1;
       }
       if (opt.tolerance > 0 && last_change <= opt.tolerance) break;
+      if (measure_ref && last_distance <= opt.ref_tolerance) break;
       if (it + 1 == iterations) break;
     }
   }
@@ -541,6 +574,7 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   if (res) {
     res->iterations = total_iters;
     res->change = last_change;
+    res->distance = last_distance;
   }
 
 done:
@@ -633,7 +667,7 @@ int gridding_batch_run(const GridBatch& b, const float2* data, const float* weig
     launch_blob(b.conv, b.table, g, b.count, stream);
     GTOMRLN_STEP(launch_check("grid_blob_kernel"));
     GTOMRLN_CUFFT_TRY(cufftExecR2C(b.r2c, b.conv, (cufftComplex*)b.convft));
-    grid_update_kernel<<<gc, T, 0, stream>>>(b.convft, b.Fw, b.Fnw, g, it + 1 < iterations, nullptr);
+    grid_update_kernel<<<gc, T, 0, stream>>>(b.convft, b.Fw, b.Fnw, g, it + 1 < iterations, nullptr, nullptr);
     GTOMRLN_STEP(launch_check("grid_update_kernel"));
   }
   grid_final_kernel<<<gc, T, 0, stream>>>(data, b.D, b.D, b.D, b.Fw, b.Fnw, b.convft, g, iterations == 0,
@@ -770,10 +804,15 @@ int gtomrln_gridding_weights(const float* d_weight, int ox, int oy, int oz, int 
                              const float* d_mlp_params, float residual_limit, double blobradius,
                              int bloborder, double blobalpha, float* d_fw, float* d_fnw,
                              int* iterations_done, double* final_change, int* warm_used,
+                             const float* d_ref_fnw, double ref_tolerance, double* final_distance,
                              void* stream) {
   clear_error();
   if (!d_fnw) return set_error(GTOMRLN_ERR_INVALID, "gridding_weights: NULL output");
+  if (d_ref_fnw && !(ref_tolerance >= 0))
+    return set_error(GTOMRLN_ERR_INVALID, "gridding_weights: negative reference tolerance");
   GridOptions opt;
+  opt.ref_fnw = d_ref_fnw;
+  opt.ref_tolerance = ref_tolerance;
   opt.tolerance = tolerance;
   opt.momentum = momentum;
   opt.mlp = d_mlp_params;
@@ -787,6 +826,7 @@ int gtomrln_gridding_weights(const float* d_weight, int ox, int oy, int oz, int 
   if (iterations_done) *iterations_done = res.iterations;
   if (final_change) *final_change = res.change;
   if (warm_used) *warm_used = res.warm_used;
+  if (final_distance) *final_distance = res.distance;
   return st;
 }
 

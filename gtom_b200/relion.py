@@ -335,18 +335,20 @@ def gridding_weights(weight, dimspadded: Dims, ori: int, paddingfactor: int = 2,
                      max_iterations: int = 1000, tolerance: float = 1e-4, momentum: float = 0.0,
                      mlp_params=None, residual_limit: float = 0.5, blobradius: float = 1.9,
                      bloborder: int = 0, blobalpha: float = 15.0, fw_out=None, fnw_out=None,
-                     stream=None):
+                     stream=None, ref_fnw=None, ref_tolerance: float = 0.0, return_distance: bool = False):
     """The gridding weights only (gtomrln_gridding_weights).  Returns
     (Fnewweight, Fweight, iterations, last change, predicted start kept);
     the weights are flat float32 CUDA tensors on the decentred
-    (P/2+1) x P x P grid, P = ori * paddingfactor."""
+    (P/2+1) x P x P grid, P = ori * paddingfactor.  With ref_fnw (weights on
+    that grid) the loop also stops once ||Fw (Fnw - ref)|| / ||Fw ref|| <=
+    ref_tolerance; return_distance appends the last such distance."""
     qx, qy, qz = (int(v) for v in dimspadded)
     P = int(ori) * int(paddingfactor)
     nc = (P // 2 + 1) * P * P
     dev = weight.device
     fnw = fnw_out if fnw_out is not None else torch.empty(nc, dtype=torch.float32, device=dev)
     fw = fw_out if fw_out is not None else torch.empty(nc, dtype=torch.float32, device=dev)
-    it, ch, used = C.c_int(0), C.c_double(0), C.c_int(0)
+    it, ch, used, dist = C.c_int(0), C.c_double(0), C.c_int(0), C.c_double(0)
     _lib.call("gtomrln_gridding_weights",
               _dev_ptr(weight, "d_weight", torch.float32, elements_fft((qx, qy, qz))),
               qx, qy, qz, int(ori), int(paddingfactor), int(max_iterations), float(tolerance),
@@ -354,7 +356,11 @@ def gridding_weights(weight, dimspadded: Dims, ori: int, paddingfactor: int = 2,
               _dev_ptr(mlp_params, "d_mlp_params", torch.float32, mlp_param_count(), optional=True),
               C.c_float(float(residual_limit)), float(blobradius), int(bloborder), float(blobalpha),
               _dev_ptr(fw, "d_fw", torch.float32, nc), _dev_ptr(fnw, "d_fnw", torch.float32, nc),
-              C.byref(it), C.byref(ch), C.byref(used), _stream(stream))
+              C.byref(it), C.byref(ch), C.byref(used),
+              _dev_ptr(ref_fnw, "ref_fnw", torch.float32, nc, optional=True), float(ref_tolerance),
+              C.byref(dist), _stream(stream))
+    if return_distance:
+        return fnw, fw, it.value, ch.value, bool(used.value), dist.value
     return fnw, fw, it.value, ch.value, bool(used.value)
 
 

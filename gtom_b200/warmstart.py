@@ -286,14 +286,19 @@ def fsc_min(a: torch.Tensor, b: torch.Tensor, box: int) -> float:
 
 
 def evaluate(params: torch.Tensor | None, box: int, dists: list, pad: int = 2,
-             tolerance: float = 1e-4, max_iterations: int = 5000, volft=None) -> list:
+             tolerance: float = 1e-4, max_iterations: int = 5000, volft=None,
+             converged_tolerance: float = 1e-4, converge_max: int = 20000) -> list:
     """For each distribution: the converged weights (momentum, relative
     change 1e-6, about the float32 floor of the change measure), then for each of MODES the iterations to `tolerance`, the
     weighted distance of the stopped weights from the converged ones, the
     wall time of the whole reconstruction through reconstruct_gridding_warm
     (CUDA events around the call, which synchronises once per iteration),
     and the map's minimum FSC to the plain map and to the map made with the
-    converged weights."""
+    converged weights.  Under "to_converged": the iterations the mode needs
+    to bring the weights within `converged_tolerance` (weighted relative L2)
+    of the converged ones, found with the library's distance measure, and
+    the wall time of the whole reconstruction run for exactly that many
+    iterations (no convergence test, so no per-iteration synchronisation)."""
     from .relion import reconstruct_gridding_warm
     P = box * pad
     D = P + 1
@@ -328,6 +333,19 @@ def evaluate(params: torch.Tensor | None, box: int, dists: list, pad: int = 2,
             torch.cuda.synchronize()
             res["ms"] = a.elapsed_time(b)
             maps[name] = m
+            _, _, k, _, _, dist = gridding_weights(w, (D, D, D), box, pad, converge_max, 0.0, mom, mlp_params=p,
+                                                   ref_fnw=ref, ref_tolerance=converged_tolerance,
+                                                   return_distance=True)
+            conv = {"iterations": k, "distance": dist, "reached": bool(dist <= converged_tolerance)}
+            if conv["reached"]:
+                m2 = torch.empty_like(out)
+                torch.cuda.synchronize()
+                a.record()
+                reconstruct_gridding_warm(data, w, m2, (box,) * 3, (D,) * 3, p, pad, k, 0.0, mom)
+                b.record()
+                torch.cuda.synchronize()
+                conv["ms"] = a.elapsed_time(b)
+            res["to_converged"] = conv
             row[name] = res
         for name, m in maps.items():
             row[name]["fsc_min_to_plain"] = fsc_min(m, maps["plain"], box)
@@ -353,6 +371,15 @@ def summarise(rows: list) -> dict:
                      if name.endswith("+mlp") else 0,
                      "speedup_vs_plain": float(np.median([r["plain"]["ms"] / r[name]["ms"] for r in rows
                                                           if name in r]))}
+        both = [r for r in rows if name in r and r[name]["to_converged"]["reached"]
+                and r["plain"]["to_converged"]["reached"]]
+        tc = [h["to_converged"] for h in have]
+        out[name]["to_converged"] = {
+            "reached": int(sum(1 for c in tc if c["reached"])), "of": len(tc),
+            "iterations": float(np.median([c["iterations"] for c in tc])),
+            "ms": float(np.median([c["ms"] for c in tc if c["reached"]])) if any(c["reached"] for c in tc) else None,
+            "speedup_vs_plain": float(np.median([r["plain"]["to_converged"]["ms"] / r[name]["to_converged"]["ms"]
+                                                 for r in both])) if both else None}
     return out
 
 

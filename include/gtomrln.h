@@ -356,13 +356,18 @@ GTOMRLN_API int gtomrln_reconstruct_gridding_warm(const float* d_dataft, const f
  * volume of dims ox x oy x oz, at least P + 1 with P = ori * paddingfactor):
  * d_fnw receives Fnewweight and d_fw (may be NULL) the decentred, masked
  * Fweight, both on the decentred (P/2+1) x P x P grid.  Used to make the
- * MLP's training pairs and to compare starts. */
+ * MLP's training pairs and to compare starts.  d_ref_fnw (may be NULL):
+ * reference weights on the same grid, e.g. converged ones; each iteration
+ * then measures the distance ||Fw (Fnw - ref)|| / ||Fw ref|| and the loop
+ * also stops once it is <= ref_tolerance (*final_distance receives the
+ * last one; the cuFFT path runs whatever path is selected). */
 GTOMRLN_API int gtomrln_gridding_weights(const float* d_weight, int ox, int oy, int oz, int ori,
                              int paddingfactor, int max_iterations, double tolerance,
                              float momentum, const float* d_mlp_params, float residual_limit,
                              double blobradius, int bloborder, double blobalpha, float* d_fw,
                              float* d_fnw, int* iterations_done, double* final_change,
-                             int* warm_used, void* stream);
+                             int* warm_used, const float* d_ref_fnw, double ref_tolerance,
+                             double* final_distance, void* stream);
 
 /* ---------------------------------------------------------------------------
  * The warm-start MLP (no reference counterpart).  28 inputs -> 64 -> 64 -> 1,

@@ -202,3 +202,24 @@ def test_trained_network_beats_the_cold_start(cuda):
             _, _, it_w, _, _ = _gridding(w, D, box, 3000, tol=1e-4, momentum=mom, params=params)
             assert it_w <= it_c, (mom, it_w, it_c)
     assert min(gains) > 1.2, gains
+
+
+@pytest.mark.parametrize("momentum", [0.0, 0.9])
+def test_distance_to_reference_weights_stops_the_loop(cuda, momentum):
+    """gtomrln_gridding_weights with reference weights: the library's
+    distance ||Fw (Fnw - ref)|| / ||Fw ref|| equals the one measured on the
+    returned weights, the loop stops at the first iteration within the
+    tolerance, and one iteration fewer is not within it."""
+    P = 64
+    vol, D = _weights(P)
+    w = torch.from_numpy(vol).cuda()
+    ref, fw, _, _, _ = _gridding(w, D, P // 2, 3000, 1e-6, 0.9)
+    tol = 1e-3
+    fnw, fw2, k, _, _, dist = G.gridding_weights(w, (D, D, D), P // 2, 2, 5000, 0.0, momentum, ref_fnw=ref,
+                                                 ref_tolerance=tol, return_distance=True)
+    assert 1 < k < 5000
+    assert dist <= tol
+    assert dist == pytest.approx(W.weighted_distance(fw2, fnw, ref), rel=1e-5)
+    _, _, k1, _, _, d1 = G.gridding_weights(w, (D, D, D), P // 2, 2, k - 1, 0.0, momentum, ref_fnw=ref,
+                                            ref_tolerance=0.0, return_distance=True)
+    assert k1 == k - 1 and d1 > tol
