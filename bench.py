@@ -323,6 +323,13 @@ def run_ours(args):
                "algorithmic_reductions": bp_reds, "ms_per_launch": round(bp_ms, 4),
                "peak_of": "measured (probe, same run)", "l2_red_peak": l2_peak,
                "frac_of_l2_red": None if not l2_peak else round(bp_rate / l2_peak, 4)}
+    # the same kernel against HBM: its measured DRAM traffic per launch over
+    # its launch time, for readers comparing against the copy bandwidth (the
+    # kernel is not HBM-bound; this says how far it is from being so)
+    if roof_bp["traffic"]:
+        dram_gbs = roof_bp["traffic"] / (bp_ms * 1e-3) / 1e9
+        roof_bp["dram_gbs"] = round(dram_gbs, 1)
+        roof_bp["dram_frac_of_hbm"] = round(dram_gbs / hbm_peak, 4)
     dominant = roof_proj if t_proj >= t_bp else roof_bp
 
     out = {"metric": "project+backproject slices/s @256^3", "value": round(value, 1),
