@@ -347,22 +347,42 @@ def run_ours(args):
            # segment kernel; the direct fallback over its list) and the
            # backprojector 6 (plan x4, segment kernel, direct fallback); the
            # binned path adds a zero fill to the projector's; the direct path
-           # launches one kernel per operator
-           "gpu_launches": {"brick": 13, "direct": 2}.get(args.path, 12) * args.steps,
+           # launches one kernel per operator; summed over the ranks
+           "gpu_launches": world * {"brick": 13, "direct": 2}.get(args.path, 12) * args.steps,
            "roofline": dominant, "rooflines": [roof_proj, roof_bp],
            "kernel_ms_per_step": {"project": round(proj_ms, 4), "backproject": round(bp_ms, 4)},
            "peaks": probe, "clocks": clocks.summary()}
 
-    if not (args.no_gridding or args.no_extras) and rank == 0:
+    # The one-GPU measurements (gridding, the next operators, the batched
+    # reconstructions, the CPU baseline) run at N = 1 only; with N ranks every
+    # rank takes the same collective steps: the end-to-end leg on all ranks
+    # between barriers, the slowest rank's time, a barrier before teardown.
+    single = world == 1
+    if single and not (args.no_gridding or args.no_extras):
         out["gridding"] = time_gridding(G, torch, acc_ft, acc_w, n, D, dev)
-    if rank == 0 and not args.no_extras:
+    if single and not args.no_extras:
         out["extensions"] = time_extensions(args, G, torch, ws, acc_ft, acc_w, dev, hbm_peak, probe)
-    if rank == 0 and not args.no_extras and args.subtomos > 0:
+    if single and not args.no_extras and args.subtomos > 0:
         out["batched_uneven"] = time_batched(args, torch, dev)
-    if rank == 0 and not args.no_extras:
-        out["e2e"] = run_e2e(args, G, torch, ws, dev)
-        out["cpu_baseline"] = cpu_baseline(args, ws)
+    if not args.no_extras:
+        if world > 1:
+            dist.barrier()
+        e2e = run_e2e(args, G, torch, ws, dev)
+        if world > 1:
+            t = torch.tensor([e2e["ms_per_step"]], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_e2e = float(t.item())
+            e2e.update({"value": round(world * e2e["batch_per_step"] / (ms_e2e * 1e-3), 1),
+                        "ms_per_step": round(ms_e2e, 3),
+                        "h2d_bytes_per_step": world * e2e["h2d_bytes_per_step"],
+                        "d2h_bytes_per_step": world * e2e["d2h_bytes_per_step"],
+                        "per_rank": "each rank copies batch_per_step particles; bytes are whole-job, "
+                                    "time the slowest rank's"})
+        out["e2e"] = e2e
+        if single:
+            out["cpu_baseline"] = cpu_baseline(args, ws)
     if world > 1:
+        dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
