@@ -94,28 +94,45 @@ __global__ void ctf_simulate_kernel(float* __restrict__ out, const float2* __res
 // element, the CTF at (sqrt(x^2 + y^2) / n, atan2(y, x)) as
 // ctf_simulate_kernel evaluates it for that address, the phase (-1)^(x+y)
 // that moves the image centre (n/2, n/2) to the origin, and the products.
-__global__ void preprocess_kernel(float2* __restrict__ ft, float* __restrict__ weights, int n,
-                                  const CtfLean* __restrict__ params) {
+// One thread per element for kPrePB consecutive particles: the element's
+// frequency, radius and azimuth are formed once, the particles' values are
+// loaded before any is used (kPrePB loads in flight), and the CTF of each
+// particle is evaluated as ctf_simulate_kernel does for that address.
+constexpr int kPrePB = 4;
+__global__ void __launch_bounds__(256, 4)
+preprocess_kernel(float2* __restrict__ ft, float* __restrict__ weights, int n, int batch,
+                  const CtfLean* __restrict__ params) {
   const int dimft = n / 2 + 1;
-  const int64_t e = (int64_t)dimft * n;
-  const int b = blockIdx.y;
-  ft += e * b;
-  if (weights) weights += e * b;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < e; i += (int64_t)gridDim.x * blockDim.x) {
-    int x = (int)(i % dimft), idy = (int)(i / dimft);
-    int y = idy <= n / 2 ? idy : idy - n;
+  const int e = dimft * n;  // the launcher keeps it below 2^31
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= e) return;
+  const int x = i % dimft, idy = i / dimft;
+  const int y = idy <= n / 2 ? idy : idy - n;
+  const bool odd = (x + idy) & 1;
+  float angle = 0.f, r = 0.f;
+  if (params) {
+    angle = atan2f((float)y, (float)x);
+    r = sqrtf((float)(x * x + y * y)) / (float)n;
+  }
+  const int b0 = blockIdx.y * kPrePB;
+  float2 v[kPrePB];
+#pragma unroll
+  for (int k = 0; k < kPrePB; k++)
+    if (b0 + k < batch) v[k] = ft[(int64_t)(b0 + k) * e + i];
+#pragma unroll
+  for (int k = 0; k < kPrePB; k++) {
+    const int b = b0 + k;
+    if (b >= batch) break;
     float c = 1.f;
     if (params) {
       const CtfLean& p = params[b];
-      float angle = atan2f((float)y, (float)x);
-      float r = sqrtf((float)(x * x + y * y)) / (float)n;
-      float ps = fmaf(p.pixeldelta, __cosf(2.0f * (angle - p.pixelangle)), p.pixelsize);
+      const float ps = fmaf(p.pixeldelta, __cosf(2.0f * (angle - p.pixelangle)), p.pixelsize);
       c = ctf_value<false, false>(__fdividef(r, ps), angle, 0.f, p);
     }
-    float s = ((x + idy) & 1) ? -c : c;
-    float2 v = ft[i];
-    ft[i] = make_float2(v.x * s, v.y * s);
-    if (weights) weights[i] = c * c;
+    const float s = odd ? -c : c;
+    const int64_t j = (int64_t)b * e + i;
+    ft[j] = make_float2(v[k].x * s, v[k].y * s);
+    if (weights) weights[j] = c * c;
   }
 }
 
@@ -199,7 +216,8 @@ int gtomrln_preprocess_particles(const float* d_images, int n, unsigned batch,
                                  const gtomrln_ctf_params_t* h_params, float* d_projft,
                                  float* d_projweights, void* stream) {
   clear_error();
-  if (n < 2 || (n & 1)) return set_error(GTOMRLN_ERR_INVALID, "preprocess_particles: n must be even and >= 2");
+  if (n < 2 || (n & 1) || n > 32768)
+    return set_error(GTOMRLN_ERR_INVALID, "preprocess_particles: n must be even, 2 .. 32768");
   if (batch == 0) return GTOMRLN_OK;
   if (!d_images || !d_projft) return set_error(GTOMRLN_ERR_INVALID, "preprocess_particles: NULL pointer");
   if (batch > 65535) return set_error(GTOMRLN_ERR_INVALID, "preprocess_particles: batch above 65535 (split it)");
@@ -219,8 +237,8 @@ int gtomrln_preprocess_particles(const float* d_images, int n, unsigned batch,
     return set_error(GTOMRLN_ERR_CUFFT, "cufftExecR2C failed (%d)", (int)r);
   }
   const int64_t e = (int64_t)(n / 2 + 1) * n;
-  dim3 grid((unsigned)std::min<int64_t>(64, (e + 255) / 256), batch);
-  preprocess_kernel<<<grid, 256, 0, s>>>((float2*)d_projft, d_projweights, n, d);
+  dim3 grid((unsigned)((e + 255) / 256), (batch + kPrePB - 1) / kPrePB);
+  preprocess_kernel<<<grid, 256, 0, s>>>((float2*)d_projft, d_projweights, n, (int)batch, d);
   cudaError_t ce = cudaGetLastError();
   pool_free(d, s);
   if (ce != cudaSuccess) return set_error(GTOMRLN_ERR_CUDA, "launch of preprocess_kernel failed: %s", cudaGetErrorString(ce));
