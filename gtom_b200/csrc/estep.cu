@@ -122,8 +122,12 @@ diff2_group_kernel(const float2* __restrict__ particle, const float* __restrict_
 // one CTA per 64 references x 64 shifts of one particle.  Chunks of 32
 // elements of c * ref and particle * shift are staged in shared memory
 // (element-major, rows padded against bank conflicts); each thread holds
-// 4 x 4 outputs (references tr + 16 k, shifts ts + 16 k), with the group
-// kernel's per-element arithmetic.
+// 4 x 4 outputs (references tr + 16 k, shifts ts + 16 k).  For the squared
+// differences both staged operands are scaled by sqrt(w) of their element,
+// so that a term w |a - b|^2 = |sqrt(w) a - sqrt(w) b|^2 costs four FP32
+// instructions instead of five (the extra rounding of the scaled operands
+// is of the order of the products' own; the expanded form, which would
+// cancel for close matches, is not used).
 constexpr int kDT = 64;        // references and shifts per tile
 constexpr int kDK = 32;        // elements per staged chunk
 constexpr int kDThreads = 256;
@@ -135,7 +139,6 @@ diff2_dense_tiled_kernel(const float2* __restrict__ particle, const float* __res
                          unsigned nshifts) {
   __shared__ float2 As[kDK][kDT + 1];  // c * ref
   __shared__ float2 Bs[kDK][kDT + 1];  // particle * shift
-  __shared__ float Ws[kDK];
   const unsigned part = blockIdx.z, r0 = blockIdx.y * kDT, s0 = blockIdx.x * kDT;
   const int tid = threadIdx.x, tr = tid >> 4, ts = tid & 15;
   const int li = tid & (kDK - 1), lrow = tid / kDK;  // loader: element li, rows lrow + 8 k
@@ -160,13 +163,17 @@ diff2_dense_tiled_kernel(const float2* __restrict__ particle, const float* __res
       rv[k] = ok && r0 + row < nrefs ? refs[elements * (r0 + row) + gi] : make_float2(0.f, 0.f);
       sv[k] = ok && s0 + row < nshifts ? shifts[elements * (s0 + row) + gi] : make_float2(0.f, 0.f);
     }
+    // sqrt(w) of the loader's element (squared differences only)
+    const float sw = CC ? 1.f : (ok ? (minvsigma2 ? sqrtf(minvsigma2[gi]) : 1.f) : 0.f);
+    const float cs = c * sw;
 #pragma unroll
     for (int k = 0; k < kDT / (kDThreads / kDK); k++) {
       const int row = lrow + k * (kDThreads / kDK);
-      As[li][row] = make_float2(rv[k].x * c, rv[k].y * c);
-      Bs[li][row] = make_float2(pv.x * sv[k].x - pv.y * sv[k].y, pv.x * sv[k].y + pv.y * sv[k].x);
+      As[li][row] = make_float2(rv[k].x * cs, rv[k].y * cs);
+      float2 bv = make_float2(pv.x * sv[k].x - pv.y * sv[k].y, pv.x * sv[k].y + pv.y * sv[k].x);
+      if (!CC) bv = make_float2(bv.x * sw, bv.y * sw);
+      Bs[li][row] = bv;
     }
-    if (tid < kDK) Ws[tid] = i0 + tid < elements ? (minvsigma2 ? minvsigma2[i0 + tid] : 1.f) : 0.f;
     __syncthreads();
 #pragma unroll 4
     for (int i = 0; i < kDK; i++) {
@@ -176,7 +183,6 @@ diff2_dense_tiled_kernel(const float2* __restrict__ particle, const float* __res
         a[k] = As[i][tr + 16 * k];
         b[k] = Bs[i][ts + 16 * k];
       }
-      const float w = Ws[i];
 #pragma unroll
       for (int x = 0; x < 4; x++) {
         if (CC) nn[x] = fmaf(a[x].x, a[x].x, fmaf(a[x].y, a[x].y, nn[x]));
@@ -186,7 +192,7 @@ diff2_dense_tiled_kernel(const float2* __restrict__ particle, const float* __res
             acc[x][y] = fmaf(a[x].x, b[y].x, fmaf(a[x].y, b[y].y, acc[x][y]));
           } else {
             const float dx = a[x].x - b[y].x, dy = a[x].y - b[y].y;
-            acc[x][y] = fmaf(w, fmaf(dx, dx, dy * dy), acc[x][y]);
+            acc[x][y] = fmaf(dx, dx, fmaf(dy, dy, acc[x][y]));
           }
         }
       }

@@ -159,3 +159,29 @@ def test_sort_and_compact(gtom_lib, cuda):
     out = torch.zeros_like(t)
     n = S.d_rlnConvertWeightsCompact(cu(x), out, x.size)
     np.testing.assert_array_equal(out.cpu().numpy()[:n], x[x > 0])
+
+
+@pytest.mark.gpu
+def test_squared_differences_close_match_accuracy(gtom_lib, cuda):
+    """A particle equal to CTF * reference 0 up to 1e-3 noise, identity
+    shift: its squared difference to that reference is ~1e-6 of the
+    operands' weighted power, and the dense (tiled) kernel still gives it to
+    1e-3 of the FP64 oracle (no cancelling expansion of |a - b|^2)."""
+    from gtom_b200.estep import d_rlnSquaredDifferences
+    rng = np.random.default_rng(7)
+    n, nr, ns = 64, 70, 66
+    e = (n // 2 + 1) * n
+    cplx = lambda *s: (rng.normal(size=s) + 1j * rng.normal(size=s)).astype(np.complex64)
+    refs = cplx(nr, e)
+    shifts = cplx(ns, e)
+    shifts[0] = 1.0
+    ctf = rng.uniform(-1, 1, (1, e)).astype(np.float32)
+    part = (ctf[0] * refs[0] + 1e-3 * cplx(e)).astype(np.complex64)[None]
+    w = rng.uniform(0.2, 1.0, e).astype(np.float32)
+    dense = torch.zeros(nr * ns, device="cuda")
+    d_rlnSquaredDifferences(cu(part), cu(w), cu(ctf), (n, n, 1), 1, cu(shifts), ns, cu(refs), nr, 1, dense, False)
+    want = E.squared_differences_dense(part, w, ctf, shifts, refs, False).ravel()
+    got = dense.cpu().numpy()
+    assert got[0] == pytest.approx(want[0], rel=1e-3)
+    assert want[0] < 1e-5 * np.median(want)
+    assert rel_l2(got, want) <= 1e-5
