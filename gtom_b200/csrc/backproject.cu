@@ -80,9 +80,8 @@ backproject_direct_kernel(float2* __restrict__ volft_base, float* __restrict__ v
   for (int k = 0; k < kBpPerThread; k++) {
     int64_t id = (int64_t)tile * kBpTile + k * kBpThreads + threadIdx.x;
     if (id >= a.elements) break;
-    int idx = (int)(id % a.dimft);
-    int idy = (int)((NDIMS == 3 ? id % a.area : id) / a.dimft);
-    int idz = NDIMS == 3 ? (int)(id / a.area) : 0;
+    int idx, idy, idz;
+    split_index(id, a.dimft, NDIMS == 3 ? a.area : a.elements, a.elements, idx, idy, idz);
     int x = idx;
     int y = idy <= half ? idy : idy - a.n;
     int z = NDIMS == 3 ? (idz <= half ? idz : idz - a.n) : 0;
@@ -555,9 +554,8 @@ backproject_shifted_kernel(float2* __restrict__ volft, float* __restrict__ volw,
   for (int k = 0; k < kBpPerThread; k++) {
     int64_t id = (int64_t)tile * kBpTile + k * kBpThreads + threadIdx.x;
     if (id >= a.elements) break;
-    int idx = (int)(id % a.dimft);
-    int idy = (int)((NDIMS == 3 ? id % a.area : id) / a.dimft);
-    int idz = NDIMS == 3 ? (int)(id / a.area) : 0;
+    int idx, idy, idz;
+    split_index(id, a.dimft, NDIMS == 3 ? a.area : a.elements, a.elements, idx, idy, idz);
     int x = idx;
     int y = idy <= rmax ? idy : idy - a.n;
     int z = NDIMS == 3 ? (idz <= rmax ? idz : idz - a.n) : 0;

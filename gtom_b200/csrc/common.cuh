@@ -119,6 +119,25 @@ __device__ __forceinline__ float lerpf(float a, float b, float t) { return fmaf(
 __device__ __forceinline__ float half_round(float v) { return __half2float(__float2half_rn(v)); }
 
 // Fire-and-forget FP32 reductions in L2 (no return value).
+// Splits a flat index into (x, row, plane) of rows of `row` elements and
+// planes of `plane` elements: 32-bit divisions when the index space stays
+// below 2^31 (every slice, volume and P grid in practice), 64-bit otherwise.
+__device__ __forceinline__ void split_index(int64_t id, int row, int64_t plane, int64_t total, int& x, int& y,
+                                            int& z) {
+  if (total < 0x7fffffffLL) {
+    const int i = (int)id, pl = (int)plane;
+    const int r = i % pl;
+    x = r % row;
+    y = r / row;
+    z = i / pl;
+  } else {
+    const int64_t r = id % plane;
+    x = (int)(r % row);
+    y = (int)(r / row);
+    z = (int)(id / plane);
+  }
+}
+
 __device__ __forceinline__ void red_add(float* p, float a) {
   asm volatile("red.relaxed.gpu.global.add.f32 [%0], %1;" ::"l"(p), "f"(a) : "memory");
 }

@@ -49,10 +49,8 @@ __global__ void grid_init_kernel(const float* __restrict__ weight, int oldx, int
   convft += b * g.nc;
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.nc) return;
-  int x = (int)(i % g.rowlen);
-  int64_t t = i / g.rowlen;
-  int y = (int)(t % g.P);
-  int z = (int)(t / g.P);
+  int x, y, z;
+  split_index(i, g.rowlen, (int64_t)g.rowlen * g.P, g.nc, x, y, z);
   int zp = z < g.P / 2 + 1 ? z : z - g.P;
   int yp = y < g.P / 2 + 1 ? y : y - g.P;
   float r = (float)(zp * zp) + (float)(yp * yp);
@@ -257,10 +255,8 @@ __global__ void grid_final_kernel(const float2* __restrict__ data, int oldx, int
   convft += b * g.nc;
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.nc) return;
-  int x = (int)(i % g.rowlen);
-  int64_t t = i / g.rowlen;
-  int y = (int)(t % g.P);
-  int z = (int)(t / g.P);
+  int x, y, z;
+  split_index(i, g.rowlen, (int64_t)g.rowlen * g.P, g.nc, x, y, z);
   int zp = z < g.P / 2 + 1 ? z : z - g.P;
   int yp = y < g.P / 2 + 1 ? y : y - g.P;
   float r = (float)(zp * zp) + (float)(yp * yp);

@@ -98,9 +98,8 @@ __device__ __forceinline__ void project_direct_tile(const Fetch& fetch, float2* 
   for (int k = 0; k < kProjPerThread; k++) {
     int64_t id = (int64_t)tile * kProjTile + k * kProjThreads + threadIdx.x;
     if (id >= a.elements) break;
-    int idx = (int)(id % a.dimft);
-    int idy = (int)((NDIMS == 3 ? id % a.area : id) / a.dimft);
-    int idz = NDIMS == 3 ? (int)(id / a.area) : 0;
+    int idx, idy, idz;
+    split_index(id, a.dimft, NDIMS == 3 ? a.area : a.elements, a.elements, idx, idy, idz);
     int x = idx;
     int y = idy <= half ? idy : idy - a.n;
     int z = idz <= half ? idz : idz - a.n;
