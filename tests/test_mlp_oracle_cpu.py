@@ -118,3 +118,29 @@ def test_momentum_reaches_the_plain_fixed_point():
     mom, ch_mom = M.gridding_iterations(fw, start, P, 2, 150, momentum=0.9)
     assert dist(mom, plain_ref) < 0.1 * dist(plain, plain_ref)
     assert ch_mom[-1] < ch_plain[-1]
+
+
+def test_warm_start_summary_of_the_converged_criterion():
+    """gtom_b200.warmstart.summarise: medians per mode, and the speed-up to
+    the converged weights taken only over distributions where both the mode
+    and the plain run reached the criterion (a run that did not is counted
+    in `reached`, not timed)."""
+    from gtom_b200 import warmstart as W
+
+    def mode(it, ms, conv_it, conv_ms, reached=True):
+        return {"iterations": it, "ms": ms, "distance_to_converged": 0.01, "fsc_min_to_plain": 1.0,
+                "fsc_min_to_converged": 0.99, "warm_used": True,
+                "to_converged": {"iterations": conv_it, "distance": 1e-4 if reached else 3e-4,
+                                 "reached": reached, **({"ms": conv_ms} if reached else {})}}
+
+    rows = [{"plain": mode(300, 100.0, 3000, 1000.0), "momentum": mode(90, 30.0, 300, 100.0)},
+            {"plain": mode(280, 90.0, 3400, 1200.0), "momentum": mode(80, 30.0, 320, 80.0)},
+            {"plain": mode(290, 95.0, 8000, None, reached=False), "momentum": mode(85, 30.0, 310, 90.0)}]
+    out = W.summarise(rows)
+    assert out["plain"]["to_converged"]["reached"] == 2 and out["plain"]["to_converged"]["of"] == 3
+    assert out["momentum"]["to_converged"]["reached"] == 3
+    assert out["momentum"]["to_converged"]["iterations"] == 310
+    # speed-ups over the two rows where plain reached it: 10x and 15x
+    assert out["momentum"]["to_converged"]["speedup_vs_plain"] == pytest.approx(12.5)
+    assert out["plain"]["to_converged"]["speedup_vs_plain"] == pytest.approx(1.0)
+    assert out["momentum"]["speedup_vs_plain"] == pytest.approx(np.median([100 / 30, 90 / 30, 95 / 30]))
