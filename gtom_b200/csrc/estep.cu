@@ -145,11 +145,16 @@ diff2_dense_tiled_kernel(const float2* __restrict__ particle, const float* __res
   const float2* pp = particle + elements * part;
   const float* cp = ctf ? ctf + elements * part : nullptr;
   float acc[4][4], nn[4];
+  // (x, y) partial sums per output as packed pairs, added at the end
+  unsigned long long acc2[4][4];
 #pragma unroll
   for (int a = 0; a < 4; a++) {
     nn[a] = 0.f;
 #pragma unroll
-    for (int b = 0; b < 4; b++) acc[a][b] = 0.f;
+    for (int b = 0; b < 4; b++) {
+      acc[a][b] = 0.f;
+      acc2[a][b] = 0ull;
+    }
   }
   for (int64_t i0 = 0; i0 < elements; i0 += kDK) {
     const int64_t gi = i0 + li;
@@ -189,16 +194,31 @@ diff2_dense_tiled_kernel(const float2* __restrict__ particle, const float* __res
 #pragma unroll
         for (int y = 0; y < 4; y++) {
           if (CC) {
-            acc[x][y] = fmaf(a[x].x, b[y].x, fmaf(a[x].y, b[y].y, acc[x][y]));
+            // (sx, sy) += (a.x b.x, a.y b.y): one packed FMA
+            const unsigned long long av = *reinterpret_cast<const unsigned long long*>(&a[x]);
+            const unsigned long long bv = *reinterpret_cast<const unsigned long long*>(&b[y]);
+            asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc2[x][y]) : "l"(av), "l"(bv));
           } else {
-            const float dx = a[x].x - b[y].x, dy = a[x].y - b[y].y;
-            acc[x][y] = fmaf(dx, dx, fmaf(dy, dy, acc[x][y]));
+            // (dx, dy) = a - b and (sx, sy) += (dx^2, dy^2) as one packed
+            // subtraction and one packed FMA (two issue slots, IEEE per lane)
+            const unsigned long long av = *reinterpret_cast<const unsigned long long*>(&a[x]);
+            const unsigned long long bv = *reinterpret_cast<const unsigned long long*>(&b[y]);
+            unsigned long long d;
+            asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(av), "l"(bv));
+            asm("fma.rn.f32x2 %0, %1, %1, %0;" : "+l"(acc2[x][y]) : "l"(d));
           }
         }
       }
     }
     __syncthreads();
   }
+#pragma unroll
+  for (int x = 0; x < 4; x++)
+#pragma unroll
+    for (int y = 0; y < 4; y++) {
+      const float2 v = *reinterpret_cast<const float2*>(&acc2[x][y]);
+      acc[x][y] = v.x + v.y;
+    }
 #pragma unroll
   for (int x = 0; x < 4; x++) {
     const unsigned r = r0 + tr + 16 * x;
