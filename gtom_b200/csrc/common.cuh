@@ -116,6 +116,21 @@ __device__ __forceinline__ float3 mat_apply(const float* m, float x, float y, fl
 // lerp of cutil_math_bugfixes.cuh:212: fma(b - a, t, a).
 __device__ __forceinline__ float lerpf(float a, float b, float t) { return fmaf(b - a, t, a); }
 
+// lerpf on both components of a complex pair at once: one packed
+// subtraction and one packed FMA (sub.rn / fma.rn per lane, so each
+// component equals lerpf's bit for bit) in two issue slots instead of four.
+__device__ __forceinline__ float2 lerp2(float2 a, float2 b, float t) {
+  unsigned long long av, bv, tv, d, r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(av) : "f"(a.x), "f"(a.y));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(bv) : "f"(b.x), "f"(b.y));
+  asm("mov.b64 %0, {%1, %1};" : "=l"(tv) : "f"(t));
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(bv), "l"(av));
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(d), "l"(tv), "l"(av));
+  float2 out;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(out.x), "=f"(out.y) : "l"(r));
+  return out;
+}
+
 __device__ __forceinline__ float half_round(float v) { return __half2float(__float2half_rn(v)); }
 
 // Fire-and-forget FP32 reductions in L2 (no return value).

@@ -40,13 +40,12 @@ __device__ __forceinline__ ProjSample project_sample(const float* m, int x, int 
 __device__ __forceinline__ float2 trilerp(const ProjSample& s, float2 d000, float2 d001, float2 d010,
                                           float2 d011, float2 d100, float2 d101, float2 d110,
                                           float2 d111) {
-  float rx00 = lerpf(d000.x, d001.x, s.fx), ix00 = lerpf(d000.y, d001.y, s.fx);
-  float rx01 = lerpf(d010.x, d011.x, s.fx), ix01 = lerpf(d010.y, d011.y, s.fx);
-  float rx10 = lerpf(d100.x, d101.x, s.fx), ix10 = lerpf(d100.y, d101.y, s.fx);
-  float rx11 = lerpf(d110.x, d111.x, s.fx), ix11 = lerpf(d110.y, d111.y, s.fx);
-  float rxy0 = lerpf(rx00, rx01, s.fy), ixy0 = lerpf(ix00, ix01, s.fy);
-  float rxy1 = lerpf(rx10, rx11, s.fy), ixy1 = lerpf(ix10, ix11, s.fy);
-  return make_float2(lerpf(rxy0, rxy1, s.fz), lerpf(ixy0, ixy1, s.fz) * s.sign);
+  // each lerp2 is lerpf on the real and the imaginary part
+  const float2 x00 = lerp2(d000, d001, s.fx), x01 = lerp2(d010, d011, s.fx);
+  const float2 x10 = lerp2(d100, d101, s.fx), x11 = lerp2(d110, d111, s.fx);
+  const float2 xy0 = lerp2(x00, x01, s.fy), xy1 = lerp2(x10, x11, s.fy);
+  const float2 v = lerp2(xy0, xy1, s.fz);
+  return make_float2(v.x, v.y * s.sign);
 }
 
 // Backprojector (src/Relion/Backproject.cu:194-238): base neighbour of the
