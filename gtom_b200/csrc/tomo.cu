@@ -25,10 +25,19 @@ namespace {
 constexpr float kTomoReach = 5.f;   // the reference's per-axis window and plane distance
 constexpr float kTomoReachDiag = 8.6602540378f;  // 5 * sqrt(3): reach along any direction
 
+// The reference is built with fast math (-use_fast_math; FastMath in its
+// Release configuration): its sine is the fast sine and its FP32 division the
+// full-range approximate one, div.full.f32, used here as well.
+__device__ __forceinline__ float fast_div(float a, float b) {
+  float r;
+  asm("div.full.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+  return r;
+}
+
 __device__ __forceinline__ float tomo_sinc(float x) {  // DeviceFunctions.cuh:11-17
   if (fabsf(x) <= 1e-4f) return 1.f;
   const float pi = 3.14159265358979323846f;
-  return __sinf(x * pi) / (x * pi);
+  return fast_div(__sinf(x * pi), x * pi);
 }
 
 // glm mat3 * vec3 and transpose(mat3) * vec3, column-major m[c*3 + r].
@@ -85,8 +94,9 @@ __global__ void tomo_kernel(float2* __restrict__ vol, int vx, int vy, int vz, co
             }
             const float dx = px - pos.x, dy = py - pos.y, dz = pz - pos.z;
             if (fabsf(dx) > kTomoReach || fabsf(dy) > kTomoReach || fabsf(dz) > kTomoReach) continue;
-            const float sample = tomo_sinc(dx) * tomo_sinc(dx / kTomoReach) * (tomo_sinc(dy) * tomo_sinc(dy / kTomoReach)) *
-                                 (tomo_sinc(dz) * tomo_sinc(dz / kTomoReach));
+            const float sample = tomo_sinc(dx) * tomo_sinc(fast_div(dx, kTomoReach)) *
+                                 (tomo_sinc(dy) * tomo_sinc(fast_div(dy, kTomoReach))) *
+                                 (tomo_sinc(dz) * tomo_sinc(fast_div(dz, kTomoReach)));
             const int64_t id = (int64_t)idy * dimft + x;
             ssum += sample;
             wsum += sample * __ldg(projw + elements * b + id);
