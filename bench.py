@@ -178,10 +178,55 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------- workload --
-def make_workload(args, device, seed):
+def synth_module():
+    """The seeded input generator (gtom_b200/synth.py: torch and numpy only)
+    loaded as a standalone module, so that the reference arm produces the
+    same inputs without importing the library's package."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("gtom_synth_standalone", ROOT / "gtom_b200" / "synth.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def bench_config(n, B, pool, P, D, world):
+    """The workload description both arms print (identical, so that the two
+    lines describe the same configuration)."""
+    return {"workload": "single-particle 256^3, padding 2: project + CTF-weighted backproject",
+            "box": n, "padding": PAD, "batch_per_step": B, "pool": pool,
+            "volume": f"{P // 2 + 1}x{P}x{P} c64 decentred",
+            "accumulators": f"{D // 2 + 1}x{D}x{D} c64 + f32 centred",
+            "l2_flush": "inputs larger than L2 (per-step data 3.96 GB)", "parallelism": f"dp{world}"}
+
+
+def make_workload(args, device, seed, impl="ours"):
+    """The bench's inputs on the GPU: the padded volume, a pool of particle
+    orientations (the reference's host matrix expression, bit for bit the
+    same in both arms), and CTF-weighted noisy particles with their CTF^2
+    weights.  The particles are projections of the volume, made by this
+    library (impl "ours") or by the reference's own projector (impl
+    "reference"), which agree bit for bit."""
     import torch
-    import gtom_b200 as G
-    from gtom_b200 import synth
+    if impl == "ours":
+        import gtom_b200 as G
+        from gtom_b200 import synth
+
+        def mats_of(ang):
+            return G.matrices_from_angles(ang, float(PAD))
+
+        def project(volft, proj, m, c):
+            G.d_rlnProject(volft, (P, P, P), proj, (n, n, 1), rmax, m, c)
+    else:
+        from oracle import refcuda
+        synth = synth_module()
+        ref = refcuda.lib()
+
+        def mats_of(ang):
+            return refcuda.matrices(ang, float(PAD))
+
+        def project(volft, proj, m, c):
+            refcuda.check(ref.ref_project(volft.data_ptr(), P, proj.data_ptr(), n, 2, rmax, m.data_ptr(), c),
+                          "reference d_rlnProject")
 
     n, P = BOX, BOX * PAD
     D = P + 1
@@ -189,11 +234,17 @@ def make_workload(args, device, seed):
     e, sp, sb = counts(n, rmax)
     rng = np.random.default_rng(seed)
     vol = synth.blob_volume(n, 2000, seed, device)
-    volft = synth.padded_half_ft(vol, PAD).reshape(-1)
+    ft = synth.padded_half_ft(vol, PAD).reshape(-1)
     del vol
+    # 64 spare zeros past the volume: the reference projector's x1 = P/2+1
+    # read can touch one element past the end (src/Relion/Project.cu:155)
+    vbuf = torch.zeros(ft.numel() + 64, dtype=torch.complex64, device=device)
+    vbuf[:ft.numel()] = ft
+    volft = vbuf[:ft.numel()]
+    del ft
     N = args.pool
     ang = synth.vmf_mixture_angles(rng, N)
-    mats = torch.from_numpy(G.matrices_from_angles(ang, float(PAD))).to(device)
+    mats = torch.from_numpy(mats_of(ang)).to(device)
     data = torch.empty((N, e), dtype=torch.complex64, device=device)
     wts = torch.empty((N, e), dtype=torch.float32, device=device)
     disk = synth.in_disk_mask(n, rmax, device).reshape(-1)
@@ -203,7 +254,7 @@ def make_workload(args, device, seed):
     proj = torch.empty((chunk, e), dtype=torch.complex64, device=device)
     for c0 in range(0, N, chunk):
         c = min(chunk, N - c0)
-        G.d_rlnProject(volft, (P, P, P), proj, (n, n, 1), rmax, mats[c0:c0 + c].reshape(-1), c)
+        project(volft, proj, mats[c0:c0 + c].reshape(-1), c)
         df = torch.from_numpy(rng.uniform(0.5, 3.0, c).astype(np.float32)).to(device)
         da = torch.from_numpy(rng.uniform(0.0, 0.1, c).astype(np.float32)).to(device)
         aa = torch.from_numpy(rng.uniform(0.0, np.pi, c).astype(np.float32)).to(device)
@@ -310,6 +361,8 @@ def run_ours(args):
                  "unit": "GB/s", "frac": round(proj_gbs / hbm_peak, 4),
                  "traffic": None if traffic.get("project_per_slice") is None
                  else int(traffic["project_per_slice"] * B),
+                 "traffic_source": "not measured in this run: ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                   "per slice from profiles/ncu_traffic.json, times the batch",
                  "algorithmic_bytes": proj_bytes, "ms_per_launch": round(proj_ms, 4),
                  "peak_of": peak_kind,
                  "l2_gather_peak_gbs": probe.get("l2_gather_gbs"),
@@ -325,6 +378,8 @@ def run_ours(args):
                "frac": None if not smem_peak else round(bp_rate / smem_peak, 4),
                "traffic": None if traffic.get("backproject_per_slice") is None
                else int(traffic["backproject_per_slice"] * B),
+               "traffic_source": "not measured in this run: ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                 "per slice from profiles/ncu_traffic.json, times the batch",
                "algorithmic_reductions": bp_reds, "ms_per_launch": round(bp_ms, 4),
                "peak_of": "measured (probe, same run)", "l2_red_peak": l2_peak,
                "frac_of_l2_red": None if not l2_peak else round(bp_rate / l2_peak, 4)}
@@ -342,11 +397,7 @@ def run_ours(args):
            "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded blob volume, vMF+uniform "
            "orientations, CTF, SNR 0.05 noise)",
-           "config": {"workload": "single-particle 256^3, padding 2: project + CTF-weighted backproject",
-                      "box": n, "padding": PAD, "batch_per_step": B, "pool": ws["N"],
-                      "volume": f"{P // 2 + 1}x{P}x{P} c64 decentred", "accumulators": f"{D // 2 + 1}x{D}x{D} "
-                      "c64 + f32 centred", "l2_flush": "inputs larger than L2 (per-step data 3.96 GB)",
-                      "parallelism": f"dp{world}"},
+           "config": bench_config(n, B, ws["N"], P, D, world),
            # per step with the default (row-segment) path: the projector launches
            # 6 kernels (plan: pairs with the zero fill, scan, fill, items; the
            # segment kernel; the direct fallback over its list) and the
@@ -369,6 +420,8 @@ def run_ours(args):
         out["extensions"] = time_extensions(args, G, torch, ws, acc_ft, acc_w, dev, hbm_peak, probe)
     if single and not args.no_extras and args.subtomos > 0:
         out["batched_uneven"] = time_batched(args, torch, dev)
+    if single and not args.no_extras:
+        out["small_config"] = small_config_ours(G, torch, dev)
     if not args.no_extras:
         if world > 1:
             dist.barrier()
@@ -392,6 +445,45 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def small_config_ours(G, torch, dev):
+    """Config 1 in full through this library: 64^3 blobs, padding 2, 1 000
+    uniform slices projected, inserted with unit CTF and weights, then the
+    10-iteration gridding reconstruction; device time per stage (CUDA
+    events, best of 5 after a warm-up)."""
+    from gtom_b200 import synth
+    n, vbuf, nv_in, mats = small_config_inputs(dev, synth, lambda a: G.matrices_from_angles(a, float(PAD)))
+    P, D, rmax, B = n * PAD, n * PAD + 1, n // 2, mats.shape[0]
+    volft = vbuf[:nv_in]
+    e = (n // 2 + 1) * n
+    nvol = (D // 2 + 1) * D * D
+    proj = torch.empty(B * e, dtype=torch.complex64, device=dev)
+    acc_ft = torch.zeros(nvol, dtype=torch.complex64, device=dev)
+    acc_w = torch.zeros(nvol, dtype=torch.float32, device=dev)
+    rec = torch.empty(n ** 3, dtype=torch.float32, device=dev)
+    m = mats.reshape(-1)
+    best = None
+    for rep in range(6):
+        acc_ft.zero_()
+        acc_w.zero_()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record()
+        G.d_rlnProject(volft, (P, P, P), proj, (n, n, 1), rmax, m, B)
+        ev[1].record()
+        G.d_rlnBackproject(acc_ft, acc_w, (D, D, D), proj, None, (n, n, 1), rmax, m, None, (1, 0, 0, 1), 0.0,
+                           False, False, B)
+        ev[2].record()
+        G.d_ReconstructGridding(acc_ft, acc_w, rec, (n,) * 3, (D,) * 3, PAD, 0, 0, 10)
+        ev[3].record()
+        torch.cuda.synchronize()
+        cur = [ev[i].elapsed_time(ev[i + 1]) for i in range(3)]
+        if rep > 0 and (best is None or sum(cur) < sum(best)):
+            best = cur
+    return {"workload": "64^3 blobs, padding 2, 1 000 uniform slices: project, backproject (unit CTF and "
+                        "weights), 10-iteration gridding",
+            "ms": {"project": round(best[0], 4), "backproject": round(best[1], 4), "gridding": round(best[2], 4),
+                   "total": round(sum(best), 4)}}
 
 
 def time_gridding(G, torch, acc_ft, acc_w, n, D, dev):
@@ -844,6 +936,16 @@ def cpu_baseline(args, ws):
 
 # ---------------------------------------------------------------- reference --
 def run_reference(args):
+    """The reference arm: the reference's kernels on this box, on the same
+    workload as the GPU arm (same seeded inputs, same batch per step, same
+    config).  The reference ships no CPU implementation of this path
+    (RELION's liblion is not vendored), so `value` is the OpenMP FP32
+    restatement of its projector and backprojector kernels on all host
+    cores; the reference's own CUDA kernels, rebuilt from its sources, are
+    timed beside it (`reference_cuda`), with its gridding reconstruction and
+    the small configuration (64^3, 1 000 slices) in full.  Nothing of the
+    library under test is loaded: the inputs come from the same seeded
+    generator, the particles from the reference's own projector."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -852,57 +954,61 @@ def run_reference(args):
     from oracle import oracle as O
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
+    B = args.batch
     a2 = argparse.Namespace(**vars(args))
-    a2.pool = max(args.cpu_sample, args.batch)
-    ws = make_workload(a2, dev, SEED)
-    count = args.cpu_sample
-    vol, data, wts, mats = cpu_sample_inputs(ws, count)
-    n, P, D, rmax = ws["n"], ws["P"], ws["D"], ws["rmax"]
-    for _ in range(min(args.warmup, 1)):
-        time_cpu_port(vol, data[:16], wts[:16], mats[:16], n, P, D, rmax)
-    t0 = time.perf_counter()
-    per = []
-    for _ in range(args.steps):
+    if a2.pool % B:
+        a2.pool = (a2.pool // B + 1) * B
+    ws = make_workload(a2, dev, SEED, impl="reference")
+    n, P, D, rmax, N = ws["n"], ws["P"], ws["D"], ws["rmax"], ws["N"]
+    vol = ws["volft"].cpu().numpy()
+
+    def batch_of(i, count):
+        s0 = (i * B) % N
+        return (ws["data"][s0:s0 + count].cpu().numpy(), ws["wts"][s0:s0 + count].cpu().numpy(),
+                ws["mats"][s0:s0 + count].cpu().numpy())
+
+    warm = min(B, 500)
+    for i in range(args.warmup):  # untimed: page-in and thread start-up on a 500-slice sample
+        time_cpu_port(vol, *batch_of(i, warm), n, P, D, rmax)
+    el = 0.0
+    for k in range(args.steps):  # each step: the full batch, host copies outside the timing
+        d, w, m = batch_of(args.warmup + k, B)
         t = time.perf_counter()
-        time_cpu_port(vol, data, wts, mats, n, P, D, rmax)
-        per.append(time.perf_counter() - t)
-    el = time.perf_counter() - t0
-    value = args.steps * count / el
+        time_cpu_port(vol, d, w, m, n, P, D, rmax)
+        el += time.perf_counter() - t
+    value = args.steps * B / el
     out = {"impl": "reference", "metric": "project+backproject slices/s @256^3", "value": round(value, 2),
            "unit": "slices/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(el / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": "single-particle 256^3, padding 2: project + CTF-weighted backproject",
-                      "box": n, "padding": PAD, "batch_per_step": count, "parallelism": "host cores"},
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded blob volume, vMF+uniform "
+           "orientations, CTF, SNR 0.05 noise)",
+           "config": bench_config(n, B, N, P, D, world),
            "cpu_baseline": {"value": round(value, 2), "unit": "slices/s", "cores": O.num_threads(),
                             "kind": "port",
-                            "sample": f"{count} slices per step; the reference ships no CPU path for this "
-                                      "(liblion is not vendored), so the OpenMP FP32 restatement of its "
-                                      "kernels runs"},
+                            "sample": f"{B} slices per step (the whole batch; warm-up steps on {warm}); the "
+                                      "reference ships no CPU path for this (liblion is not vendored), so "
+                                      "the OpenMP FP32 restatement of its kernels runs"},
            "e2e": {"value": round(value, 2), "unit": "slices/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     rc = reference_cuda(args, ws, dev)
     if rc is not None:
         out["reference_cuda"] = rc
+        out["small_config"] = small_config_reference(dev)
     print(json.dumps(out), flush=True)
 
 
 def reference_cuda(args, ws, dev):
     """Times the reference's own CUDA kernels (rebuilt from its sources for
-    sm_100a into oracle/_ref/) on the same workload, for the GPU-to-GPU ratio."""
-    import ctypes as C
+    sm_100a into oracle/_ref/) on the same workload: d_rlnProject and
+    d_rlnBackproject of one batch, then d_ReconstructGridding (10
+    iterations, P = 512) of the accumulated volume."""
     import torch
-    from oracle import oracle as O
-    if not O.REF_PATH.exists():
+    from oracle import refcuda
+    if not refcuda.available():
         return None
-    ref = C.CDLL(str(O.REF_PATH))
-    p, i, f = C.c_void_p, C.c_int, C.c_float
-    ref.ref_project.argtypes = [p, i, p, i, i, i, p, i]
-    ref.ref_backproject.argtypes = [p, p, i, p, p, i, i, i, p, p, f, f, f, f, f, i, i, i]
+    ref = refcuda.lib()
     n, P, D, rmax, e = ws["n"], ws["P"], ws["D"], ws["rmax"], ws["e"]
     B = min(args.batch, ws["N"])
-    vol = torch.zeros(ws["volft"].numel() + 64, dtype=torch.complex64, device=dev)
-    vol[: ws["volft"].numel()] = ws["volft"]
     proj = torch.empty(B * e, dtype=torch.complex64, device=dev)
     nvol = (D // 2 + 1) * D * D
     acc_ft = torch.zeros(nvol, dtype=torch.complex64, device=dev)
@@ -910,28 +1016,129 @@ def reference_cuda(args, ws, dev):
     m = ws["mats"][:B].contiguous()
     t = []
     for rep in range(3):
+        acc_ft.zero_()
+        acc_w.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        rc1 = ref.ref_project(vol.data_ptr(), P, proj.data_ptr(), n, 2, rmax, m.data_ptr(), B)
+        refcuda.check(ref.ref_project(ws["volft"].data_ptr(), P, proj.data_ptr(), n, 2, rmax, m.data_ptr(), B),
+                      "reference d_rlnProject")
         t1 = time.perf_counter()
-        rc2 = ref.ref_backproject(acc_ft.data_ptr(), acc_w.data_ptr(), D, ws["data"].data_ptr(),
-                                  ws["wts"].data_ptr(), n, 2, rmax, m.data_ptr(), None, 1, 0, 0, 1, 0.0, 0, 0, B)
+        refcuda.check(ref.ref_backproject(acc_ft.data_ptr(), acc_w.data_ptr(), D, ws["data"].data_ptr(),
+                                          ws["wts"].data_ptr(), n, 2, rmax, m.data_ptr(), None, 1, 0, 0, 1, 0.0,
+                                          0, 0, B), "reference d_rlnBackproject")
         t2 = time.perf_counter()
-        if rc1 or rc2:
-            return {"error": f"reference CUDA returned {rc1}, {rc2}"}
         t.append((t1 - t0, t2 - t1))
     tp = min(x[0] for x in t)
     tb = min(x[1] for x in t)
+    rec = torch.empty(n ** 3, dtype=torch.float32, device=dev)
+    tg = []
+    for rep in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        refcuda.check(ref.ref_reconstruct_gridding(acc_ft.data_ptr(), acc_w.data_ptr(), rec.data_ptr(), n, D, PAD,
+                                                   10, 1.9, 0, 15.0), "reference d_ReconstructGridding")
+        tg.append(time.perf_counter() - t0)
     return {"value": round(B / (tp + tb), 1), "unit": "slices/s", "batch": B,
             "project_ms": round(tp * 1e3, 3), "backproject_ms": round(tb * 1e3, 3),
-            "how": "reference d_rlnProject / d_rlnBackproject (matrix overloads) rebuilt from source for "
-                   "sm_100a with its own flags; each call synchronises (as the reference does)"}
+            "gridding_10it_ms": round(min(tg) * 1e3, 3),
+            "how": "reference d_rlnProject / d_rlnBackproject (matrix overloads) and d_ReconstructGridding "
+                   "(10 iterations, P = 512, its own cuFFT plans per call) rebuilt from source for sm_100a "
+                   "with its own flags; each call synchronises (as the reference does); best of 3 / 2"}
+
+
+SMALL_BOX = 64
+
+
+def small_config_inputs(dev, synth, mats_of):
+    """The small plain configuration: a 64^3 volume of 200 Gaussian blobs
+    (sigma U(1.5, 4) voxels, amplitude U(0.2, 1), centres within radius 28),
+    padding 2, 1 000 slices at uniform SO(3) orientations."""
+    import torch
+    n = SMALL_BOX
+    rng = np.random.default_rng(1001)
+    vol = synth.blob_volume(n, 200, 1001, dev, radius_frac=28.0 / n)
+    ft = synth.padded_half_ft(vol, PAD).reshape(-1)
+    vbuf = torch.zeros(ft.numel() + 64, dtype=torch.complex64, device=dev)
+    vbuf[:ft.numel()] = ft
+    ang = synth.vmf_mixture_angles(rng, 1000, uniform_frac=1.0)
+    mats = torch.from_numpy(mats_of(ang)).to(dev)
+    return n, vbuf, ft.numel(), mats
+
+
+def small_config_reference(dev):
+    """Config 1 in full through the reference: its CUDA kernels (project,
+    backproject with unit CTF and weights, 10-iteration gridding) and the CPU
+    port (projector and backprojector restated, gridding in the FP64 numpy
+    restatement) on the host cores."""
+    import torch
+    from oracle import oracle as O
+    from oracle import refcuda
+    ref = refcuda.lib()
+    n, vbuf, nv_in, mats = small_config_inputs(dev, synth_module(), lambda a: refcuda.matrices(a, float(PAD)))
+    P, D, rmax, B = n * PAD, n * PAD + 1, n // 2, mats.shape[0]
+    e = (n // 2 + 1) * n
+    nvol = (D // 2 + 1) * D * D
+    proj = torch.empty(B * e, dtype=torch.complex64, device=dev)
+    acc_ft = torch.zeros(nvol, dtype=torch.complex64, device=dev)
+    acc_w = torch.zeros(nvol, dtype=torch.float32, device=dev)
+    rec = torch.empty(n ** 3, dtype=torch.float32, device=dev)
+    best = None
+    for rep in range(3):
+        acc_ft.zero_()
+        acc_w.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        refcuda.check(ref.ref_project(vbuf.data_ptr(), P, proj.data_ptr(), n, 2, rmax, mats.data_ptr(), B), "project")
+        t1 = time.perf_counter()
+        refcuda.check(ref.ref_backproject(acc_ft.data_ptr(), acc_w.data_ptr(), D, proj.data_ptr(), None, n, 2, rmax,
+                                          mats.data_ptr(), None, 1, 0, 0, 1, 0.0, 0, 0, B), "backproject")
+        t2 = time.perf_counter()
+        refcuda.check(ref.ref_reconstruct_gridding(acc_ft.data_ptr(), acc_w.data_ptr(), rec.data_ptr(), n, D, PAD,
+                                                   10, 1.9, 0, 15.0), "gridding")
+        t3 = time.perf_counter()
+        cur = (t1 - t0, t2 - t1, t3 - t2)
+        best = cur if best is None or sum(cur) < sum(best) else best
+    vol = vbuf[:nv_in].cpu().numpy()
+    m = mats.cpu().numpy()
+    t0 = time.perf_counter()
+    p = O.project(vol, P, n, rmax, m, fp32=True)
+    t1 = time.perf_counter()
+    vf, vw = np.zeros(nvol, np.complex64), np.zeros(nvol, np.float32)
+    O.backproject(vf, vw, D, p, None, n, rmax, m, decentered=False, fp32=True)
+    t2 = time.perf_counter()
+    O.reconstruct_gridding(vf.reshape(D, D, D // 2 + 1), vw.reshape(D, D, D // 2 + 1), n, (D, D, D), PAD)
+    t3 = time.perf_counter()
+    return {"workload": "64^3 blobs, padding 2, 1 000 uniform slices: project, backproject (unit CTF and "
+                        "weights), 10-iteration gridding",
+            "reference_cuda_ms": {"project": round(best[0] * 1e3, 3), "backproject": round(best[1] * 1e3, 3),
+                                  "gridding": round(best[2] * 1e3, 3), "total": round(sum(best) * 1e3, 3)},
+            "cpu_port_ms": {"project": round((t1 - t0) * 1e3, 1), "backproject": round((t2 - t1) * 1e3, 1),
+                            "gridding_fp64_numpy": round((t3 - t2) * 1e3, 1), "total": round((t3 - t0) * 1e3, 1),
+                            "cores": O.num_threads()}}
+
+
+PROBE_SRC = ROOT / "bench_probe" / "l2_probe.cu"
+PROBE_LIB = ROOT / "bench_probe" / "libbench_probe.so"
+
+
+def build_probe() -> Path:
+    """Compiles the roofline microbenchmarks (bench_probe/l2_probe.cu, bench
+    only: the product library neither contains nor loads them) for sm_100a
+    when the library is missing or older than its source."""
+    import subprocess
+    if not PROBE_LIB.exists() or PROBE_LIB.stat().st_mtime < PROBE_SRC.stat().st_mtime:
+        cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+        nvcc = str(Path(cuda) / "bin" / "nvcc") if (Path(cuda) / "bin" / "nvcc").exists() else "nvcc"
+        subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+                        "-Xcompiler", "-fPIC", "-shared", "-o", str(PROBE_LIB), str(PROBE_SRC)], check=True)
+    return PROBE_LIB
 
 
 def l2_probe():
     import ctypes as C
-    path = ROOT / "gtom_b200" / "lib" / "libgtomrln_probe.so"
-    if not path.exists():
+    try:
+        path = build_probe()
+    except Exception:
         return {}
     L = C.CDLL(str(path))
     L.gtomrln_probe_l2_red.restype = C.c_double

@@ -6,8 +6,8 @@
 //     buffer, the access pattern of the projector's corner fetches,
 //   * shared-memory update rates (FP32 / int32 / int64 atomics, plain
 //     read-add-write) and the CUDA cores' FP32 FMA rate.
-// Built into a separate library (gtom_b200/lib/libgtomrln_probe.so); the
-// product library does not contain it.
+// Bench-only: bench.py builds it into bench_probe/libbench_probe.so; the
+// product library (gtom_b200/) neither contains nor loads it.
 #include <cuda_runtime.h>
 #include <cstdint>
 

@@ -22,7 +22,6 @@ CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIBDIR = PKG / "lib"
 LIB = LIBDIR / "libgtomrln.so"
-PROBE_LIB = LIBDIR / "libgtomrln_probe.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
@@ -75,10 +74,6 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     objs = [OBJ / (s.stem + ".o") for s in srcs]
     if force or jobs or _stale(LIB, objs):
         _run([nvcc, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcufft"], verbose)
-    # Roofline probes (L2 reduction / gather rates) live in their own library.
-    probe_srcs = sorted((CSRC / "probe").glob("*.cu"))
-    if probe_srcs and (force or _stale(PROBE_LIB, probe_srcs)):
-        _run([nvcc, *ARCH, *NVFLAGS, "-shared", "-o", str(PROBE_LIB), *map(str, probe_srcs)], verbose)
     return LIB
 
 

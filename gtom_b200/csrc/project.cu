@@ -10,7 +10,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
-#include <mutex>
 #include <type_traits>
 
 #include "brick.cuh"
@@ -460,25 +459,20 @@ constexpr unsigned kNoAllocMaxBatch = 4096;
 static __device__ __align__(256) float g_noalloc_matrices[kNoAllocMaxBatch * 9];
 
 // In host code g_noalloc_matrices is only a host-side stand-in; the device
-// address comes from cudaGetSymbolAddress, looked up once per device with
-// that device current.
-static std::mutex g_noalloc_mutex;
-static float* g_noalloc_ptr[64] = {};
-
+// address comes from cudaGetSymbolAddress with the calling device current.
+// It is looked up on every call rather than cached: the lookup is cheap once
+// the module is loaded, and a cached address would go stale if the caller
+// reset the device (cudaDeviceReset) and the module were loaded again
+// elsewhere.
 static int noalloc_matrices(float** out) {
-  int dev = 0;
-  GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return set_error(GTOMRLN_ERR_INVALID, "device index %d out of range", dev);
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_matrices);
-    if (e != cudaSuccess)
-      return set_error(GTOMRLN_ERR_CUDA, "cudaGetSymbolAddress of the fixed matrix array failed: %s",
-                       cudaGetErrorString(e));
-    g_noalloc_ptr[dev] = (float*)p;
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_matrices);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(GTOMRLN_ERR_CUDA, "cudaGetSymbolAddress of the fixed matrix array failed: %s",
+                     cudaGetErrorString(e));
   }
-  *out = g_noalloc_ptr[dev];
+  *out = (float*)p;
   return GTOMRLN_OK;
 }
 
@@ -507,16 +501,20 @@ int gtomrln_project_angles_noalloc(const float* d_volumeft, int vx, int vy, int 
   float* d_mats = nullptr;
   st = noalloc_matrices(&d_mats);
   if (st) return st;
-  // Host staging without allocation: a fixed per-thread buffer.
+  // Host side without allocation: the matrices are built in a fixed
+  // per-thread buffer and carried to the array as kernel parameters (at most
+  // 4096 * 9 floats, five launches), so the upload holds no reference to
+  // host memory after this call returns and no copy engine is involved.
   static thread_local float h_mats[kNoAllocMaxBatch * 9];
   matrices_from_angles(h_angles, supersample, batch, h_mats);
   cudaStream_t s = (cudaStream_t)stream;
   // Every matrix the kernel reads is rewritten here, so nothing left from an
-  // earlier call needs clearing.  The copy is ordered on `s` after earlier
+  // earlier call needs clearing.  The upload is ordered on `s` after earlier
   // work on `s`; calls on different streams that overlap on the GPU race for
-  // the shared array.
-  GTOMRLN_CUDA_TRY(cudaMemcpyAsync(d_mats, h_mats, sizeof(float) * 9 * (size_t)batch,
-                                   cudaMemcpyHostToDevice, s));
+  // the shared array.  The projection always takes the direct kernel: the
+  // brick kernels need plan scratch, which this entry point does not allocate.
+  st = upload_via_params(d_mats, h_mats, 9 * (size_t)batch, s);
+  if (st) return st;
   ArrayFetch f{(const float2*)d_volumeft, a.P, a.P / 2 + 1, a.nvox - 1};
   return launch_project(f, ndp, d_proj, d_mats, a, batch, s);
 }

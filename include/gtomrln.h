@@ -142,10 +142,14 @@ GTOMRLN_API int gtomrln_project_tex(unsigned long long t_volumeRe, unsigned long
  * instead and allocates nothing.  Limit: batch <= 4096 slices per call
  * (larger batches return GTOMRLN_ERR_INVALID; split them).  The array costs
  * every device that loads the library 147,456 bytes until the process exits.
- * The first call on a device looks up the array's device address; make it
- * before any stream capture.  All calls share the one array: calls ordered
- * on one stream are safe, calls on different streams that overlap on the
- * GPU race.  Results equal gtomrln_project_angles's. */
+ * Each call looks up the array's device address (on the first call on a
+ * device this loads the library's device code); make the first call on a
+ * device before any stream capture.  The matrices travel to the array as
+ * kernel parameters, and the projection always runs the direct kernel (the
+ * brick kernels would need plan scratch).  All calls share the one array,
+ * which keeps the last call's matrices: calls ordered on one stream are
+ * safe, calls on different streams that overlap on the GPU race.  Results
+ * equal gtomrln_project_angles's. */
 GTOMRLN_API int gtomrln_project_angles_noalloc(const float* d_volumeft, int vx, int vy, int vz,
                                    float* d_proj, int px, int py, int pz, const float* h_angles,
                                    float supersample, unsigned batch, void* stream);

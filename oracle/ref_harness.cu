@@ -18,6 +18,17 @@ using namespace gtom;
 
 extern "C" {
 
+// The host matrices of the h_angles overloads (src/Relion/Project.cu:14-16,
+// src/Relion/Backproject.cu:29-31): the same expression, column-major glm
+// layout, 9 floats per slice.
+int ref_matrices(float* h_angles, float supersample, int batch, float* h_matrices) {
+  for (int i = 0; i < batch; i++) {
+    glm::mat3 m = glm::transpose(Matrix3Euler(((tfloat3*)h_angles)[i])) * Matrix3Scale(supersample);
+    memcpy(h_matrices + 9 * (size_t)i, &m, sizeof(glm::mat3));
+  }
+  return 0;
+}
+
 // include/Relion.cuh:35 -> src/Relion/Project.cu:25-43
 int ref_project(float* d_volumeft, int P, float* d_proj, int n, int ndims, int rmax,
                 float* d_matrices, int batch) {

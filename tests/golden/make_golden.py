@@ -15,7 +15,6 @@ that the fixtures keep.
 """
 from __future__ import annotations
 
-import ctypes as C
 import sys
 from pathlib import Path
 
@@ -26,31 +25,11 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from oracle import oracle as O  # noqa: E402
+from oracle import refcuda  # noqa: E402
 from tests.synthdata import blob_volume_ft, random_angles  # noqa: E402
 
-REF = C.CDLL(str(O.REF_PATH))
-_p, _i, _f, _d = C.c_void_p, C.c_int, C.c_float, C.c_double
-REF.ref_project.argtypes = [_p, _i, _p, _i, _i, _i, _p, _i]
-REF.ref_project_angles.argtypes = [_p, _i, _p, _i, _i, _p, _f, _i]
-REF.ref_backproject.argtypes = [_p, _p, _i, _p, _p, _i, _i, _i, _p, _p, _f, _f, _f, _f, _f, _i, _i, _i]
-REF.ref_backproject_angles.argtypes = [_p, _p, _i, _p, _p, _i, _i, _i, _p, _p, _f, _f, _f, _f, _f,
-                                       _f, _i, _i, _i]
-REF.ref_reconstruct_gridding.argtypes = [_p, _p, _p, _i, _i, _i, _i, _d, _i, _d]
-REF.ref_project_shifted.argtypes = [_p, _i, _p, _i, _i, _i, _p, _p, _p, _i]
-REF.ref_backproject_shifted.argtypes = [_p, _p, _i, _p, _p, _i, _i, _i, _p, _p, _p, _i]
-REF.ref_ctf_simulate.argtypes = [_p, _p, _p, _p, _i, _i, _i, _i]
-REF.ref_convert_weights_dense.argtypes = [_p, _i, _i, _i, _i, _p, _p, _p]
-REF.ref_backproject_tomo.argtypes = [_p, _i, _p, _p, _i, _i, _p, _i]
-REF.ref_convert_weights_sparse.argtypes = [_p, _p, _p, _i, _i, _i, _p, _p, _p]
-REF.ref_diff_remap_dense.argtypes = [_p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _p, _p, _i]
-REF.ref_diff_remap_sparse.argtypes = [_p, _p, _p, _p, _p, _i, _i, _i, _i, _p, _p, _i]
-REF.ref_create_minvsigma2s.argtypes = [_p, _p, _i, _p, _f]
-REF.ref_store_weights_add.argtypes = [_p, _p, _p, _p, _p, _i, _i, _p, _f, _f, _p, _p, _p, _p, _p, _p, _p, _i]
-
-
-def _ok(rc: int, what: str) -> None:
-    if rc != 0:
-        raise RuntimeError(f"{what}: CUDA error {rc}")
+REF = refcuda.lib()
+_ok = refcuda.check
 
 
 def dev(a: np.ndarray, extra: int = 0) -> torch.Tensor:

@@ -24,7 +24,8 @@ def fsc(a: np.ndarray, b: np.ndarray, nshells: int | None = None) -> np.ndarray:
     """Fourier shell correlation of two real cubes, one value per integer shell
     up to Nyquist."""
     n = a.shape[0]
-    fa, fb = np.fft.rfftn(a), np.fft.rfftn(b)
+    # float64 throughout: the shell sums of |F|^2 of large maps overflow float32
+    fa, fb = np.fft.rfftn(np.asarray(a, np.float64)), np.fft.rfftn(np.asarray(b, np.float64))
     k = np.fft.fftfreq(n) * n
     kx = np.arange(n // 2 + 1)
     r = np.sqrt(k[:, None, None] ** 2 + k[None, :, None] ** 2 + kx[None, None, :] ** 2)
