@@ -47,29 +47,82 @@ void matrices_from_angles(const float* angles, float s, unsigned batch, float* o
   }
 }
 
-// One pool per device.  Freed scratch stays mapped in the pool (no release
-// threshold) so that repeated calls reuse it instead of remapping gigabytes
-// each time; gtomrln_release_caches() returns it to the device.
-static std::mutex g_pool_mutex;
-static std::vector<cudaMemPool_t> g_pools;
+// The context id through the driver's cuCtxGetCurrent / cuCtxGetId, looked
+// up once through the runtime (no link against the driver library).
+namespace {
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
+std::once_flag g_ctx_once;
+CtxGetCurrentFn g_ctx_current = nullptr;
+CtxGetIdFn g_ctx_id = nullptr;
+}  // namespace
+
+unsigned long long context_id() {
+  std::call_once(g_ctx_once, [] {
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void**)&g_ctx_current, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      g_ctx_current = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", (void**)&g_ctx_id, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      g_ctx_id = nullptr;
+    cudaGetLastError();
+  });
+  if (!g_ctx_current || !g_ctx_id) return 0;
+  void* ctx = nullptr;
+  if (g_ctx_current(&ctx) != 0 || !ctx) {
+    // no context current yet (or it was destroyed): the runtime creates the
+    // device's primary context and makes it current
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaSetDevice(dev) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    if (g_ctx_current(&ctx) != 0 || !ctx) return 0;
+  }
+  unsigned long long id = 0;
+  return g_ctx_id(ctx, &id) == 0 ? id : 0;
+}
+
+// One pool per device and context.  Freed scratch stays mapped in the pool
+// (no release threshold) so that repeated calls reuse it instead of
+// remapping gigabytes each time; gtomrln_release_caches() returns it to the
+// device and destroys the pool.
+namespace {
+struct PoolEntry {
+  int dev;
+  unsigned long long ctx;
+  cudaMemPool_t pool;
+};
+std::mutex g_pool_mutex;
+std::vector<PoolEntry> g_pools;
+}  // namespace
 
 static int get_pool(cudaMemPool_t* out) {
   int dev = 0;
   GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long ctx = context_id();
   std::lock_guard<std::mutex> lock(g_pool_mutex);
-  if ((int)g_pools.size() <= dev) g_pools.resize(dev + 1, nullptr);
-  if (!g_pools[dev]) {
-    cudaMemPoolProps props = {};
-    props.allocType = cudaMemAllocationTypePinned;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = dev;
-    cudaMemPool_t pool;
-    GTOMRLN_CUDA_TRY(cudaMemPoolCreate(&pool, &props));
-    uint64_t threshold = UINT64_MAX;
-    GTOMRLN_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
-    g_pools[dev] = pool;
+  for (size_t i = 0; i < g_pools.size(); i++) {
+    if (g_pools[i].dev != dev) continue;
+    if (g_pools[i].ctx == ctx) {
+      *out = g_pools[i].pool;
+      return GTOMRLN_OK;
+    }
+    // made in a context that no longer exists: its memory went with it
+    g_pools.erase(g_pools.begin() + i);
+    break;
   }
-  *out = g_pools[dev];
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool;
+  GTOMRLN_CUDA_TRY(cudaMemPoolCreate(&pool, &props));
+  uint64_t threshold = UINT64_MAX;
+  GTOMRLN_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+  g_pools.push_back({dev, ctx, pool});
+  *out = pool;
   return GTOMRLN_OK;
 }
 
@@ -107,6 +160,7 @@ int pool_free(void* ptr, cudaStream_t stream) {
 namespace {
 struct ScratchSlot {
   int dev;
+  unsigned long long ctx;
   cudaStream_t stream;
   void* ptr;
   size_t bytes;
@@ -126,14 +180,19 @@ int scratch_alloc(void** ptr, size_t bytes, cudaStream_t stream) {
   if (cs != cudaStreamCaptureStatusNone) return pool_alloc(ptr, bytes, stream);
   int dev = 0;
   GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long ctx = context_id();
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  // slots of this device made in an earlier context are gone with it
+  g_scratch.erase(std::remove_if(g_scratch.begin(), g_scratch.end(),
+                                 [&](const ScratchSlot& s) { return s.dev == dev && s.ctx != ctx; }),
+                  g_scratch.end());
   ScratchSlot* slot = nullptr;
   for (auto& s : g_scratch)
     if (s.dev == dev && s.stream == stream) slot = &s;
   if (!slot) {
     cudaEvent_t ev;
     GTOMRLN_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    g_scratch.push_back({dev, stream, nullptr, 0, false, ev});
+    g_scratch.push_back({dev, ctx, stream, nullptr, 0, false, ev});
     slot = &g_scratch.back();
   }
   if (slot->busy) return pool_alloc(ptr, bytes, stream);
@@ -183,6 +242,7 @@ namespace {
 constexpr int kStageSlots = 8;
 struct StageSlot {
   int dev;
+  unsigned long long ctx;
   void* ptr;
   size_t cap;
   cudaEvent_t done;
@@ -196,18 +256,30 @@ unsigned g_stage_turn = 0;
 int stage_acquire(size_t bytes, void** ptr, int* slot) {
   int dev = 0;
   GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long ctx = context_id();
   StageSlot* s = nullptr;
   int idx = -1;
   {
     std::lock_guard<std::mutex> lock(g_stage_mutex);
     std::vector<int> mine;
-    for (int i = 0; i < (int)g_stage.size(); i++)
-      if (g_stage[i].dev == dev) mine.push_back(i);
+    for (int i = 0; i < (int)g_stage.size(); i++) {
+      StageSlot& t = g_stage[i];
+      if (t.dev != dev) continue;
+      if (t.ctx != ctx) {
+        // made in a context that no longer exists (its pinned memory and
+        // event went with it): retire the slot for good
+        t.dev = -1;
+        t.ptr = nullptr;
+        t.cap = 0;
+        continue;
+      }
+      mine.push_back(i);
+    }
     if (mine.empty()) {
       for (int k = 0; k < kStageSlots; k++) {
         cudaEvent_t ev;
         GTOMRLN_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        g_stage.push_back({dev, nullptr, 0, ev, false});
+        g_stage.push_back({dev, ctx, nullptr, 0, ev, false});
         mine.push_back((int)g_stage.size() - 1);
       }
     }
@@ -282,27 +354,30 @@ int upload_via_params(float* dst, const float* src, size_t count, cudaStream_t s
   return GTOMRLN_OK;
 }
 
-// Frees the idle staging slots' pinned memory on device dev (after a device
-// synchronisation); the slots and their events stay.
-static void release_stage(int dev) {
+// Frees the idle staging slots' pinned memory of the current context on
+// device dev (after a device synchronisation); the slots and their events
+// stay.
+static void release_stage(int dev, unsigned long long ctx) {
   std::lock_guard<std::mutex> lock(g_stage_mutex);
   for (auto& s : g_stage)
-    if (s.dev == dev && !s.busy && s.ptr) {
+    if (s.dev == dev && s.ctx == ctx && !s.busy && s.ptr) {
       cudaFreeHost(s.ptr);
       s.ptr = nullptr;
       s.cap = 0;
     }
 }
 
-// Frees the idle scratch slots of device dev (after a device synchronisation).
-static int release_scratch(int dev) {
+// Frees the idle scratch slots of the current context on device dev (after
+// a device synchronisation) and forgets those of earlier contexts.
+static int release_scratch(int dev, unsigned long long ctx) {
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
   std::vector<ScratchSlot> keep;
   for (auto& s : g_scratch) {
-    if (s.dev != dev || s.busy) {
+    if (s.dev != dev || (s.ctx == ctx && s.busy)) {
       keep.push_back(s);
       continue;
     }
+    if (s.ctx != ctx) continue;  // gone with its context
     if (s.ptr) {
       GTOMRLN_CUDA_TRY(cudaFreeAsync(s.ptr, 0));
       GTOMRLN_CUDA_TRY(cudaStreamSynchronize(0));
@@ -313,12 +388,45 @@ static int release_scratch(int dev) {
   return GTOMRLN_OK;
 }
 
-int release_gridding_plans();  // gridding.cu
-int release_ctf_plans();       // ctf.cu
+// Trims and destroys the memory pool of the current context on device dev,
+// and forgets pools of earlier contexts there.
+static int release_pool(int dev, unsigned long long ctx) {
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  std::vector<PoolEntry> keep;
+  int st = GTOMRLN_OK;
+  for (auto& p : g_pools) {
+    if (p.dev != dev) {
+      keep.push_back(p);
+      continue;
+    }
+    if (p.ctx != ctx) continue;
+    cudaError_t e = cudaMemPoolTrimTo(p.pool, 0);
+    if (e == cudaSuccess) e = cudaMemPoolDestroy(p.pool);
+    if (e != cudaSuccess && !st) st = set_error(GTOMRLN_ERR_CUDA, "memory pool release: %s", cudaGetErrorString(e));
+  }
+  g_pools.swap(keep);
+  return st;
+}
+
+int release_gridding_caches(int dev, unsigned long long ctx);  // gridding.cu
+int release_ctf_plans(int dev, unsigned long long ctx);        // ctf.cu
+int release_brick_orders(int dev, unsigned long long ctx);     // brick_plan.cu
+int release_gridfft_tables(int dev, unsigned long long ctx);   // gridfft.cu
 
 static std::atomic<int> g_path[3] = {{GTOMRLN_PATH_AUTO}, {GTOMRLN_PATH_AUTO}, {GTOMRLN_PATH_AUTO}};
 
 int path_choice(int op) { return (op >= 0 && op <= 2) ? g_path[op].load() : GTOMRLN_PATH_AUTO; }
+
+// Crossovers measured at padding 2 (direct vs row-segment, ms):
+// backprojector  n = 128: 1 000 slices 0.48 vs 0.76, 3 000: 1.40 vs 1.97,
+//                10 000: 4.56 vs 3.23; n = 192: 300 slices 0.64 vs 0.52;
+//                n = 96, 10 000: 2.65 vs 2.97;
+// projector      n = 192: 3 000 slices 0.86 vs 1.05, 10 000: 2.99 vs 2.08;
+//                n = 256: 300 slices 0.26 vs 0.50, 1 000: 0.83 vs 0.72.
+bool brick_path_pays(int op, int V, unsigned batch) {
+  if (op == GTOMRLN_OP_BACKPROJECT) return (V >= 384 && batch >= 300) || (V >= 256 && batch >= 6000);
+  return (V >= 512 && batch >= 1000) || (V >= 384 && batch >= 6000);
+}
 
 // Defaults measured on the B200 at 256^3 (padding 2) with 10,000-slice
 // batches (row-segment variants; the largest bricks whose shared memory fits
@@ -343,19 +451,19 @@ int gtomrln_version(void) { return 100; }
 const char* gtomrln_last_error(void) { return g_last_error.c_str(); }
 
 int gtomrln_release_caches(void) {
-  int st = release_gridding_plans();
-  if (st) return st;
-  st = release_ctf_plans();
-  if (st) return st;
+  clear_error();
   int dev = 0;
   GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long ctx = context_id();
   GTOMRLN_CUDA_TRY(cudaDeviceSynchronize());
-  st = release_scratch(dev);
+  int st = release_gridding_caches(dev, ctx);
+  if (!st) st = release_ctf_plans(dev, ctx);
+  if (!st) st = release_brick_orders(dev, ctx);
+  if (!st) st = release_gridfft_tables(dev, ctx);
+  if (!st) st = release_scratch(dev, ctx);
   if (st) return st;
-  release_stage(dev);
-  std::lock_guard<std::mutex> lock(g_pool_mutex);
-  if ((int)g_pools.size() > dev && g_pools[dev]) GTOMRLN_CUDA_TRY(cudaMemPoolTrimTo(g_pools[dev], 0));
-  return GTOMRLN_OK;
+  release_stage(dev, ctx);
+  return release_pool(dev, ctx);
 }
 
 int gtomrln_set_path(int op, int path) {

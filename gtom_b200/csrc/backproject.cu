@@ -156,7 +156,6 @@ backproject_direct_kernel(float2* __restrict__ volft_base, float* __restrict__ v
 // the brick's only one and the voxel has no alias (decentred y or z = +-V/2
 // share storage), otherwise with vector L2 reductions.
 // ---------------------------------------------------------------------------
-constexpr unsigned kBrickMinBatch = 32;
 
 // Adds a brick's shared-memory accumulators to the volume: plain
 // read-add-write when the work item is the brick's only one and the voxel has
@@ -804,7 +803,7 @@ static int backproject_launch(float* d_volumeft, float* d_volumeweights, int vx,
   if (ndp == 2 && vx == vy && vx == vz && vx >= 4 && !d_ivolume && mag.x == 1.f && mag.y == 0.f &&
       mag.z == 0.f && mag.w == 1.f && a.ewalddiaminv == 0.f && (d_volumeft || d_volumeweights) &&
       (choice == GTOMRLN_PATH_BRICK || choice == GTOMRLN_PATH_SEGMENT ||
-       (choice == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch)))
+       (choice == GTOMRLN_PATH_AUTO && brick_path_pays(GTOMRLN_OP_BACKPROJECT, vx, batch))))
     return backproject_brick(d_volumeft, d_volumeweights, d_projft, d_projweights, d_matrices, a, (int)rmax,
                              decentered, square, batch, stream, choice == GTOMRLN_PATH_BRICK ? 0 : 1);
 
@@ -899,7 +898,7 @@ int gtomrln_backproject_shifted(float* d_volumeft, float* d_volumeweights, int v
   const int choice = path_choice(GTOMRLN_OP_BACKPROJECT);
   if (ndp == 2 && vx == vy && vx == vz && vx >= 4 && (d_volumeft || d_volumeweights) &&
       (choice == GTOMRLN_PATH_BRICK || choice == GTOMRLN_PATH_SEGMENT ||
-       (choice == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch)))
+       (choice == GTOMRLN_PATH_AUTO && brick_path_pays(GTOMRLN_OP_BACKPROJECT, vx, batch))))
     return backproject_shifted_brick(d_volumeft, d_volumeweights, d_projft, d_projweights, d_matrices, d_shifts,
                                      d_globalweights, a, (int)rmax, batch, (cudaStream_t)stream);
   dim3 grid((unsigned)(a.tiles * (int64_t)batch));

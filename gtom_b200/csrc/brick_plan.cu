@@ -406,14 +406,30 @@ __global__ void plan_items_kernel(const int* __restrict__ counts, const int* __r
     items[item_off[b] + k] = {b, offsets[b] + k * chunk, min(chunk, c - k * chunk), nch == 1 ? 1 : 0};
 }
 
-// Brick visiting order per grid, cached on each device.
+// Brick visiting order per grid, cached per device and context.
 static std::mutex g_order_mutex;
-static std::map<std::tuple<int, int, int, int, int, int>, int*> g_orders;
+static std::map<std::tuple<int, unsigned long long, int, int, int, int, int>, int*> g_orders;
+
+// Frees the orders of the current context on device dev and forgets those of
+// earlier contexts there (gone with their context).
+int release_brick_orders(int dev, unsigned long long ctx) {
+  std::lock_guard<std::mutex> lock(g_order_mutex);
+  for (auto it = g_orders.begin(); it != g_orders.end();) {
+    if (std::get<0>(it->first) != dev) {
+      ++it;
+      continue;
+    }
+    if (std::get<1>(it->first) == ctx) cudaFree(it->second);
+    it = g_orders.erase(it);
+  }
+  return GTOMRLN_OK;
+}
 
 static int brick_order(const BrickGrid& g, const int** out) {
   int dev = 0;
   GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
-  auto key = std::make_tuple(dev, g.V, g.B, g.nbx, g.nby, g.ylo);
+  const unsigned long long ctx = context_id();
+  auto key = std::make_tuple(dev, ctx, g.V, g.B, g.nbx, g.nby, g.ylo);
   std::lock_guard<std::mutex> lock(g_order_mutex);
   auto it = g_orders.find(key);
   if (it != g_orders.end()) {

@@ -47,12 +47,28 @@ void matrices_from_angles(const float* angles, float supersample, unsigned batch
 // Implementation chosen for op (GTOMRLN_OP_*) by gtomrln_set_path.
 int path_choice(int op);
 
+// Whether GTOMRLN_PATH_AUTO takes the brick-major (row-segment) kernels for
+// op on a cubic volume of edge V and a batch of 2D slices: they win once the
+// volume no longer fits in L2 and the batch amortises their plan, while the
+// direct kernels, whose gathers and reductions then stay in L2, win on
+// smaller volumes.  Thresholds from a B200 sweep of boxes 32-256 (V = 2n
+// or 2n + 1) and batches 100-10 000 (abi.cu).
+bool brick_path_pays(int op, int V, unsigned batch);
+
 // Launch shape of the brick kernels for op: brick edge in voxels, threads
 // per CTA, and the most slices one work item takes (gtomrln_set_brick_tuning).
 struct BrickTuning {
   int edge, threads, chunk;
 };
 BrickTuning brick_tuning(int op);
+
+// Unique id of the calling thread's current CUDA context (the device's
+// primary context, made current if no context is), 0 if it cannot be
+// determined.  The library's per-device caches (memory pool, scratch and
+// staging slots, FFT plans, tables) are keyed on it, so that nothing made in
+// a context that the caller has since destroyed (cudaDeviceReset) is used
+// again: a new context never shares an id with an earlier one.
+unsigned long long context_id();
 
 // Stream-ordered device scratch from the library's memory pool.
 int pool_alloc(void** ptr, size_t bytes, cudaStream_t stream);

@@ -137,20 +137,30 @@ preprocess_kernel(float2* __restrict__ ft, float* __restrict__ weights, int n, i
 }
 
 static std::mutex g_ctf_mutex;
-static std::map<std::tuple<int, int, unsigned>, cufftHandle> g_r2c_plans;  // (device, n, batch)
+// (device, context, n, batch)
+static std::map<std::tuple<int, unsigned long long, int, unsigned>, cufftHandle> g_r2c_plans;
 
-int release_ctf_plans() {
+// Destroys the plans of the current context on device dev and forgets those
+// of earlier contexts there (gone with their context).
+int release_ctf_plans(int dev, unsigned long long ctx) {
   std::lock_guard<std::mutex> lock(g_ctf_mutex);
-  for (auto& kv : g_r2c_plans) cufftDestroy(kv.second);
-  g_r2c_plans.clear();
+  for (auto it = g_r2c_plans.begin(); it != g_r2c_plans.end();) {
+    if (std::get<0>(it->first) != dev) {
+      ++it;
+      continue;
+    }
+    if (std::get<1>(it->first) == ctx) cufftDestroy(it->second);
+    it = g_r2c_plans.erase(it);
+  }
   return GTOMRLN_OK;
 }
 
 static int r2c_plan(int n, unsigned batch, cufftHandle* out) {
   int dev = 0;
   GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long ctx = context_id();
   std::lock_guard<std::mutex> lock(g_ctf_mutex);
-  auto key = std::make_tuple(dev, n, batch);
+  auto key = std::make_tuple(dev, ctx, n, batch);
   auto it = g_r2c_plans.find(key);
   if (it != g_r2c_plans.end()) {
     *out = it->second;

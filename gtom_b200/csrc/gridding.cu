@@ -316,13 +316,14 @@ struct PlanPair {
   cufftHandle r2c = 0, c2r = 0;
 };
 static std::mutex g_plan_mutex;
-static std::map<std::pair<int, int>, PlanPair> g_plans;  // (device, P)
+static std::map<std::tuple<int, unsigned long long, int>, PlanPair> g_plans;  // (device, context, P)
 
 static int get_plans(int P, PlanPair* out) {
   int dev = 0;
   GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long ctx = context_id();
   std::lock_guard<std::mutex> lock(g_plan_mutex);
-  auto it = g_plans.find({dev, P});
+  auto it = g_plans.find(std::make_tuple(dev, ctx, P));
   if (it != g_plans.end()) {
     *out = it->second;
     return GTOMRLN_OK;
@@ -335,24 +336,44 @@ static int get_plans(int P, PlanPair* out) {
     cufftDestroy(pp.r2c);
     return set_error(GTOMRLN_ERR_CUFFT, "cufftPlan3d C2R %d^3 failed (%d)", P, (int)r);
   }
-  g_plans[{dev, P}] = pp;
+  g_plans[std::make_tuple(dev, ctx, P)] = pp;
   *out = pp;
   return GTOMRLN_OK;
 }
 
-int release_gridding_plans() {
-  std::lock_guard<std::mutex> lock(g_plan_mutex);
-  for (auto& kv : g_plans) {
-    cufftDestroy(kv.second.r2c);
-    cufftDestroy(kv.second.c2r);
+
+// Blob tables are cached per (device, context, radius, alpha, order).
+static std::mutex g_table_mutex;
+static std::map<std::tuple<int, unsigned long long, double, double, int>, float*> g_tables;
+
+// Destroys the plans and frees the tables of the current context on device
+// dev, and forgets those of earlier contexts there (gone with their context).
+int release_gridding_caches(int dev, unsigned long long ctx) {
+  {
+    std::lock_guard<std::mutex> lock(g_plan_mutex);
+    for (auto it = g_plans.begin(); it != g_plans.end();) {
+      if (std::get<0>(it->first) != dev) {
+        ++it;
+        continue;
+      }
+      if (std::get<1>(it->first) == ctx) {
+        cufftDestroy(it->second.r2c);
+        cufftDestroy(it->second.c2r);
+      }
+      it = g_plans.erase(it);
+    }
   }
-  g_plans.clear();
+  std::lock_guard<std::mutex> lock(g_table_mutex);
+  for (auto it = g_tables.begin(); it != g_tables.end();) {
+    if (std::get<0>(it->first) != dev) {
+      ++it;
+      continue;
+    }
+    if (std::get<1>(it->first) == ctx) cudaFree(it->second);
+    it = g_tables.erase(it);
+  }
   return GTOMRLN_OK;
 }
-
-// Blob tables are cached per (device, radius, alpha, order).
-static std::mutex g_table_mutex;
-static std::map<std::tuple<int, double, double, int>, float*> g_tables;
 
 int build_blob_table(double radius, double alpha, int order, int nsamples, float* out) {
   if (order != 0 && order != 2)
@@ -369,8 +390,9 @@ int build_blob_table(double radius, double alpha, int order, int nsamples, float
 static int get_table(double radius, double alpha, int order, const float** out) {
   int dev = 0;
   GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long ctx = context_id();
   std::lock_guard<std::mutex> lock(g_table_mutex);
-  auto key = std::make_tuple(dev, radius, alpha, order);
+  auto key = std::make_tuple(dev, ctx, radius, alpha, order);
   auto it = g_tables.find(key);
   if (it != g_tables.end()) {
     *out = it->second;

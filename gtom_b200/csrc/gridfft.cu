@@ -55,15 +55,17 @@ namespace {
 constexpr int kColsPerCta = 16;  // x columns per CTA (z pass) and per cluster rank (plane pass)
 constexpr int kRowsPerCta = 32;  // y rows per cluster rank in the plane pass
 
-// Twiddle table exp(-2 pi i m / N), m < N, per (device, N), built in double.
+// Twiddle table exp(-2 pi i m / N), m < N, per (device, context, N), built
+// in double.
 std::mutex g_tw_mutex;
-std::map<std::pair<int, int>, float2*> g_tw;
+std::map<std::tuple<int, unsigned long long, int>, float2*> g_tw;
 
 int twiddles(int N, const float2** out) {
   int dev = 0;
   GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long ctx = context_id();
   std::lock_guard<std::mutex> lock(g_tw_mutex);
-  auto key = std::make_pair(dev, N);
+  auto key = std::make_tuple(dev, ctx, N);
   auto it = g_tw.find(key);
   if (it != g_tw.end()) {
     *out = it->second;
@@ -80,6 +82,21 @@ int twiddles(int N, const float2** out) {
   GTOMRLN_CUDA_TRY(cudaMemcpy(d, h.data(), sizeof(float2) * N, cudaMemcpyHostToDevice));
   g_tw[key] = d;
   *out = d;
+  return GTOMRLN_OK;
+}
+
+// Frees the twiddle tables of the current context on device dev and
+// forgets those of earlier contexts there (gone with their context).
+int release_tables(int dev, unsigned long long ctx) {
+  std::lock_guard<std::mutex> lock(g_tw_mutex);
+  for (auto it = g_tw.begin(); it != g_tw.end();) {
+    if (std::get<0>(it->first) != dev) {
+      ++it;
+      continue;
+    }
+    if (std::get<1>(it->first) == ctx) cudaFree(it->second);
+    it = g_tw.erase(it);
+  }
   return GTOMRLN_OK;
 }
 
@@ -467,14 +484,15 @@ cudaLaunchConfig_t xy_config(int count, cudaStream_t stream, cudaLaunchAttribute
 template <int N>
 bool xy_fits() {
   static std::mutex m;
-  static std::map<int, bool> cache;
+  static std::map<std::pair<int, unsigned long long>, bool> cache;  // (device, context)
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
+  const auto key = std::make_pair(dev, context_id());
   std::lock_guard<std::mutex> lock(m);
-  auto it = cache.find(dev);
+  auto it = cache.find(key);
   if (it != cache.end()) return it->second;
   bool ok = false;
   const int zs = (int)z_smem<N>();
@@ -493,7 +511,7 @@ bool xy_fits() {
          twiddles(N, &tw) == GTOMRLN_OK;
   }
   cudaGetLastError();
-  cache[dev] = ok;
+  cache[key] = ok;
   return ok;
 }
 
@@ -565,5 +583,9 @@ int gridfft_iteration(float2* data, const GridGeom& g, int count, const float* t
     default: return set_error(GTOMRLN_ERR_INVALID, "fused gridding: grid %d not supported", g.P);
   }
 }
+
+// Frees the fused transforms' tables of the current context on device dev
+// (gtomrln_release_caches).
+int release_gridfft_tables(int dev, unsigned long long ctx) { return release_tables(dev, ctx); }
 
 }  // namespace gtomrln

@@ -340,7 +340,6 @@ __global__ void project_zero_kernel(float2* __restrict__ proj, ProjArgs a, int64
   }
 }
 
-constexpr unsigned kBrickMinBatch = 32;
 
 // The brick path: plan, zero fill outside rmax, brick kernel, and the direct
 // kernel for any slice the plan could not take.  Nothing synchronises.  A
@@ -531,7 +530,7 @@ int gtomrln_project(const float* d_volumeft, int vx, int vy, int vz, float* d_pr
   const int choice = path_choice(GTOMRLN_OP_PROJECT);
   if (ndp == 2 && vx == vy && vx == vz && vx >= 4 &&
       (choice == GTOMRLN_PATH_BRICK || choice == GTOMRLN_PATH_SEGMENT ||
-       (choice == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch)))
+       (choice == GTOMRLN_PATH_AUTO && brick_path_pays(GTOMRLN_OP_PROJECT, vx, batch))))
     return project_brick(d_volumeft, d_proj, d_matrices, a, batch, (cudaStream_t)stream,
                          choice == GTOMRLN_PATH_BRICK ? 0 : 1);
   ArrayFetch f{(const float2*)d_volumeft, a.P, a.P / 2 + 1, a.nvox - 1};
@@ -591,7 +590,7 @@ int gtomrln_project_shifted(const float* d_volumeft, int vx, int vy, int vz, flo
   const int choice = path_choice(GTOMRLN_OP_PROJECT);
   if (ndp == 2 && vx == vy && vx == vz && vx >= 4 &&
       (choice == GTOMRLN_PATH_BRICK || choice == GTOMRLN_PATH_SEGMENT ||
-       (choice == GTOMRLN_PATH_AUTO && batch >= kBrickMinBatch)))
+       (choice == GTOMRLN_PATH_AUTO && brick_path_pays(GTOMRLN_OP_PROJECT, vx, batch))))
     return project_brick(d_volumeft, d_proj, d_matrices, a, batch, (cudaStream_t)stream, 1,
                          ShiftPost{d_shifts, d_globalweights});
   ArrayFetch f{(const float2*)d_volumeft, a.P, a.P / 2 + 1, a.nvox - 1};

@@ -65,8 +65,10 @@ GTOMRLN_API int gtomrln_release_caches(void);
 /* Extension (no reference counterpart): choose the implementation of an
  * operation for the calling process.  op: GTOMRLN_OP_PROJECT or
  * GTOMRLN_OP_BACKPROJECT; path: GTOMRLN_PATH_AUTO (default: brick-major with
- * row segments for batches of 32 or more 2D slices whose geometry allows
- * it, else direct),
+ * row segments for 2D slices whose geometry allows it, once the volume is
+ * too large for L2 and the batch amortises the plan — backprojector: edge
+ * >= 384 and >= 300 slices, or edge >= 256 and >= 6 000; projector: edge
+ * >= 512 and >= 1 000, or edge >= 384 and >= 6 000 — else direct),
  * GTOMRLN_PATH_DIRECT (one thread per slice element, global gathers /
  * reductions), GTOMRLN_PATH_BRICK (brick-major, shared-memory staging, pixels
  * binned per brick by a planning pass; falls back to direct where the
