@@ -74,6 +74,11 @@ def parse_args():
                     help="slices timed on the host cores (about 10 s of work on 16 threads)")
     ap.add_argument("--subtomos", type=int, default=512,
                     help="sub-tomograms of the batched uneven-box workload (0 skips it)")
+    ap.add_argument("--config5", action="store_true",
+                    help="instead of the bench: the large combined configuration (400^3, padding 2, "
+                         "2 half-maps x 4 classes) end to end on one GPU")
+    ap.add_argument("--c5-particles", type=int, default=1000000)
+    ap.add_argument("--c5-chunk", type=int, default=5000)
     return ap.parse_args()
 
 
@@ -598,6 +603,25 @@ def time_extensions(args, G, torch, ws, acc_ft, acc_w, dev, hbm_peak, probe):
                                   "g_reductions_per_s": round(reds / (ms * 1e-3) / 1e9, 1),
                                   "frac_of_smem_atomic": None if not sm else round(reds / (ms * 1e-3) / 1e9 / sm, 4),
                                   "frac_of_l2_red_v2": None if not l2 else round(reds / (ms * 1e-3) / 1e9 / l2, 4)}
+    # the general insertion (Backproject.cu:57-63, 145-152, 183-189): a 1.2 %
+    # anisotropic magnification, the Ewald curvature of 300 kV electrons at
+    # 1 A/pixel (sphere radius n / 0.0197 pixels, supersampled by 2) and two
+    # target volumes (half-maps) chosen per particle, against the plain
+    # insertion of the same particles into one volume
+    iv = torch.from_numpy(rng.integers(0, 2, B).astype(np.int32)).to(dev)
+    nvox = (D // 2 + 1) * D * D
+    g_ft = torch.zeros(2 * nvox, dtype=torch.complex64, device=dev)
+    g_w = torch.zeros(2 * nvox, dtype=torch.float32, device=dev)
+    data, wts = ws["data"][:B].reshape(-1), ws["wts"][:B].reshape(-1)
+    ms_plain = timed(lambda: G.d_rlnBackproject(acc_ft, acc_w, (D, D, D), data, wts, (n, n, 1), rmax, m, None,
+                                                (1, 0, 0, 1), 0.0, False, False, B))
+    ms_gen = timed(lambda: G.d_rlnBackproject(g_ft, g_w, (D, D, D), data, wts, (n, n, 1), rmax, m, iv,
+                                              (1.012, 0.004, -0.006, 0.993), 2.0 * n / 0.0197, False, False, B))
+    res["backproject_general"] = {"slices_per_s": round(B / (ms_gen * 1e-3), 1), "ms": round(ms_gen, 3),
+                                  "plain_ms": round(ms_plain, 3), "ratio_to_plain": round(ms_gen / ms_plain, 3),
+                                  "geometry": "magnification (1.012, 0.004, -0.006, 0.993), Ewald radius "
+                                              f"{2.0 * n / 0.0197:.0f} px, 2 volumes by d_ivolume"}
+    del g_ft, g_w
     imgs = torch.randn((B, n, n), device=dev)
     params = [dict(defocus=-float(d) * 1e-6) for d in rng.uniform(0.5, 3.0, B)]
     from gtom_b200.ctf import ctf_params
@@ -1217,10 +1241,143 @@ def run_sweep(args):
     print(json.dumps({"sweep": out, "path": args.path, "batch": B, "box": n, "padding": PAD}), flush=True)
 
 
+def run_config5(args):
+    """The large combined configuration on one B200: a 400^3 FP32 blob
+    volume per class (2 000 Gaussians each), padding 2 (complex64
+    401 x 800 x 800 per class), and 1 000 000 400 x 400 particles split into
+    2 half-maps x 4 classes of 40 / 30 / 20 / 10 %, with CTFs and noise as
+    in the single-particle workload (SNR 0.05).  The particles are generated
+    on the GPU in chunks (projected from their class, CTF, noise; 965 GB in
+    all, never resident at once) and every chunk is inserted into the eight
+    centred 801^3 accumulators with one backprojection call whose d_ivolume
+    selects the volume (2 class + half) per particle, the row-segment kernel
+    with one work item per (volume, brick).  Then each of the eight volumes
+    is reconstructed with the gridding correction from the learned warm
+    start and the momentum update to a relative change of 1e-4 (P = 800,
+    cuFFT transforms).  Reported: insertion slices/s (device time of the
+    insertion calls alone), generation time, per-volume gridding time and
+    iterations, the 10-iteration plain gridding at P = 800 for scale, and
+    the device memory in use at its peak against the GPU's total."""
+    import torch
+    import gtom_b200 as G
+    from gtom_b200 import synth
+    from gtom_b200 import warmstart as WS
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    n, P, D = 400, 800, 801
+    rmax, e = n // 2, (n // 2 + 1) * n
+    nvox = (D // 2 + 1) * D * D
+    fracs = np.array([0.4, 0.3, 0.2, 0.1])
+    total, chunk = args.c5_particles, args.c5_chunk
+    rng = np.random.default_rng(1005)
+    peak = [0]
+
+    def note_memory():
+        free, tot = torch.cuda.mem_get_info()
+        peak[0] = max(peak[0], tot - free)
+        return tot
+
+    t0 = time.perf_counter()
+    vols = []
+    for c in range(4):
+        v = synth.blob_volume(n, 2000, 2000 + c, dev)
+        vols.append(synth.padded_half_ft(v, PAD).reshape(-1))
+        del v
+        torch.cuda.empty_cache()
+    torch.cuda.synchronize()
+    t_vols = time.perf_counter() - t0
+    acc_ft = torch.zeros(8 * nvox, dtype=torch.complex64, device=dev)
+    acc_w = torch.zeros(8 * nvox, dtype=torch.float32, device=dev)
+    proj = torch.empty((chunk, e), dtype=torch.complex64, device=dev)
+    disk = synth.in_disk_mask(n, rmax, dev).reshape(-1)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1005)
+    ev = []
+    per_volume = np.zeros(8, np.int64)
+    t0 = time.perf_counter()
+    for c0 in range(0, total, chunk):
+        cnt = min(chunk, total - c0)
+        counts = rng.multinomial(cnt, fracs)
+        cls = np.repeat(np.arange(4), counts)
+        ivol = (2 * cls + rng.integers(0, 2, cnt)).astype(np.int32)
+        np.add.at(per_volume, ivol, 1)
+        mats = torch.from_numpy(G.matrices_from_angles(synth.vmf_mixture_angles(rng, cnt), float(PAD))).to(dev)
+        s0 = 0
+        for c in range(4):
+            k = int(counts[c])
+            if k:
+                G.d_rlnProject(vols[c], (P, P, P), proj[s0:s0 + k].reshape(-1), (n, n, 1), rmax,
+                               mats[s0:s0 + k].reshape(-1), k)
+            s0 += k
+        df = torch.from_numpy(rng.uniform(0.5, 3.0, cnt).astype(np.float32)).to(dev)
+        da = torch.from_numpy(rng.uniform(0.0, 0.1, cnt).astype(np.float32)).to(dev)
+        aa = torch.from_numpy(rng.uniform(0.0, np.pi, cnt).astype(np.float32)).to(dev)
+        ctf = synth.ctf_half(n, df, da, aa).reshape(cnt, e)
+        sig = proj[:cnt] * ctf
+        pw = (sig.abs() ** 2 * disk).sum(1, keepdim=True) / disk.sum()
+        sd = torch.sqrt(pw / 0.05 / 2)
+        data = (sig + torch.complex(torch.randn((cnt, e), device=dev, generator=gen),
+                                    torch.randn((cnt, e), device=dev, generator=gen)) * sd) * ctf
+        wts = ctf * ctf
+        del sig
+        d_iv = torch.from_numpy(ivol).to(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        G.d_rlnBackproject(acc_ft, acc_w, (D, D, D), data.reshape(-1), wts.reshape(-1), (n, n, 1), rmax,
+                           mats.reshape(-1), d_iv, (1, 0, 0, 1), 0.0, False, False, cnt)
+        b.record()
+        ev.append((a, b))
+        if c0 == 0:
+            torch.cuda.synchronize()
+            note_memory()
+        del data, wts, ctf
+    torch.cuda.synchronize()
+    t_all = time.perf_counter() - t0
+    ins_ms = sum(a.elapsed_time(b) for a, b in ev)
+    note_memory()
+    del proj, vols
+    torch.cuda.empty_cache()
+    p128 = WS.load_params(128, dev)
+    out = torch.empty(n ** 3, dtype=torch.float32, device=dev)
+    grid = []
+    for v in range(8):
+        sl = slice(v * nvox, (v + 1) * nvox)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        it, ch, used = G.reconstruct_gridding_warm(acc_ft[sl], acc_w[sl], out, (n,) * 3, (D,) * 3, p128, PAD, 1000,
+                                                   1e-4, 0.9)
+        b.record()
+        torch.cuda.synchronize()
+        note_memory()
+        grid.append({"volume": v, "class": v // 2, "half": v % 2, "particles": int(per_volume[v]),
+                     "iterations": it, "final_change": ch, "learned_start_kept": used,
+                     "ms": round(a.elapsed_time(b), 2)})
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    G.d_ReconstructGridding(acc_ft[:nvox], acc_w[:nvox], out, (n,) * 3, (D,) * 3, PAD, 0, 0, 10)
+    b.record()
+    torch.cuda.synchronize()
+    tot = note_memory()
+    print(json.dumps({
+        "config": "large combined: 400^3 blob volume per class, padding 2, 1 000 000 particles of 400^2 in 2 "
+                  "half-maps x 4 classes (40/30/20/10 %), CTF, SNR 0.05; one insertion call per chunk into 8 "
+                  "volumes by d_ivolume; learned warm start + momentum gridding per volume to change 1e-4",
+        "particles": total, "chunk": chunk,
+        "insert_slices_per_s": round(total / (ins_ms * 1e-3), 1), "insert_ms": round(ins_ms, 1),
+        "generate_and_insert_s": round(t_all, 1), "class_volumes_s": round(t_vols, 1),
+        "gridding": grid, "gridding_total_ms": round(sum(g["ms"] for g in grid), 1),
+        "gridding_10it_plain_ms": round(a.elapsed_time(b), 2),
+        "peak_device_memory_gb": round(peak[0] / 1e9, 2), "device_memory_gb": round(tot / 1e9, 2),
+        "accumulators_gb": round(8 * nvox * 12 / 1e9, 2)}), flush=True)
+
+
 def main():
     args = parse_args()
     if args.sweep:
         run_sweep(args)
+        return
+    if args.config5:
+        run_config5(args)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -9,6 +9,7 @@
 // of the trilinear weights, Friedel mirroring, the second insertion on the
 // x = 0 plane and the clamps are the reference's, step for step.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 
 #include "brick.cuh"
@@ -71,7 +72,11 @@ backproject_direct_kernel(float2* __restrict__ volft_base, float* __restrict__ v
 #pragma unroll
   for (int i = 0; i < 9; i++) m[i] = __ldg(mats + 9 * (int64_t)slice + i);
   if (ivolume) {
-    int64_t off = (int64_t)__ldg(ivolume + slice) * a.nvox;
+    // a negative index would address memory before the volumes (the
+    // reference writes there); such a slice is skipped
+    const int iv = __ldg(ivolume + slice);
+    if (iv < 0) continue;
+    int64_t off = (int64_t)iv * a.nvox;
     if (volft) volft += off;
     if (volw) volw += off;
   }
@@ -319,11 +324,22 @@ backproject_brick_kernel(float2* __restrict__ volft, float* __restrict__ volw,
 // and the second insertions on the x = 0 plane.  Each target of each pixel
 // is added once, by the pair of its brick on the side of its conjugation,
 // with the weights and values of the binned variant.
-template <bool DECENTERED, bool SQUARE>
+//
+// GEN (centred output only): the general geometry of the reference's
+// insertion — a magnification of the pixel coordinates, the Ewald curvature
+// and a target volume per slice (Backproject.cu:57-63, 145-152, 183-189).
+// A work item's key is volume * nbricks + brick; the row segments walk the
+// magnified map u c0' + v c1' with every box widened by the curvature's
+// reach, and each candidate is kept only if the reference's magnified
+// radius test passes, so the samples and targets are the direct kernel's.
+// The grid reaches one voxel past the volume (kept samples come within
+// rmax * scale of the origin) and the flush folds those voxels onto the
+// edge faces with the reference's clamps.
+template <bool DECENTERED, bool SQUARE, bool GEN>
 __global__ void __launch_bounds__(1024)
-backproject_segment_kernel(float2* __restrict__ volft, float* __restrict__ volw,
+backproject_segment_kernel(float2* __restrict__ volft_base, float* __restrict__ volw_base,
                            const float2* __restrict__ projft, const float* __restrict__ projw,
-                           const float* __restrict__ mats, BpArgs a, BrickGrid g, PixelSet px,
+                           const float* __restrict__ mats, BpArgs a, BrickGrid g, PixelSet px, SliceGeom gm,
                            const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
                            const int* __restrict__ slices, int* __restrict__ counter) {
   extern __shared__ float acc[];
@@ -348,7 +364,10 @@ backproject_segment_kernel(float2* __restrict__ volft, float* __restrict__ volw,
     const int w = item_s;
     if (w >= nitems) break;
     const BrickItem it = items[w];
-    const int3 o = brick_origin(g, it.brick);
+    const int vol = GEN ? it.brick / g.nbricks : 0;
+    const int3 o = brick_origin(g, it.brick - vol * g.nbricks);
+    float2* volft = volft_base && GEN ? volft_base + (int64_t)vol * a.nvox : volft_base;
+    float* volw = volw_base && GEN ? volw_base + (int64_t)vol * a.nvox : volw_base;
 
     // warps take the item's pairs one at a time, the next one's slice
     // fetched before the current one is processed
@@ -365,16 +384,26 @@ backproject_segment_kernel(float2* __restrict__ volft, float* __restrict__ volw,
       float m[9];
 #pragma unroll
       for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
+      float me[9];
+      if (GEN) effective_matrix(m, gm, me);
+      const float widen = GEN ? curvature_reach(m, gm, px.pmax) : 0.f;
       const int64_t sbase = a.elements * slice;
 #pragma unroll 1
       for (int side = 0; side < 2; side++) {
-        const SegBox box = seg_box(m, side, o, B, 1.f);
+        const SegBox box = seg_box(GEN ? me : m, side, o, B, 1.f, widen);
         const bool plane0 = side == 1 && o.x == 0;  // second insertions can land in this brick
         seg_for_each_pixel(box, px, [&](int u, int v, bool valid) {
           if (!valid) return;
+          float qx = (float)u, qy = (float)v, qz = 0.f;
+          if (GEN) {  // Backproject.cu:176-192, as backproject_direct_kernel
+            qx = fmaf(a.mag.x, (float)u, a.mag.z * (float)v);
+            qy = fmaf(a.mag.y, (float)u, a.mag.w * (float)v);
+            qz = a.ewalddiaminv * (float)(u * u + v * v);
+            if ((int)fmaf(qz, qz, fmaf(qx, qx, qy * qy)) >= a.rmax2) return;
+          }
           const int idy = v < 0 ? v + a.n : v;
           const int64_t id = sbase + (int64_t)idy * a.dimft + u;
-          BpSample s = backproject_sample(m, (float)u, (float)v, 0.f);
+          BpSample s = backproject_sample(m, qx, qy, qz);
           const float2 val = projft ? __ldg(projft + id) : make_float2(1.f, 0.f);
           const float pw = projw ? __ldg(projw + id) : 1.f;
           if (side == 0) {
@@ -435,7 +464,7 @@ backproject_segment_kernel(float2* __restrict__ volft, float* __restrict__ volw,
     __syncthreads();
 
     // flush the brick into the volume
-    bp_flush_brick<DECENTERED>(volft, volw, are, aim, aw, B, RS, PS, o, V, a.rowlen, it.exclusive != 0);
+    bp_flush_brick<DECENTERED, GEN>(volft, volw, are, aim, aw, B, RS, PS, o, V, a.rowlen, it.exclusive != 0);
   }
 }
 
@@ -461,25 +490,68 @@ static void launch_bp_direct_any(dim3 grid, cudaStream_t stream, float2* vf, flo
   }
 }
 
+// Square of the smallest singular value of the 2x2 magnification (columns
+// (x, y) and (z, w)).
+static double mag_smin2(float4 mag) {
+  const double m00 = mag.x, m10 = mag.y, m01 = mag.z, m11 = mag.w;
+  const double p = m00 * m00 + m10 * m10, q = m01 * m01 + m11 * m11, r = m00 * m01 + m10 * m11;
+  return 0.5 * (p + q) - std::sqrt(0.25 * (p - q) * (p - q) + r * r);
+}
+
+// Largest volume index of a device array, through the pool (one small
+// kernel and a read-back that waits for the stream).
+__global__ void max_index_kernel(const int* __restrict__ iv, unsigned n, int* __restrict__ out) {
+  int m = INT_MIN;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = max(m, iv[i]);
+  for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+static int device_max_index(const int* d_iv, unsigned n, cudaStream_t stream, int* out) {
+  int* d = nullptr;
+  int st = pool_alloc((void**)&d, sizeof(int), stream);
+  if (st) return st;
+  const int init = INT_MIN;
+  int h = INT_MIN;
+  cudaError_t e = cudaMemcpyAsync(d, &init, sizeof(int), cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) {
+    max_index_kernel<<<std::min(1024u, (n + 255) / 256), 256, 0, stream>>>(d_iv, n, d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  pool_free(d, stream);
+  if (e != cudaSuccess) return set_error(GTOMRLN_ERR_CUDA, "volume index read-back: %s", cudaGetErrorString(e));
+  *out = h;
+  return GTOMRLN_OK;
+}
+
 // The brick path: plan, brick kernel, and the direct kernel for any slice the
-// plan could not take.  Nothing synchronises.
+// plan could not take.  Nothing synchronises.  gen: magnification, Ewald
+// curvature or per-slice volumes (centred output, row segments only;
+// d_ivolume values in [0, nvol)).
 static int backproject_brick(float* d_volumeft, float* d_volumeweights, const float* d_projft,
                              const float* d_projweights, const float* d_mats, const BpArgs& a,
                              int rmax, int decentered, int square, unsigned batch, cudaStream_t stream,
-                             int segments) {
+                             int segments, bool gen = false, const int* d_ivolume = nullptr, int nvol = 1) {
   const int V = a.P;
   // Neighbours stay inside x [0, V/2] and y, z [-V/2, yhi] (no clamp, no
-  // wrap beyond the reference's) while every sample radius is below limit.
+  // wrap beyond the reference's) while every sample radius is below limit;
+  // the general geometry's grid reaches one voxel further and its flush
+  // folds that voxel onto the edge with the reference's clamps.
   const int yhi = decentered ? V / 2 : V - 1 - V / 2;
-  const float limit = (float)std::min(V / 2, yhi) - 1e-4f;
+  const int ext = gen ? 1 : 0;
+  const float limit = (float)(std::min(V / 2, yhi) + ext) - 1e-4f;
   const BrickTuning tune = brick_tuning(GTOMRLN_OP_BACKPROJECT);
-  BrickGrid g = make_brick_grid(V, tune.edge, V / 2, -(V / 2), yhi);
+  BrickGrid g = make_brick_grid(V, tune.edge, V / 2 + ext, -(V / 2) - ext, yhi + ext);
   size_t smem = sizeof(float) * 3 * (size_t)tune.edge * (tune.edge + 1) * (tune.edge + 1);
   auto kern = decentered ? (square ? backproject_brick_kernel<true, true> : backproject_brick_kernel<true, false>)
                          : (square ? backproject_brick_kernel<false, true> : backproject_brick_kernel<false, false>);
-  auto skern = decentered
-                   ? (square ? backproject_segment_kernel<true, true> : backproject_segment_kernel<true, false>)
-                   : (square ? backproject_segment_kernel<false, true> : backproject_segment_kernel<false, false>);
+  auto skern = gen ? (square ? backproject_segment_kernel<false, true, true>
+                             : backproject_segment_kernel<false, false, true>)
+               : decentered
+                   ? (square ? backproject_segment_kernel<true, true, false> : backproject_segment_kernel<true, false, false>)
+                   : (square ? backproject_segment_kernel<false, true, false> : backproject_segment_kernel<false, false, false>);
   cudaError_t e = segments ? cudaFuncSetAttribute(skern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
                            : cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess)
@@ -499,20 +571,35 @@ static int backproject_brick(float* d_volumeft, float* d_volumeweights, const fl
   px.rmax2 = a.rmax2;
   px.strict = 1;
   px.pmax = std::sqrt((float)std::max(0, rmax * rmax - 1));
+  SliceGeom gm;
+  if (gen) {
+    // The samples kept have |q| < rmax with q the magnified coordinates, so
+    // the pixels to visit lie within rmax / (smallest singular value of the
+    // magnification); the kernel applies the exact test.
+    const double rp = (double)rmax / std::sqrt(mag_smin2(a.mag));
+    const double lim2 = 2.0 * (double)(a.n / 2 + 1) * (a.n / 2 + 1);  // beyond every pixel of the slice
+    px.rmax2 = (int)std::min(lim2, std::floor(rp * rp * (1.0 + 1e-6)) + 2.0);
+    px.pmax = (float)std::sqrt((double)px.rmax2) * (1.f + 1e-6f);
+    gm.mag = a.mag;
+    gm.curve = a.ewalddiaminv;
+    gm.ivolume = d_ivolume;
+    gm.nvol = nvol;
+    gm.qmax = std::sqrt((float)a.rmax2) * (1.f + 1e-6f);
+  }
   BrickPlan plan;
   int st = build_brick_plan(GTOMRLN_OP_BACKPROJECT, d_mats, (int)batch, g, px, limit, tune.chunk, stream, &plan,
-                            segments);
+                            segments, nullptr, gm);
   if (st) return st;
   if (segments)
     skern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
-        (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, a, g, px,
+        (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, a, g, px, gm,
         plan.items, plan.nitems, plan.pairs, plan.counter);
   else
     kern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
         (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, a, g, plan.items,
         plan.nitems, plan.pairs, plan.bins, plan.entries, plan.counter);
   launch_bp_direct_any(dim3(sms * 4), stream, (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft,
-                       d_projweights, d_mats, nullptr, a, plan.fallback, plan.nfallback, 2, decentered, square);
+                       d_projweights, d_mats, d_ivolume, a, plan.fallback, plan.nfallback, 2, decentered, square);
   e = cudaGetLastError();
   free_brick_plan(&plan, stream);
   if (e != cudaSuccess)
@@ -766,11 +853,13 @@ static int backproject_shifted_brick(float* d_volumeft, float* d_volumeweights, 
   return GTOMRLN_OK;
 }
 
+// nvol_hint: the number of volumes d_ivolume indexes when the caller knows it
+// (the host-array overload), <= 0 when not.
 static int backproject_launch(float* d_volumeft, float* d_volumeweights, int vx, int vy, int vz,
                               const float* d_projft, const float* d_projweights, int px, int py,
                               int pz, unsigned rmax, const float* d_matrices, const int* d_ivolume,
                               float4 mag, float ewaldradiussuper, int decentered, int square,
-                              unsigned batch, cudaStream_t stream) {
+                              unsigned batch, cudaStream_t stream, int nvol_hint = 0) {
   int ndv = dimension_count(vx, vy, vz), ndp = dimension_count(px, py, pz);
   if (ndv < ndp)
     return set_error(GTOMRLN_ERR_INVALID,
@@ -800,12 +889,42 @@ static int backproject_launch(float* d_volumeft, float* d_volumeweights, int vx,
     return set_error(GTOMRLN_ERR_INVALID, "backproject: batch too large for one launch");
 
   const int choice = path_choice(GTOMRLN_OP_BACKPROJECT);
-  if (ndp == 2 && vx == vy && vx == vz && vx >= 4 && !d_ivolume && mag.x == 1.f && mag.y == 0.f &&
-      mag.z == 0.f && mag.w == 1.f && a.ewalddiaminv == 0.f && (d_volumeft || d_volumeweights) &&
-      (choice == GTOMRLN_PATH_BRICK || choice == GTOMRLN_PATH_SEGMENT ||
-       (choice == GTOMRLN_PATH_AUTO && brick_path_pays(GTOMRLN_OP_BACKPROJECT, vx, batch))))
+  const bool plain = !d_ivolume && mag.x == 1.f && mag.y == 0.f && mag.z == 0.f && mag.w == 1.f &&
+                     a.ewalddiaminv == 0.f;
+  const bool brick = ndp == 2 && vx == vy && vx == vz && vx >= 4 && (d_volumeft || d_volumeweights) &&
+                     (choice == GTOMRLN_PATH_BRICK || choice == GTOMRLN_PATH_SEGMENT ||
+                      (choice == GTOMRLN_PATH_AUTO && brick_path_pays(GTOMRLN_OP_BACKPROJECT, vx, batch)));
+  if (brick && plain)
     return backproject_brick(d_volumeft, d_volumeweights, d_projft, d_projweights, d_matrices, a, (int)rmax,
                              decentered, square, batch, stream, choice == GTOMRLN_PATH_BRICK ? 0 : 1);
+  // The general geometry (magnification, Ewald curvature, per-slice volumes)
+  // takes the row-segment kernel for centred output when the magnification
+  // is well conditioned; per-slice volumes need their count (from the host
+  // array, else read back from the device, which waits for the stream and
+  // is skipped under stream capture).
+  if (brick && !decentered && choice != GTOMRLN_PATH_BRICK && mag_smin2(mag) > 1e-4 &&
+      std::fabs(a.ewalddiaminv) < 1.f) {
+    int nvol = 1;
+    if (d_ivolume) {
+      nvol = nvol_hint;
+      if (nvol <= 0) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) {
+          cudaGetLastError();
+          cs = cudaStreamCaptureStatusActive;
+        }
+        int mx = -1;
+        if (cs == cudaStreamCaptureStatusNone) {
+          int st = device_max_index(d_ivolume, batch, stream, &mx);
+          if (st) return st;
+        }
+        nvol = mx + 1;
+      }
+    }
+    if (nvol >= 1 && nvol <= 4096)
+      return backproject_brick(d_volumeft, d_volumeweights, d_projft, d_projweights, d_matrices, a, (int)rmax,
+                               decentered, square, batch, stream, 1, true, d_ivolume, nvol);
+  }
 
   launch_bp_direct_any(dim3((unsigned)(a.tiles * (int64_t)batch)), stream, (float2*)d_volumeft, d_volumeweights,
                        (const float2*)d_projft, d_projweights, d_matrices, d_ivolume, a, nullptr, nullptr, ndp,
@@ -853,10 +972,12 @@ int gtomrln_backproject_angles(float* d_volumeft, float* d_volumeweights, int vx
         return set_error(GTOMRLN_ERR_CUDA, "ivolume upload failed: %s", cudaGetErrorString(e));
       }
     }
+    int hint = 0;
+    if (h_ivolume && batch) hint = *std::max_element(h_ivolume, h_ivolume + batch) + 1;
     int st = backproject_launch(d_volumeft, d_volumeweights, vx, vy, vz, d_projft, d_projweights,
                                 px, py, pz, rmax, d_m, d_iv, make_float4(mag_x, mag_y, mag_z, mag_w),
                                 ewaldradius * supersample, outputdecentered, squareinterpweights,
-                                batch, s);
+                                batch, s, hint);
     int st2 = pool_free(d_iv, s);
     return st ? st : st2;
   });

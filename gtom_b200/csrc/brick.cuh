@@ -103,9 +103,43 @@ struct PixelSet {
   float pmax;        // largest |pixel| in the set
 };
 
+// Slice geometry beyond a plain matrix (the backprojector's general case,
+// Backproject.cu:57-63, 145-152, 183-189): an in-plane magnification applied
+// to the pixel coordinates before the matrix, the Ewald-sphere curvature
+// z = curve * (x^2 + y^2) along the matrix's third column, and a target
+// volume per slice.  Defaults describe the plain case.
+struct SliceGeom {
+  float4 mag = make_float4(1.f, 0.f, 0.f, 1.f);  // columns of the 2x2 magnification
+  float curve = 0.f;            // 1 / (2 R); 0 = flat slices
+  const int* ivolume = nullptr;  // per-slice volume index (device), or none
+  int nvol = 1;                  // volumes the plan spans (ivolume values in [0, nvol))
+  float qmax = -1.f;  // bound on |q| of the samples kept (magnified radius test); < 0: the pixel set's pmax
+};
+
+// The map pixel (u, v) -> u c0' + v c1' of the enumeration: the matrix's
+// first two columns through the magnification (c0' = mag.x c0 + mag.y c1,
+// c1' = mag.z c0 + mag.w c1), third column unchanged.
+__device__ __forceinline__ void effective_matrix(const float* m, const SliceGeom& gm, float* me) {
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    me[r] = fmaf(gm.mag.x, m[r], gm.mag.y * m[3 + r]);
+    me[3 + r] = fmaf(gm.mag.z, m[r], gm.mag.w * m[3 + r]);
+    me[6 + r] = m[6 + r];
+  }
+}
+
+// Largest displacement (voxels, any axis) of a sample from the flat map by
+// the curvature, over pixels of radius <= pmax: curve pmax^2 max|c2_r|.
+__device__ __forceinline__ float curvature_reach(const float* m, const SliceGeom& gm, float pmax) {
+  if (gm.curve == 0.f) return 0.f;
+  const float c2 = fmaxf(fabsf(m[6]), fmaxf(fabsf(m[7]), fabsf(m[8])));
+  return fabsf(gm.curve) * pmax * pmax * c2 * (1.f + 1e-5f) + 1e-4f;
+}
+
 // Per-call plan, all in device memory.
 struct BrickPlan {
   BrickGrid g;
+  int nvol = 1;  // work-item keys are volume * g.nbricks + brick
   int batch = 0;
   int max_items = 0;
   BrickItem* items = nullptr;
@@ -131,9 +165,13 @@ struct BrickPlan {
 // With a segment plan, zero_out (the projector's output, complex, elements
 // per slice as px) receives the zeros outside px's radius for every planned
 // slice, in the plan's own per-slice pass.
+// geom (segment plans only): magnification, curvature and per-slice volumes
+// of the backprojector's general case; the plan then lists one pair per
+// (slice, volume-brick key) and its enumeration boxes are widened by the
+// curvature's reach.
 int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g, const PixelSet& px,
                      float limit, int chunk, cudaStream_t stream, BrickPlan* plan, int segments = 0,
-                     void* zero_out = nullptr);
+                     void* zero_out = nullptr, const SliceGeom& geom = SliceGeom());
 int free_brick_plan(BrickPlan* plan, cudaStream_t stream);
 
 // Pixel id -> signed slice coordinates (FFT order in y).

@@ -257,24 +257,33 @@ bin_slices_kernel(const float* __restrict__ mats, BrickGrid g, PixelSet px, floa
 // slice's plane within the radius its samples reach.  Each becomes a bin
 // without entries; the brick kernel finds the pixels by row segments
 // (segment.cuh).  Positions of a slice lie on the plane through the origin
-// spanned by the first two matrix columns and within plane_scale * pmax of
-// the origin, mirrored positions too, so the list covers every brick a
-// pixel of the slice (or its mirror) can reach.
+// spanned by the first two (magnified) matrix columns and within
+// plane_scale * pmax of the origin, mirrored positions too, so the list
+// covers every brick a pixel of the slice (or its mirror) can reach; with
+// the Ewald curvature the samples leave the plane by at most its reach,
+// which widens every box.  With per-slice volumes a pair's key is
+// volume * nbricks + brick; a slice whose volume index is outside
+// [0, nvol) takes the direct path.
 constexpr int kPairThreads = 256;
 __global__ void __launch_bounds__(kPairThreads)
 segment_pairs_kernel(const float* __restrict__ mats, BrickGrid g, float pmax, float limit, float below,
                      PixelBin* __restrict__ bins, int64_t bins_cap, unsigned long long* __restrict__ counters,
                      int* __restrict__ brick_pairs, int* __restrict__ fallback, int* __restrict__ nfallback,
-                     float2* __restrict__ zero_out, PixelSet zpx) {
+                     float2* __restrict__ zero_out, PixelSet zpx, SliceGeom gm) {
   extern __shared__ int hits[];  // brick ids of this slice
   __shared__ int s_n;
   __shared__ long long s_base;
   const int slice = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
-  float m[9];
+  float m0[9], m[9];
 #pragma unroll
-  for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
-  const float scale = plane_scale(m);
-  if (!(scale * pmax < limit)) {  // uniform over the block
+  for (int k = 0; k < 9; k++) m0[k] = __ldg(mats + 9 * (int64_t)slice + k);
+  effective_matrix(m0, gm, m);
+  // Samples kept lie within R of the origin: |q| <= qmax in the plane of the
+  // matrix's first two columns, plus the curvature's reach along the third.
+  const float widen = curvature_reach(m0, gm, pmax);
+  const float R = plane_scale(m0) * (gm.qmax < 0.f ? pmax : gm.qmax) + widen;
+  const int vol = gm.ivolume ? __ldg(gm.ivolume + slice) : 0;
+  if (!(R < limit) || vol < 0 || vol >= gm.nvol) {  // uniform over the block
     if (tid == 0) fallback[atomicAdd(nfallback, 1)] = slice;
     return;
   }
@@ -293,9 +302,8 @@ segment_pairs_kernel(const float* __restrict__ mats, BrickGrid g, float pmax, fl
   if (tid == 0) s_n = 0;
   __syncthreads();
   const float n0 = m[1] * m[5] - m[2] * m[4], n1 = m[2] * m[3] - m[0] * m[5], n2 = m[0] * m[4] - m[1] * m[3];
-  const float R = scale * pmax;
   const float R2 = R * R * (1.f + 1e-5f) + 1e-3f;
-  const float lo_pad = below + kSegMargin, hi_pad = (float)g.B + kSegMargin;
+  const float lo_pad = below + widen + kSegMargin, hi_pad = (float)g.B + widen + kSegMargin;
   for (int base = 0; base < g.nbricks; base += kPairThreads) {
     const int b = base + tid;
     bool hit = false;
@@ -329,7 +337,7 @@ segment_pairs_kernel(const float* __restrict__ mats, BrickGrid g, float pmax, fl
     return;
   }
   for (int k = tid; k < nh; k += kPairThreads) {
-    const int b = hits[k];
+    const int b = vol * g.nbricks + hits[k];
     bins[s_base + k] = {slice, 0, 0, b, 0, 0, 0, 0};
     atomicAdd(brick_pairs + b, 1);
   }
@@ -339,16 +347,19 @@ segment_pairs_kernel(const float* __restrict__ mats, BrickGrid g, float pmax, fl
 // origin); writes bin-list offsets, per-brick item offsets and the item count.
 constexpr int kScanThreads = 1024;
 __global__ void __launch_bounds__(kScanThreads)
-pairs_scan_kernel(const int* __restrict__ counts, const int* __restrict__ order, int nbricks, int chunk,
+pairs_scan_kernel(const int* __restrict__ counts, const int* __restrict__ order, int nbricks, int nvol, int chunk,
                   int* __restrict__ offsets, int* __restrict__ item_off, int* __restrict__ cursor,
                   int* __restrict__ nitems) {
   __shared__ int s_c[kScanThreads], s_i[kScanThreads];
   __shared__ int carry_c, carry_i;
   if (threadIdx.x == 0) carry_c = carry_i = 0;
   __syncthreads();
-  for (int base = 0; base < nbricks; base += kScanThreads) {
+  // keys volume * nbricks + brick, the volumes interleaved brick by brick so
+  // that every volume's central bricks start first
+  const int nkeys = nbricks * nvol;
+  for (int base = 0; base < nkeys; base += kScanThreads) {
     int t = base + threadIdx.x;
-    int b = t < nbricks ? order[t] : -1;
+    int b = t < nkeys ? (t % nvol) * nbricks + order[t / nvol] : -1;
     int c = b >= 0 ? counts[b] : 0;
     int ni = (c + chunk - 1) / chunk;
     s_c[threadIdx.x] = c;
@@ -455,9 +466,13 @@ static int brick_order(const BrickGrid& g, const int** out) {
 
 int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g, const PixelSet& px,
                      float limit, int chunk, cudaStream_t stream, BrickPlan* plan, int segments,
-                     void* zero_out) {
+                     void* zero_out, const SliceGeom& geom) {
   plan->g = g;
+  plan->nvol = geom.nvol;
   plan->batch = batch;
+  if (geom.nvol < 1 || (!segments && (geom.nvol != 1 || geom.curve != 0.f || geom.mag.x != 1.f ||
+                                      geom.mag.y != 0.f || geom.mag.z != 0.f || geom.mag.w != 1.f)))
+    return set_error(GTOMRLN_ERR_INVALID, "brick plan: the binning plan takes plain slices of one volume only");
   size_t hist_bytes = 2 * sizeof(int) * (size_t)g.nbricks;
   if (hist_bytes > 200 * 1024)
     return set_error(GTOMRLN_ERR_INVALID, "brick grid of %d bricks too fine for the binning plan", g.nbricks);
@@ -497,9 +512,11 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
   int64_t bins_cap = std::max<int64_t>(1, (int64_t)batch * per_slice);
   if (entries_cap > 0x7fffffffLL || bins_cap > 0x7fffffffLL)
     return set_error(GTOMRLN_ERR_INVALID, "brick plan too large for one call; split the batch");
-  int64_t cap_items = (int64_t)g.nbricks + bins_cap / chunk + 1;
+  const int64_t nkeys = (int64_t)g.nbricks * geom.nvol;  // work-item keys: volume * nbricks + brick
+  if (nkeys > 0x7fffffffLL) return set_error(GTOMRLN_ERR_INVALID, "brick plan: too many volumes");
+  int64_t cap_items = nkeys + bins_cap / chunk + 1;
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-  size_t nb = (size_t)g.nbricks;
+  size_t nb = (size_t)nkeys;
   size_t o_counts = 0;
   size_t o_offsets = o_counts + al(nb * 4);
   size_t o_itemoff = o_offsets + al(nb * 4);
@@ -540,7 +557,7 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
       cudaFuncSetAttribute(segment_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
       segment_pairs_kernel<<<batch, kPairThreads, smem_bytes, stream>>>(
           d_mats, g, px.pmax, limit, below, plan->bins, bins_cap, counters, counts, plan->fallback,
-          plan->nfallback, (float2*)zero_out, px);
+          plan->nfallback, (float2*)zero_out, px, geom);
     } else if (op == GTOMRLN_OP_PROJECT) {
       cudaFuncSetAttribute(bin_slices_kernel<GTOMRLN_OP_PROJECT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem_bytes);
@@ -554,15 +571,15 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
           d_mats, g, px, limit, plan->entries, entries_cap, plan->bins, bins_cap, counters, counts,
           plan->fallback, plan->nfallback, use_codes);
     }
-    pairs_scan_kernel<<<1, kScanThreads, 0, stream>>>(counts, d_order, g.nbricks, chunk, offsets, item_off,
-                                                      cursor, plan->nitems);
+    pairs_scan_kernel<<<1, kScanThreads, 0, stream>>>(counts, d_order, g.nbricks, geom.nvol, chunk, offsets,
+                                                      item_off, cursor, plan->nitems);
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     pairs_fill_kernel<<<sms * 4, 256, 0, stream>>>(plan->bins, counters, bins_cap, counts, offsets, cursor,
                                                    plan->pairs, segments);
-    plan_items_kernel<<<(g.nbricks + 255) / 256, 256, 0, stream>>>(counts, offsets, item_off, g.nbricks, chunk,
-                                                                   plan->items);
+    plan_items_kernel<<<(int)((nkeys + 255) / 256), 256, 0, stream>>>(counts, offsets, item_off, (int)nkeys, chunk,
+                                                                      plan->items);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess) {

@@ -182,14 +182,6 @@ __device__ __forceinline__ void red_add4(float* p, float a, float b, float c, fl
                : "memory");
 }
 
-// Slice element id -> signed Fourier coordinates (Project.cu:103-109).
-struct SliceGeom {
-  int n;         // dimsproj.x
-  int dimft;     // n/2 + 1
-  int64_t area;  // dimft * n
-  int64_t elements;
-};
-
 // Copies host-built matrices to stream-ordered scratch, runs fn, frees.
 template <class Fn>
 inline int with_device_matrices(const float* h_angles, float supersample, unsigned batch,

@@ -160,15 +160,17 @@ __device__ __forceinline__ void seg_for_each_pixel(const SegBox& b, const PixelS
 }
 
 // The box of brick origin o, edge B, widened by `below` voxels on the low
-// side and by the margin on both, for side 0 (positions) or side 1
-// (negated positions) of matrix m.
-__device__ __forceinline__ SegBox seg_box(const float* m, int side, int3 o, int B, float below) {
+// side, by `widen` (a bound on how far samples leave the flat map, e.g. by
+// the Ewald curvature) and the margin on both, for side 0 (positions) or
+// side 1 (negated positions) of matrix m.
+__device__ __forceinline__ SegBox seg_box(const float* m, int side, int3 o, int B, float below,
+                                          float widen = 0.f) {
   SegBox b;
   b.m = m;
   b.sg = side ? -1.f : 1.f;
   b.o = o;
-  b.below = below + kSegMargin;
-  b.above = (float)B + kSegMargin;
+  b.below = below + widen + kSegMargin;
+  b.above = (float)B + widen + kSegMargin;
   return b;
 }
 

@@ -181,3 +181,46 @@ def test_segment_paths_on_general_geometry(cuda, kind, edge):
     finally:
         set_brick_tuning("project")
         set_brick_tuning("backproject")
+
+
+@pytest.mark.parametrize("case", [
+    dict(mag=(1.03, 0.02, -0.01, 0.97)),
+    dict(ewald=30.0),
+    dict(nvol=3),
+    dict(mag=(0.98, -0.015, 0.02, 1.025), ewald=-45.0, nvol=2, sq=True),
+    dict(mag=(1.01, 0.0, 0.0, 1.01), ewald=60.0, nvol=4, n=64, V=129, batch=200),
+])
+def test_segment_backprojector_general_geometry(cuda, case):
+    """Magnification, Ewald curvature and per-slice volumes on the row-segment
+    backprojector (centred output): the same contributions as the oracle's
+    single-precision port of Backproject3DtoNDKernel, including the samples
+    that come within one voxel of the volume's edge (folded by the clamps)."""
+    from gtom_b200 import d_rlnBackproject
+    c = dict(mag=(1, 0, 0, 1), ewald=0.0, nvol=1, sq=False, n=48, V=97, batch=300)
+    c.update(case)
+    n, V, batch, nvol = c["n"], c["V"], c["batch"], c["nvol"]
+    rng = np.random.default_rng(n + batch + nvol)
+    mats = O.matrices_f64(random_angles(rng, batch), 2.0).astype(np.float32)
+    e = O.elements_fft(n)
+    projft = (rng.normal(size=(batch, e)) + 1j * rng.normal(size=(batch, e))).astype(np.complex64)
+    projw = rng.uniform(0.1, 1, size=(batch, e)).astype(np.float32)
+    ivol = rng.integers(0, nvol, batch).astype(np.int32) if nvol > 1 else None
+    nv = (V // 2 + 1) * V * V * nvol
+    got = {}
+    for path in ("direct", "segment"):
+        _paths("auto", path)
+        vf = torch.zeros(nv, dtype=torch.complex64, device="cuda")
+        vw = torch.zeros(nv, dtype=torch.float32, device="cuda")
+        d_rlnBackproject(vf, vw, (V, V, V), torch.from_numpy(projft).cuda().reshape(-1),
+                         torch.from_numpy(projw).cuda().reshape(-1), (n, n, 1), n // 2,
+                         torch.from_numpy(mats).cuda().reshape(-1),
+                         None if ivol is None else torch.from_numpy(ivol).cuda(), c["mag"], c["ewald"], False,
+                         c["sq"], batch)
+        torch.cuda.synchronize()
+        got[path] = (vf.cpu().numpy(), vw.cpu().numpy())
+    of, ow = np.zeros(nv, np.complex64), np.zeros(nv, np.float32)
+    O.backproject(of, ow, V, projft, projw, n, n // 2, mats, ivolume=ivol, magnification=c["mag"],
+                  ewaldradiussuper=c["ewald"], decentered=False, square=c["sq"], fp32=True)
+    for path, (gf, gw) in got.items():
+        assert rel_l2(gf, of) <= 1e-5, path
+        assert rel_l2(gw, ow) <= 1e-5, path
