@@ -341,7 +341,7 @@ backproject_segment_kernel(float2* __restrict__ volft_base, float* __restrict__ 
                            const float2* __restrict__ projft, const float* __restrict__ projw,
                            const float* __restrict__ mats, BpArgs a, BrickGrid g, PixelSet px, SliceGeom gm,
                            const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
-                           const int* __restrict__ slices, int* __restrict__ counter) {
+                           const int* __restrict__ pairs, const PixelBin* __restrict__ bins, int* __restrict__ counter) {
   extern __shared__ float acc[];
   __shared__ int item_s, next_s;
   const int nitems = *nitems_ptr;
@@ -377,10 +377,11 @@ backproject_segment_kernel(float2* __restrict__ volft_base, float* __restrict__ 
       return __shfl_sync(0xffffffffu, j, 0);
     };
     int j = take();
-    int slice = j < it.count ? __ldg(slices + it.offset + j) : 0;
+    int4 pr = j < it.count ? seg_pair(bins, pairs, it.offset + j) : make_int4(0, kSegNoRows, kSegNoRows, 0);
     while (j < it.count) {
       const int jn = take();
-      const int next = jn < it.count ? __ldg(slices + it.offset + jn) : 0;
+      const int4 nx = jn < it.count ? seg_pair(bins, pairs, it.offset + jn) : make_int4(0, kSegNoRows, kSegNoRows, 0);
+      const int slice = pr.x;
       float m[9];
 #pragma unroll
       for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
@@ -390,9 +391,12 @@ backproject_segment_kernel(float2* __restrict__ volft_base, float* __restrict__ 
       const int64_t sbase = a.elements * slice;
 #pragma unroll 1
       for (int side = 0; side < 2; side++) {
+        int vlo, vhi;
+        seg_unpack_rows(side ? pr.z : pr.y, vlo, vhi);
+        if (vlo > vhi) continue;  // no pixel of this side
         const SegBox box = seg_box(GEN ? me : m, side, o, B, 1.f, widen);
         const bool plane0 = side == 1 && o.x == 0;  // second insertions can land in this brick
-        seg_for_each_pixel(box, px, [&](int u, int v, bool valid) {
+        seg_for_each_pixel_rows(box, px, vlo, vhi, [&](int u, int v, bool valid) {
           if (!valid) return;
           float qx = (float)u, qy = (float)v, qz = 0.f;
           if (GEN) {  // Backproject.cu:176-192, as backproject_direct_kernel
@@ -459,7 +463,7 @@ backproject_segment_kernel(float2* __restrict__ volft_base, float* __restrict__ 
         });
       }
       j = jn;
-      slice = next;
+      pr = nx;
     }
     __syncthreads();
 
@@ -593,7 +597,7 @@ static int backproject_brick(float* d_volumeft, float* d_volumeweights, const fl
   if (segments)
     skern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
         (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, a, g, px, gm,
-        plan.items, plan.nitems, plan.pairs, plan.counter);
+        plan.items, plan.nitems, plan.pairs, plan.bins, plan.counter);
   else
     kern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
         (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, a, g, plan.items,
@@ -710,7 +714,7 @@ backproject_shifted_segment_kernel(float2* __restrict__ volft, float* __restrict
                                    const float* __restrict__ mats, const float* __restrict__ shifts,
                                    const float* __restrict__ gweights, BpArgs a, BrickGrid g, PixelSet px,
                                    const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
-                                   const int* __restrict__ slices, int* __restrict__ counter) {
+                                   const int* __restrict__ pairs, const PixelBin* __restrict__ bins, int* __restrict__ counter) {
   extern __shared__ float acc[];
   __shared__ int item_s, next_s;
   const int nitems = *nitems_ptr;
@@ -738,10 +742,11 @@ backproject_shifted_segment_kernel(float2* __restrict__ volft, float* __restrict
       return __shfl_sync(0xffffffffu, j, 0);
     };
     int j = take();
-    int slice = j < it.count ? __ldg(slices + it.offset + j) : 0;
+    int4 pr = j < it.count ? seg_pair(bins, pairs, it.offset + j) : make_int4(0, kSegNoRows, kSegNoRows, 0);
     while (j < it.count) {
       const int jn = take();
-      const int next = jn < it.count ? __ldg(slices + it.offset + jn) : 0;
+      const int4 nx = jn < it.count ? seg_pair(bins, pairs, it.offset + jn) : make_int4(0, kSegNoRows, kSegNoRows, 0);
+      const int slice = pr.x;
       float m[9];
 #pragma unroll
       for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
@@ -750,8 +755,11 @@ backproject_shifted_segment_kernel(float2* __restrict__ volft, float* __restrict
       const int64_t sbase = a.elements * slice;
 #pragma unroll 1
       for (int side = 0; side < 2; side++) {
+        int vlo, vhi;
+        seg_unpack_rows(side ? pr.z : pr.y, vlo, vhi);
+        if (vlo > vhi) continue;  // no pixel of this side
         const SegBox box = seg_box(m, side, o, B, 1.f);
-        seg_for_each_pixel(box, px, [&](int u, int v, bool valid) {
+        seg_for_each_pixel_rows(box, px, vlo, vhi, [&](int u, int v, bool valid) {
           if (!valid) return;
           float3 pos = mat_apply(m, (float)u, (float)v, 0.f);
           const bool flip = pos.x + 1e-5f < 0.f;
@@ -799,7 +807,7 @@ backproject_shifted_segment_kernel(float2* __restrict__ volft, float* __restrict
         });
       }
       j = jn;
-      slice = next;
+      pr = nx;
     }
     __syncthreads();
     bp_flush_brick<false, true>(volft, volw, are, aim, aw, B, RS, PS, o, V, a.rowlen, it.exclusive != 0);
@@ -841,7 +849,7 @@ static int backproject_shifted_brick(float* d_volumeft, float* d_volumeweights, 
   if (st) return st;
   backproject_shifted_segment_kernel<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
       (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, d_shifts, d_gweights,
-      a, g, px, plan.items, plan.nitems, plan.pairs, plan.counter);
+      a, g, px, plan.items, plan.nitems, plan.pairs, plan.bins, plan.counter);
   backproject_shifted_kernel<2><<<sms * 4, kBpThreads, 0, stream>>>(
       (float2*)d_volumeft, d_volumeweights, (const float2*)d_projft, d_projweights, d_mats, d_shifts, d_gweights,
       a, rmax, plan.fallback, plan.nfallback);

@@ -39,7 +39,9 @@ struct BrickItem {
 // A (slice, brick) bin: `count` pixel ids starting at entries[start]; the
 // first `interior` of them are pixels whose whole 2x2x2 target cube (direct
 // or mirrored, away from the x = 0 plane) lies inside the brick, so a warp
-// can treat them with one branch-free path.
+// can treat them with one branch-free path.  In a segment plan the bin
+// lists no pixels: start and count hold the packed row ranges of the
+// pair's side 0 and side 1 (seg_pack_rows).
 struct PixelBin {
   int slice, start, count, brick, interior, pad0, pad1, pad2;
 };
@@ -144,7 +146,7 @@ struct BrickPlan {
   int max_items = 0;
   BrickItem* items = nullptr;
   int* nitems = nullptr;      // number of valid items
-  int* pairs = nullptr;       // per brick: indices into bins (segment plan: slices)
+  int* pairs = nullptr;       // per brick: indices into bins
   PixelBin* bins = nullptr;
   int* entries = nullptr;     // pixel ids, grouped by bin
   int* counter = nullptr;     // work counter of the persistent kernel (starts at 0)

@@ -336,9 +336,22 @@ segment_pairs_kernel(const float* __restrict__ mats, BrickGrid g, float pmax, fl
     if (tid == 0) fallback[atomicAdd(nfallback, 1)] = slice;
     return;
   }
+  // Each pair carries the row range of its two sides (the brick's box as the
+  // brick kernels build it: widened by `below` on the low side, by the
+  // curvature's reach and the margin on all), so that the kernels neither
+  // recompute it per warp nor walk a side with no pixels.
   for (int k = tid; k < nh; k += kPairThreads) {
-    const int b = vol * g.nbricks + hits[k];
-    bins[s_base + k] = {slice, 0, 0, b, 0, 0, 0, 0};
+    const int local = hits[k];
+    const int3 o = brick_origin(g, local);
+    int rows[2];
+#pragma unroll
+    for (int side = 0; side < 2; side++) {
+      const SegBox box = seg_box(m, side, o, g.B, below, widen);
+      int vlo, vhi;
+      rows[side] = seg_rows(box, zpx, vlo, vhi) ? seg_pack_rows(vlo, vhi) : kSegNoRows;
+    }
+    const int b = vol * g.nbricks + local;
+    bins[s_base + k] = {slice, rows[0], rows[1], b, 0, 0, 0, 0};
     atomicAdd(brick_pairs + b, 1);
   }
 }
@@ -388,20 +401,19 @@ pairs_scan_kernel(const int* __restrict__ counts, const int* __restrict__ order,
   if (threadIdx.x == 0) *nitems = carry_i;
 }
 
-// Groups the bins by brick: pairs[offsets[b] ..] lists brick b's bins (the
-// binning plan) or directly their slices (the segment plan, whose bins carry
-// nothing else), so that a kernel reaches the slice in one load.
+// Groups the bins by brick: pairs[offsets[b] ..] lists the bins of brick (or
+// volume-brick key) b.
 __global__ void pairs_fill_kernel(const PixelBin* __restrict__ bins,
                                   const unsigned long long* __restrict__ counters, int64_t bins_cap,
                                   const int* __restrict__ counts, const int* __restrict__ offsets,
-                                  int* __restrict__ cursor, int* __restrict__ pairs, int store_slice) {
+                                  int* __restrict__ cursor, int* __restrict__ pairs) {
   int64_t nb = (int64_t)min(counters[1], (unsigned long long)bins_cap);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb;
        i += (int64_t)gridDim.x * blockDim.x) {
     int b = bins[i].brick;
     if (b < 0) continue;  // reserved by a slice that fell back
     int s = atomicAdd(cursor + b, 1);
-    if (s < counts[b]) pairs[offsets[b] + s] = store_slice ? bins[i].slice : (int)i;
+    if (s < counts[b]) pairs[offsets[b] + s] = (int)i;
   }
 }
 
@@ -577,7 +589,7 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     pairs_fill_kernel<<<sms * 4, 256, 0, stream>>>(plan->bins, counters, bins_cap, counts, offsets, cursor,
-                                                   plan->pairs, segments);
+                                                   plan->pairs);
     plan_items_kernel<<<(int)((nkeys + 255) / 256), 256, 0, stream>>>(counts, offsets, item_off, (int)nkeys, chunk,
                                                                       plan->items);
     e = cudaGetLastError();

@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(1024)
 project_segment_kernel(const float2* __restrict__ vol, float2* __restrict__ proj,
                        const float* __restrict__ mats, ProjArgs a, BrickGrid g, PixelSet px,
                        const BrickItem* __restrict__ items, const int* __restrict__ nitems_ptr,
-                       const int* __restrict__ slices, int* __restrict__ counter, Post post = Post()) {
+                       const int* __restrict__ pairs, const PixelBin* __restrict__ bins, int* __restrict__ counter, Post post = Post()) {
   extern __shared__ float2 tile[];
   __shared__ int item_s, next_s;
   const int nitems = *nitems_ptr;
@@ -287,18 +287,22 @@ project_segment_kernel(const float2* __restrict__ vol, float2* __restrict__ proj
       return __shfl_sync(0xffffffffu, j, 0);
     };
     int j = take();
-    int slice = j < it.count ? __ldg(slices + it.offset + j) : 0;
+    int4 pr = j < it.count ? seg_pair(bins, pairs, it.offset + j) : make_int4(0, kSegNoRows, kSegNoRows, 0);
     while (j < it.count) {
       const int jn = take();
-      const int next = jn < it.count ? __ldg(slices + it.offset + jn) : 0;
+      const int4 nx = jn < it.count ? seg_pair(bins, pairs, it.offset + jn) : make_int4(0, kSegNoRows, kSegNoRows, 0);
+      const int slice = pr.x;
       float m[9];
 #pragma unroll
       for (int k = 0; k < 9; k++) m[k] = __ldg(mats + 9 * (int64_t)slice + k);
       float2* out = proj + a.elements * slice;
 #pragma unroll 1
       for (int side = 0; side < 2; side++) {
+        int vlo, vhi;
+        seg_unpack_rows(side ? pr.z : pr.y, vlo, vhi);
+        if (vlo > vhi) continue;  // no pixel of this side
         const SegBox box = seg_box(m, side, o, B, 0.f);
-        seg_for_each_pixel(box, px, [&](int u, int v, bool valid) {
+        seg_for_each_pixel_rows(box, px, vlo, vhi, [&](int u, int v, bool valid) {
           if (!valid) return;
           ProjSample s = project_sample(m, u, v, 0);
           if ((s.sign < 0.f) != (side == 1)) return;  // the other side's pixel
@@ -313,7 +317,7 @@ project_segment_kernel(const float2* __restrict__ vol, float2* __restrict__ proj
         });
       }
       j = jn;
-      slice = next;
+      pr = nx;
     }
   }
 }
@@ -388,7 +392,7 @@ static int project_brick(const float* d_volumeft, float* d_proj, const float* d_
   if (segments)
     kern<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
         (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, px, plan.items, plan.nitems, plan.pairs,
-        plan.counter, post);
+        plan.bins, plan.counter, post);
   else
     project_brick_kernel<<<sms * std::max(occ, 1), tune.threads, smem, stream>>>(
         (const float2*)d_volumeft, (float2*)d_proj, d_mats, a, g, plan.items, plan.nitems, plan.pairs, plan.bins,

@@ -119,15 +119,31 @@ __device__ __forceinline__ void seg_row(const SegBox& b, const PixelSet& px, int
   ub = min((int)floorf(umax), min(seg_isqrt(rem), px.dimft - 1));
 }
 
+// Row range of a (slice, brick, side) as the plan stores it: vlo in the low
+// and vhi in the high 16 bits; an empty side as vlo = 1, vhi = 0.
+__host__ __device__ __forceinline__ int seg_pack_rows(int vlo, int vhi) {
+  return (int)(((unsigned)vlo & 0xffffu) | ((unsigned)vhi << 16));
+}
+__device__ __forceinline__ void seg_unpack_rows(int packed, int& vlo, int& vhi) {
+  vlo = (int)(short)(packed & 0xffff);
+  vhi = packed >> 16;
+}
+constexpr int kSegNoRows = (int)(1u | (0u << 16));
+
+// A segment plan's pair k: (slice, packed rows of side 0, of side 1, brick).
+__device__ __forceinline__ int4 seg_pair(const PixelBin* __restrict__ bins, const int* __restrict__ pairs,
+                                         int k) {
+  return __ldg(reinterpret_cast<const int4*>(bins + __ldg(pairs + k)));
+}
+
 // Calls f(u, v, valid) once per lane per wave of 32 candidate pixels of the
-// box (valid false on idle lanes of the last wave).  Warp-synchronous: all
-// 32 lanes must call it together with the same box; f may use warp
-// collectives.
+// box in rows vlo .. vhi (from seg_rows; valid false on idle lanes of the
+// last wave).  Warp-synchronous: all 32 lanes must call it together with the
+// same box; f may use warp collectives.
 template <class F>
-__device__ __forceinline__ void seg_for_each_pixel(const SegBox& b, const PixelSet& px, F&& f) {
+__device__ __forceinline__ void seg_for_each_pixel_rows(const SegBox& b, const PixelSet& px, int vlo, int vhi,
+                                                        F&& f) {
   const int lane = threadIdx.x & 31;
-  int vlo, vhi;
-  if (!seg_rows(b, px, vlo, vhi)) return;
   for (int vb = vlo; vb <= vhi; vb += 32) {
     const int v = vb + lane;
     int ua = 1, ub = 0;
@@ -157,6 +173,14 @@ __device__ __forceinline__ void seg_for_each_pixel(const SegBox& b, const PixelS
       f(valid ? ra + (k - rs) : 0, valid ? rv : 0, valid);
     }
   }
+}
+
+// The same, finding the row range first.
+template <class F>
+__device__ __forceinline__ void seg_for_each_pixel(const SegBox& b, const PixelSet& px, F&& f) {
+  int vlo, vhi;
+  if (!seg_rows(b, px, vlo, vhi)) return;
+  seg_for_each_pixel_rows(b, px, vlo, vhi, f);
 }
 
 // The box of brick origin o, edge B, widened by `below` voxels on the low
