@@ -379,20 +379,26 @@ def run_ours(args):
                  "gather_bytes": gather_bytes,
                  "gather_gbs": round(gather_bytes / (proj_ms * 1e-3) / 1e9, 1),
                  "l2_gather_peak_gbs": probe.get("l2_gather_gbs")}
-    # The brick backprojector privatises every FP32 reduction in shared memory,
-    # so its ceiling is the shared-memory FP32 atomic rate; the L2 reduction
-    # rate (the direct kernel's ceiling) is reported beside it.
+    # The segment backprojector privatises every reduction in shared memory
+    # and accumulates most work items in fixed point (int32 shared atomics),
+    # the rest with FP32 ones: its ceiling is the int32 shared-memory atomic
+    # rate, with the FP32 one and the L2 reduction rate (the direct kernel's
+    # ceiling) beside it.
+    i32_peak = probe.get("smem_i32_atomic_gadds")
     smem_peak = probe.get("smem_f32_atomic_gadds")
     l2_peak = probe.get("l2_red_v2_gadds") or probe.get("l2_red_gadds")
     roof_bp = {"kernel": "backproject", "bound": "smem_atomic", "achieved": round(bp_rate, 2),
-               "peak": smem_peak, "unit": "G FP32 reductions/s",
-               "frac": None if not smem_peak else round(bp_rate / smem_peak, 4),
+               "peak": i32_peak, "unit": "G reductions/s",
+               "frac": None if not i32_peak else round(bp_rate / i32_peak, 4),
                "traffic": None if traffic.get("backproject_per_slice") is None
                else int(traffic["backproject_per_slice"] * B),
                "traffic_source": "not measured in this run: ncu dram__bytes_read.sum + dram__bytes_write.sum "
                                  "per slice from profiles/ncu_traffic.json, times the batch",
                "algorithmic_reductions": bp_reds, "ms_per_launch": round(bp_ms, 4),
-               "peak_of": "measured (probe, same run)", "l2_red_peak": l2_peak,
+               "peak_of": "measured int32 shared-memory atomic rate (probe, same run)",
+               "fp32_smem_atomic_peak": smem_peak,
+               "frac_of_fp32_smem_atomic": None if not smem_peak else round(bp_rate / smem_peak, 4),
+               "l2_red_peak": l2_peak,
                "frac_of_l2_red": None if not l2_peak else round(bp_rate / l2_peak, 4)}
     # the same kernel against HBM: its measured DRAM traffic per launch over
     # its launch time, for readers comparing against the copy bandwidth (the

@@ -470,7 +470,8 @@ int gtomrln_set_path(int op, int path) {
   clear_error();
   const bool grid = op == GTOMRLN_OP_GRIDDING;
   if ((op != GTOMRLN_OP_PROJECT && op != GTOMRLN_OP_BACKPROJECT && !grid) || path < GTOMRLN_PATH_AUTO ||
-      (!grid && path > GTOMRLN_PATH_SEGMENT) ||
+      (!grid && path > GTOMRLN_PATH_SEGMENT &&
+       !(op == GTOMRLN_OP_BACKPROJECT && path == GTOMRLN_PATH_SEGMENT_FP32)) ||
       (grid && path != GTOMRLN_PATH_AUTO && path != GTOMRLN_PATH_DIRECT && path != GTOMRLN_PATH_FUSED))
     return set_error(GTOMRLN_ERR_INVALID, "set_path: unknown op %d or path %d", op, path);
   g_path[op].store(path);

@@ -370,13 +370,15 @@ def mlp_param_count() -> int:
 
 
 _OPS = {"project": 0, "backproject": 1, "gridding": 2}
-_PATHS = {"auto": 0, "direct": 1, "brick": 2, "segment": 3, "fused": 4}
+_PATHS = {"auto": 0, "direct": 1, "brick": 2, "segment": 3, "fused": 4, "segment_fp32": 5}
 
 
 def set_path(op: str, path: str) -> None:
     """Selects the implementation of "project" or "backproject" for this
     process: "auto" (default), "direct", "brick" (pixels binned per brick) or
-    "segment" (pixels found per brick by row segments); of "gridding": "auto"
+    "segment" (pixels found per brick by row segments; the backprojector's
+    accumulates each work item in fixed point first), for "backproject" also
+    "segment_fp32" (row segments, FP32 atomics only); of "gridding": "auto"
     or "direct" (cuFFT transforms) or "fused" (two fused passes per iteration
     with the library's own transforms on power-of-two grids)
     (gtomrln_set_path)."""

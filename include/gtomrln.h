@@ -88,6 +88,11 @@ GTOMRLN_API int gtomrln_release_caches(void);
 #define GTOMRLN_PATH_BRICK 2
 #define GTOMRLN_PATH_SEGMENT 3
 #define GTOMRLN_PATH_FUSED 4
+/* op GTOMRLN_OP_BACKPROJECT: the row-segment kernel with FP32 shared-memory
+ * atomics only (GTOMRLN_PATH_SEGMENT and AUTO first accumulate each work
+ * item in fixed point with int32 atomics, at the FP32 path's accuracy, and
+ * fall back to FP32 for an item whose sums could overflow). */
+#define GTOMRLN_PATH_SEGMENT_FP32 5
 GTOMRLN_API int gtomrln_set_path(int op, int path);
 
 /* Extension (no reference counterpart): launch shape of the brick-major
