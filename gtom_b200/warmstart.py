@@ -193,6 +193,108 @@ def make_training_set(weights, ori: int, pad: int = 2, tolerance: float = 1e-6,
                        eligible=torch.cat(elig), converged=conv)
 
 
+@dataclass
+class FeatureRows:
+    """Training rows sampled from many distributions: raw features (n, 28),
+    targets log(Fnw * s) and loss weights (mean 1 per distribution)."""
+    X: torch.Tensor
+    target: torch.Tensor
+    weight: torch.Tensor
+    converged: list = field(default_factory=list)
+
+
+def make_feature_rows(weights, ori: int, pad: int = 2, rows_per_dist: int = 60000, tolerance: float = 1e-6,
+                      max_iterations: int = 5000, momentum: float = 0.9, count: int | None = None,
+                      device="cuda", seed: int = 0) -> FeatureRows:
+    """As make_training_set, but keeping only `rows_per_dist` randomly chosen
+    trained voxels of each distribution, as feature rows, so that thousands
+    of distributions fit in memory (a full stack takes ~100 MB per
+    distribution at P = 256; 60 000 rows take 7 MB)."""
+    P = ori * pad
+    D = P + 1
+    nd = len(weights) if count is None else int(count)
+    dev = torch.device(device)
+    mask = sphere_mask(P, dev)
+    X = torch.zeros((nd * rows_per_dist, N_IN), dtype=torch.float32, device=dev)
+    T = torch.zeros(nd * rows_per_dist, dtype=torch.float32, device=dev)
+    Wt = torch.zeros(nd * rows_per_dist, dtype=torch.float32, device=dev)
+    g = torch.Generator(device=dev)
+    conv = []
+    for d, w in enumerate(weights):
+        fnw, fw, it, ch, _ = gridding_weights(w, (D, D, D), ori, pad, max_iterations, tolerance, momentum)
+        conv.append((it, ch))
+        sel = mask & (fw > 0)
+        idx = torch.nonzero(sel).squeeze(1)
+        if idx.numel() == 0:
+            continue
+        s = float(fw[sel].double().mean())
+        g.manual_seed(seed * 100003 + d)
+        pick = idx[torch.randint(idx.numel(), (rows_per_dist,), generator=g, device=dev)]
+        one = TrainingSet(P=P, fw=fw, target=fnw, weight=fnw, inv_scale=torch.tensor([1.0 / s], device=dev),
+                          eligible=pick)
+        lo = d * rows_per_dist
+        X[lo:lo + rows_per_dist] = volume_features(one, pick)
+        T[lo:lo + rows_per_dist] = torch.log(torch.clamp(fnw[pick] * s, min=math.exp(LOG_FLOOR)))
+        lw = (fw[sel] * fnw[sel]) ** 2
+        m = float(lw.double().mean())
+        if m > 0:
+            Wt[lo:lo + rows_per_dist] = (fw[pick] * fnw[pick]) ** 2 / m
+    return FeatureRows(X=X, target=T, weight=Wt, converged=conv)
+
+
+def init_params_rows(rows: FeatureRows, seed: int = 0, sample: int = 200000) -> torch.Tensor:
+    """init_params on feature rows."""
+    g = torch.Generator(device=rows.X.device)
+    g.manual_seed(seed)
+    pick = torch.randint(rows.X.shape[0], (min(sample, rows.X.shape[0]),), generator=g, device=rows.X.device)
+    f = rows.X[pick].double()
+    mu = f.mean(0)
+    sd = f.std(0).clamp_min(1e-3)
+    rng = np.random.default_rng(seed)
+    p = np.zeros(mlp_param_count(), np.float32)
+    p[:N_IN] = mu.cpu().numpy()
+    p[N_IN:2 * N_IN] = (1.0 / sd).cpu().numpy()
+    o = OFF_W1
+    p[o:o + N_HID * N_IN] = rng.normal(0, math.sqrt(2 / N_IN), N_HID * N_IN)
+    o += N_HID * N_IN + N_HID
+    p[o:o + N_HID * N_HID] = rng.normal(0, math.sqrt(2 / N_HID), N_HID * N_HID)
+    o += N_HID * N_HID + N_HID
+    p[o:o + N_HID] = rng.normal(0, math.sqrt(1 / N_HID), N_HID)
+    return torch.from_numpy(p).to(rows.X.device)
+
+
+def train_rows(rows: FeatureRows, params: torch.Tensor, steps: int = 3000, batch: int = 32768,
+               lr: float = 2e-3, lr_final: float = 1e-4, seed: int = 0, log_every: int = 0) -> list:
+    """train() on feature rows: minibatches gathered from the rows, gradients
+    by the library's hand-written backward kernel (gtomrln_mlp_gradients)."""
+    dev = params.device
+    n = mlp_param_count()
+    grad = torch.zeros(n, dtype=torch.float32, device=dev)
+    m = torch.zeros(n, dtype=torch.float32, device=dev)
+    v = torch.zeros(n, dtype=torch.float32, device=dev)
+    loss = torch.zeros(1, dtype=torch.float32, device=dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    losses = []
+    nr = rows.X.shape[0]
+    for step in range(1, steps + 1):
+        idx = torch.randint(nr, (batch,), generator=g, device=dev)
+        xb, tb, wb = rows.X[idx].contiguous(), rows.target[idx].contiguous(), rows.weight[idx].contiguous()
+        loss.zero_()
+        _lib.call("gtomrln_mlp_gradients", C.c_void_p(params.data_ptr()), C.c_void_p(xb.data_ptr()),
+                  C.c_void_p(tb.data_ptr()), C.c_void_p(wb.data_ptr()), batch, C.c_float(1.0 / batch),
+                  C.c_void_p(grad.data_ptr()), C.c_void_p(loss.data_ptr()), stream)
+        t = (step - 1) / max(1, steps - 1)
+        rate = lr_final + 0.5 * (lr - lr_final) * (1 + math.cos(math.pi * t))
+        _lib.call("gtomrln_mlp_adam", C.c_void_p(params.data_ptr()), C.c_void_p(grad.data_ptr()),
+                  C.c_void_p(m.data_ptr()), C.c_void_p(v.data_ptr()), step, C.c_float(rate),
+                  C.c_float(0.9), C.c_float(0.999), C.c_float(1e-8), stream)
+        if (log_every and step % log_every == 0) or step == steps:
+            losses.append(float(loss.item()))
+    return losses
+
+
 def volume_features(ts: TrainingSet, index: torch.Tensor) -> torch.Tensor:
     """Raw features (n, 28) of stack voxels `index` (int64 CUDA tensor)."""
     n = index.numel()
@@ -404,6 +506,9 @@ def main(argv=None) -> None:
     ap.add_argument("--batch", type=int, default=32768)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--max-voxels", type=int, default=400000, help="trained voxels kept per distribution")
+    ap.add_argument("--rows-per-dist", type=int, default=0,
+                    help="train on this many sampled feature rows per distribution instead of whole stacks "
+                         "(fits thousands of distributions)")
     ap.add_argument("--seed", type=int, default=1004)
     ap.add_argument("--save", action="store_true", help="store the parameters under gtom_b200/data/")
     ap.add_argument("--load", action="store_true", help="evaluate the stored parameters (no training)")
@@ -420,14 +525,23 @@ def main(argv=None) -> None:
             raise SystemExit(f"no stored parameters for box {a.box}")
         return _evaluate_and_report(a, params, held, rep)
     t0 = time.perf_counter()
-    ts = make_training_set((sampling_weights(a.box, d, a.pad) for d in train_d), a.box, a.pad,
-                           count=len(train_d), max_voxels=a.max_voxels)
+    if a.rows_per_dist:
+        ts = make_feature_rows((sampling_weights(a.box, d, a.pad) for d in train_d), a.box, a.pad,
+                               rows_per_dist=a.rows_per_dist, count=len(train_d), seed=a.seed)
+        rep["rows"] = int(ts.X.shape[0])
+    else:
+        ts = make_training_set((sampling_weights(a.box, d, a.pad) for d in train_d), a.box, a.pad,
+                               count=len(train_d), max_voxels=a.max_voxels)
     torch.cuda.synchronize()
     rep["make_training_set_s"] = round(time.perf_counter() - t0, 1)
     rep["reference_iterations_median"] = float(np.median([c[0] for c in ts.converged]))
-    params = init_params(ts, seed=a.seed)
     t0 = time.perf_counter()
-    losses = train(ts, params, steps=a.steps, batch=a.batch, lr=a.lr, log_every=max(1, a.steps // 20))
+    if a.rows_per_dist:
+        params = init_params_rows(ts, seed=a.seed)
+        losses = train_rows(ts, params, steps=a.steps, batch=a.batch, lr=a.lr, log_every=max(1, a.steps // 20))
+    else:
+        params = init_params(ts, seed=a.seed)
+        losses = train(ts, params, steps=a.steps, batch=a.batch, lr=a.lr, log_every=max(1, a.steps // 20))
     torch.cuda.synchronize()
     rep["train_s"] = round(time.perf_counter() - t0, 1)
     rep["losses"] = [round(x, 5) for x in losses]
