@@ -412,6 +412,7 @@ int release_gridding_caches(int dev, unsigned long long ctx);  // gridding.cu
 int release_ctf_plans(int dev, unsigned long long ctx);        // ctf.cu
 int release_brick_orders(int dev, unsigned long long ctx);     // brick_plan.cu
 int release_gridfft_tables(int dev, unsigned long long ctx);   // gridfft.cu
+int release_gridsym_caches(int dev, unsigned long long ctx);   // gridsym.cu
 
 static std::atomic<int> g_path[3] = {{GTOMRLN_PATH_AUTO}, {GTOMRLN_PATH_AUTO}, {GTOMRLN_PATH_AUTO}};
 
@@ -460,6 +461,7 @@ int gtomrln_release_caches(void) {
   if (!st) st = release_ctf_plans(dev, ctx);
   if (!st) st = release_brick_orders(dev, ctx);
   if (!st) st = release_gridfft_tables(dev, ctx);
+  if (!st) st = release_gridsym_caches(dev, ctx);
   if (!st) st = release_scratch(dev, ctx);
   if (st) return st;
   release_stage(dev, ctx);
@@ -472,7 +474,8 @@ int gtomrln_set_path(int op, int path) {
   if ((op != GTOMRLN_OP_PROJECT && op != GTOMRLN_OP_BACKPROJECT && !grid) || path < GTOMRLN_PATH_AUTO ||
       (!grid && path > GTOMRLN_PATH_SEGMENT &&
        !(op == GTOMRLN_OP_BACKPROJECT && path == GTOMRLN_PATH_SEGMENT_FP32)) ||
-      (grid && path != GTOMRLN_PATH_AUTO && path != GTOMRLN_PATH_DIRECT && path != GTOMRLN_PATH_FUSED))
+      (grid && path != GTOMRLN_PATH_AUTO && path != GTOMRLN_PATH_DIRECT && path != GTOMRLN_PATH_FUSED &&
+       path != GTOMRLN_PATH_SYMMETRIC))
     return set_error(GTOMRLN_ERR_INVALID, "set_path: unknown op %d or path %d", op, path);
   g_path[op].store(path);
   return GTOMRLN_OK;

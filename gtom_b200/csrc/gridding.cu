@@ -497,11 +497,13 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   bool warm_live = warm;
   const int T = 256;
   unsigned bc = (unsigned)((g.nc + T - 1) / T);
-  // The fused FFT iteration (gridfft.cu) for power-of-two grids when the
-  // caller chose it; the final map always uses cuFFT.
-  const bool fused = path_choice(GTOMRLN_OP_GRIDDING) == GTOMRLN_PATH_FUSED && !measure_ref &&
-                     gridfft_available(P, 1);
-  bool need_first = true;  // the fused loop starts with the inverse transform along z
+  // The symmetric-spectrum iteration (gridsym.cu) or the fused FFT
+  // iteration (gridfft.cu) for power-of-two grids when the caller chose
+  // one; the final map always uses cuFFT.
+  const int gpath = path_choice(GTOMRLN_OP_GRIDDING);
+  const bool sym = gpath == GTOMRLN_PATH_SYMMETRIC && gridsym_available(P);
+  const bool fused = !sym && gpath == GTOMRLN_PATH_FUSED && !measure_ref && gridfft_available(P, 1);
+  bool need_first = true;  // both start with a transform along z
 
   GTOMRLN_STEP(pool_alloc((void**)&convft, g.nc * sizeof(float2), stream));
   GTOMRLN_STEP(pool_alloc((void**)&conv, g.nr * sizeof(float), stream));
@@ -528,7 +530,13 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   for (int it = 0; it < iterations; it++) {
     // the residual check of a predicted start needs the first change
     double* ch = (opt.tolerance > 0 || measure_ref || (warm_live && it == 0)) ? change : nullptr;
-    if (fused) {
+    if (sym) {
+      if (need_first) GTOMRLN_STEP(gridsym_first(convft, g, 1, Fw, Fnw, momentum ? V : nullptr, stream));
+      need_first = false;
+      if (ch) GTOMRLN_CUDA_TRY(cudaMemsetAsync(ch, 0, sizeof(h_change), stream));
+      GTOMRLN_STEP(gridsym_iteration(convft, g, 1, table, Fw, Fnw, momentum ? V : nullptr, opt.momentum,
+                                     it + 1 < iterations, ch, opt.ref_fnw, stream));
+    } else if (fused) {
       if (need_first) GTOMRLN_STEP(gridfft_first(convft, g, 1, stream));
       need_first = false;
       if (ch) GTOMRLN_CUDA_TRY(cudaMemsetAsync(ch, 0, sizeof(h_change), stream));

@@ -44,6 +44,7 @@
 #include <tuple>
 #include <vector>
 
+#include "fftcore.cuh"
 #include "gridfft.cuh"
 
 namespace cg = cooperative_groups;
@@ -98,53 +99,6 @@ int release_tables(int dev, unsigned long long ctx) {
     it = g_tw.erase(it);
   }
   return GTOMRLN_OK;
-}
-
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(fmaf(a.x, b.x, -(a.y * b.y)), fmaf(a.x, b.y, a.y * b.x));
-}
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-// times -i (forward) or +i (inverse)
-template <bool INV>
-__device__ __forceinline__ float2 mul_mi(float2 a) {
-  return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
-}
-
-// In-register DFT of length R, forward (exp(-2 pi i nk/R)) or inverse.
-template <int R, bool INV>
-__device__ __forceinline__ void dft(float2* v) {
-  if (R == 2) {
-    const float2 t = v[0];
-    v[0] = cadd(t, v[1]);
-    v[1] = csub(t, v[1]);
-  } else if (R == 4) {
-    const float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
-    const float2 a2 = cadd(v[1], v[3]), a3 = mul_mi<INV>(csub(v[1], v[3]));
-    v[0] = cadd(a0, a2);
-    v[2] = csub(a0, a2);
-    v[1] = cadd(a1, a3);
-    v[3] = csub(a1, a3);
-  } else {  // R == 8: two DFT-4 of the even and odd elements, then W8^k
-    float2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
-    dft<4, INV>(e);
-    dft<4, INV>(o);
-    const float h = 0.70710678118654752440f;
-    // W8^1, W8^2, W8^3 (forward: (1-i)/sqrt2, -i, (-1-i)/sqrt2; inverse: conjugates)
-    const float2 o1 = INV ? make_float2((o[1].x - o[1].y) * h, (o[1].x + o[1].y) * h)
-                          : make_float2((o[1].x + o[1].y) * h, (o[1].y - o[1].x) * h);
-    const float2 o2 = mul_mi<INV>(o[2]);
-    const float2 o3 = INV ? make_float2(-(o[3].x + o[3].y) * h, (o[3].x - o[3].y) * h)
-                          : make_float2((o[3].y - o[3].x) * h, -(o[3].x + o[3].y) * h);
-    v[0] = cadd(e[0], o[0]);
-    v[4] = csub(e[0], o[0]);
-    v[1] = cadd(e[1], o1);
-    v[5] = csub(e[1], o1);
-    v[2] = cadd(e[2], o2);
-    v[6] = csub(e[2], o2);
-    v[3] = cadd(e[3], o3);
-    v[7] = csub(e[3], o3);
-  }
 }
 
 // Shared-memory layout of a transform: element i at i + i/8 (one spare
@@ -587,5 +541,7 @@ int gridfft_iteration(float2* data, const GridGeom& g, int count, const float* t
 // Frees the fused transforms' tables of the current context on device dev
 // (gtomrln_release_caches).
 int release_gridfft_tables(int dev, unsigned long long ctx) { return release_tables(dev, ctx); }
+
+int fft_twiddles(int N, const float2** out) { return twiddles(N, out); }
 
 }  // namespace gtomrln

@@ -103,4 +103,29 @@ int gridfft_first(float2* data, const GridGeom& g, int count, cudaStream_t strea
 int gridfft_iteration(float2* data, const GridGeom& g, int count, const float* table, const float* Fw,
                       float* Fnw, float* V, float beta, bool write_next, double* change, cudaStream_t stream);
 
+// Twiddle table e(-2 pi i m / N), m < N, on the current device (built once
+// per device, context and N in double precision; freed by the library's
+// cache release).
+int fft_twiddles(int N, const float2** out);
+
+// ------------------------------------------- symmetric-spectrum path --
+// The iteration on the Hermitian half along z of the real spectrum
+// (gridsym.cu): four passes over a (P/2+1) x P x (P/2+1) complex work array
+// W (which fits in the cuFFT path's spectrum buffer).  Power-of-two grids
+// P = 64 .. 512.
+
+bool gridsym_available(int P);
+// W <- transform along z of S = Fw * Fnw (Fw * V when V is non-null), the
+// start of the loop.
+int gridsym_first(float2* W, const GridGeom& g, int count, const float* Fw, float* Fnw, float* V,
+                  cudaStream_t stream);
+// One iteration: transforms along y, x (with the blob) and y, then along
+// z with the update of Fnw (and V with momentum beta > 0); change (one
+// volume) accumulates the convergence sums when non-null, and with ref also
+// the distance to the reference weights ref; with write_next, W <- the
+// transform along z of the next iteration's Fw * Fnw (Fw * V).
+int gridsym_iteration(float2* W, const GridGeom& g, int count, const float* table, const float* Fw, float* Fnw,
+                      float* V, float beta, bool write_next, double* change, const float* ref,
+                      cudaStream_t stream);
+
 }  // namespace gtomrln

@@ -370,7 +370,7 @@ def mlp_param_count() -> int:
 
 
 _OPS = {"project": 0, "backproject": 1, "gridding": 2}
-_PATHS = {"auto": 0, "direct": 1, "brick": 2, "segment": 3, "fused": 4, "segment_fp32": 5}
+_PATHS = {"auto": 0, "direct": 1, "brick": 2, "segment": 3, "fused": 4, "segment_fp32": 5, "symmetric": 6}
 
 
 def set_path(op: str, path: str) -> None:
@@ -379,8 +379,10 @@ def set_path(op: str, path: str) -> None:
     "segment" (pixels found per brick by row segments; the backprojector's
     accumulates each work item in fixed point first), for "backproject" also
     "segment_fp32" (row segments, FP32 atomics only); of "gridding": "auto"
-    or "direct" (cuFFT transforms) or "fused" (two fused passes per iteration
-    with the library's own transforms on power-of-two grids)
+    or "direct" (cuFFT transforms), "fused" (two fused passes per iteration
+    with the library's own transforms on power-of-two grids) or "symmetric"
+    (four passes over the Hermitian half along z of the real iterated
+    spectrum, the library's own transforms, power-of-two grids)
     (gtomrln_set_path)."""
     _lib.call("gtomrln_set_path", _OPS[op], _PATHS[path])
 

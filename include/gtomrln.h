@@ -93,6 +93,10 @@ GTOMRLN_API int gtomrln_release_caches(void);
  * item in fixed point with int32 atomics, at the FP32 path's accuracy, and
  * fall back to FP32 for an item whose sums could overflow). */
 #define GTOMRLN_PATH_SEGMENT_FP32 5
+/* op GTOMRLN_OP_GRIDDING: each iteration as four streaming passes over the
+ * Hermitian half along z of the (real) iterated spectrum, with the library's
+ * own transforms, on power-of-two grids P = 64 .. 512 (cuFFT elsewhere). */
+#define GTOMRLN_PATH_SYMMETRIC 6
 GTOMRLN_API int gtomrln_set_path(int op, int path);
 
 /* Extension (no reference counterpart): launch shape of the brick-major

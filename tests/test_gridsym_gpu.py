@@ -1,0 +1,144 @@
+"""The symmetric-spectrum gridding iteration (gtom_b200/csrc/gridsym.cu:
+four passes per iteration over the Hermitian half along z of the real
+iterated spectrum, with the library's own transforms) against the cuFFT path
+and the FP64 oracle on the same inputs.
+
+Both paths compute the reference's iteration (RecFourier.cu:158-171); they
+differ only in how the FP32 transforms round, so the weights after one
+iteration agree to ~1e-6 and the maps after 10 iterations to relative L2
+1e-5 (the bar here, tighter than the 1e-4 of reconstructions against the
+reference).  Against the FP64 oracle the bar is the reconstructions' 1e-4."""
+import numpy as np
+import pytest
+import torch
+
+import gtom_b200 as G
+from oracle import oracle as O
+from tests.helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _inputs(ori, pad=2, seed=0):
+    """Centred accumulators of a synthetic backprojection: blob data, smooth
+    positive weights inside the padded sphere (symmetric on the x = 0 plane,
+    as the backprojector's second insertions make them)."""
+    rng = np.random.default_rng(seed + ori)
+    D = ori * pad + 1
+    z, y, x = np.meshgrid(np.arange(D) - D // 2, np.arange(D) - D // 2, np.arange(D // 2 + 1), indexing="ij")
+    r = np.sqrt(x ** 2 + y ** 2 + z ** 2)
+    w = (np.where(r < ori * pad / 2, 1.0 + 30.0 * np.exp(-r / (ori / 3)), 0.0)
+         * rng.uniform(0.8, 1.2, r.shape)).astype(np.float32)
+    w[:, :, 0] = 0.5 * (w[:, :, 0] + w[::-1, ::-1, 0])
+    data = ((rng.normal(size=r.shape) + 1j * rng.normal(size=r.shape)) * w * np.exp(-r / ori)).astype(np.complex64)
+    return data, w, D
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda().reshape(-1)
+
+
+def _on(path, fn):
+    G.set_path("gridding", path)
+    try:
+        out = fn()
+        torch.cuda.synchronize()
+        return out
+    finally:
+        G.set_path("gridding", "auto")
+
+
+@pytest.mark.parametrize("ori", [32, 64, 128, 256])
+def test_symmetric_gridding_matches_cufft(gtom_lib, cuda, ori):
+    data, w, D = _inputs(ori)
+    d_data, d_w = _dev(data), _dev(w)
+    maps = {}
+    for path in ("direct", "symmetric"):
+        out = torch.full((ori ** 3,), float("nan"), device="cuda")
+        _on(path, lambda: G.d_ReconstructGridding(d_data, d_w, out, (ori,) * 3, (D,) * 3, 2, 0, 0, 10))
+        maps[path] = out.cpu().numpy()
+    assert np.all(np.isfinite(maps["symmetric"]))
+    assert rel_l2(maps["symmetric"], maps["direct"]) <= 1e-5
+
+
+@pytest.mark.parametrize("iterations", [1, 3])
+def test_symmetric_weights_match_cufft(gtom_lib, cuda, iterations):
+    """The gridding weights themselves after a few iterations."""
+    ori = 64
+    data, w, D = _inputs(ori, seed=3)
+    d_w = _dev(w)
+    fnw = {}
+    for path in ("direct", "symmetric"):
+        fnw[path] = _on(path, lambda: G.gridding_weights(d_w, (D,) * 3, ori, 2, iterations, 0.0))[0].cpu().numpy()
+    assert rel_l2(fnw["symmetric"], fnw["direct"]) <= 2e-6
+
+
+@pytest.mark.parametrize("ori,iterations", [(16, 10), (24, 3), (32, 10)])
+def test_symmetric_gridding_matches_oracle(gtom_lib, cuda, ori, iterations):
+    """FP64 oracle (numpy pocketfft restatement of RecFourier.cu:98-241);
+    ori 24 is a grid the path does not take (P = 48): cuFFT runs there."""
+    data, w, D = _inputs(ori, seed=7)
+    out = torch.zeros(ori ** 3, device="cuda")
+    _on("symmetric", lambda: G.d_ReconstructGridding(_dev(data), _dev(w), out, (ori,) * 3, (D,) * 3, 2, 0, 0,
+                                                     iterations))
+    ref = O.reconstruct_gridding(data, w, ori, (D, D, D), 2, iterations=iterations)
+    assert rel_l2(out.cpu().numpy().reshape(ori, ori, ori), ref) <= 1e-4
+
+
+@pytest.mark.parametrize("momentum", [0.0, 0.9])
+def test_symmetric_long_runs_match_cufft(gtom_lib, cuda, momentum):
+    """60 iterations (plain and with momentum), then to a change of 1e-4:
+    the two paths may stop one iteration apart, and one iteration moves the
+    weights by ~1e-4, so the stopped maps agree to 1e-3."""
+    ori = 64
+    data, w, D = _inputs(ori, seed=5)
+    d_data, d_w = _dev(data), _dev(w)
+    res = {}
+    for path in ("direct", "symmetric"):
+        fixed = torch.zeros(ori ** 3, device="cuda")
+        _on(path, lambda: G.reconstruct_gridding_warm(d_data, d_w, fixed, (ori,) * 3, (D,) * 3, None, 2, 60, 0.0,
+                                                      momentum))
+        out = torch.zeros(ori ** 3, device="cuda")
+        it, ch, _ = _on(path, lambda: G.reconstruct_gridding_warm(d_data, d_w, out, (ori,) * 3, (D,) * 3, None, 2,
+                                                                  400, 1e-4, momentum))
+        res[path] = (it, ch, out.cpu().numpy(), fixed.cpu().numpy())
+    assert rel_l2(res["symmetric"][3], res["direct"][3]) <= 1e-4
+    assert abs(res["symmetric"][0] - res["direct"][0]) <= 1
+    assert res["symmetric"][1] <= 1e-4 and res["direct"][1] <= 1e-4
+    assert rel_l2(res["symmetric"][2], res["direct"][2]) <= 1e-3
+
+
+def test_symmetric_distance_to_reference_weights(gtom_lib, cuda):
+    """The distance measure ||Fw (Fnw - ref)|| / ||Fw ref|| accumulated by
+    the z pass equals the cuFFT path's update kernel's, and stops the loop at
+    the same iteration (within one)."""
+    ori = 64
+    data, w, D = _inputs(ori, seed=9)
+    d_w = _dev(w)
+    ref = _on("direct", lambda: G.gridding_weights(d_w, (D,) * 3, ori, 2, 400, 0.0, momentum=0.9))[0]
+    got = {}
+    for path in ("direct", "symmetric"):
+        got[path] = _on(path, lambda: G.gridding_weights(d_w, (D,) * 3, ori, 2, 1000, 0.0, ref_fnw=ref,
+                                                         ref_tolerance=1e-2, return_distance=True))
+    it_d, it_s = got["direct"][2], got["symmetric"][2]
+    assert abs(it_d - it_s) <= 1 and it_d < 1000
+    assert got["symmetric"][5] <= 1e-2
+
+
+def test_symmetric_warm_start(gtom_lib, cuda):
+    """The learned start (the committed 128^3 network) on the symmetric
+    path: same decision on the predicted start and the same map as cuFFT's
+    within the long-run bar."""
+    from gtom_b200 import warmstart as WS
+    ori = 64
+    data, w, D = _inputs(ori, seed=11)
+    d_data, d_w = _dev(data), _dev(w)
+    params = WS.load_params(128, torch.device("cuda"))
+    res = {}
+    for path in ("direct", "symmetric"):
+        out = torch.zeros(ori ** 3, device="cuda")
+        it, ch, used = _on(path, lambda: G.reconstruct_gridding_warm(d_data, d_w, out, (ori,) * 3, (D,) * 3, params,
+                                                                     2, 30, 0.0, 0.9))
+        res[path] = (used, out.cpu().numpy())
+    assert res["symmetric"][0] == res["direct"][0]
+    assert rel_l2(res["symmetric"][1], res["direct"][1]) <= 1e-4
