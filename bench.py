@@ -513,11 +513,39 @@ def time_gridding(G, torch, acc_ft, acc_w, n, D, dev):
     b.record()
     torch.cuda.synchronize()
     ms10 = a.elapsed_time(b)
+    a.record()
+    G.d_ReconstructGridding(acc_ft, acc_w, out, (n,) * 3, (D,) * 3, PAD, 0, 0, 1)
+    b.record()
+    torch.cuda.synchronize()
+    ms1 = a.elapsed_time(b)
     P = n * PAD
     nc, nr = (P // 2 + 1) * P * P, P ** 3
     compulsory = 12 * nc + 8 * nr
-    res = {"ms_10_iterations": round(ms10, 3), "P": P, "compulsory_bytes_per_iteration": compulsory,
-           "to_1e-4": {}}
+    # the default path on this grid: four passes over the (P/2+1) x P x
+    # (P/2+1) complex work array W (16 B per element each) plus Fw in and Fnw
+    # in and out (12 B per spectrum element) per iteration
+    nw = (P // 2 + 1) * P * (P // 2 + 1)
+    sym_bytes = 4 * 16 * nw + 12 * nc
+    per_it = (ms10 - ms1) / 9
+    res = {"ms_10_iterations": round(ms10, 3), "ms_per_iteration": round(per_it, 4), "P": P,
+           "path": "symmetric (four passes over the Hermitian half along z)" if P in (64, 128, 256, 512) else "cufft",
+           "compulsory_bytes_per_iteration": compulsory, "path_bytes_per_iteration": sym_bytes,
+           "path_gbs": round(sym_bytes / (per_it * 1e-3) / 1e9, 1), "to_1e-4": {}}
+    hbm, hbm_kind = measured_peaks()
+    res["path_frac_of_hbm"] = round(sym_bytes / (per_it * 1e-3) / 1e9 / hbm, 4)
+    res["hbm_peak"] = {"gbs": hbm, "of": hbm_kind}
+    # the cuFFT path (GTOMRLN_PATH_DIRECT) on the same accumulators, for scale
+    G.set_path("gridding", "direct")
+    try:
+        G.d_ReconstructGridding(acc_ft, acc_w, out, (n,) * 3, (D,) * 3, PAD, 0, 0, 1)
+        torch.cuda.synchronize()
+        a.record()
+        G.d_ReconstructGridding(acc_ft, acc_w, out, (n,) * 3, (D,) * 3, PAD, 0, 0, 10)
+        b.record()
+        torch.cuda.synchronize()
+        res["ms_10_iterations_cufft"] = round(a.elapsed_time(b), 3)
+    finally:
+        G.set_path("gridding", "auto")
     # to a relative change of 1e-4: the reference's update from its sphere-mask
     # start, the momentum update, and both from the learned start (the
     # network trained at 128^3; its inputs are scale- and radius-normalised)

@@ -24,6 +24,7 @@ struct GridBatch {
   cufftHandle r2c = 0, c2r = 0;
   const float* table = nullptr;
   bool fused = false;  // the fused FFT iteration is prepared (outside any capture) and available
+  bool sym = false;    // the symmetric-spectrum iteration is prepared (outside any capture) and available
 };
 
 // Allocates the stacks (cudaMalloc) and makes the batched plans.

@@ -497,11 +497,11 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   bool warm_live = warm;
   const int T = 256;
   unsigned bc = (unsigned)((g.nc + T - 1) / T);
-  // The symmetric-spectrum iteration (gridsym.cu) or the fused FFT
-  // iteration (gridfft.cu) for power-of-two grids when the caller chose
-  // one; the final map always uses cuFFT.
+  // The symmetric-spectrum iteration (gridsym.cu; default on power-of-two
+  // grids P = 64 .. 512) or, when the caller chose it, the fused FFT
+  // iteration (gridfft.cu); cuFFT transforms otherwise and for the final map.
   const int gpath = path_choice(GTOMRLN_OP_GRIDDING);
-  const bool sym = gpath == GTOMRLN_PATH_SYMMETRIC && gridsym_available(P);
+  const bool sym = (gpath == GTOMRLN_PATH_SYMMETRIC || gpath == GTOMRLN_PATH_AUTO) && gridsym_available(P);
   const bool fused = !sym && gpath == GTOMRLN_PATH_FUSED && !measure_ref && gridfft_available(P, 1);
   bool need_first = true;  // both start with a transform along z
 
@@ -632,6 +632,11 @@ int gridding_batch_prepare(GridBatch* gb, int count, int ori, int pad, double bl
   // decided (and its tables and kernel attributes set up) here, outside the
   // stream capture of gridding_batch_run
   b.fused = gridfft_available(b.P, count);
+  b.sym = gridsym_available(b.P);
+  if (b.sym) {
+    st = gridsym_prepare(b.P);
+    if (st) return st;
+  }
   *gb = b;  // so that gridding_batch_free releases what was made on failure
   GTOMRLN_CUDA_TRY(cudaMalloc(&gb->convft, count * nc * sizeof(float2)));
   GTOMRLN_CUDA_TRY(cudaMalloc(&gb->conv, count * nr * sizeof(float)));
@@ -676,14 +681,22 @@ int gridding_batch_run(const GridBatch& b, const float2* data, const float* weig
   const int T = 256;
   dim3 gc((unsigned)((g.nc + T - 1) / T), (unsigned)b.count);
   int st = GTOMRLN_OK;
-  const bool fused = b.fused && path_choice(GTOMRLN_OP_GRIDDING) == GTOMRLN_PATH_FUSED;
+  const int gpath = path_choice(GTOMRLN_OP_GRIDDING);
+  const bool sym = b.sym && (gpath == GTOMRLN_PATH_AUTO || gpath == GTOMRLN_PATH_SYMMETRIC);
+  const bool fused = !sym && b.fused && gpath == GTOMRLN_PATH_FUSED;
   GTOMRLN_CUFFT_TRY(cufftSetStream(b.r2c, stream));
   GTOMRLN_CUFFT_TRY(cufftSetStream(b.c2r, stream));
   grid_init_kernel<<<gc, T, 0, stream>>>(weight, b.D, b.D, b.D, b.Fw, b.Fnw, b.convft, g, maskr2,
                                          iterations > 0, b.wstride);
   GTOMRLN_STEP(launch_check("grid_init_kernel"));
   if (fused && iterations > 0) GTOMRLN_STEP(gridfft_first(b.convft, g, b.count, stream));
+  if (sym && iterations > 0) GTOMRLN_STEP(gridsym_first(b.convft, g, b.count, b.Fw, b.Fnw, nullptr, stream));
   for (int it = 0; it < iterations; it++) {
+    if (sym) {
+      GTOMRLN_STEP(gridsym_iteration(b.convft, g, b.count, b.table, b.Fw, b.Fnw, nullptr, 0.f,
+                                     it + 1 < iterations, nullptr, nullptr, stream));
+      continue;
+    }
     if (fused) {
       GTOMRLN_STEP(gridfft_iteration(b.convft, g, b.count, b.table, b.Fw, b.Fnw, nullptr, 0.f,
                                      it + 1 < iterations, nullptr, stream));

@@ -49,13 +49,16 @@ __device__ __forceinline__ float grid_update_value(float c, float old) {
 
 // The same update applied at the extrapolated point v (momentum in the
 // logarithm of the weights): nw = min(1e20, v / max(1e-4, c)) and the next
-// extrapolation ext = min(1e20, nw (nw / old)^beta).
+// extrapolation ext = min(1e20, nw (nw / old)^beta).  The extrapolation is a
+// heuristic of this library (its fixed points are the plain update's), so
+// its power runs on the fast intrinsics (__fdividef, __powf: relative error
+// ~1e-6 on ratios near 1); the update itself keeps the reference's division.
 __device__ __forceinline__ void grid_update_momentum_value(float c, float old, float v, float beta, float& nw,
                                                            float& ext) {
   const float w = fmaxf(1e-4f, c);
   nw = fminf(1e20f, v / w);
   ext = nw;
-  if (old > 0.f && nw > 0.f) ext = fminf(1e20f, nw * powf(nw / old, beta));
+  if (old > 0.f && nw > 0.f) ext = fminf(1e20f, nw * __powf(__fdividef(nw, old), beta));
 }
 
 // Adds the block's (d2, o2) to change[0..1] (one atomic pair per block).
@@ -115,6 +118,9 @@ int fft_twiddles(int N, const float2** out);
 // P = 64 .. 512.
 
 bool gridsym_available(int P);
+// Launch attributes and twiddle table of grid P on the current device, made
+// ahead of a stream capture (later calls only look them up).
+int gridsym_prepare(int P);
 // W <- transform along z of S = Fw * Fnw (Fw * V when V is non-null), the
 // start of the loop.
 int gridsym_first(float2* W, const GridGeom& g, int count, const float* Fw, float* Fnw, float* V,

@@ -37,14 +37,24 @@
 // element): 2.97 GB at P = 512, against ~8 GB for cuFFT's passes plus the
 // blob and update kernels.
 //
-// The real transforms of length P run as complex transforms of length P/2
-// on the packed pairs (x(2n), x(2n+1)) with the usual pre- and post-
-// twiddles; the complex transforms are Stockham radix-8 (radix-4/2 last
-// stage) FFTs over 16 columns in shared memory (element n of column c at
-// n * 17 + c: conflict-free for the column-wise stages and for the row-wise
-// loads of the x pass), 16 threads per column, twiddles read from a table
-// e(-m/P) computed in double precision.  All transforms are unnormalised,
-// as cuFFT's; the 1/P^3 of the reference's C2R rides with the blob.
+// Transforms.  A real transform of length P runs as a complex transform of
+// length H = P/2 on the packed pairs (x(2n), x(2n+1)) with the usual pre-
+// and post-twiddles.  A complex transform of length N = N1 N2 is a four-step
+// FFT over N2 threads per column: thread t holds the elements t + N2 m
+// (m < N1) in registers, loaded straight from HBM; it transforms them with an
+// in-register N1-point DFT, multiplies by e(-+ t k1 / N), exchanges through
+// shared memory once (each thread then holds N1/N2 values of k1 for all N2
+// threads' elements), and finishes with N1/N2 in-register N2-point DFTs, which
+// leaves it holding the outputs t + N2 m again: loads and stores take the
+// same coalesced pattern and the data crosses shared memory once per
+// transform.  In the x pass the N2 threads of a row are consecutive lanes of
+// one warp, so its exchanges need only the warp and the partners k, H - k of
+// the pre- and post-twiddles are shuffles; in the y and z passes the lanes
+// run over 16 consecutive columns (coalesced along x).  Twiddles come from a
+// table e(-m/P) computed in double precision (runtime factors) and from
+// compile-time constants (inside the in-register DFTs).  All transforms are
+// unnormalised, as cuFFT's; the 1/P^3 of the reference's C2R rides with the
+// blob.
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -58,12 +68,80 @@ namespace gtomrln {
 
 namespace {
 
-constexpr int kCols = 16;          // columns (rows in the x pass) per CTA
-constexpr int kPitch = kCols + 1;  // shared-memory stride of element index n, in float2
-constexpr int kThreads = 256;      // 16 threads per column
+constexpr int kCols = 16;          // columns (y and z passes) or rows (x pass) per CTA
+constexpr int kPitch = kCols + 1;  // shared-memory stride between element indices (y, z passes), in float2
 
-// Twiddle e(-m/N) (forward) or e(+m/N) (INV) of an N-point transform from
-// the table e(-j/P) of the working grid, N = P/S.
+// ---------------------------------------------- compile-time twiddles --
+constexpr double kPiD = 3.14159265358979323846264338327950288;
+
+// sin and cos by their Taylor series after reduction to [-pi, pi] (the
+// remaining error is far below FP32 rounding); compile-time only.
+constexpr double ce_sin(double x) {
+  while (x > kPiD) x -= 2 * kPiD;
+  while (x < -kPiD) x += 2 * kPiD;
+  double term = x, sum = x;
+  for (int k = 1; k < 20; k++) {
+    term *= -x * x / ((2.0 * k) * (2.0 * k + 1.0));
+    sum += term;
+  }
+  return sum;
+}
+constexpr double ce_cos(double x) { return ce_sin(x + kPiD / 2); }
+
+// In-register DFT of length N (power of two), unnormalised, forward
+// (exp(-)) or inverse (exp(+)), natural order in and out: radix-2
+// decimation in time down to the radix-8/4/2 kernels of fftcore.cuh, with
+// the combining twiddles as constants.
+template <int N, bool INV>
+__device__ __forceinline__ void dftr(float2* v) {
+  if constexpr (N <= 8) {
+    dft<N, INV>(v);
+  } else {
+    float2 e[N / 2], o[N / 2];
+#pragma unroll
+    for (int i = 0; i < N / 2; i++) {
+      e[i] = v[2 * i];
+      o[i] = v[2 * i + 1];
+    }
+    dftr<N / 2, INV>(e);
+    dftr<N / 2, INV>(o);
+#pragma unroll
+    for (int k = 0; k < N / 2; k++) {
+      const float wr = (float)ce_cos(2 * kPiD * k / N);
+      const float wi = (float)(INV ? ce_sin(2 * kPiD * k / N) : -ce_sin(2 * kPiD * k / N));
+      const float2 t = k == 0 ? o[0] : cmul(o[k], make_float2(wr, wi));
+      v[k] = cadd(e[k], t);
+      v[k + N / 2] = csub(e[k], t);
+    }
+  }
+}
+
+// ------------------------------------------------------ four-step FFT --
+// N = N1 N2 with N2 threads per column and N1 a multiple of N2.
+template <int N>
+struct Split;
+template <>
+struct Split<32> {
+  static constexpr int N1 = 8, N2 = 4;
+};
+template <>
+struct Split<64> {
+  static constexpr int N1 = 8, N2 = 8;
+};
+template <>
+struct Split<128> {
+  static constexpr int N1 = 16, N2 = 8;
+};
+template <>
+struct Split<256> {
+  static constexpr int N1 = 16, N2 = 16;
+};
+template <>
+struct Split<512> {
+  static constexpr int N1 = 32, N2 = 16;
+};
+
+// Runtime twiddle e(-m/N) (or e(+m/N), INV) from the table e(-j/P), N = P/S.
 template <int S, bool INV>
 __device__ __forceinline__ float2 twiddle(const float2* tw, int m) {
   float2 w = tw[m * S];
@@ -71,134 +149,88 @@ __device__ __forceinline__ float2 twiddle(const float2* tw, int m) {
   return w;
 }
 
-template <int N, int Ns>
-constexpr int stage_radix() {
-  return N / Ns >= 8 ? 8 : N / Ns;
+// Shared-memory places of the exchange: element (k1, n2) of the transform of
+// column c.  Columns-fast (y, z passes: lanes run over 16 columns and two
+// threads, each half-warp's access contiguous) or rows (x pass: lanes run
+// over the N2 threads of a row, each row in its own block; the odd stride
+// N1 + 1 keeps both the write and the read conflict-free).
+template <int N1, int N2, bool ROWS>
+__device__ __forceinline__ int xplace(int k1, int n2, int c) {
+  if constexpr (ROWS)
+    return c * (N2 * (N1 + 1)) + n2 * (N1 + 1) + k1;
+  else
+    return (n2 * N1 + k1) * kPitch + c;
 }
 
-// Stockham stages from sub-transform length Ns on over the CTA's 16
-// columns (column c, thread t of the column's 16): each butterfly reads R
-// elements, applies the twiddles and a radix-R DFT, and writes its R
-// outputs to their sorted places; all reads of a stage precede all its
-// writes (barrier), so the transform runs in place.
-template <int N, int S, bool INV, int Ns>
-__device__ __forceinline__ void fft_stages(float2* s, const float2* tw, int c, int t) {
-  if constexpr (Ns < N) {
-    constexpr int R = stage_radix<N, Ns>();
-    constexpr int NB = N / R;                    // butterflies per column
-    constexpr int Q = (NB + kCols - 1) / kCols;  // per thread
-    float2 v[Q][R];
+// The four-step transform of one column (thread t of its N2 threads holds
+// elements t + N2 m in v[m]; afterwards outputs t + N2 m in v[m]).  ROWS:
+// the column's threads share a warp and synchronise as a warp; else the
+// block synchronises (every thread of the block must call it).  Begins with
+// a barrier, so the exchange buffer may still be in use by the caller.
+template <int N, bool INV, bool ROWS, int S>
+__device__ __forceinline__ void four_step(float2* v, float2* xb, const float2* tw, int t, int c) {
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2, J = N1 / N2;
+  dftr<N1, INV>(v);
 #pragma unroll
-    for (int q = 0; q < Q; q++) {
-      const int j = t + kCols * q;
-      if (NB % kCols == 0 || j < NB) {
+  for (int k1 = 1; k1 < N1; k1++) v[k1] = cmul(v[k1], twiddle<S, INV>(tw, t * k1));
+  if (ROWS) __syncwarp(); else __syncthreads();
 #pragma unroll
-        for (int r = 0; r < R; r++) v[q][r] = s[(j + r * NB) * kPitch + c];
-        const int k = j & (Ns - 1);
+  for (int k1 = 0; k1 < N1; k1++) xb[xplace<N1, N2, ROWS>(k1, t, c)] = v[k1];
+  if (ROWS) __syncwarp(); else __syncthreads();
 #pragma unroll
-        for (int r = 1; r < R; r++) v[q][r] = cmul(v[q][r], twiddle<S, INV>(tw, r * k * (N / (Ns * R))));
-        dft<R, INV>(v[q]);
-      }
-    }
-    __syncthreads();
+  for (int j = 0; j < J; j++) {
+    float2 u[N2];
 #pragma unroll
-    for (int q = 0; q < Q; q++) {
-      const int j = t + kCols * q;
-      if (NB % kCols == 0 || j < NB) {
-        const int k = j & (Ns - 1);
-        const int d = (j - k) * R + k;
+    for (int n2 = 0; n2 < N2; n2++) u[n2] = xb[xplace<N1, N2, ROWS>(t + N2 * j, n2, c)];
+    dftr<N2, INV>(u);
 #pragma unroll
-        for (int r = 0; r < R; r++) s[(d + r * Ns) * kPitch + c] = v[q][r];
-      }
-    }
-    __syncthreads();
-    fft_stages<N, S, INV, Ns * R>(s, tw, c, t);
+    for (int k2 = 0; k2 < N2; k2++) v[j + J * k2] = u[k2];
   }
 }
 
-// N-point transforms (unnormalised; INV: exp(+)) of the 16 columns.  The
-// data must be in place (barrier before); ends with a barrier.
-template <int N, int S, bool INV>
-__device__ __forceinline__ void fft_cols(float2* s, const float2* tw, int c, int t) {
-  fft_stages<N, S, INV, 1>(s, tw, c, t);
+// The pre-twiddle of a Hermitian-to-real transform of length P = 2H as an
+// H-point complex transform: Z(k) = (X(k) + conj X(H-k)) + i e(sg k/P)
+// (X(k) - conj X(H-k)) (sg = +1: the inverse C2R; -1: the forward sum); the
+// H-point transform of the same sign then gives x(2n) = Re z(n),
+// x(2n+1) = Im z(n).
+template <bool PLUS>
+__device__ __forceinline__ float2 c2r_pre(float2 xk, float2 xm, float2 w) {
+  if (PLUS) w.y = -w.y;  // the table holds e(-k/P)
+  const float2 a = make_float2(xk.x + xm.x, xk.y - xm.y);  // X(k) + conj X(H-k)
+  const float2 b = make_float2(xk.x - xm.x, xk.y + xm.y);  // X(k) - conj X(H-k)
+  const float2 wb = cmul(w, b);
+  return make_float2(a.x - wb.y, a.y + wb.x);  // a + i wb
 }
 
-// Pre-twiddle of a Hermitian-to-real transform of length P computed as a
-// complex transform of length H = P/2: from the half spectrum X(0..H) of a
-// column, Z(k) = (X(k) + conj X(H-k)) + i e(sg k/P) (X(k) - conj X(H-k)),
-// k < H (sg = +1: the inverse C2R, sg = -1: the forward sum).  The H-point
-// transform of the same sign then gives x(2n) = Re z(n), x(2n+1) = Im z(n).
-// In place; thread t of the column takes the pairs (k, H-k), k <= H/2.
-template <int H, bool PLUS>
-__device__ __forceinline__ void c2r_pre(float2* s, const float2* tw, int c, int t) {
-  for (int k = t; k <= H / 2; k += kCols) {
-    const float2 xk = s[k * kPitch + c], xm = s[(H - k) * kPitch + c];
-    // e(sg k/P) with sg = +1 for PLUS, -1 otherwise; the table holds e(-j/P)
-    float2 w = tw[k];
-    if (PLUS) w.y = -w.y;
-    {
-      const float2 a = make_float2(xk.x + xm.x, xk.y - xm.y);  // X(k) + conj X(H-k)
-      const float2 b = make_float2(xk.x - xm.x, xk.y + xm.y);  // X(k) - conj X(H-k)
-      const float2 wb = cmul(w, b);
-      s[k * kPitch + c] = make_float2(a.x - wb.y, a.y + wb.x);  // a + i wb
-    }
-    if (k != 0 && 2 * k != H) {
-      // the partner H-k: e(sg (H-k)/P) = -conj e(sg k/P)
-      const float2 w2 = make_float2(-w.x, w.y);
-      const float2 a = make_float2(xm.x + xk.x, xm.y - xk.y);
-      const float2 b = make_float2(xm.x - xk.x, xm.y + xk.y);
-      const float2 wb = cmul(w2, b);
-      s[(H - k) * kPitch + c] = make_float2(a.x - wb.y, a.y + wb.x);
-    }
-  }
-  __syncthreads();
-}
-
-// Post-twiddle of a real-to-Hermitian transform of length P computed as a
-// complex transform of length H of the packed pairs z(n) = x(2n) + i x(2n+1):
-// Y(k) = (Z(k) + conj Z(H-k)) / 2 - (i/2) e(sg k/P) (Z(k) - conj Z(H-k)),
-// k = 0 .. H (Z indices mod H; sg = -1: the forward R2C, sg = +1: the
-// transform with exp(+)).  In place, Y(H) into row H.
-template <int H, bool PLUS>
-__device__ __forceinline__ void r2c_post(float2* s, const float2* tw, int c, int t) {
-  for (int k = t; k <= H / 2; k += kCols) {
-    const int km = k == 0 ? 0 : H - k;
-    const float2 zk = s[k * kPitch + c], zm = s[km * kPitch + c];
-    float2 w = tw[k];
-    if (PLUS) w.y = -w.y;
-    {
-      const float2 a = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));  // (Z(k) + conj Z(H-k)) / 2
-      const float2 b = make_float2(0.5f * (zk.x - zm.x), 0.5f * (zk.y + zm.y));  // (Z(k) - conj Z(H-k)) / 2
-      const float2 wb = cmul(w, b);
-      s[k * kPitch + c] = make_float2(a.x + wb.y, a.y - wb.x);  // a - i wb
-    }
-    // partner: H-k (k > 0), or H itself for k = 0, with e(sg (H-k)/P) = -conj e(sg k/P)
-    if (2 * k != H) {
-      const int kp = H - k;
-      const float2 w2 = make_float2(-w.x, w.y);
-      const float2 a = make_float2(0.5f * (zm.x + zk.x), 0.5f * (zm.y - zk.y));
-      const float2 b = make_float2(0.5f * (zm.x - zk.x), 0.5f * (zm.y + zk.y));
-      const float2 wb = cmul(w2, b);
-      s[kp * kPitch + c] = make_float2(a.x + wb.y, a.y - wb.x);
-    }
-  }
-  __syncthreads();
+// The post-twiddle of a real-to-Hermitian transform of length P computed as
+// an H-point complex transform of the packed pairs: Y(k) = (Z(k) + conj
+// Z(H-k)) / 2 - (i/2) e(sg k/P) (Z(k) - conj Z(H-k)) (Z indices mod H;
+// sg = -1: the forward R2C; +1: exp(+)).  Y(H) = Re Z(0) - Im Z(0).
+template <bool PLUS>
+__device__ __forceinline__ float2 r2c_post(float2 zk, float2 zm, float2 w) {
+  if (PLUS) w.y = -w.y;
+  const float2 a = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+  const float2 b = make_float2(0.5f * (zk.x - zm.x), 0.5f * (zk.y + zm.y));
+  const float2 wb = cmul(w, b);
+  return make_float2(a.x + wb.y, a.y - wb.x);  // a - i wb
 }
 
 __device__ __forceinline__ void load_twiddles(float2* tw, const float2* __restrict__ twg, int P) {
   for (int m = threadIdx.x; m < P; m += blockDim.x) tw[m] = __ldg(twg + m);
 }
 
-// The transform along y of W (INV: exp(+), the inverse of the C2R; else
-// the forward of the R2C).  Grid: (tiles, volumes); tiles are 16
-// consecutive x < P/2 at one z, then x = P/2 at 16 consecutive z.
+// ------------------------------------------------------------ y pass --
+// The transform along y of W (INV: exp(+), the inverse of the C2R; else the
+// forward of the R2C).  Grid: (tiles, volumes); tiles are 16 consecutive
+// x < P/2 at one z, then x = P/2 at 16 consecutive z.  16 N2 threads.
 template <int P, bool INV>
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kCols * Split<P>::N2, 2)
 gridsym_y_kernel(float2* __restrict__ W, const float2* __restrict__ twg) {
   constexpr int H = P / 2, R = H + 1;
+  constexpr int N1 = Split<P>::N1, N2 = Split<P>::N2;
   extern __shared__ float2 smem[];
   float2* tw = smem;
-  float2* s = smem + P;
+  float2* xb = smem + P;
   load_twiddles(tw, twg, P);
   const int c = threadIdx.x & (kCols - 1), t = threadIdx.x / kCols;
   constexpr int kMain = (H / kCols) * (H + 1);
@@ -216,76 +248,70 @@ gridsym_y_kernel(float2* __restrict__ W, const float2* __restrict__ twg) {
     cs = (int64_t)P * R;
     ncols = min(kCols, H + 1 - z0);
   }
-  float2* col = W + (int64_t)blockIdx.y * ((int64_t)(H + 1) * P * R) + base + c * cs;
   const bool in = c < ncols;
-  constexpr int U = P / kCols;  // elements per thread
-  constexpr int UB = U < 8 ? U : 8;
+  float2* col = W + (int64_t)blockIdx.y * ((int64_t)(H + 1) * P * R) + base + (in ? c * cs : 0);
+  float2 v[N1];
 #pragma unroll
-  for (int u0 = 0; u0 < U; u0 += UB) {
-    float2 v[UB];
-#pragma unroll
-    for (int u = 0; u < UB; u++) v[u] = in ? col[(int64_t)(t + kCols * (u0 + u)) * R] : make_float2(0.f, 0.f);
-#pragma unroll
-    for (int u = 0; u < UB; u++) s[(t + kCols * (u0 + u)) * kPitch + c] = v[u];
-  }
-  __syncthreads();
-  fft_cols<P, 1, INV>(s, tw, c, t);
+  for (int m = 0; m < N1; m++) v[m] = in ? col[(int64_t)(t + N2 * m) * R] : make_float2(0.f, 0.f);
+  __syncthreads();  // twiddles in place
+  four_step<P, INV, false, 1>(v, xb, tw, t, c);
   if (in) {
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      const int n = t + kCols * u;
-      col[(int64_t)n * R] = s[n * kPitch + c];
-    }
+    for (int m = 0; m < N1; m++) col[(int64_t)(t + N2 * m) * R] = v[m];
   }
 }
 
+// ------------------------------------------------------------ x pass --
 // Per row (y, z), z <= P/2: C2R along x, times blob(r) / P^3, R2C along x.
-// Grid: ((P/2 + 1) P / 16, volumes); a CTA takes 16 consecutive rows.
+// Grid: ((P/2 + 1) P / 16, volumes); a CTA takes 16 consecutive rows, the
+// N2 threads of a row consecutive lanes.
 template <int P>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kCols * Split<P / 2>::N2, 3)
 gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const float* __restrict__ table,
                  float inv_n, float funcsampling) {
   constexpr int H = P / 2, R = H + 1;
+  constexpr int N1 = Split<H>::N1, N2 = Split<H>::N2;
   extern __shared__ float2 smem[];
   float2* tw = smem;
-  float2* s = smem + P;
-  float* stab = reinterpret_cast<float*>(s + (H + 1) * kPitch);
+  float2* xb = smem + P;
   load_twiddles(tw, twg, P);
-  for (int i = threadIdx.x; i < kBlobSamples; i += blockDim.x) stab[i] = __ldg(table + i);
-  const int c = threadIdx.x & (kCols - 1), t = threadIdx.x / kCols;
-  const int64_t row0 = (int64_t)blockIdx.x * kCols;
-  float2* rows = W + (int64_t)blockIdx.y * ((int64_t)(H + 1) * P * R) + row0 * R;
-  // the 16 rows are 16 R consecutive elements
-  constexpr int E = kCols * R;
-  for (int e0 = 0; e0 < E; e0 += 4 * kThreads) {
-    float2 v[4];
+  const int t = threadIdx.x % N2, r = threadIdx.x / N2;
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned partner = (lane & ~(unsigned)(N2 - 1)) | ((unsigned)(N2 - t) & (N2 - 1));
+  const int64_t rg = (int64_t)blockIdx.x * kCols + r;  // z * P + y
+  float2* row = W + (int64_t)blockIdx.y * ((int64_t)(H + 1) * P * R) + rg * R;
+  float2 v[N1];
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const int e = e0 + u * kThreads + threadIdx.x;
-      if (e < E) v[u] = rows[e];
+  for (int m = 0; m < N1; m++) v[m] = row[t + N2 * m];
+  const float2 xH = t == 0 ? row[H] : make_float2(0.f, 0.f);
+  __syncthreads();  // twiddles in place
+  // pre-twiddle of the C2R: the partner H - k of k = t + N2 m is element
+  // N1-1-m of thread N2-t (t > 0), or element N1-m (H for m = 0) of thread 0
+  // (into a second array: the partners' elements are read after this
+  // thread's own have been replaced)
+  {
+    float2 z[N1];
+#pragma unroll
+    for (int m = 0; m < N1; m++) {
+      const float2 sh = make_float2(__shfl_sync(0xffffffffu, v[N1 - 1 - m].x, partner),
+                                    __shfl_sync(0xffffffffu, v[N1 - 1 - m].y, partner));
+      const float2 xm = t != 0 ? sh : (m == 0 ? xH : v[(N1 - m) % N1]);
+      z[m] = c2r_pre<true>(v[m], xm, tw[t + N2 * m]);
     }
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const int e = e0 + u * kThreads + threadIdx.x;
-      if (e < E) {
-        const int r = e / R, x = e - r * R;
-        s[x * kPitch + r] = v[u];
-      }
-    }
+    for (int m = 0; m < N1; m++) v[m] = z[m];
   }
-  __syncthreads();
-  c2r_pre<H, true>(s, tw, c, t);
-  fft_cols<H, 2, true>(s, tw, c, t);
+  four_step<H, true, true, 2>(v, xb, tw, t, r);
   {
     // blob: grid_blob_kernel's table index (radius sqrt(x^2 + y^2 + z^2) / P
     // / funcsampling in FP32 with the row part formed first)
-    const int rg = (int)(row0 + c);  // z * P + y
-    const int z = rg / P, y = rg - z * P;
+    const int z = (int)(rg / P), y = (int)(rg - (int64_t)z * P);
     const int zp = z < H ? z : z - P, yp = y < H ? y : y - P;
     const float cyz = (float)(yp * yp + zp * zp);
     const float inv_p = __frcp_rn((float)P);
-    for (int n = t; n < H; n += kCols) {
-      float2 v = s[n * kPitch + c];
+#pragma unroll
+    for (int m = 0; m < N1; m++) {
+      const int n = t + N2 * m;
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         const int x = 2 * n + h;
@@ -293,24 +319,29 @@ gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const f
         const float sq = sqrtf(xp * xp + cyz);
         int ti = (int)((sq * inv_p) / funcsampling);
         ti = ti < kBlobSamples - 1 ? ti : kBlobSamples - 1;
-        if (h == 0) v.x = v.x * inv_n * stab[ti];
-        else v.y = v.y * inv_n * stab[ti];
+        const float bv = __ldg(table + ti);
+        if (h == 0) v[m].x = v[m].x * inv_n * bv;
+        else v[m].y = v[m].y * inv_n * bv;
       }
-      s[n * kPitch + c] = v;
     }
   }
-  __syncthreads();
-  fft_cols<H, 2, false>(s, tw, c, t);
-  r2c_post<H, false>(s, tw, c, t);
-  for (int e0 = 0; e0 < E; e0 += kThreads) {
-    const int e = e0 + threadIdx.x;
-    if (e < E) {
-      const int r = e / R, x = e - r * R;
-      rows[e] = s[x * kPitch + r];
-    }
+  four_step<H, false, true, 2>(v, xb, tw, t, r);
+  // post-twiddle of the R2C: partner (H - k) mod H as above (thread 0:
+  // element 0 for m = 0, else N1 - m)
+  float2 y[N1];
+#pragma unroll
+  for (int m = 0; m < N1; m++) {
+    const float2 sh = make_float2(__shfl_sync(0xffffffffu, v[N1 - 1 - m].x, partner),
+                                  __shfl_sync(0xffffffffu, v[N1 - 1 - m].y, partner));
+    const float2 zm = t != 0 ? sh : v[(N1 - m) % N1];
+    y[m] = r2c_post<false>(v[m], zm, tw[t + N2 * m]);
   }
+#pragma unroll
+  for (int m = 0; m < N1; m++) row[t + N2 * m] = y[m];
+  if (t == 0) row[H] = make_float2(v[0].x - v[0].y, 0.f);
 }
 
+// ------------------------------------------------------------ z pass --
 enum : int { kZFirst = 0, kZIter = 1 };
 
 // Per column (x, y) along z.  kZFirst: the real-to-Hermitian transform
@@ -321,89 +352,92 @@ enum : int { kZFirst = 0, kZIter = 1 };
 // to reference weights as well.  Grid: (tiles, volumes); tiles are 16
 // consecutive x < P/2 at one y, then x = P/2 at 16 consecutive y.
 template <int P, int MODE, bool MOM>
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kCols * Split<P / 2>::N2, 3)
 gridsym_z_kernel(float2* __restrict__ W, const float* __restrict__ Fw, float* __restrict__ Fnw,
                  float* __restrict__ V, const float2* __restrict__ twg, float beta, int write_next,
                  double* __restrict__ change, const float* __restrict__ ref) {
   constexpr int H = P / 2, R = H + 1;
+  constexpr int N1 = Split<H>::N1, N2 = Split<H>::N2;
   constexpr int64_t NC = (int64_t)R * P * P;        // spectrum elements per volume
   constexpr int64_t NW = (int64_t)(H + 1) * P * R;  // W elements per volume
+  constexpr int64_t ES = (int64_t)P * R;            // element stride along z (W and the weights)
   extern __shared__ float2 smem[];
   float2* tw = smem;
-  float2* s = smem + P;
+  float2* xb = smem + P;
   load_twiddles(tw, twg, P);
   const int c = threadIdx.x & (kCols - 1), t = threadIdx.x / kCols;
   constexpr int kMain = P * (H / kCols);
   const int b = blockIdx.x;
   int64_t base, cs;
-  int ncols;
   if (b < kMain) {
     const int y = b / (H / kCols), xt = b - y * (H / kCols);
     base = (int64_t)y * R + xt * kCols;
     cs = 1;
-    ncols = kCols;
   } else {
-    const int y0 = (b - kMain) * kCols;
-    base = (int64_t)y0 * R + H;
+    base = (int64_t)(b - kMain) * kCols * R + H;
     cs = R;
-    ncols = min(kCols, P - y0);
   }
-  constexpr int64_t ES = (int64_t)P * R;  // element stride along z (W and the weights)
-  const bool in = c < ncols;
   const int64_t vol = blockIdx.y;
   float2* wc = W + vol * NW + base + c * cs;
   const int64_t wo = vol * NC + base + c * cs;
+  float2 v[N1];
   if (MODE == kZIter) {
-    constexpr int U = (H + 1 + kCols - 1) / kCols;
+    float2 xH = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      const int z = t + kCols * u;
-      if (z <= H) s[z * kPitch + c] = in ? wc[z * ES] : make_float2(0.f, 0.f);
-    }
+    for (int m = 0; m < N1; m++) v[m] = wc[(t + N2 * m) * ES];
+    if (t == 0) xH = wc[H * ES];
+    // pre-twiddle (exp(-) sum) with the partners H - k through shared memory
+    __syncthreads();  // twiddles in place
+#pragma unroll
+    for (int m = 0; m < N1; m++) xb[(t + N2 * m) * kPitch + c] = v[m];
+    if (t == 0) xb[H * kPitch + c] = xH;
     __syncthreads();
-    c2r_pre<H, false>(s, tw, c, t);
-    fft_cols<H, 2, false>(s, tw, c, t);
+#pragma unroll
+    for (int m = 0; m < N1; m++) {
+      const int k = t + N2 * m;
+      v[m] = c2r_pre<false>(v[m], xb[(H - k) * kPitch + c], tw[k]);
+    }
+    four_step<H, false, false, 2>(v, xb, tw, t, c);
   }
-  // the update (kZIter) and S = Fw * Fnw (Fw * V), pairs (S(2n), S(2n+1))
+  // the update (kZIter) and S = Fw * Fnw (Fw * V): element n = t + N2 m of
+  // the packed pairs is (S(2n), S(2n+1))
   double d2 = 0, o2 = 0, r2 = 0, q2 = 0;
-  constexpr int NQ = H / kCols;  // pairs (2n, 2n+1) per thread
-  constexpr int CH = NQ < 4 ? NQ : 4;
   const bool dist = MODE == kZIter && change && ref;
-#pragma unroll 1
-  for (int q0 = 0; q0 < NQ; q0 += CH) {
+  constexpr int CH = N1 < 2 ? N1 : 2;
+#pragma unroll
+  for (int m0 = 0; m0 < N1; m0 += CH) {
     // loads of CH pairs first (in flight together), then the updates
     float fw[CH][2], old[CH][2], vv[CH][2], rf[CH][2];
 #pragma unroll
     for (int q = 0; q < CH; q++) {
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        const int64_t gi = wo + (int64_t)(2 * (t + kCols * (q0 + q)) + h) * ES;
-        fw[q][h] = in ? __ldg(Fw + gi) : 0.f;
-        old[q][h] = in && (MODE == kZIter || !MOM) ? Fnw[gi] : 0.f;
-        vv[q][h] = in && MOM ? V[gi] : 0.f;
-        rf[q][h] = in && dist ? __ldg(ref + gi) : 0.f;
+        const int64_t gi = wo + (int64_t)(2 * (t + N2 * (m0 + q)) + h) * ES;
+        fw[q][h] = __ldg(Fw + gi);
+        old[q][h] = MODE == kZIter || !MOM ? Fnw[gi] : 0.f;
+        vv[q][h] = MOM ? V[gi] : 0.f;
+        rf[q][h] = dist ? __ldg(ref + gi) : 0.f;
       }
     }
 #pragma unroll
     for (int q = 0; q < CH; q++) {
-      const int n = t + kCols * (q0 + q);
-      const float2 cv = MODE == kZIter ? s[n * kPitch + c] : make_float2(0.f, 0.f);
+      const int m = m0 + q;
       float sv[2];
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        const int64_t gi = wo + (int64_t)(2 * n + h) * ES;
+        const int64_t gi = wo + (int64_t)(2 * (t + N2 * m) + h) * ES;
         float next;
         if (MODE == kZIter) {
-          const float cval = h ? cv.y : cv.x;
+          const float cval = h ? v[m].y : v[m].x;
           float nw;
           if (MOM) {
             grid_update_momentum_value(cval, old[q][h], vv[q][h], beta, nw, next);
-            if (in) V[gi] = next;
+            V[gi] = next;
           } else {
             nw = grid_update_value(cval, old[q][h]);
             next = nw;
           }
-          if (in) Fnw[gi] = nw;
+          Fnw[gi] = nw;
           if (change) {
             const double d = (double)fw[q][h] * ((double)nw - (double)old[q][h]);
             const double o = (double)fw[q][h] * (double)old[q][h];
@@ -421,7 +455,7 @@ gridsym_z_kernel(float2* __restrict__ W, const float* __restrict__ Fw, float* __
         }
         sv[h] = fw[q][h] * next;
       }
-      s[n * kPitch + c] = make_float2(sv[0], sv[1]);
+      v[m] = make_float2(sv[0], sv[1]);
     }
   }
   if (MODE == kZIter && change) {
@@ -431,23 +465,34 @@ gridsym_z_kernel(float2* __restrict__ W, const float* __restrict__ Fw, float* __
       grid_change_reduce(r2, q2, change + 2);
     }
   }
-  __syncthreads();
   if (MODE == kZIter && !write_next) return;  // uniform
-  fft_cols<H, 2, true>(s, tw, c, t);
-  r2c_post<H, true>(s, tw, c, t);
-  if (in) {
-    for (int z = t; z <= H; z += kCols) wc[z * ES] = s[z * kPitch + c];
+  if (MODE == kZFirst) __syncthreads();  // twiddles in place
+  four_step<H, true, false, 2>(v, xb, tw, t, c);
+  // post-twiddle (exp(+)) with the partners (H - k) mod H through shared memory
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < N1; m++) xb[(t + N2 * m) * kPitch + c] = v[m];
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < N1; m++) {
+    const int k = t + N2 * m, km = k == 0 ? 0 : H - k;
+    wc[k * ES] = r2c_post<true>(v[m], xb[km * kPitch + c], tw[k]);
   }
+  if (t == 0) wc[H * ES] = make_float2(v[0].x - v[0].y, 0.f);
 }
 
+// ------------------------------------------------------------- launch --
 template <int P>
 struct SymSizes {
   static constexpr int H = P / 2;
+  static constexpr int y_threads = kCols * Split<P>::N2;
+  static constexpr int xz_threads = kCols * Split<H>::N2;
   static constexpr int y_tiles = (H / kCols) * (H + 1) + (H + 1 + kCols - 1) / kCols;
   static constexpr int x_tiles = (H + 1) * P / kCols;
   static constexpr int z_tiles = P * (H / kCols) + P / kCols;
+  // twiddle table + exchange buffer
   static constexpr size_t y_smem = sizeof(float2) * (P + (size_t)P * kPitch);
-  static constexpr size_t x_smem = sizeof(float2) * (P + (size_t)(H + 1) * kPitch) + sizeof(float) * kBlobSamples;
+  static constexpr size_t x_smem = sizeof(float2) * (P + (size_t)kCols * Split<H>::N2 * (Split<H>::N1 + 1));
   static constexpr size_t z_smem = sizeof(float2) * (P + (size_t)(H + 1) * kPitch);
 };
 
@@ -477,11 +522,11 @@ int run_first(float2* W, int count, const float* Fw, float* Fnw, float* V, const
   using Z = SymSizes<P>;
   const dim3 grid(Z::z_tiles, count);
   if (V)
-    gridsym_z_kernel<P, kZFirst, true><<<grid, kThreads, Z::z_smem, stream>>>(W, Fw, Fnw, V, tw, 0.f, 1,
-                                                                              nullptr, nullptr);
+    gridsym_z_kernel<P, kZFirst, true><<<grid, Z::xz_threads, Z::z_smem, stream>>>(W, Fw, Fnw, V, tw, 0.f, 1,
+                                                                                   nullptr, nullptr);
   else
-    gridsym_z_kernel<P, kZFirst, false><<<grid, kThreads, Z::z_smem, stream>>>(W, Fw, Fnw, V, tw, 0.f, 1,
-                                                                               nullptr, nullptr);
+    gridsym_z_kernel<P, kZFirst, false><<<grid, Z::xz_threads, Z::z_smem, stream>>>(W, Fw, Fnw, V, tw, 0.f, 1,
+                                                                                    nullptr, nullptr);
   GTOMRLN_LAUNCH_CHECK("gridsym_z_kernel (first)");
   return GTOMRLN_OK;
 }
@@ -492,20 +537,20 @@ int run_iteration(float2* W, int count, const float* table, const float* Fw, flo
   using Z = SymSizes<P>;
   const float inv_n = 1.0f / ((float)P * (float)P * (float)P);
   const float funcsampling = (float)(0.5 / kBlobSamples);
-  gridsym_y_kernel<P, true><<<dim3(Z::y_tiles, count), kThreads, Z::y_smem, stream>>>(W, tw);
+  gridsym_y_kernel<P, true><<<dim3(Z::y_tiles, count), Z::y_threads, Z::y_smem, stream>>>(W, tw);
   GTOMRLN_LAUNCH_CHECK("gridsym_y_kernel (inverse)");
-  gridsym_x_kernel<P><<<dim3(Z::x_tiles, count), kThreads, Z::x_smem, stream>>>(W, tw, table, inv_n,
-                                                                                funcsampling);
+  gridsym_x_kernel<P><<<dim3(Z::x_tiles, count), Z::xz_threads, Z::x_smem, stream>>>(W, tw, table, inv_n,
+                                                                                     funcsampling);
   GTOMRLN_LAUNCH_CHECK("gridsym_x_kernel");
-  gridsym_y_kernel<P, false><<<dim3(Z::y_tiles, count), kThreads, Z::y_smem, stream>>>(W, tw);
+  gridsym_y_kernel<P, false><<<dim3(Z::y_tiles, count), Z::y_threads, Z::y_smem, stream>>>(W, tw);
   GTOMRLN_LAUNCH_CHECK("gridsym_y_kernel (forward)");
   const dim3 grid(Z::z_tiles, count);
   if (V)
-    gridsym_z_kernel<P, kZIter, true><<<grid, kThreads, Z::z_smem, stream>>>(W, Fw, Fnw, V, tw, beta,
-                                                                             write_next, change, ref);
+    gridsym_z_kernel<P, kZIter, true><<<grid, Z::xz_threads, Z::z_smem, stream>>>(W, Fw, Fnw, V, tw, beta,
+                                                                                  write_next, change, ref);
   else
-    gridsym_z_kernel<P, kZIter, false><<<grid, kThreads, Z::z_smem, stream>>>(W, Fw, Fnw, V, tw, beta,
-                                                                              write_next, change, ref);
+    gridsym_z_kernel<P, kZIter, false><<<grid, Z::xz_threads, Z::z_smem, stream>>>(W, Fw, Fnw, V, tw, beta,
+                                                                                   write_next, change, ref);
   GTOMRLN_LAUNCH_CHECK("gridsym_z_kernel");
   return GTOMRLN_OK;
 }
@@ -540,6 +585,13 @@ int ensure_attributes(int P) {
 
 bool gridsym_available(int P) { return P == 64 || P == 128 || P == 256 || P == 512; }
 
+int gridsym_prepare(int P) {
+  int st = ensure_attributes(P);
+  if (st) return st;
+  const float2* tw = nullptr;
+  return fft_twiddles(P, &tw);
+}
+
 int gridsym_first(float2* W, const GridGeom& g, int count, const float* Fw, float* Fnw, float* V,
                   cudaStream_t stream) {
   int st = ensure_attributes(g.P);
@@ -564,6 +616,8 @@ int gridsym_iteration(float2* W, const GridGeom& g, int count, const float* tabl
   });
 }
 
+// Forgets the launch attributes set on device dev (a context reset drops
+// them with the context).
 int release_gridsym_caches(int dev, unsigned long long /*ctx*/) {
   std::lock_guard<std::mutex> lock(g_attr_mutex);
   for (auto it = g_attr_done.begin(); it != g_attr_done.end();) {

@@ -379,11 +379,11 @@ def set_path(op: str, path: str) -> None:
     "segment" (pixels found per brick by row segments; the backprojector's
     accumulates each work item in fixed point first), for "backproject" also
     "segment_fp32" (row segments, FP32 atomics only); of "gridding": "auto"
-    or "direct" (cuFFT transforms), "fused" (two fused passes per iteration
-    with the library's own transforms on power-of-two grids) or "symmetric"
-    (four passes over the Hermitian half along z of the real iterated
-    spectrum, the library's own transforms, power-of-two grids)
-    (gtomrln_set_path)."""
+    (default: "symmetric" on power-of-two grids P = 64 .. 512, cuFFT
+    elsewhere), "direct" (cuFFT transforms), "fused" (two fused passes per
+    iteration with the library's own transforms on power-of-two grids) or
+    "symmetric" (four passes over the Hermitian half along z of the real
+    iterated spectrum, the library's own transforms) (gtomrln_set_path)."""
     _lib.call("gtomrln_set_path", _OPS[op], _PATHS[path])
 
 

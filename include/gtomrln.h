@@ -77,11 +77,12 @@ GTOMRLN_API int gtomrln_release_caches(void);
  * the same per-sample arithmetic. */
 #define GTOMRLN_OP_PROJECT 0
 #define GTOMRLN_OP_BACKPROJECT 1
-/* op GTOMRLN_OP_GRIDDING: GTOMRLN_PATH_AUTO (default) and
- * GTOMRLN_PATH_DIRECT run the gridding iterations' 3D transforms with cuFFT;
- * GTOMRLN_PATH_FUSED runs each iteration as two fused passes with the
- * library's own transforms on power-of-two grids P = 64 .. 512 (cuFFT
- * elsewhere). */
+/* op GTOMRLN_OP_GRIDDING: GTOMRLN_PATH_AUTO (default) runs the gridding
+ * iterations as GTOMRLN_PATH_SYMMETRIC (below) on power-of-two grids
+ * P = 64 .. 512 and with cuFFT's 3D transforms elsewhere;
+ * GTOMRLN_PATH_DIRECT always uses cuFFT; GTOMRLN_PATH_FUSED runs each
+ * iteration as two fused passes with the library's own transforms on
+ * power-of-two grids P = 64 .. 512 (cuFFT elsewhere). */
 #define GTOMRLN_OP_GRIDDING 2
 #define GTOMRLN_PATH_AUTO 0
 #define GTOMRLN_PATH_DIRECT 1
