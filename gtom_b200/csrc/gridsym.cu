@@ -88,30 +88,82 @@ constexpr double ce_sin(double x) {
 }
 constexpr double ce_cos(double x) { return ce_sin(x + kPiD / 2); }
 
-// In-register DFT of length N (power of two), unnormalised, forward
-// (exp(-)) or inverse (exp(+)), natural order in and out: radix-2
-// decimation in time down to the radix-8/4/2 kernels of fftcore.cuh, with
-// the combining twiddles as constants.
+// Odd prime DFT of length R in registers (R = 3, 5), unnormalised, forward
+// (exp(-)) or inverse (exp(+)): X(k) = a(0) + sum over n = 1 .. (R-1)/2 of
+// (a(n) + a(R-n)) cos(2 pi k n / R) -+ i (a(n) - a(R-n)) sin(2 pi k n / R).
+template <int R, bool INV>
+__device__ __forceinline__ void dft_odd(float2* v) {
+  float2 sp[(R - 1) / 2], sm[(R - 1) / 2];
+#pragma unroll
+  for (int n = 1; n <= (R - 1) / 2; n++) {
+    sp[n - 1] = cadd(v[n], v[R - n]);
+    sm[n - 1] = csub(v[n], v[R - n]);
+  }
+  float2 out[R];
+  out[0] = v[0];
+#pragma unroll
+  for (int n = 0; n < (R - 1) / 2; n++) out[0] = cadd(out[0], sp[n]);
+#pragma unroll
+  for (int k = 1; k < R; k++) {
+    float2 re = v[0], im = make_float2(0.f, 0.f);  // re: cosine part, im: sine part (before the factor -+i)
+#pragma unroll
+    for (int n = 1; n <= (R - 1) / 2; n++) {
+      const float cs = (float)ce_cos(2 * kPiD * ((k * n) % R) / R);
+      const float sn = (float)ce_sin(2 * kPiD * ((k * n) % R) / R);
+      re = make_float2(fmaf(cs, sp[n - 1].x, re.x), fmaf(cs, sp[n - 1].y, re.y));
+      im = make_float2(fmaf(sn, sm[n - 1].x, im.x), fmaf(sn, sm[n - 1].y, im.y));
+    }
+    // forward: re - i im; inverse: re + i im
+    out[k] = INV ? make_float2(re.x - im.y, re.y + im.x) : make_float2(re.x + im.y, re.y - im.x);
+  }
+#pragma unroll
+  for (int k = 0; k < R; k++) v[k] = out[k];
+}
+
+// In-register DFT of length N (factors 2, 3, 5), unnormalised, forward
+// (exp(-)) or inverse (exp(+)), natural order in and out: decimation in
+// time by the smallest factor (2, then 3, then 5) down to the radix-8/4/2
+// kernels of fftcore.cuh and the odd prime kernels above, with the
+// combining twiddles as constants.
 template <int N, bool INV>
 __device__ __forceinline__ void dftr(float2* v) {
-  if constexpr (N <= 8) {
+  if constexpr (N == 1) {
+    return;
+  } else if constexpr (N == 2 || N == 4 || N == 8) {
     dft<N, INV>(v);
+  } else if constexpr (N == 3 || N == 5) {
+    dft_odd<N, INV>(v);
   } else {
-    float2 e[N / 2], o[N / 2];
+    constexpr int R = N % 2 == 0 ? 2 : (N % 3 == 0 ? 3 : 5);
+    constexpr int M = N / R;
+    static_assert(M * R == N, "dftr: lengths with factors 2, 3 and 5 only");
+    float2 sub[R][M];
 #pragma unroll
-    for (int i = 0; i < N / 2; i++) {
-      e[i] = v[2 * i];
-      o[i] = v[2 * i + 1];
-    }
-    dftr<N / 2, INV>(e);
-    dftr<N / 2, INV>(o);
+    for (int r = 0; r < R; r++)
 #pragma unroll
-    for (int k = 0; k < N / 2; k++) {
-      const float wr = (float)ce_cos(2 * kPiD * k / N);
-      const float wi = (float)(INV ? ce_sin(2 * kPiD * k / N) : -ce_sin(2 * kPiD * k / N));
-      const float2 t = k == 0 ? o[0] : cmul(o[k], make_float2(wr, wi));
-      v[k] = cadd(e[k], t);
-      v[k + N / 2] = csub(e[k], t);
+      for (int i = 0; i < M; i++) sub[r][i] = v[R * i + r];
+#pragma unroll
+    for (int r = 0; r < R; r++) dftr<M, INV>(sub[r]);
+#pragma unroll
+    for (int k = 0; k < M; k++) {
+      float2 u[R];
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        if (r * k == 0) {
+          u[r] = sub[r][k];
+        } else {
+          const float wr = (float)ce_cos(2 * kPiD * r * k / N);
+          const float wi = (float)(INV ? ce_sin(2 * kPiD * r * k / N) : -ce_sin(2 * kPiD * r * k / N));
+          u[r] = cmul(sub[r][k], make_float2(wr, wi));
+        }
+      }
+      if constexpr (R == 2) {
+        dft<2, INV>(u);
+      } else {
+        dft_odd<R, INV>(u);
+      }
+#pragma unroll
+      for (int q = 0; q < R; q++) v[k + M * q] = u[q];
     }
   }
 }
@@ -120,26 +172,22 @@ __device__ __forceinline__ void dftr(float2* v) {
 // N = N1 N2 with N2 threads per column and N1 a multiple of N2.
 template <int N>
 struct Split;
-template <>
-struct Split<32> {
-  static constexpr int N1 = 8, N2 = 4;
-};
-template <>
-struct Split<64> {
-  static constexpr int N1 = 8, N2 = 8;
-};
-template <>
-struct Split<128> {
-  static constexpr int N1 = 16, N2 = 8;
-};
-template <>
-struct Split<256> {
-  static constexpr int N1 = 16, N2 = 16;
-};
-template <>
-struct Split<512> {
-  static constexpr int N1 = 32, N2 = 16;
-};
+#define GTOMRLN_SPLIT(N_, A_, B_)            \
+  template <>                               \
+  struct Split<N_> {                        \
+    static constexpr int N1 = A_, N2 = B_;  \
+  };
+GTOMRLN_SPLIT(32, 8, 4)
+GTOMRLN_SPLIT(48, 12, 4)
+GTOMRLN_SPLIT(64, 8, 8)
+GTOMRLN_SPLIT(96, 24, 4)
+GTOMRLN_SPLIT(128, 16, 8)
+GTOMRLN_SPLIT(192, 24, 8)
+GTOMRLN_SPLIT(256, 16, 16)
+GTOMRLN_SPLIT(400, 20, 20)
+GTOMRLN_SPLIT(512, 32, 16)
+GTOMRLN_SPLIT(800, 40, 20)
+#undef GTOMRLN_SPLIT
 
 // Runtime twiddle e(-m/N) (or e(+m/N), INV) from the table e(-j/P), N = P/S.
 template <int S, bool INV>
@@ -164,19 +212,21 @@ __device__ __forceinline__ int xplace(int k1, int n2, int c) {
 
 // The four-step transform of one column (thread t of its N2 threads holds
 // elements t + N2 m in v[m]; afterwards outputs t + N2 m in v[m]).  ROWS:
-// the column's threads share a warp and synchronise as a warp; else the
-// block synchronises (every thread of the block must call it).  Begins with
-// a barrier, so the exchange buffer may still be in use by the caller.
-template <int N, bool INV, bool ROWS, int S>
+// the row layout of xplace.  WSYNC: the column's threads share a warp and
+// synchronise as a warp; else the block synchronises (every thread of the
+// block must call it).  Begins with a barrier, so the exchange buffer may
+// still be in use by the caller.
+template <int N, bool INV, bool ROWS, bool WSYNC, int S>
 __device__ __forceinline__ void four_step(float2* v, float2* xb, const float2* tw, int t, int c) {
   constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2, J = N1 / N2;
+  static_assert(J * N2 == N1, "four_step: N1 must be a multiple of N2");
   dftr<N1, INV>(v);
 #pragma unroll
   for (int k1 = 1; k1 < N1; k1++) v[k1] = cmul(v[k1], twiddle<S, INV>(tw, t * k1));
-  if (ROWS) __syncwarp(); else __syncthreads();
+  if (WSYNC) __syncwarp(); else __syncthreads();
 #pragma unroll
   for (int k1 = 0; k1 < N1; k1++) xb[xplace<N1, N2, ROWS>(k1, t, c)] = v[k1];
-  if (ROWS) __syncwarp(); else __syncthreads();
+  if (WSYNC) __syncwarp(); else __syncthreads();
 #pragma unroll
   for (int j = 0; j < J; j++) {
     float2 u[N2];
@@ -224,7 +274,7 @@ __device__ __forceinline__ void load_twiddles(float2* tw, const float2* __restri
 // forward of the R2C).  Grid: (tiles, volumes); tiles are 16 consecutive
 // x < P/2 at one z, then x = P/2 at 16 consecutive z.  16 N2 threads.
 template <int P, bool INV>
-__global__ void __launch_bounds__(kCols * Split<P>::N2, 2)
+__global__ void __launch_bounds__(kCols * Split<P>::N2, (P > 512 ? 1 : 2))
 gridsym_y_kernel(float2* __restrict__ W, const float2* __restrict__ twg) {
   constexpr int H = P / 2, R = H + 1;
   constexpr int N1 = Split<P>::N1, N2 = Split<P>::N2;
@@ -254,7 +304,7 @@ gridsym_y_kernel(float2* __restrict__ W, const float2* __restrict__ twg) {
 #pragma unroll
   for (int m = 0; m < N1; m++) v[m] = in ? col[(int64_t)(t + N2 * m) * R] : make_float2(0.f, 0.f);
   __syncthreads();  // twiddles in place
-  four_step<P, INV, false, 1>(v, xb, tw, t, c);
+  four_step<P, INV, false, false, 1>(v, xb, tw, t, c);
   if (in) {
 #pragma unroll
     for (int m = 0; m < N1; m++) col[(int64_t)(t + N2 * m) * R] = v[m];
@@ -264,20 +314,26 @@ gridsym_y_kernel(float2* __restrict__ W, const float2* __restrict__ twg) {
 // ------------------------------------------------------------ x pass --
 // Per row (y, z), z <= P/2: C2R along x, times blob(r) / P^3, R2C along x.
 // Grid: ((P/2 + 1) P / 16, volumes); a CTA takes 16 consecutive rows, the
-// N2 threads of a row consecutive lanes.
+// N2 threads of a row consecutive lanes.  Where N2 divides 32 a row lies in
+// one warp (warp-synchronous exchanges, shuffles for the Hermitian
+// partners); else (P = 800) the block synchronises and the partners go
+// through shared memory.
 template <int P>
-__global__ void __launch_bounds__(kCols * Split<P / 2>::N2, 3)
+__global__ void __launch_bounds__(kCols * Split<P / 2>::N2, (P > 512 ? 2 : 3))
 gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const float* __restrict__ table,
                  float inv_n, float funcsampling) {
   constexpr int H = P / 2, R = H + 1;
   constexpr int N1 = Split<H>::N1, N2 = Split<H>::N2;
+  constexpr bool WROW = 32 % N2 == 0;    // a row's threads within one warp
+  constexpr int XS = N2 * (N1 + 1);      // a row's block of the exchange buffer
+  constexpr bool POW2 = (P & (P - 1)) == 0;
   extern __shared__ float2 smem[];
   float2* tw = smem;
   float2* xb = smem + P;
   load_twiddles(tw, twg, P);
   const int t = threadIdx.x % N2, r = threadIdx.x / N2;
   const unsigned lane = threadIdx.x & 31;
-  const unsigned partner = (lane & ~(unsigned)(N2 - 1)) | ((unsigned)(N2 - t) & (N2 - 1));
+  const unsigned partner = WROW ? (lane & ~(unsigned)(N2 - 1)) | ((unsigned)(N2 - t) & (N2 - 1)) : lane;
   const int64_t rg = (int64_t)blockIdx.x * kCols + r;  // z * P + y
   float2* row = W + (int64_t)blockIdx.y * ((int64_t)(H + 1) * P * R) + rg * R;
   float2 v[N1];
@@ -285,26 +341,39 @@ gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const f
   for (int m = 0; m < N1; m++) v[m] = row[t + N2 * m];
   const float2 xH = t == 0 ? row[H] : make_float2(0.f, 0.f);
   __syncthreads();  // twiddles in place
-  // pre-twiddle of the C2R: the partner H - k of k = t + N2 m is element
+  // pre-twiddle of the C2R.  The partner H - k of k = t + N2 m is element
   // N1-1-m of thread N2-t (t > 0), or element N1-m (H for m = 0) of thread 0
   // (into a second array: the partners' elements are read after this
   // thread's own have been replaced)
   {
     float2 z[N1];
+    if constexpr (WROW) {
 #pragma unroll
-    for (int m = 0; m < N1; m++) {
-      const float2 sh = make_float2(__shfl_sync(0xffffffffu, v[N1 - 1 - m].x, partner),
-                                    __shfl_sync(0xffffffffu, v[N1 - 1 - m].y, partner));
-      const float2 xm = t != 0 ? sh : (m == 0 ? xH : v[(N1 - m) % N1]);
-      z[m] = c2r_pre<true>(v[m], xm, tw[t + N2 * m]);
+      for (int m = 0; m < N1; m++) {
+        const float2 sh = make_float2(__shfl_sync(0xffffffffu, v[N1 - 1 - m].x, partner),
+                                      __shfl_sync(0xffffffffu, v[N1 - 1 - m].y, partner));
+        const float2 xm = t != 0 ? sh : (m == 0 ? xH : v[(N1 - m) % N1]);
+        z[m] = c2r_pre<true>(v[m], xm, tw[t + N2 * m]);
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < N1; m++) xb[r * XS + t + N2 * m] = v[m];
+      if (t == 0) xb[r * XS + H] = xH;
+      __syncthreads();
+#pragma unroll
+      for (int m = 0; m < N1; m++) {
+        const int k = t + N2 * m;
+        z[m] = c2r_pre<true>(v[m], xb[r * XS + H - k], tw[k]);
+      }
     }
 #pragma unroll
     for (int m = 0; m < N1; m++) v[m] = z[m];
   }
-  four_step<H, true, true, 2>(v, xb, tw, t, r);
+  four_step<H, true, true, WROW, 2>(v, xb, tw, t, r);
   {
     // blob: grid_blob_kernel's table index (radius sqrt(x^2 + y^2 + z^2) / P
-    // / funcsampling in FP32 with the row part formed first)
+    // / funcsampling in FP32 with the row part formed first; the division by
+    // a power-of-two P as the multiplication by its exact reciprocal)
     const int z = (int)(rg / P), y = (int)(rg - (int64_t)z * P);
     const int zp = z < H ? z : z - P, yp = y < H ? y : y - P;
     const float cyz = (float)(yp * yp + zp * zp);
@@ -317,7 +386,7 @@ gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const f
         const int x = 2 * n + h;
         const float xp = (float)(x < H ? x : x - P);
         const float sq = sqrtf(xp * xp + cyz);
-        int ti = (int)((sq * inv_p) / funcsampling);
+        int ti = (int)((POW2 ? sq * inv_p : sq / (float)P) / funcsampling);
         ti = ti < kBlobSamples - 1 ? ti : kBlobSamples - 1;
         const float bv = __ldg(table + ti);
         if (h == 0) v[m].x = v[m].x * inv_n * bv;
@@ -325,16 +394,28 @@ gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const f
       }
     }
   }
-  four_step<H, false, true, 2>(v, xb, tw, t, r);
+  four_step<H, false, true, WROW, 2>(v, xb, tw, t, r);
   // post-twiddle of the R2C: partner (H - k) mod H as above (thread 0:
   // element 0 for m = 0, else N1 - m)
   float2 y[N1];
+  if constexpr (WROW) {
 #pragma unroll
-  for (int m = 0; m < N1; m++) {
-    const float2 sh = make_float2(__shfl_sync(0xffffffffu, v[N1 - 1 - m].x, partner),
-                                  __shfl_sync(0xffffffffu, v[N1 - 1 - m].y, partner));
-    const float2 zm = t != 0 ? sh : v[(N1 - m) % N1];
-    y[m] = r2c_post<false>(v[m], zm, tw[t + N2 * m]);
+    for (int m = 0; m < N1; m++) {
+      const float2 sh = make_float2(__shfl_sync(0xffffffffu, v[N1 - 1 - m].x, partner),
+                                    __shfl_sync(0xffffffffu, v[N1 - 1 - m].y, partner));
+      const float2 zm = t != 0 ? sh : v[(N1 - m) % N1];
+      y[m] = r2c_post<false>(v[m], zm, tw[t + N2 * m]);
+    }
+  } else {
+    __syncthreads();  // the exchange buffer is free
+#pragma unroll
+    for (int m = 0; m < N1; m++) xb[r * XS + t + N2 * m] = v[m];
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < N1; m++) {
+      const int k = t + N2 * m;
+      y[m] = r2c_post<false>(v[m], xb[r * XS + (k == 0 ? 0 : H - k)], tw[k]);
+    }
   }
 #pragma unroll
   for (int m = 0; m < N1; m++) row[t + N2 * m] = y[m];
@@ -352,7 +433,7 @@ enum : int { kZFirst = 0, kZIter = 1 };
 // to reference weights as well.  Grid: (tiles, volumes); tiles are 16
 // consecutive x < P/2 at one y, then x = P/2 at 16 consecutive y.
 template <int P, int MODE, bool MOM>
-__global__ void __launch_bounds__(kCols * Split<P / 2>::N2, 3)
+__global__ void __launch_bounds__(kCols * Split<P / 2>::N2, (P > 512 ? 2 : 3))
 gridsym_z_kernel(float2* __restrict__ W, const float* __restrict__ Fw, float* __restrict__ Fnw,
                  float* __restrict__ V, const float2* __restrict__ twg, float beta, int write_next,
                  double* __restrict__ change, const float* __restrict__ ref) {
@@ -397,7 +478,7 @@ gridsym_z_kernel(float2* __restrict__ W, const float* __restrict__ Fw, float* __
       const int k = t + N2 * m;
       v[m] = c2r_pre<false>(v[m], xb[(H - k) * kPitch + c], tw[k]);
     }
-    four_step<H, false, false, 2>(v, xb, tw, t, c);
+    four_step<H, false, false, false, 2>(v, xb, tw, t, c);
   }
   // the update (kZIter) and S = Fw * Fnw (Fw * V): element n = t + N2 m of
   // the packed pairs is (S(2n), S(2n+1))
@@ -467,7 +548,7 @@ gridsym_z_kernel(float2* __restrict__ W, const float* __restrict__ Fw, float* __
   }
   if (MODE == kZIter && !write_next) return;  // uniform
   if (MODE == kZFirst) __syncthreads();  // twiddles in place
-  four_step<H, true, false, 2>(v, xb, tw, t, c);
+  four_step<H, true, false, false, 2>(v, xb, tw, t, c);
   // post-twiddle (exp(+)) with the partners (H - k) mod H through shared memory
   __syncthreads();
 #pragma unroll
@@ -560,9 +641,12 @@ template <typename F>
 int with_grid(int P, F&& f) {
   switch (P) {
     case 64: return f(std::integral_constant<int, 64>());
+    case 96: return f(std::integral_constant<int, 96>());
     case 128: return f(std::integral_constant<int, 128>());
+    case 192: return f(std::integral_constant<int, 192>());
     case 256: return f(std::integral_constant<int, 256>());
     case 512: return f(std::integral_constant<int, 512>());
+    case 800: return f(std::integral_constant<int, 800>());
     default: return set_error(GTOMRLN_ERR_INVALID, "gridsym: unsupported grid %d", P);
   }
 }
@@ -583,7 +667,9 @@ int ensure_attributes(int P) {
 
 }  // namespace
 
-bool gridsym_available(int P) { return P == 64 || P == 128 || P == 256 || P == 512; }
+bool gridsym_available(int P) {
+  return P == 64 || P == 96 || P == 128 || P == 192 || P == 256 || P == 512 || P == 800;
+}
 
 int gridsym_prepare(int P) {
   int st = ensure_attributes(P);

@@ -1,7 +1,8 @@
 """The symmetric-spectrum gridding iteration (gtom_b200/csrc/gridsym.cu:
 four passes per iteration over the Hermitian half along z of the real
 iterated spectrum, with the library's own transforms) against the cuFFT path
-and the FP64 oracle on the same inputs.
+and the FP64 oracle on the same inputs, on every grid it takes: powers of two
+P = 64 .. 512 and the mixed-radix P = 96, 192 (radix 3) and 800 (radix 5).
 
 Both paths compute the reference's iteration (RecFourier.cu:158-171); they
 differ only in how the FP32 transforms round, so the weights after one
@@ -48,7 +49,7 @@ def _on(path, fn):
         G.set_path("gridding", "auto")
 
 
-@pytest.mark.parametrize("ori", [32, 64, 128, 256])
+@pytest.mark.parametrize("ori", [32, 48, 64, 96, 128, 256])
 def test_symmetric_gridding_matches_cufft(gtom_lib, cuda, ori):
     data, w, D = _inputs(ori)
     d_data, d_w = _dev(data), _dev(w)
@@ -142,3 +143,33 @@ def test_symmetric_warm_start(gtom_lib, cuda):
         res[path] = (used, out.cpu().numpy())
     assert res["symmetric"][0] == res["direct"][0]
     assert rel_l2(res["symmetric"][1], res["direct"][1]) <= 1e-4
+
+
+def test_symmetric_gridding_matches_cufft_at_800(gtom_lib, cuda):
+    """P = 800 (400^3 at padding 2, the large combined configuration's grid;
+    radix-5 transforms, rows of the x pass spanning warps), 3 iterations;
+    inputs made on the GPU (2.6 GB of accumulators)."""
+    ori, pad = 400, 2
+    D = ori * pad + 1
+    g = torch.Generator(device="cuda")
+    g.manual_seed(800)
+    z = torch.arange(D, device="cuda", dtype=torch.float32) - D // 2
+    x = torch.arange(D // 2 + 1, device="cuda", dtype=torch.float32)
+    r = torch.sqrt(z[:, None, None] ** 2 + z[None, :, None] ** 2 + x[None, None, :] ** 2)
+    w = torch.where(r < ori * pad / 2, 1.0 + 30.0 * torch.exp(-r / (ori / 3)), torch.zeros_like(r))
+    w = w * (0.8 + 0.4 * torch.rand(w.shape, device="cuda", generator=g))
+    w[:, :, 0] = 0.5 * (w[:, :, 0] + torch.flip(w[:, :, 0], (0, 1)))
+    data = torch.complex(torch.randn(w.shape, device="cuda", generator=g),
+                         torch.randn(w.shape, device="cuda", generator=g)) * (w * torch.exp(-r / ori))
+    del r
+    d_w, d_data = w.reshape(-1).contiguous(), data.reshape(-1).contiguous()
+    del w, data
+    maps = {}
+    for path in ("direct", "symmetric"):
+        out = torch.full((ori ** 3,), float("nan"), device="cuda")
+        _on(path, lambda: G.d_ReconstructGridding(d_data, d_w, out, (ori,) * 3, (D,) * 3, pad, 0, 0, 3))
+        maps[path] = out
+    assert torch.isfinite(maps["symmetric"]).all()
+    err = (torch.linalg.vector_norm(maps["symmetric"] - maps["direct"]) /
+           torch.linalg.vector_norm(maps["direct"])).item()
+    assert err <= 1e-5, err
