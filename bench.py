@@ -1294,7 +1294,7 @@ def run_config5(args):
     with one work item per (volume, brick).  Then each of the eight volumes
     is reconstructed with the gridding correction from the learned warm
     start and the momentum update to a relative change of 1e-4 (P = 800,
-    cuFFT transforms).  Reported: insertion slices/s (device time of the
+    the symmetric-spectrum iteration with radix-5 transforms).  Reported: insertion slices/s (device time of the
     insertion calls alone), generation time, per-volume gridding time and
     iterations, the 10-iteration plain gridding at P = 800 for scale, and
     the device memory in use at its peak against the GPU's total."""
@@ -1379,6 +1379,10 @@ def run_config5(args):
     torch.cuda.empty_cache()
     p128 = WS.load_params(128, dev)
     out = torch.empty(n ** 3, dtype=torch.float32, device=dev)
+    # one untimed short run first: the final transform's plan, the tables and
+    # the pool's buffers are made once per grid
+    G.reconstruct_gridding_warm(acc_ft[:nvox], acc_w[:nvox], out, (n,) * 3, (D,) * 3, p128, PAD, 2, 0.0, 0.9)
+    torch.cuda.synchronize()
     grid = []
     for v in range(8):
         sl = slice(v * nvox, (v + 1) * nvox)
