@@ -151,6 +151,14 @@ __device__ __forceinline__ void dftr(float2* v) {
       for (int r = 0; r < R; r++) {
         if (r * k == 0) {
           u[r] = sub[r][k];
+        } else if (4 * r * k == N) {
+          u[r] = mul_mi<INV>(sub[r][k]);  // e(-+1/4) = -+i
+        } else if (8 * r * k == N || 8 * r * k == 3 * N) {
+          // e(-+1/8), e(-+3/8): (1 -+ i)/sqrt2, (-1 -+ i)/sqrt2, four operations
+          const float h = 0.70710678118654752440f;
+          const float2 a = sub[r][k];
+          const float2 p = 8 * r * k == N ? a : mul_mi<INV>(a);  // e(-+3/8) = -+i e(-+1/8)
+          u[r] = INV ? make_float2((p.x - p.y) * h, (p.x + p.y) * h) : make_float2((p.x + p.y) * h, (p.y - p.x) * h);
         } else {
           const float wr = (float)ce_cos(2 * kPiD * r * k / N);
           const float wi = (float)(INV ? ce_sin(2 * kPiD * r * k / N) : -ce_sin(2 * kPiD * r * k / N));
