@@ -179,8 +179,14 @@ def test_trained_network_beats_the_cold_start(cuda):
     """Train on 12 distributions at box 32 (P = 64) with the library's own
     kernels; then on 4 held-out distributions the predicted start must be
     closer to the converged weights than the cold start after the same
-    number of plain iterations, and reach the 1e-4 tolerance in no more
-    iterations (plain and momentum forms)."""
+    number of plain iterations (10: the criterion of the converged weights,
+    measured early, where the network's gain lies), and reach the 1e-4
+    change in no more iterations (plain and momentum forms).  What it does
+    not gain is asserted nowhere because it is not there: to within 1e-4 of
+    the converged weights the learned start takes as long as the cold one
+    (1.00x plain, 0.95x with momentum on the 200 held-out distributions of
+    the 128^3 workload), the remaining error being the iteration's slow,
+    non-local modes."""
     box, pad = 32, 2
     D = box * pad + 1
     rng = np.random.default_rng(2024)
