@@ -96,7 +96,7 @@ grid_blob_kernel(float* __restrict__ conv, const float* __restrict__ table, Grid
     // HOIST (P <= 4096): grid_blob_index's radius with the conversions
     // hoisted: xp^2 + yp^2 + zp^2 is then an integer below 2^24, exact in
     // FP32 however it is summed, so the row part yp^2 + zp^2 is formed once
-    // per row and only the square root, the division and the truncation
+    // per row and only the square root, the divisions and the truncation
     // remain per voxel
     const int zp = z < P / 2 ? z : z - P;
     float c[kBlobRows];
@@ -105,8 +105,6 @@ grid_blob_kernel(float* __restrict__ conv, const float* __restrict__ table, Grid
       const int y = y0 + r, yp = y < P / 2 ? y : y - P;
       c[r] = (float)(yp * yp + zp * zp);
     }
-    const bool pow2 = (P & (P - 1)) == 0;
-    const float inv_p = __frcp_rn((float)P);
     for (int x = threadIdx.x; x < P; x += blockDim.x) {
       float* col = conv + (plane * P + y0) * P + x;
       float v[kBlobRows];
@@ -120,10 +118,7 @@ grid_blob_kernel(float* __restrict__ conv, const float* __restrict__ table, Grid
         if (r >= rows) break;
         int ti;
         if (HOIST) {
-          const float sq = sqrtf(xx + c[r]);
-          const float rr = (pow2 ? sq * inv_p : sq / (float)P) / funcsampling;
-          ti = (int)rr;
-          ti = ti < kBlobSamples - 1 ? ti : kBlobSamples - 1;
+          ti = grid_blob_index_sq(xx + c[r], (float)P, funcsampling);
         } else {
           ti = grid_blob_index(P, x, y0 + r, z, funcsampling);
         }

@@ -16,20 +16,36 @@ struct GridGeom {
   int64_t nr;    // P^3 real elements
 };
 
+// The reference's gridding is compiled with fast math (-use_fast_math,
+// CMakeLists.txt:36): its FP32 square root is the approximate one and its
+// FP32 division the full-range approximate one, both flushing denormals.
+// The gridding kernels here use the same instructions for the reference's
+// blob radius and weight update.
+__device__ __forceinline__ float grid_sqrt(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float grid_div(float a, float b) {
+  float r;
+  asm("div.full.ftz.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+  return r;
+}
+
 // PrecomputeBlobKernel's table index (RecFourier.cu:243-262) at real-space
-// voxel (x, y, z) of the P grid, the radius evaluated as the reference does:
-// sqrt(r^2) / P / funcsampling in FP32.  For a power-of-two P the division by
-// P is the multiplication by its reciprocal (exact: a power of two), which
-// leaves one division per voxel.
+// voxel (x, y, z) of the P grid, the radius evaluated as the reference's
+// build does: sqrt(xp^2 + yp^2 + zp^2) / P / funcsampling with its fast-math
+// square root and divisions (the squares are integers below 2^24, exact in
+// FP32 however they are summed).
+__device__ __forceinline__ int grid_blob_index_sq(float r2, float P, float funcsampling) {
+  const int ti = (int)grid_div(grid_div(grid_sqrt(r2), P), funcsampling);
+  return ti < kBlobSamples - 1 ? ti : kBlobSamples - 1;
+}
 __device__ __forceinline__ int grid_blob_index(int P, int x, int y, int z, float funcsampling) {
   const int zp = z < P / 2 ? z : z - P;
   const int yp = y < P / 2 ? y : y - P;
   const float xp = (float)(x < P / 2 ? x : x - P);
-  const float s = sqrtf(xp * xp + (float)(yp * yp) + (float)(zp * zp));
-  const float sp = (P & (P - 1)) == 0 ? s * __frcp_rn((float)P) : s / (float)P;
-  const float r = sp / funcsampling;
-  const int ti = (int)r;
-  return ti < kBlobSamples - 1 ? ti : kBlobSamples - 1;
+  return grid_blob_index_sq(xp * xp + (float)(yp * yp) + (float)(zp * zp), (float)P, funcsampling);
 }
 
 // The table value there, read from global memory.  Lanes at consecutive x
@@ -41,10 +57,11 @@ __device__ __forceinline__ float grid_blob_at(const float* __restrict__ table, i
 }
 
 // Iteration2Kernel (RecFourier.cu:293-308) for one voxel: the new
-// Fnewweight from the real part c of the convolved spectrum.
+// Fnewweight from the real part c of the convolved spectrum (the division
+// as the reference's fast-math build does it).
 __device__ __forceinline__ float grid_update_value(float c, float old) {
   const float w = fmaxf(1e-4f, c);
-  return fminf(1e20f, old / w);
+  return fminf(1e20f, grid_div(old, w));
 }
 
 // The same update applied at the extrapolated point v (momentum in the
@@ -56,7 +73,7 @@ __device__ __forceinline__ float grid_update_value(float c, float old) {
 __device__ __forceinline__ void grid_update_momentum_value(float c, float old, float v, float beta, float& nw,
                                                            float& ext) {
   const float w = fmaxf(1e-4f, c);
-  nw = fminf(1e20f, v / w);
+  nw = fminf(1e20f, grid_div(v, w));
   ext = nw;
   if (old > 0.f && nw > 0.f) ext = fminf(1e20f, nw * __powf(__fdividef(nw, old), beta));
 }

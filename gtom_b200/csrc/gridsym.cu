@@ -334,7 +334,6 @@ gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const f
   constexpr int N1 = Split<H>::N1, N2 = Split<H>::N2;
   constexpr bool WROW = 32 % N2 == 0;    // a row's threads within one warp
   constexpr int XS = N2 * (N1 + 1);      // a row's block of the exchange buffer
-  constexpr bool POW2 = (P & (P - 1)) == 0;
   extern __shared__ float2 smem[];
   float2* tw = smem;
   float2* xb = smem + P;
@@ -379,13 +378,12 @@ gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const f
   }
   four_step<H, true, true, WROW, 2>(v, xb, tw, t, r);
   {
-    // blob: grid_blob_kernel's table index (radius sqrt(x^2 + y^2 + z^2) / P
-    // / funcsampling in FP32 with the row part formed first; the division by
-    // a power-of-two P as the multiplication by its exact reciprocal)
+    // blob: grid_blob_kernel's table index (the reference's radius
+    // sqrt(x^2 + y^2 + z^2) / P / funcsampling with its fast-math square root
+    // and divisions, the row part formed first)
     const int z = (int)(rg / P), y = (int)(rg - (int64_t)z * P);
     const int zp = z < H ? z : z - P, yp = y < H ? y : y - P;
     const float cyz = (float)(yp * yp + zp * zp);
-    const float inv_p = __frcp_rn((float)P);
 #pragma unroll
     for (int m = 0; m < N1; m++) {
       const int n = t + N2 * m;
@@ -393,9 +391,7 @@ gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const f
       for (int h = 0; h < 2; h++) {
         const int x = 2 * n + h;
         const float xp = (float)(x < H ? x : x - P);
-        const float sq = sqrtf(xp * xp + cyz);
-        int ti = (int)((POW2 ? sq * inv_p : sq / (float)P) / funcsampling);
-        ti = ti < kBlobSamples - 1 ? ti : kBlobSamples - 1;
+        const int ti = grid_blob_index_sq(xp * xp + cyz, (float)P, funcsampling);
         const float bv = __ldg(table + ti);
         if (h == 0) v[m].x = v[m].x * inv_n * bv;
         else v[m].y = v[m].y * inv_n * bv;
