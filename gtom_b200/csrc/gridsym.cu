@@ -346,7 +346,10 @@ gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const f
   float2 v[N1];
 #pragma unroll
   for (int m = 0; m < N1; m++) v[m] = row[t + N2 * m];
-  const float2 xH = t == 0 ? row[H] : make_float2(0.f, 0.f);
+  // a C2R takes the x = 0 and x = P/2 terms as real (their imaginary parts,
+  // zero for a Hermitian spectrum, are dropped as cuFFT's C2R drops them)
+  const float2 xH = t == 0 ? make_float2(row[H].x, 0.f) : make_float2(0.f, 0.f);
+  if (t == 0) v[0].y = 0.f;
   __syncthreads();  // twiddles in place
   // pre-twiddle of the C2R.  The partner H - k of k = t + N2 m is element
   // N1-1-m of thread N2-t (t > 0), or element N1-m (H for m = 0) of thread 0
@@ -470,7 +473,12 @@ gridsym_z_kernel(float2* __restrict__ W, const float* __restrict__ Fw, float* __
     float2 xH = make_float2(0.f, 0.f);
 #pragma unroll
     for (int m = 0; m < N1; m++) v[m] = wc[(t + N2 * m) * ES];
-    if (t == 0) xH = wc[H * ES];
+    // the z = 0 and z = P/2 terms of a Hermitian column are real (their
+    // imaginary parts are rounding, dropped as a C2R drops them)
+    if (t == 0) {
+      xH = make_float2(wc[H * ES].x, 0.f);
+      v[0].y = 0.f;
+    }
     // pre-twiddle (exp(-) sum) with the partners H - k through shared memory
     __syncthreads();  // twiddles in place
 #pragma unroll
