@@ -1136,7 +1136,9 @@ static int backproject_launch(float* d_volumeft, float* d_volumeweights, int vx,
   const int choice = path_choice(GTOMRLN_OP_BACKPROJECT);
   const bool plain = !d_ivolume && mag.x == 1.f && mag.y == 0.f && mag.z == 0.f && mag.w == 1.f &&
                      a.ewalddiaminv == 0.f;
-  const bool brick = ndp == 2 && vx == vy && vx == vz && vx >= 4 && (d_volumeft || d_volumeweights) &&
+  // (the brick plans' integer square roots take radii below 4 096: seg_isqrt)
+  const bool brick = ndp == 2 && vx == vy && vx == vz && vx >= 4 && a.rmax2 <= (1 << 24) &&
+                     (d_volumeft || d_volumeweights) &&
                      (choice == GTOMRLN_PATH_BRICK || choice == GTOMRLN_PATH_SEGMENT ||
                       choice == GTOMRLN_PATH_SEGMENT_FP32 ||
                       (choice == GTOMRLN_PATH_AUTO && brick_path_pays(GTOMRLN_OP_BACKPROJECT, vx, batch)));
@@ -1265,7 +1267,7 @@ int gtomrln_backproject_shifted(float* d_volumeft, float* d_volumeweights, int v
   if ((int64_t)a.tiles * batch > 0x7fffffffLL)
     return set_error(GTOMRLN_ERR_INVALID, "backproject_shifted: batch too large for one launch");
   const int choice = path_choice(GTOMRLN_OP_BACKPROJECT);
-  if (ndp == 2 && vx == vy && vx == vz && vx >= 4 && (d_volumeft || d_volumeweights) &&
+  if (ndp == 2 && vx == vy && vx == vz && vx >= 4 && a.rmax2 <= (1 << 24) && (d_volumeft || d_volumeweights) &&
       (choice == GTOMRLN_PATH_BRICK || choice == GTOMRLN_PATH_SEGMENT ||
        (choice == GTOMRLN_PATH_AUTO && brick_path_pays(GTOMRLN_OP_BACKPROJECT, vx, batch))))
     return backproject_shifted_brick(d_volumeft, d_volumeweights, d_projft, d_projweights, d_matrices, d_shifts,

@@ -532,7 +532,8 @@ int gtomrln_project(const float* d_volumeft, int vx, int vy, int vz, float* d_pr
   if (batch && (!d_volumeft || !d_proj || !d_matrices))
     return set_error(GTOMRLN_ERR_INVALID, "project: NULL device pointer");
   const int choice = path_choice(GTOMRLN_OP_PROJECT);
-  if (ndp == 2 && vx == vy && vx == vz && vx >= 4 &&
+  // the brick plans' integer square roots take radii below 4 096 (seg_isqrt)
+  if (ndp == 2 && vx == vy && vx == vz && vx >= 4 && a.rmax2 <= (1 << 24) &&
       (choice == GTOMRLN_PATH_BRICK || choice == GTOMRLN_PATH_SEGMENT ||
        (choice == GTOMRLN_PATH_AUTO && brick_path_pays(GTOMRLN_OP_PROJECT, vx, batch))))
     return project_brick(d_volumeft, d_proj, d_matrices, a, batch, (cudaStream_t)stream,
@@ -592,7 +593,8 @@ int gtomrln_project_shifted(const float* d_volumeft, int vx, int vy, int vz, flo
   if (batch && (!d_volumeft || !d_proj || !d_matrices || !d_shifts || !d_globalweights))
     return set_error(GTOMRLN_ERR_INVALID, "project_shifted: NULL device pointer");
   const int choice = path_choice(GTOMRLN_OP_PROJECT);
-  if (ndp == 2 && vx == vy && vx == vz && vx >= 4 &&
+  // the brick plans' integer square roots take radii below 4 096 (seg_isqrt)
+  if (ndp == 2 && vx == vy && vx == vz && vx >= 4 && a.rmax2 <= (1 << 24) &&
       (choice == GTOMRLN_PATH_BRICK || choice == GTOMRLN_PATH_SEGMENT ||
        (choice == GTOMRLN_PATH_AUTO && brick_path_pays(GTOMRLN_OP_PROJECT, vx, batch))))
     return project_brick(d_volumeft, d_proj, d_matrices, a, batch, (cudaStream_t)stream, 1,

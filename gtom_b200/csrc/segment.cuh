@@ -43,11 +43,22 @@ struct SegBox {
   __device__ __forceinline__ float hi(int r) const { return org(r) + above; }
 };
 
-// Largest u with u^2 <= rem (rem >= 0), exactly.
+// Largest u with u^2 <= rem (0 <= rem < 2^24: radii below 4 096), exactly:
+// the approximate square root is within a unit of the truth there, which the
+// two integer corrections absorb.
 __device__ __forceinline__ int seg_isqrt(int rem) {
-  int r = (int)sqrtf((float)rem);
+  float f;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(f) : "f"((float)rem));
+  int r = (int)f;
   r -= r * r > rem;
   r += (r + 1) * (r + 1) <= rem;
+  return r;
+}
+
+// Approximate reciprocal (a few ulp), for bounds that a margin widens.
+__device__ __forceinline__ float seg_rcp(float a) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
   return r;
 }
 
@@ -89,8 +100,8 @@ __device__ __forceinline__ bool seg_rows(const SegBox& b, const PixelSet& px, in
 }
 
 // Pixel interval [ua, ub] of row v holding the box, clipped to the pixel set
-// (ub < ua when empty).  The bounds multiply by the correctly rounded
-// reciprocal of the column entry: one more rounding, far inside the margin.
+// (ub < ua when empty).  The bounds multiply by the approximate reciprocal of
+// the column entry: a few more ulp, far inside the margin.
 __device__ __forceinline__ void seg_row(const SegBox& b, const PixelSet& px, int v, int& ua, int& ub) {
   float umin = -1.f, umax = (float)px.dimft;
 #pragma unroll
@@ -100,7 +111,7 @@ __device__ __forceinline__ void seg_row(const SegBox& b, const PixelSet& px, int
     // |a| <= 1e-20 moves a * u by < 1e-16 over the row: a u-free test, which
     // the margin keeps conservative (and 1 / a stays finite otherwise)
     if (fabsf(a) > 1e-20f) {
-      const float ra = __frcp_rn(a);
+      const float ra = seg_rcp(a);
       const float e0 = l * ra, e1 = h * ra;
       umin = fmaxf(umin, fminf(e0, e1));
       umax = fminf(umax, fmaxf(e0, e1));
