@@ -512,8 +512,10 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   GTOMRLN_CUFFT_TRY(cufftSetStream(plans.r2c, stream));
   GTOMRLN_CUFFT_TRY(cufftSetStream(plans.c2r, stream));
 
+  // the first iteration's spectrum Fw * Fnw: the cuFFT and fused loops read
+  // it; the symmetric loop makes its own first transform from Fw and Fnw
   grid_init_kernel<<<bc, T, 0, stream>>>(d_weight, oldx, oldy, oldz, Fw, Fnw, convft, g, maskr2,
-                                         iterations > 0 && !warm, 0);
+                                         iterations > 0 && !warm && !sym, 0);
   GTOMRLN_STEP(launch_check("grid_init_kernel"));
   if (warm) {
     GTOMRLN_CUDA_TRY(cudaMemsetAsync(sums, 0, 2 * sizeof(double), stream));
@@ -561,7 +563,7 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
         if (!(last_change <= (double)opt.residual_limit)) {
           // Rejected predicted start: the cold start (sphere mask) from scratch.
           grid_init_kernel<<<bc, T, 0, stream>>>(d_weight, oldx, oldy, oldz, Fw, Fnw, convft, g,
-                                                 maskr2, 1, 0);
+                                                 maskr2, !sym, 0);
           GTOMRLN_STEP(launch_check("grid_init_kernel"));
           need_first = true;
           if (momentum)
@@ -682,7 +684,7 @@ int gridding_batch_run(const GridBatch& b, const float2* data, const float* weig
   GTOMRLN_CUFFT_TRY(cufftSetStream(b.r2c, stream));
   GTOMRLN_CUFFT_TRY(cufftSetStream(b.c2r, stream));
   grid_init_kernel<<<gc, T, 0, stream>>>(weight, b.D, b.D, b.D, b.Fw, b.Fnw, b.convft, g, maskr2,
-                                         iterations > 0, b.wstride);
+                                         iterations > 0 && !sym, b.wstride);
   GTOMRLN_STEP(launch_check("grid_init_kernel"));
   if (fused && iterations > 0) GTOMRLN_STEP(gridfft_first(b.convft, g, b.count, stream));
   if (sym && iterations > 0) GTOMRLN_STEP(gridsym_first(b.convft, g, b.count, b.Fw, b.Fnw, nullptr, stream));
