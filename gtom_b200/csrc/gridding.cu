@@ -252,31 +252,7 @@ __global__ void grid_final_kernel(const float2* __restrict__ data, int oldx, int
   if (i >= g.nc) return;
   int x, y, z;
   split_index(i, g.rowlen, (int64_t)g.rowlen * g.P, g.nc, x, y, z);
-  int zp = z < g.P / 2 + 1 ? z : z - g.P;
-  int yp = y < g.P / 2 + 1 ? y : y - g.P;
-  float r = (float)(zp * zp) + (float)(yp * yp);
-  float rr = r + (float)(x * x);
-  float mask = rr < (float)(g.P * g.P / 4) ? 1.f : 0.f;
-  int zi = zp + oldz / 2, yi = yp + oldy / 2;
-  float2 v = make_float2(0.f, 0.f);
-  if (zi >= 0 && zi < oldz && yi >= 0 && yi < oldy && x < oldx / 2 + 1) {
-    v = __ldg(data + ((int64_t)zi * oldy + yi) * (oldx / 2 + 1) + x);
-    v.x *= mask;
-    v.y *= mask;
-  }
-  if (divide) {
-    float inv = 1.0f / fmaxf(fabsf(Fw[i]), 1e-4f);  // Arithmetics.cu:310-311
-    v.x *= inv;
-    v.y *= inv;
-  } else {
-    float f = Fnw[i];
-    v.x *= f;
-    v.y *= f;
-  }
-  if ((x + y + z) & 1) {
-    v.x = -v.x;
-    v.y = -v.y;
-  }
+  const float2 v = grid_final_value(data, oldx, oldy, oldz, Fw, Fnw, g.P, x, y, z, i, divide != 0);
   convft[i] = v;
 }
 
@@ -294,16 +270,8 @@ __global__ void grid_crop_kernel(const float* __restrict__ conv, float* __restri
   int64_t t = i / ori;
   int y = (int)(t % ori);
   int z = (int)(t / ori);
-  float v = conv[((int64_t)(z + off) * P + (y + off)) * P + (x + off)];
-  int yy = (y - ori / 2) * (y - ori / 2);
-  int zz = (z - ori / 2) * (z - ori / 2);
-  float xx = (float)(x - ori / 2);
-  float r = sqrtf(xx * xx + (float)yy + (float)zz) / (float)P;
-  if (r > 0) {
-    float s = fabsf(r) <= 1e-4f ? 1.f : sinpif(r) / (r * 3.14159265358979f);
-    v /= s * s;
-  }
-  out[i] = v * scale;
+  const float v = conv[((int64_t)(z + off) * P + (y + off)) * P + (x + off)];
+  out[i] = grid_crop_value(v, x, y, z, ori, P, scale);
 }
 
 // ----------------------------------------------------------------- plans --
@@ -470,12 +438,6 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   int st = get_table(radius * pad, alpha, order, &table);
   if (st) return st;
   PlanPair plans;
-  if (!planf || !planb) {
-    st = get_plans(P, &plans);
-    if (st) return st;
-  }
-  if (planf) plans.r2c = planf;
-  if (planb) plans.c2r = planb;
 
   const bool warm = opt.mlp != nullptr && iterations > 0;
   const bool momentum = opt.momentum > 0.f;
@@ -499,9 +461,14 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   const bool sym = (gpath == GTOMRLN_PATH_SYMMETRIC || gpath == GTOMRLN_PATH_AUTO) && gridsym_available(P);
   const bool fused = !sym && gpath == GTOMRLN_PATH_FUSED && !measure_ref && gridfft_available(P, 1);
   bool need_first = true;  // both start with a transform along z
+  if (!sym) {  // the symmetric path makes the final map with its own transforms too
+    if (!planf || !planb) GTOMRLN_STEP(get_plans(P, &plans));
+    if (planf) plans.r2c = planf;
+    if (planb) plans.c2r = planb;
+  }
 
   GTOMRLN_STEP(pool_alloc((void**)&convft, g.nc * sizeof(float2), stream));
-  GTOMRLN_STEP(pool_alloc((void**)&conv, g.nr * sizeof(float), stream));
+  if (!sym) GTOMRLN_STEP(pool_alloc((void**)&conv, g.nr * sizeof(float), stream));
   GTOMRLN_STEP(pool_alloc((void**)&Fw, g.nc * sizeof(float), stream));
   GTOMRLN_STEP(pool_alloc((void**)&Fnw, g.nc * sizeof(float), stream));
   if (momentum) GTOMRLN_STEP(pool_alloc((void**)&V, g.nc * sizeof(float), stream));
@@ -509,8 +476,10 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
     GTOMRLN_STEP(pool_alloc((void**)&change, sizeof(h_change), stream));
   if (warm) GTOMRLN_STEP(pool_alloc((void**)&sums, 2 * sizeof(double), stream));
 
-  GTOMRLN_CUFFT_TRY(cufftSetStream(plans.r2c, stream));
-  GTOMRLN_CUFFT_TRY(cufftSetStream(plans.c2r, stream));
+  if (!sym) {
+    GTOMRLN_CUFFT_TRY(cufftSetStream(plans.r2c, stream));
+    GTOMRLN_CUFFT_TRY(cufftSetStream(plans.c2r, stream));
+  }
 
   // the first iteration's spectrum Fw * Fnw: the cuFFT and fused loops read
   // it; the symmetric loop makes its own first transform from Fw and Fnw
@@ -584,7 +553,11 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
     GTOMRLN_CUDA_TRY(cudaMemcpyAsync(opt.out_fw, Fw, g.nc * sizeof(float), cudaMemcpyDeviceToDevice, stream));
   if (opt.out_fnw)
     GTOMRLN_CUDA_TRY(cudaMemcpyAsync(opt.out_fnw, Fnw, g.nc * sizeof(float), cudaMemcpyDeviceToDevice, stream));
-  if (!opt.weights_only) {
+  if (!opt.weights_only && sym) {
+    GTOMRLN_STEP(gridsym_final(convft, g, 1, (const float2*)d_dataft, oldx, oldy, oldz, 0, Fw, Fnw,
+                               iterations == 0, ori, 1.0f / (float)(pad * pad * pad * ori), d_out, nullptr,
+                               stream));
+  } else if (!opt.weights_only) {
     grid_final_kernel<<<bc, T, 0, stream>>>((const float2*)d_dataft, oldx, oldy, oldz, Fw, Fnw,
                                             convft, g, iterations == 0, 0);
     GTOMRLN_STEP(launch_check("grid_final_kernel"));
@@ -705,6 +678,12 @@ int gridding_batch_run(const GridBatch& b, const float2* data, const float* weig
     GTOMRLN_CUFFT_TRY(cufftExecR2C(b.r2c, b.conv, (cufftComplex*)b.convft));
     grid_update_kernel<<<gc, T, 0, stream>>>(b.convft, b.Fw, b.Fnw, g, it + 1 < iterations, nullptr, nullptr);
     GTOMRLN_STEP(launch_check("grid_update_kernel"));
+  }
+  if (sym) {
+    GTOMRLN_STEP(gridsym_final(b.convft, g, b.count, data, b.D, b.D, b.D, b.wstride, b.Fw, b.Fnw,
+                               iterations == 0, b.ori, 1.0f / (float)(b.pad * b.pad * b.pad * b.ori), nullptr,
+                               outs, stream));
+    goto done;
   }
   grid_final_kernel<<<gc, T, 0, stream>>>(data, b.D, b.D, b.D, b.Fw, b.Fnw, b.convft, g, iterations == 0,
                                           b.wstride);

@@ -78,6 +78,59 @@ __device__ __forceinline__ void grid_update_momentum_value(float c, float old, f
   if (old > 0.f && nw > 0.f) ext = fminf(1e20f, nw * __powf(__fdividef(nw, old), beta));
 }
 
+// One element (x, y, z) of the final spectrum, before its inverse
+// transform: DecenterKernel<tcomplex> of the centred input data
+// (RecFourier.cu:175-179: the masked sample of the old (oldx, oldy, oldz)
+// box), times Fnewweight (RecFourier.cu:206) or divided by
+// max(|Fweight|, 1e-4) when no iteration ran (RecFourier.cu:200-202), then
+// d_Shift by P/2 in every axis (RecFourier.cu:213-214), the factor
+// (-1)^(x+y+z).  i: the element's index on the P grid (rows of P/2 + 1).
+__device__ __forceinline__ float2 grid_final_value(const float2* __restrict__ data, int oldx, int oldy, int oldz,
+                                                   const float* __restrict__ Fw, const float* __restrict__ Fnw,
+                                                   int P, int x, int y, int z, int64_t i, bool divide) {
+  const int zp = z < P / 2 + 1 ? z : z - P;
+  const int yp = y < P / 2 + 1 ? y : y - P;
+  const float r = (float)(zp * zp) + (float)(yp * yp);
+  const float rr = r + (float)(x * x);
+  const float mask = rr < (float)(P * P / 4) ? 1.f : 0.f;
+  const int zi = zp + oldz / 2, yi = yp + oldy / 2;
+  float2 v = make_float2(0.f, 0.f);
+  if (zi >= 0 && zi < oldz && yi >= 0 && yi < oldy && x < oldx / 2 + 1) {
+    v = __ldg(data + ((int64_t)zi * oldy + yi) * (oldx / 2 + 1) + x);
+    v.x *= mask;
+    v.y *= mask;
+  }
+  if (divide) {
+    const float inv = 1.0f / fmaxf(fabsf(Fw[i]), 1e-4f);  // Arithmetics.cu:310-311
+    v.x *= inv;
+    v.y *= inv;
+  } else {
+    const float f = Fnw[i];
+    v.x *= f;
+    v.y *= f;
+  }
+  if ((x + y + z) & 1) {
+    v.x = -v.x;
+    v.y = -v.y;
+  }
+  return v;
+}
+
+// The map value at (x, y, z) of the ori^3 output from the real grid's value
+// v at its centred position: CorrectGriddingKernel's division by sinc^2(r/P)
+// (RecFourier.cu:310-332) and the final scale (RecFourier.cu:237).
+__device__ __forceinline__ float grid_crop_value(float v, int x, int y, int z, int ori, int P, float scale) {
+  const int yy = (y - ori / 2) * (y - ori / 2);
+  const int zz = (z - ori / 2) * (z - ori / 2);
+  const float xx = (float)(x - ori / 2);
+  const float r = sqrtf(xx * xx + (float)yy + (float)zz) / (float)P;
+  if (r > 0) {
+    const float s = fabsf(r) <= 1e-4f ? 1.f : sinpif(r) / (r * 3.14159265358979f);
+    v /= s * s;
+  }
+  return v * scale;
+}
+
 // Adds the block's (d2, o2) to change[0..1] (one atomic pair per block).
 __device__ __forceinline__ void grid_change_reduce(double d2, double o2, double* change) {
   for (int off = 16; off > 0; off >>= 1) {
@@ -150,5 +203,16 @@ int gridsym_first(float2* W, const GridGeom& g, int count, const float* Fw, floa
 int gridsym_iteration(float2* W, const GridGeom& g, int count, const float* table, const float* Fw, float* Fnw,
                       float* V, float beta, bool write_next, double* change, const float* ref,
                       cudaStream_t stream);
+// The final map: the corrected data's inverse transform (decentred and
+// centred per element from the caller's centred data of box (oldx, oldy,
+// oldz), volumes wstride apart; times Fnw, or divided by max(|Fw|, 1e-4)
+// when divide), cropped to the central ori^3 and gridding-corrected, times
+// scale, into out (or outs[volume]).  T needs (P/2+1) P ori complex
+// elements per volume (it fits in the loop's W buffer).  The x = 0 and
+// x = P/2 terms of each transformed row are taken as real: a spectrum whose
+// x = 0 plane is not Hermitian is transformed by its Hermitian part.
+int gridsym_final(float2* T, const GridGeom& g, int count, const float2* data, int oldx, int oldy, int oldz,
+                  int64_t wstride, const float* Fw, const float* Fnw, bool divide, int ori, float scale, float* out,
+                  float* const* outs, cudaStream_t stream);
 
 }  // namespace gtomrln

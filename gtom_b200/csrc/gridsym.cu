@@ -574,6 +574,179 @@ gridsym_z_kernel(float2* __restrict__ W, const float* __restrict__ Fw, float* __
   if (t == 0) wc[H * ES] = make_float2(v[0].x - v[0].y, 0.f);
 }
 
+// -------------------------------------------------------- final map --
+// The final C2R of the corrected data (RecFourier.cu:175-216), cropped to
+// the central ori^3 of the P grid (Padding.cu:22-42) and gridding-corrected
+// (RecFourier.cu:310-332), as three passes of the same transforms: only the
+// z planes and y rows of the crop are ever written.  T: the work array,
+// (P/2+1) x P x ori complex per volume, layout [zc][y][x] (rows of P/2 + 1),
+// inside the loop's W buffer.
+struct FinalArgs {
+  const float2* data;  // centred input spectra (old box), volume stride wstride
+  int oldx, oldy, oldz;
+  int64_t wstride;
+  const float* Fw;     // P-grid weights, volume stride (P/2+1) P P
+  const float* Fnw;
+  int divide;          // no iteration ran: divide by max(|Fw|, 1e-4)
+  int ori, off;        // output box and its offset in the P grid
+  float scale;
+  float* out;          // ori^3 output (one volume), or
+  float* const* outs;  // one output per volume
+};
+
+// Pass 1, per column (x, y) along z: the final spectrum's elements
+// (grid_final_value, straight from the caller's data), inverse transform,
+// the crop's z planes written.  Tiles as in gridsym_z_kernel.
+template <int P>
+__global__ void __launch_bounds__(kCols * Split<P>::N2, (P > 512 ? 1 : 2))
+gridsym_final_z_kernel(float2* __restrict__ T, FinalArgs f, const float2* __restrict__ twg) {
+  constexpr int H = P / 2, R = H + 1;
+  constexpr int N1 = Split<P>::N1, N2 = Split<P>::N2;
+  constexpr int64_t NC = (int64_t)R * P * P;
+  extern __shared__ float2 smem[];
+  float2* tw = smem;
+  float2* xb = smem + P;
+  load_twiddles(tw, twg, P);
+  const int c = threadIdx.x & (kCols - 1), t = threadIdx.x / kCols;
+  constexpr int kMain = P * (H / kCols);
+  const int b = blockIdx.x;
+  int x, y;
+  if (b < kMain) {
+    y = b / (H / kCols);
+    x = (b - y * (H / kCols)) * kCols + c;
+  } else {
+    y = (b - kMain) * kCols + c;
+    x = H;
+  }
+  const int64_t vol = blockIdx.y;
+  const float2* data = f.data + vol * f.wstride;
+  const float* Fw = f.Fw + vol * NC;
+  const float* Fnw = f.Fnw + vol * NC;
+  float2* tv = T + vol * ((int64_t)R * P * f.ori);
+  float2 v[N1];
+#pragma unroll
+  for (int m = 0; m < N1; m++) {
+    const int z = t + N2 * m;
+    v[m] = grid_final_value(data, f.oldx, f.oldy, f.oldz, Fw, Fnw, P, x, y, z, ((int64_t)z * P + y) * R + x,
+                            f.divide != 0);
+  }
+  __syncthreads();  // twiddles in place
+  four_step<P, true, false, false, 1>(v, xb, tw, t, c);
+#pragma unroll
+  for (int m = 0; m < N1; m++) {
+    const int z = t + N2 * m - f.off;
+    if ((unsigned)z < (unsigned)f.ori) tv[((int64_t)z * P + y) * R + x] = v[m];
+  }
+}
+
+// Pass 2, per column (x, zc) along y: inverse transform, the crop's rows
+// written to rows 0 .. ori-1 of the plane (each CTA has read its whole
+// column before it writes).  Tiles: 16 consecutive x < P/2 at one zc, then
+// x = P/2 at 16 consecutive zc.
+template <int P>
+__global__ void __launch_bounds__(kCols * Split<P>::N2, (P > 512 ? 1 : 2))
+gridsym_final_y_kernel(float2* __restrict__ T, int ori, int off, const float2* __restrict__ twg) {
+  constexpr int H = P / 2, R = H + 1;
+  constexpr int N1 = Split<P>::N1, N2 = Split<P>::N2;
+  extern __shared__ float2 smem[];
+  float2* tw = smem;
+  float2* xb = smem + P;
+  load_twiddles(tw, twg, P);
+  const int c = threadIdx.x & (kCols - 1), t = threadIdx.x / kCols;
+  const int kMain = (H / kCols) * ori;
+  const int b = blockIdx.x;
+  int zc, x;
+  if (b < kMain) {
+    zc = b / (H / kCols);
+    x = (b - zc * (H / kCols)) * kCols + c;
+  } else {
+    zc = (b - kMain) * kCols + c;
+    x = H;
+  }
+  const bool in = zc < ori;
+  float2* col = T + (int64_t)blockIdx.y * ((int64_t)R * P * ori) + (in ? ((int64_t)zc * P * R + x) : 0);
+  float2 v[N1];
+#pragma unroll
+  for (int m = 0; m < N1; m++) v[m] = in ? col[(int64_t)(t + N2 * m) * R] : make_float2(0.f, 0.f);
+  __syncthreads();  // twiddles in place
+  four_step<P, true, false, false, 1>(v, xb, tw, t, c);
+  if (in) {
+#pragma unroll
+    for (int m = 0; m < N1; m++) {
+      const int yc = t + N2 * m - off;
+      if ((unsigned)yc < (unsigned)ori) col[(int64_t)yc * R] = v[m];
+    }
+  }
+}
+
+// Pass 3, per row (yc, zc): C2R along x (the x = 0 and x = P/2 terms taken
+// as real), the crop's x, the gridding correction and scale.  A CTA takes
+// 16 consecutive rows of the ori x ori crop (rows past it idle).
+template <int P>
+__global__ void __launch_bounds__(kCols * Split<P / 2>::N2, (P > 512 ? 2 : 3))
+gridsym_final_x_kernel(const float2* __restrict__ T, FinalArgs f, const float2* __restrict__ twg) {
+  constexpr int H = P / 2, R = H + 1;
+  constexpr int N1 = Split<H>::N1, N2 = Split<H>::N2;
+  constexpr bool WROW = 32 % N2 == 0;
+  constexpr int XS = N2 * (N1 + 1);
+  extern __shared__ float2 smem[];
+  float2* tw = smem;
+  float2* xb = smem + P;
+  load_twiddles(tw, twg, P);
+  const int t = threadIdx.x % N2, r = threadIdx.x / N2;
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned partner = WROW ? (lane & ~(unsigned)(N2 - 1)) | ((unsigned)(N2 - t) & (N2 - 1)) : lane;
+  const int ori = f.ori;
+  const int64_t rr = (int64_t)blockIdx.x * kCols + r;  // zc * ori + yc
+  const bool in = rr < (int64_t)ori * ori;
+  const int zc = in ? (int)(rr / ori) : 0, yc = in ? (int)(rr - (int64_t)zc * ori) : 0;
+  const int64_t vol = blockIdx.y;
+  const float2* row = T + vol * ((int64_t)R * P * ori) + ((int64_t)zc * P + yc) * R;
+  float2 v[N1];
+#pragma unroll
+  for (int m = 0; m < N1; m++) v[m] = in ? row[t + N2 * m] : make_float2(0.f, 0.f);
+  const float2 xH = t == 0 && in ? make_float2(row[H].x, 0.f) : make_float2(0.f, 0.f);
+  if (t == 0) v[0].y = 0.f;
+  __syncthreads();  // twiddles in place
+  {
+    float2 z[N1];
+    if constexpr (WROW) {
+#pragma unroll
+      for (int m = 0; m < N1; m++) {
+        const float2 sh = make_float2(__shfl_sync(0xffffffffu, v[N1 - 1 - m].x, partner),
+                                      __shfl_sync(0xffffffffu, v[N1 - 1 - m].y, partner));
+        const float2 xm = t != 0 ? sh : (m == 0 ? xH : v[(N1 - m) % N1]);
+        z[m] = c2r_pre<true>(v[m], xm, tw[t + N2 * m]);
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < N1; m++) xb[r * XS + t + N2 * m] = v[m];
+      if (t == 0) xb[r * XS + H] = xH;
+      __syncthreads();
+#pragma unroll
+      for (int m = 0; m < N1; m++) {
+        const int k = t + N2 * m;
+        z[m] = c2r_pre<true>(v[m], xb[r * XS + H - k], tw[k]);
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < N1; m++) v[m] = z[m];
+  }
+  four_step<H, true, true, WROW, 2>(v, xb, tw, t, r);
+  if (!in) return;  // after the last collective of the row's warp / block
+  float* out = f.outs ? f.outs[vol] : f.out;
+  float* orow = out + ((int64_t)zc * ori + yc) * ori;
+#pragma unroll
+  for (int m = 0; m < N1; m++) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int xc = 2 * (t + N2 * m) + h - f.off;
+      if ((unsigned)xc < (unsigned)ori)
+        orow[xc] = grid_crop_value(h ? v[m].y : v[m].x, xc, yc, zc, ori, P, f.scale);
+    }
+  }
+}
+
 // ------------------------------------------------------------- launch --
 template <int P>
 struct SymSizes {
@@ -592,6 +765,12 @@ struct SymSizes {
 template <int P>
 int set_attributes() {
   using Z = SymSizes<P>;
+  GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(gridsym_final_z_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)Z::y_smem));
+  GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(gridsym_final_y_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)Z::y_smem));
+  GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(gridsym_final_x_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)Z::x_smem));
   GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(gridsym_y_kernel<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)Z::y_smem));
   GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(gridsym_y_kernel<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -645,6 +824,21 @@ int run_iteration(float2* W, int count, const float* table, const float* Fw, flo
     gridsym_z_kernel<P, kZIter, false><<<grid, Z::xz_threads, Z::z_smem, stream>>>(W, Fw, Fnw, V, tw, beta,
                                                                                    write_next, change, ref);
   GTOMRLN_LAUNCH_CHECK("gridsym_z_kernel");
+  return GTOMRLN_OK;
+}
+
+template <int P>
+int run_final(float2* T, int count, const FinalArgs& f, const float2* tw, cudaStream_t stream) {
+  using Z = SymSizes<P>;
+  constexpr int H = P / 2;
+  gridsym_final_z_kernel<P><<<dim3(Z::z_tiles, count), Z::y_threads, Z::y_smem, stream>>>(T, f, tw);
+  GTOMRLN_LAUNCH_CHECK("gridsym_final_z_kernel");
+  const unsigned ytiles = (unsigned)((H / kCols) * f.ori + (f.ori + kCols - 1) / kCols);
+  gridsym_final_y_kernel<P><<<dim3(ytiles, count), Z::y_threads, Z::y_smem, stream>>>(T, f.ori, f.off, tw);
+  GTOMRLN_LAUNCH_CHECK("gridsym_final_y_kernel");
+  const unsigned xtiles = (unsigned)(((int64_t)f.ori * f.ori + kCols - 1) / kCols);
+  gridsym_final_x_kernel<P><<<dim3(xtiles, count), Z::xz_threads, Z::x_smem, stream>>>(T, f, tw);
+  GTOMRLN_LAUNCH_CHECK("gridsym_final_x_kernel");
   return GTOMRLN_OK;
 }
 
@@ -712,6 +906,32 @@ int gridsym_iteration(float2* W, const GridGeom& g, int count, const float* tabl
     return run_iteration<decltype(p)::value>(W, count, table, Fw, Fnw, V, beta, write_next, change, ref, tw,
                                              stream);
   });
+}
+
+int gridsym_final(float2* T, const GridGeom& g, int count, const float2* data, int oldx, int oldy, int oldz,
+                  int64_t wstride, const float* Fw, const float* Fnw, bool divide, int ori, float scale, float* out,
+                  float* const* outs, cudaStream_t stream) {
+  if (ori <= 0 || ori > g.P) return set_error(GTOMRLN_ERR_INVALID, "gridsym_final: output box %d", ori);
+  int st = ensure_attributes(g.P);
+  if (st) return st;
+  const float2* tw = nullptr;
+  st = fft_twiddles(g.P, &tw);
+  if (st) return st;
+  FinalArgs f;
+  f.data = data;
+  f.oldx = oldx;
+  f.oldy = oldy;
+  f.oldz = oldz;
+  f.wstride = wstride;
+  f.Fw = Fw;
+  f.Fnw = Fnw;
+  f.divide = divide ? 1 : 0;
+  f.ori = ori;
+  f.off = g.P / 2 - ori / 2;
+  f.scale = scale;
+  f.out = out;
+  f.outs = outs;
+  return with_grid(g.P, [&](auto p) { return run_final<decltype(p)::value>(T, count, f, tw, stream); });
 }
 
 // Forgets the launch attributes set on device dev (a context reset drops

@@ -20,10 +20,12 @@ from tests.helpers import rel_l2
 pytestmark = pytest.mark.gpu
 
 
-def _inputs(ori, pad=2, seed=0):
+def _inputs(ori, pad=2, seed=0, hermitian=True):
     """Centred accumulators of a synthetic backprojection: blob data, smooth
-    positive weights inside the padded sphere (symmetric on the x = 0 plane,
-    as the backprojector's second insertions make them)."""
+    positive weights inside the padded sphere, both Hermitian on the x = 0
+    plane (w(-y, -z) = w(y, z), data(-y, -z) = conj data(y, z)), as the
+    backprojector's second insertions make them; hermitian=False leaves the
+    data's x = 0 plane as drawn."""
     rng = np.random.default_rng(seed + ori)
     D = ori * pad + 1
     z, y, x = np.meshgrid(np.arange(D) - D // 2, np.arange(D) - D // 2, np.arange(D // 2 + 1), indexing="ij")
@@ -32,6 +34,8 @@ def _inputs(ori, pad=2, seed=0):
          * rng.uniform(0.8, 1.2, r.shape)).astype(np.float32)
     w[:, :, 0] = 0.5 * (w[:, :, 0] + w[::-1, ::-1, 0])
     data = ((rng.normal(size=r.shape) + 1j * rng.normal(size=r.shape)) * w * np.exp(-r / ori)).astype(np.complex64)
+    if hermitian:
+        data[:, :, 0] = 0.5 * (data[:, :, 0] + np.conj(data[::-1, ::-1, 0]))
     return data, w, D
 
 
@@ -74,10 +78,11 @@ def test_symmetric_weights_match_cufft(gtom_lib, cuda, iterations):
     assert rel_l2(fnw["symmetric"], fnw["direct"]) <= 2e-6
 
 
-@pytest.mark.parametrize("ori,iterations", [(16, 10), (24, 3), (32, 10)])
+@pytest.mark.parametrize("ori,iterations", [(16, 10), (24, 3), (32, 10), (32, 0), (48, 2)])
 def test_symmetric_gridding_matches_oracle(gtom_lib, cuda, ori, iterations):
     """FP64 oracle (numpy pocketfft restatement of RecFourier.cu:98-241);
-    ori 24 is a grid the path does not take (P = 48): cuFFT runs there."""
+    ori 24 is a grid the path does not take (P = 48): cuFFT runs there.
+    0 iterations: the final map divides by max(|Fw|, 1e-4)."""
     data, w, D = _inputs(ori, seed=7)
     out = torch.zeros(ori ** 3, device="cuda")
     _on("symmetric", lambda: G.d_ReconstructGridding(_dev(data), _dev(w), out, (ori,) * 3, (D,) * 3, 2, 0, 0,
@@ -148,7 +153,7 @@ def test_symmetric_warm_start(gtom_lib, cuda):
 def test_symmetric_gridding_matches_cufft_at_800(gtom_lib, cuda):
     """P = 800 (400^3 at padding 2, the large combined configuration's grid;
     radix-5 transforms, rows of the x pass spanning warps), 3 iterations;
-    inputs made on the GPU (2.6 GB of accumulators)."""
+    inputs made on the GPU (2.6 GB of accumulators), Hermitian on x = 0."""
     ori, pad = 400, 2
     D = ori * pad + 1
     g = torch.Generator(device="cuda")
@@ -161,6 +166,7 @@ def test_symmetric_gridding_matches_cufft_at_800(gtom_lib, cuda):
     w[:, :, 0] = 0.5 * (w[:, :, 0] + torch.flip(w[:, :, 0], (0, 1)))
     data = torch.complex(torch.randn(w.shape, device="cuda", generator=g),
                          torch.randn(w.shape, device="cuda", generator=g)) * (w * torch.exp(-r / ori))
+    data[:, :, 0] = 0.5 * (data[:, :, 0] + torch.flip(data[:, :, 0], (0, 1)).conj())
     del r
     d_w, d_data = w.reshape(-1).contiguous(), data.reshape(-1).contiguous()
     del w, data
@@ -175,21 +181,34 @@ def test_symmetric_gridding_matches_cufft_at_800(gtom_lib, cuda):
     assert err <= 1e-5, err
 
 
-def test_symmetric_gridding_takes_asymmetric_weights_as_cufft_does(gtom_lib, cuda):
+def test_symmetric_gridding_takes_asymmetric_weights_as_the_oracle(gtom_lib, cuda):
     """Weights whose x = 0 plane is not symmetric (a caller's own, not a
-    backprojection's): the C2R of both paths takes the plane's symmetric part
-    (the x = 0 and x = P/2 terms of each transformed row as real), so the maps
-    still agree."""
-    ori = 64
+    backprojection's): every C2R of the path takes the x = 0 and x = P/2
+    terms of each transformed row as real, i.e. transforms the Hermitian part
+    of the plane, as numpy's irfftn in the oracle does."""
+    ori = 32
     data, w, D = _inputs(ori, seed=13)
     rng = np.random.default_rng(13)
     w = w.copy()
     w[:, :, 0] *= rng.uniform(0.7, 1.3, w[:, :, 0].shape).astype(np.float32)
-    d_data, d_w = _dev(data), _dev(w)
-    maps = {}
-    for path in ("direct", "symmetric"):
-        out = torch.full((ori ** 3,), float("nan"), device="cuda")
-        _on(path, lambda: G.d_ReconstructGridding(d_data, d_w, out, (ori,) * 3, (D,) * 3, 2, 0, 0, 10))
-        maps[path] = out.cpu().numpy()
-    assert np.all(np.isfinite(maps["symmetric"]))
-    assert rel_l2(maps["symmetric"], maps["direct"]) <= 1e-5
+    out = torch.full((ori ** 3,), float("nan"), device="cuda")
+    _on("symmetric", lambda: G.d_ReconstructGridding(_dev(data), _dev(w), out, (ori,) * 3, (D,) * 3, 2, 0, 0, 10))
+    ref = O.reconstruct_gridding(data, w, ori, (D, D, D), 2, iterations=10)
+    got = out.cpu().numpy().reshape(ori, ori, ori)
+    assert np.all(np.isfinite(got))
+    assert rel_l2(got, ref) <= 1e-4
+
+
+def test_symmetric_final_map_of_non_hermitian_data_follows_the_oracle(gtom_lib, cuda):
+    """Data whose x = 0 plane is not Hermitian: the final transform takes its
+    Hermitian part, as numpy's irfftn in the oracle does.  (cuFFT's 3D C2R
+    is not specified on such input, and its result differs from the oracle's
+    at P = 128 and 256; a backprojection's data is Hermitian there.)"""
+    ori = 64
+    data, w, D = _inputs(ori, seed=17, hermitian=False)
+    out = torch.full((ori ** 3,), float("nan"), device="cuda")
+    _on("symmetric", lambda: G.d_ReconstructGridding(_dev(data), _dev(w), out, (ori,) * 3, (D,) * 3, 2, 0, 0, 2))
+    ref = O.reconstruct_gridding(data, w, ori, (D, D, D), 2, iterations=2)
+    got = out.cpu().numpy().reshape(ori, ori, ori)
+    assert np.all(np.isfinite(got))
+    assert rel_l2(got, ref) <= 1e-4
