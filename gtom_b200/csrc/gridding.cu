@@ -38,34 +38,41 @@ double kaiser_fourier_value(double w, double a, double alpha, int m);  // below
 // RecFourier.cu:264-285 (DecenterKernel) for the weights + SphereMask.cu:167-189
 // (Fnewweight = 1 inside r^2 < (r_max*pad)^2) + Iteration1Kernel
 // (RecFourier.cu:287-291).  old* are the centred input dims.
-__global__ void grid_init_kernel(const float* __restrict__ weight, int oldx, int oldy, int oldz,
-                                 float* __restrict__ Fw, float* __restrict__ Fnw,
-                                 float2* __restrict__ convft, GridGeom g, int maskr2,
-                                 int write_conv, int64_t wstride) {
+// One warp per (y, z) row of the P grid (lanes along x; grid (rows / 8,
+// volumes), 256 threads): the row's decentring and radii once, no index
+// divisions per element.
+constexpr int kInitWarps = 8;
+__global__ void __launch_bounds__(32 * kInitWarps)
+grid_init_kernel(const float* __restrict__ weight, int oldx, int oldy, int oldz, float* __restrict__ Fw,
+                 float* __restrict__ Fnw, float2* __restrict__ convft, GridGeom g, int maskr2, int write_conv,
+                 int64_t wstride) {
   const int64_t b = blockIdx.y;  // volume of a batch (stacks of equal volumes)
   weight += b * wstride;
   Fw += b * g.nc;
   Fnw += b * g.nc;
   convft += b * g.nc;
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= g.nc) return;
-  int x, y, z;
-  split_index(i, g.rowlen, (int64_t)g.rowlen * g.P, g.nc, x, y, z);
-  int zp = z < g.P / 2 + 1 ? z : z - g.P;
-  int yp = y < g.P / 2 + 1 ? y : y - g.P;
-  float r = (float)(zp * zp) + (float)(yp * yp);
-  float rr = r + (float)(x * x);
-  float mask = rr < (float)(g.P * g.P / 4) ? 1.f : 0.f;
-  int zi = zp + oldz / 2, yi = yp + oldy / 2;
-  float w = 0.f;
-  if (zi >= 0 && zi < oldz && yi >= 0 && yi < oldy && x < oldx / 2 + 1)
-    w = __ldg(weight + ((int64_t)zi * oldy + yi) * (oldx / 2 + 1) + x) * mask;
-  Fw[i] = w;
-  // SphereMaskFTKernel uses y < dims.y/2+1 ? y : y - dims.x, the same split.
-  int r2 = x * x + yp * yp + zp * zp;
-  float nw = r2 < maskr2 ? 1.f : 0.f;
-  Fnw[i] = nw;
-  if (write_conv) convft[i] = make_float2(w * nw, 0.f);
+  const int row = blockIdx.x * kInitWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (row >= g.P * g.P) return;
+  const int z = row / g.P, y = row - z * g.P;
+  const int zp = z < g.P / 2 + 1 ? z : z - g.P;
+  const int yp = y < g.P / 2 + 1 ? y : y - g.P;
+  const float r = (float)(zp * zp) + (float)(yp * yp);
+  const int zi = zp + oldz / 2, yi = yp + oldy / 2;
+  const bool in_yz = zi >= 0 && zi < oldz && yi >= 0 && yi < oldy;
+  const float* wrow = weight + (in_yz ? ((int64_t)zi * oldy + yi) * (oldx / 2 + 1) : 0);
+  const int64_t base = (int64_t)row * g.rowlen;
+  const int yz2 = yp * yp + zp * zp;
+  for (int x = lane; x < g.rowlen; x += 32) {
+    const float rr = r + (float)(x * x);
+    const float mask = rr < (float)(g.P * g.P / 4) ? 1.f : 0.f;
+    float w = 0.f;
+    if (in_yz && x < oldx / 2 + 1) w = __ldg(wrow + x) * mask;
+    Fw[base + x] = w;
+    // SphereMaskFTKernel uses y < dims.y/2+1 ? y : y - dims.x, the same split.
+    const float nw = x * x + yz2 < maskr2 ? 1.f : 0.f;
+    Fnw[base + x] = nw;
+    if (write_conv) convft[base + x] = make_float2(w * nw, 0.f);
+  }
 }
 
 // conv <- (conv * 1/P^3) * blob(r): d_IFFTC2R's renormalisation
@@ -454,6 +461,7 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
   bool warm_live = warm;
   const int T = 256;
   unsigned bc = (unsigned)((g.nc + T - 1) / T);
+  const unsigned init_blocks = (unsigned)((P * P + kInitWarps - 1) / kInitWarps);
   // The symmetric-spectrum iteration (gridsym.cu; default on power-of-two
   // grids P = 64 .. 512) or, when the caller chose it, the fused FFT
   // iteration (gridfft.cu); cuFFT transforms otherwise and for the final map.
@@ -483,8 +491,8 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
 
   // the first iteration's spectrum Fw * Fnw: the cuFFT and fused loops read
   // it; the symmetric loop makes its own first transform from Fw and Fnw
-  grid_init_kernel<<<bc, T, 0, stream>>>(d_weight, oldx, oldy, oldz, Fw, Fnw, convft, g, maskr2,
-                                         iterations > 0 && !warm && !sym, 0);
+  grid_init_kernel<<<init_blocks, 32 * kInitWarps, 0, stream>>>(d_weight, oldx, oldy, oldz, Fw, Fnw, convft, g,
+                                                                maskr2, iterations > 0 && !warm && !sym, 0);
   GTOMRLN_STEP(launch_check("grid_init_kernel"));
   if (warm) {
     GTOMRLN_CUDA_TRY(cudaMemsetAsync(sums, 0, 2 * sizeof(double), stream));
@@ -531,8 +539,8 @@ static int reconstruct(const float* d_dataft, const float* d_weight, float* d_ou
         warm_live = false;
         if (!(last_change <= (double)opt.residual_limit)) {
           // Rejected predicted start: the cold start (sphere mask) from scratch.
-          grid_init_kernel<<<bc, T, 0, stream>>>(d_weight, oldx, oldy, oldz, Fw, Fnw, convft, g,
-                                                 maskr2, !sym, 0);
+          grid_init_kernel<<<init_blocks, 32 * kInitWarps, 0, stream>>>(d_weight, oldx, oldy, oldz, Fw, Fnw,
+                                                                        convft, g, maskr2, !sym, 0);
           GTOMRLN_STEP(launch_check("grid_init_kernel"));
           need_first = true;
           if (momentum)
@@ -650,13 +658,14 @@ int gridding_batch_run(const GridBatch& b, const float2* data, const float* weig
   const int maskr2 = (r_max * b.pad) * (r_max * b.pad);
   const int T = 256;
   dim3 gc((unsigned)((g.nc + T - 1) / T), (unsigned)b.count);
+  const dim3 gi((unsigned)((b.P * b.P + kInitWarps - 1) / kInitWarps), (unsigned)b.count);
   int st = GTOMRLN_OK;
   const int gpath = path_choice(GTOMRLN_OP_GRIDDING);
   const bool sym = b.sym && (gpath == GTOMRLN_PATH_AUTO || gpath == GTOMRLN_PATH_SYMMETRIC);
   const bool fused = !sym && b.fused && gpath == GTOMRLN_PATH_FUSED;
   GTOMRLN_CUFFT_TRY(cufftSetStream(b.r2c, stream));
   GTOMRLN_CUFFT_TRY(cufftSetStream(b.c2r, stream));
-  grid_init_kernel<<<gc, T, 0, stream>>>(weight, b.D, b.D, b.D, b.Fw, b.Fnw, b.convft, g, maskr2,
+  grid_init_kernel<<<gi, 32 * kInitWarps, 0, stream>>>(weight, b.D, b.D, b.D, b.Fw, b.Fnw, b.convft, g, maskr2,
                                          iterations > 0 && !sym, b.wstride);
   GTOMRLN_STEP(launch_check("grid_init_kernel"));
   if (fused && iterations > 0) GTOMRLN_STEP(gridfft_first(b.convft, g, b.count, stream));

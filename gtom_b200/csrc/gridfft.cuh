@@ -84,36 +84,47 @@ __device__ __forceinline__ void grid_update_momentum_value(float c, float old, f
 // box), times Fnewweight (RecFourier.cu:206) or divided by
 // max(|Fweight|, 1e-4) when no iteration ran (RecFourier.cu:200-202), then
 // d_Shift by P/2 in every axis (RecFourier.cu:213-214), the factor
-// (-1)^(x+y+z).  i: the element's index on the P grid (rows of P/2 + 1).
-__device__ __forceinline__ float2 grid_final_value(const float2* __restrict__ data, int oldx, int oldy, int oldz,
-                                                   const float* __restrict__ Fw, const float* __restrict__ Fnw,
-                                                   int P, int x, int y, int z, int64_t i, bool divide) {
+// (-1)^(x+y+z).  In two steps, so that callers can issue their loads
+// first: grid_final_source gives the element's index in the input box (-1:
+// outside it, the value 0), grid_final_apply the value from the sample v
+// and the weight w (Fw[i] when divide, else Fnw[i]; i: the element's index
+// on the P grid, rows of P/2 + 1).
+__device__ __forceinline__ int64_t grid_final_source(int oldx, int oldy, int oldz, int P, int x, int y, int z) {
+  const int zp = z < P / 2 + 1 ? z : z - P;
+  const int yp = y < P / 2 + 1 ? y : y - P;
+  const int zi = zp + oldz / 2, yi = yp + oldy / 2;
+  if (zi >= 0 && zi < oldz && yi >= 0 && yi < oldy && x < oldx / 2 + 1)
+    return ((int64_t)zi * oldy + yi) * (oldx / 2 + 1) + x;
+  return -1;
+}
+__device__ __forceinline__ float2 grid_final_apply(float2 v, float w, int P, int x, int y, int z, bool divide) {
   const int zp = z < P / 2 + 1 ? z : z - P;
   const int yp = y < P / 2 + 1 ? y : y - P;
   const float r = (float)(zp * zp) + (float)(yp * yp);
   const float rr = r + (float)(x * x);
   const float mask = rr < (float)(P * P / 4) ? 1.f : 0.f;
-  const int zi = zp + oldz / 2, yi = yp + oldy / 2;
-  float2 v = make_float2(0.f, 0.f);
-  if (zi >= 0 && zi < oldz && yi >= 0 && yi < oldy && x < oldx / 2 + 1) {
-    v = __ldg(data + ((int64_t)zi * oldy + yi) * (oldx / 2 + 1) + x);
-    v.x *= mask;
-    v.y *= mask;
-  }
+  v.x *= mask;
+  v.y *= mask;
   if (divide) {
-    const float inv = 1.0f / fmaxf(fabsf(Fw[i]), 1e-4f);  // Arithmetics.cu:310-311
+    const float inv = 1.0f / fmaxf(fabsf(w), 1e-4f);  // Arithmetics.cu:310-311
     v.x *= inv;
     v.y *= inv;
   } else {
-    const float f = Fnw[i];
-    v.x *= f;
-    v.y *= f;
+    v.x *= w;
+    v.y *= w;
   }
   if ((x + y + z) & 1) {
     v.x = -v.x;
     v.y = -v.y;
   }
   return v;
+}
+__device__ __forceinline__ float2 grid_final_value(const float2* __restrict__ data, int oldx, int oldy, int oldz,
+                                                   const float* __restrict__ Fw, const float* __restrict__ Fnw,
+                                                   int P, int x, int y, int z, int64_t i, bool divide) {
+  const int64_t src = grid_final_source(oldx, oldy, oldz, P, x, y, z);
+  const float2 v = src >= 0 ? __ldg(data + src) : make_float2(0.f, 0.f);
+  return grid_final_apply(v, divide ? Fw[i] : Fnw[i], P, x, y, z, divide);
 }
 
 // The map value at (x, y, z) of the ori^3 output from the real grid's value

@@ -19,13 +19,15 @@
 // are zero up to rounding; the kept real parts are the same sums.
 //
 // Per iteration (W: the (P/2+1) x P x (P/2+1) complex work array, layout
-// [z][y][x] with rows of P/2 + 1 like the reference's spectra):
-//   gridsym_y_kernel<INV>  inverse transform along y of W (columns of 16
-//                          consecutive x at one z, or of x = P/2 at 16 z);
+// [z][y][x] with rows of P/2 + 2, the last element padding, so that rows
+// start on 16-byte boundaries as tensor copies need):
+//   gridsym_y_tma_kernel<INV>  inverse transform along y of W (columns of 16
+//                          consecutive x at one z, staged in shared memory
+//                          by tensor copies, or of x = P/2 at 16 z);
 //   gridsym_x_kernel       per row (y, z): C2R along x, times blob(r)/P^3
 //                          (IFFT.cu:36-46 normalisation, RecFourier.cu:
 //                          243-262 table), R2C along x;
-//   gridsym_y_kernel<FWD>  forward transform along y;
+//   gridsym_y_tma_kernel<FWD>  forward transform along y;
 //   gridsym_z_kernel       per column (x, y): Hermitian-to-real transform
 //                          along z (the real part of the R2C), Iteration2
 //                          (the weight update, plain or with momentum, the
@@ -55,7 +57,10 @@
 // compile-time constants (inside the in-register DFTs).  All transforms are
 // unnormalised, as cuFFT's; the 1/P^3 of the reference's C2R rides with the
 // blob.
+#include <cuda.h>  // CUtensorMap and its enums (the encoder is looked up at run time)
+
 #include <algorithm>
+#include <cstdint>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -246,6 +251,42 @@ __device__ __forceinline__ void four_step(float2* v, float2* xb, const float2* t
   }
 }
 
+// The same transform with the exchange in J = N1/N2 rounds of N2 x N2 values
+// per column (round j: the outputs k1 = N2 j .. N2 j + N2 - 1 of every
+// thread's N1-point DFT), so that the exchange buffer holds 16 N2^2 values
+// instead of 16 N; columns-fast layout (16 columns per element, each
+// half-warp's access one 128-byte row).  Round j's N2-point DFTs return
+// X(k1 + N1 k2), k1 = N2 j + t, i.e. outputs t + N2 (j + J k2), written back
+// into the registers the round's inputs left and renamed at the end.
+template <int N, bool INV>
+__device__ __forceinline__ void four_step_rounds(float2* v, float2* xb, const float2* tw, int t, int c) {
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2, J = N1 / N2;
+  static_assert(J * N2 == N1, "four_step_rounds: N1 must be a multiple of N2");
+  dftr<N1, INV>(v);
+#pragma unroll
+  for (int k1 = 1; k1 < N1; k1++) v[k1] = cmul(v[k1], twiddle<1, INV>(tw, t * k1));
+#pragma unroll
+  for (int j = 0; j < J; j++) {
+    __syncthreads();  // the previous round's (or the caller's) reads of xb are done
+#pragma unroll
+    for (int k = 0; k < N2; k++) xb[(t * N2 + k) * kCols + c] = v[N2 * j + k];
+    __syncthreads();
+    float2 u[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; n2++) u[n2] = xb[(n2 * N2 + t) * kCols + c];
+    dftr<N2, INV>(u);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) v[N2 * j + k2] = u[k2];
+  }
+  float2 w[N1];
+#pragma unroll
+  for (int j = 0; j < J; j++)
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) w[j + J * k2] = v[N2 * j + k2];
+#pragma unroll
+  for (int m = 0; m < N1; m++) v[m] = w[m];
+}
+
 // The pre-twiddle of a Hermitian-to-real transform of length P = 2H as an
 // H-point complex transform: Z(k) = (X(k) + conj X(H-k)) + i e(sg k/P)
 // (X(k) - conj X(H-k)) (sg = +1: the inverse C2R; -1: the forward sum); the
@@ -277,45 +318,179 @@ __device__ __forceinline__ void load_twiddles(float2* tw, const float2* __restri
   for (int m = threadIdx.x; m < P; m += blockDim.x) tw[m] = __ldg(twg + m);
 }
 
+// ------------------------------------------------------- TMA staging --
+// Tensor copies global -> shared completed on an mbarrier (no multicast, no
+// cluster).  Every wait is bounded: after kWaitLimitNs without completion
+// the kernel records a fault (g_gridsym_fault), which the final map turns
+// into NaN output.
+constexpr unsigned long long kWaitLimitNs = 1000000000ull;  // 1 s
+__device__ int g_gridsym_fault;
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits for the phase of the given parity; false after kWaitLimitNs.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > kWaitLimitNs) return false;
+  }
+}
+// Orders this thread's earlier shared-memory accesses (and, after a CTA
+// barrier, the CTA's) before the following tensor copy's writes.
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_addr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+      : "memory");
+}
+
 // ------------------------------------------------------------ y pass --
-// The transform along y of W (INV: exp(+), the inverse of the C2R; else the
-// forward of the R2C).  Grid: (tiles, volumes); tiles are 16 consecutive
-// x < P/2 at one z, then x = P/2 at 16 consecutive z.  16 N2 threads.
+// W's rows hold P/2 + 2 complex elements (the last one padding), so that
+// every row starts on a 16-byte boundary, as tensor copies need.
+template <int P>
+constexpr int w_pitch() { return P / 2 + 2; }
+
+// Sizes of the staged y pass: a tile (16 columns x P rows) arrives as NB
+// tensor boxes of BOX rows (a box has at most 256 rows).
+template <int P>
+struct YStage {
+  static constexpr int NB = (P + 255) / 256;
+  static constexpr int BOX = P / NB;
+  static_assert(BOX * NB == P && BOX <= 256, "YStage: rows must split into equal boxes");
+  static constexpr int N2 = Split<P>::N2;
+  static constexpr size_t stage_bytes = sizeof(float2) * kCols * P;
+  static constexpr size_t xb_bytes = sizeof(float2) * kCols * N2 * N2;
+  // 1 KB for aligning the staging buffer, staging, exchange, twiddles
+  static constexpr size_t smem = 1024 + stage_bytes + xb_bytes + sizeof(float2) * P;
+};
+
+// The y pass, persistent, over nyq + tiles work units: first the columns
+// x = P/2 (16 consecutive z of one volume per unit, plain loads), then the
+// tiles of 16 consecutive x < P/2 at one (volume, z), each of which arrives
+// in shared memory by tensor copies (map: W as floats, dims {2 (P/2+2), P,
+// (P/2+1) volumes}, box {32, BOX, 1}).  CTA i starts with unit i and takes
+// the next from a counter as soon as it holds its current unit in
+// registers, starting the next tile's copy then, so the copy runs during the
+// transform and the stores and the slower x = P/2 units leave no tail.  The
+// counter and the count of finished CTAs sit in the padding element of W's
+// first row (the last CTA zeroes both for the next launch; the first
+// transform zeroes them once).  The transform is four_step_rounds (the
+// exchange buffer and the staging buffer fit two CTAs per SM at P = 512).
 template <int P, bool INV>
 __global__ void __launch_bounds__(kCols * Split<P>::N2, (P > 512 ? 1 : 2))
-gridsym_y_kernel(float2* __restrict__ W, const float2* __restrict__ twg) {
-  constexpr int H = P / 2, R = H + 1;
+gridsym_y_tma_kernel(const __grid_constant__ CUtensorMap map, float2* __restrict__ W,
+                     const float2* __restrict__ twg, int tiles, int nyq) {
+  using Y = YStage<P>;
+  constexpr int H = P / 2, RW = w_pitch<P>();
   constexpr int N1 = Split<P>::N1, N2 = Split<P>::N2;
-  extern __shared__ float2 smem[];
-  float2* tw = smem;
-  float2* xb = smem + P;
+  constexpr int XT = H / kCols;                    // tiles per (volume, z)
+  constexpr int NQ = (H + 1 + kCols - 1) / kCols;  // x = P/2 units per volume
+  extern __shared__ unsigned char sraw[];
+  __shared__ unsigned long long bar;
+  __shared__ int next_s;
+  float2* stage = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(sraw) + 1023) & ~(uintptr_t)1023);
+  float2* xb = stage + kCols * P;
+  float2* tw = xb + kCols * N2 * N2;
+  int* sched = reinterpret_cast<int*>(W + H + 1);  // {counter, finished CTAs}
   load_twiddles(tw, twg, P);
   const int c = threadIdx.x & (kCols - 1), t = threadIdx.x / kCols;
-  constexpr int kMain = (H / kCols) * (H + 1);
-  const int b = blockIdx.x;
-  int64_t base, cs;
-  int ncols;
-  if (b < kMain) {
-    const int z = b / (H / kCols), xt = b - z * (H / kCols);
-    base = (int64_t)z * P * R + xt * kCols;
-    cs = 1;
-    ncols = kCols;
-  } else {
-    const int z0 = (b - kMain) * kCols;
-    base = (int64_t)z0 * P * R + H;
-    cs = (int64_t)P * R;
-    ncols = min(kCols, H + 1 - z0);
+  const int total = nyq + tiles;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  auto issue = [&](int tile) {  // one thread
+    const int vz = tile / XT, xt = tile - vz * XT;
+    fence_proxy_async();
+    mbar_expect_tx(&bar, (unsigned)Y::stage_bytes);
+#pragma unroll
+    for (int k = 0; k < Y::NB; k++)
+      tma_load_3d(stage + k * Y::BOX * kCols, &map, xt * 2 * kCols, k * Y::BOX, vz, &bar);
+  };
+  // the next unit, and its copy when it is a tile (one thread)
+  auto take_next = [&]() {
+    const int u = (int)gridDim.x + atomicAdd(sched, 1);
+    next_s = u;
+    if (u >= nyq && u < total) issue(u - nyq);
+  };
+  int u = blockIdx.x;
+  if (threadIdx.x == 0 && u >= nyq && u < total) issue(u - nyq);
+  unsigned parity = 0;
+  bool fault = false;
+  while (u < total) {
+    float2 v[N1];
+    float2* col;
+    bool in = true;
+    if (u >= nyq) {
+      const bool ok = mbar_wait(&bar, parity);
+      if (!__syncthreads_and(ok)) {
+        if (threadIdx.x == 0) atomicExch(&g_gridsym_fault, 1);
+        mbar_wait(&bar, parity);  // once more for the copy in flight, then leave
+        fault = true;
+        break;
+      }
+      parity ^= 1u;
+#pragma unroll
+      for (int m = 0; m < N1; m++) v[m] = stage[(t + N2 * m) * kCols + c];
+      __syncthreads();  // the staging buffer is read
+      if (threadIdx.x == 0) take_next();
+      const int tile = u - nyq, vz = tile / XT, xt = tile - vz * XT;
+      col = W + (int64_t)vz * P * RW + xt * kCols + c;
+    } else {
+      const int vol = u / NQ, z = (u - vol * NQ) * kCols + c;
+      in = z <= H;
+      col = W + ((int64_t)vol * (H + 1) + (in ? z : 0)) * P * RW + H;
+#pragma unroll
+      for (int m = 0; m < N1; m++) v[m] = in ? col[(int64_t)(t + N2 * m) * RW] : make_float2(0.f, 0.f);
+      __syncthreads();  // every thread has read next_s
+      if (threadIdx.x == 0) take_next();
+    }
+    four_step_rounds<P, INV>(v, xb, tw, t, c);  // begins with a CTA barrier: next_s is visible after it
+    if (in) {
+#pragma unroll
+      for (int m = 0; m < N1; m++) col[(int64_t)(t + N2 * m) * RW] = v[m];
+    }
+    u = next_s;
   }
-  const bool in = c < ncols;
-  float2* col = W + (int64_t)blockIdx.y * ((int64_t)(H + 1) * P * R) + base + (in ? c * cs : 0);
-  float2 v[N1];
-#pragma unroll
-  for (int m = 0; m < N1; m++) v[m] = in ? col[(int64_t)(t + N2 * m) * R] : make_float2(0.f, 0.f);
-  __syncthreads();  // twiddles in place
-  four_step<P, INV, false, false, 1>(v, xb, tw, t, c);
-  if (in) {
-#pragma unroll
-    for (int m = 0; m < N1; m++) col[(int64_t)(t + N2 * m) * R] = v[m];
+  // the last CTA to finish zeroes the counter for the next launch (a CTA
+  // leaves the loop only once the counter is past the last unit)
+  __syncthreads();
+  if (threadIdx.x == 0 && !fault) {
+    __threadfence();
+    if (atomicAdd(sched + 1, 1) == (int)gridDim.x - 1) {
+      sched[0] = 0;
+      sched[1] = 0;
+      __threadfence();
+    }
   }
 }
 
@@ -330,7 +505,7 @@ template <int P>
 __global__ void __launch_bounds__(kCols * Split<P / 2>::N2, (P > 512 ? 2 : 3))
 gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const float* __restrict__ table,
                  float inv_n, float funcsampling) {
-  constexpr int H = P / 2, R = H + 1;
+  constexpr int H = P / 2, RW = w_pitch<P>();
   constexpr int N1 = Split<H>::N1, N2 = Split<H>::N2;
   constexpr bool WROW = 32 % N2 == 0;    // a row's threads within one warp
   constexpr int XS = N2 * (N1 + 1);      // a row's block of the exchange buffer
@@ -342,7 +517,7 @@ gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const f
   const unsigned lane = threadIdx.x & 31;
   const unsigned partner = WROW ? (lane & ~(unsigned)(N2 - 1)) | ((unsigned)(N2 - t) & (N2 - 1)) : lane;
   const int64_t rg = (int64_t)blockIdx.x * kCols + r;  // z * P + y
-  float2* row = W + (int64_t)blockIdx.y * ((int64_t)(H + 1) * P * R) + rg * R;
+  float2* row = W + (int64_t)blockIdx.y * ((int64_t)(H + 1) * P * RW) + rg * RW;
   float2 v[N1];
 #pragma unroll
   for (int m = 0; m < N1; m++) v[m] = row[t + N2 * m];
@@ -444,11 +619,12 @@ __global__ void __launch_bounds__(kCols * Split<P / 2>::N2, (P > 512 ? 2 : 3))
 gridsym_z_kernel(float2* __restrict__ W, const float* __restrict__ Fw, float* __restrict__ Fnw,
                  float* __restrict__ V, const float2* __restrict__ twg, float beta, int write_next,
                  double* __restrict__ change, const float* __restrict__ ref) {
-  constexpr int H = P / 2, R = H + 1;
+  constexpr int H = P / 2, R = H + 1, RW = w_pitch<P>();
   constexpr int N1 = Split<H>::N1, N2 = Split<H>::N2;
-  constexpr int64_t NC = (int64_t)R * P * P;        // spectrum elements per volume
-  constexpr int64_t NW = (int64_t)(H + 1) * P * R;  // W elements per volume
-  constexpr int64_t ES = (int64_t)P * R;            // element stride along z (W and the weights)
+  constexpr int64_t NC = (int64_t)R * P * P;         // spectrum elements per volume
+  constexpr int64_t NW = (int64_t)(H + 1) * P * RW;  // W elements per volume
+  constexpr int64_t ES = (int64_t)P * R;             // element stride along z of the weights
+  constexpr int64_t EW = (int64_t)P * RW;            // and of W
   extern __shared__ float2 smem[];
   float2* tw = smem;
   float2* xb = smem + P;
@@ -456,27 +632,32 @@ gridsym_z_kernel(float2* __restrict__ W, const float* __restrict__ Fw, float* __
   const int c = threadIdx.x & (kCols - 1), t = threadIdx.x / kCols;
   constexpr int kMain = P * (H / kCols);
   const int b = blockIdx.x;
-  int64_t base, cs;
+  int x, y;
   if (b < kMain) {
-    const int y = b / (H / kCols), xt = b - y * (H / kCols);
-    base = (int64_t)y * R + xt * kCols;
-    cs = 1;
+    y = b / (H / kCols);
+    x = (b - y * (H / kCols)) * kCols + c;
   } else {
-    base = (int64_t)(b - kMain) * kCols * R + H;
-    cs = R;
+    y = (b - kMain) * kCols + c;
+    x = H;
   }
   const int64_t vol = blockIdx.y;
-  float2* wc = W + vol * NW + base + c * cs;
-  const int64_t wo = vol * NC + base + c * cs;
+  if (MODE == kZFirst && b == 0 && vol == 0 && threadIdx.x == 0) {
+    // the y pass's work counter (padding of W's first row): zero for its first launch
+    int* sched = reinterpret_cast<int*>(W + H + 1);
+    sched[0] = 0;
+    sched[1] = 0;
+  }
+  float2* wc = W + vol * NW + (int64_t)y * RW + x;
+  const int64_t wo = vol * NC + (int64_t)y * R + x;
   float2 v[N1];
   if (MODE == kZIter) {
     float2 xH = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int m = 0; m < N1; m++) v[m] = wc[(t + N2 * m) * ES];
+    for (int m = 0; m < N1; m++) v[m] = wc[(t + N2 * m) * EW];
     // the z = 0 and z = P/2 terms of a Hermitian column are real (their
     // imaginary parts are rounding, dropped as a C2R drops them)
     if (t == 0) {
-      xH = make_float2(wc[H * ES].x, 0.f);
+      xH = make_float2(wc[H * EW].x, 0.f);
       v[0].y = 0.f;
     }
     // pre-twiddle (exp(-) sum) with the partners H - k through shared memory
@@ -569,9 +750,9 @@ gridsym_z_kernel(float2* __restrict__ W, const float* __restrict__ Fw, float* __
 #pragma unroll
   for (int m = 0; m < N1; m++) {
     const int k = t + N2 * m, km = k == 0 ? 0 : H - k;
-    wc[k * ES] = r2c_post<true>(v[m], xb[km * kPitch + c], tw[k]);
+    wc[k * EW] = r2c_post<true>(v[m], xb[km * kPitch + c], tw[k]);
   }
-  if (t == 0) wc[H * ES] = make_float2(v[0].x - v[0].y, 0.f);
+  if (t == 0) wc[H * EW] = make_float2(v[0].x - v[0].y, 0.f);
 }
 
 // -------------------------------------------------------- final map --
@@ -623,12 +804,26 @@ gridsym_final_z_kernel(float2* __restrict__ T, FinalArgs f, const float2* __rest
   const float* Fw = f.Fw + vol * NC;
   const float* Fnw = f.Fnw + vol * NC;
   float2* tv = T + vol * ((int64_t)R * P * f.ori);
+  // the loads of CH elements first (an index outside the input box reads
+  // element 0, zeroed after), then their corrections
+  const float* wsrc = f.divide ? Fw : Fnw;
+  constexpr int CH = N1 <= 20 ? N1 : (N1 % 20 == 0 ? 20 : (N1 % 16 == 0 ? 16 : 12));
+  static_assert(N1 % CH == 0, "gridsym_final_z_kernel: chunks");
   float2 v[N1];
 #pragma unroll
-  for (int m = 0; m < N1; m++) {
-    const int z = t + N2 * m;
-    v[m] = grid_final_value(data, f.oldx, f.oldy, f.oldz, Fw, Fnw, P, x, y, z, ((int64_t)z * P + y) * R + x,
-                            f.divide != 0);
+  for (int m0 = 0; m0 < N1; m0 += CH) {
+    float wt[CH];
+#pragma unroll
+    for (int q = 0; q < CH; q++) {
+      const int z = t + N2 * (m0 + q);
+      const int64_t src = grid_final_source(f.oldx, f.oldy, f.oldz, P, x, y, z);
+      v[m0 + q] = __ldg(data + (src >= 0 ? src : 0));
+      if (src < 0) v[m0 + q] = make_float2(0.f, 0.f);
+      wt[q] = __ldg(wsrc + ((int64_t)z * P + y) * R + x);
+    }
+#pragma unroll
+    for (int q = 0; q < CH; q++)
+      v[m0 + q] = grid_final_apply(v[m0 + q], wt[q], P, x, y, t + N2 * (m0 + q), f.divide != 0);
   }
   __syncthreads();  // twiddles in place
   four_step<P, true, false, false, 1>(v, xb, tw, t, c);
@@ -734,6 +929,8 @@ gridsym_final_x_kernel(const float2* __restrict__ T, FinalArgs f, const float2* 
   }
   four_step<H, true, true, WROW, 2>(v, xb, tw, t, r);
   if (!in) return;  // after the last collective of the row's warp / block
+  // a y pass whose tensor copies did not complete left W unusable: NaN map
+  const bool fault = g_gridsym_fault != 0;
   float* out = f.outs ? f.outs[vol] : f.out;
   float* orow = out + ((int64_t)zc * ori + yc) * ori;
 #pragma unroll
@@ -742,7 +939,8 @@ gridsym_final_x_kernel(const float2* __restrict__ T, FinalArgs f, const float2* 
     for (int h = 0; h < 2; h++) {
       const int xc = 2 * (t + N2 * m) + h - f.off;
       if ((unsigned)xc < (unsigned)ori)
-        orow[xc] = grid_crop_value(h ? v[m].y : v[m].x, xc, yc, zc, ori, P, f.scale);
+        orow[xc] = fault ? __int_as_float(0x7fc00000) : grid_crop_value(h ? v[m].y : v[m].x, xc, yc, zc, ori, P,
+                                                                        f.scale);
     }
   }
 }
@@ -765,16 +963,16 @@ struct SymSizes {
 template <int P>
 int set_attributes() {
   using Z = SymSizes<P>;
+  GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(gridsym_y_tma_kernel<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)YStage<P>::smem));
+  GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(gridsym_y_tma_kernel<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)YStage<P>::smem));
   GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(gridsym_final_z_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)Z::y_smem));
   GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(gridsym_final_y_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)Z::y_smem));
   GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(gridsym_final_x_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)Z::x_smem));
-  GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(gridsym_y_kernel<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)Z::y_smem));
-  GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(gridsym_y_kernel<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)Z::y_smem));
   GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(gridsym_x_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)Z::x_smem));
   GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(gridsym_z_kernel<P, kZFirst, false>,
@@ -785,6 +983,66 @@ int set_attributes() {
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Z::z_smem));
   GTOMRLN_CUDA_TRY(cudaFuncSetAttribute(gridsym_z_kernel<P, kZIter, true>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Z::z_smem));
+  return GTOMRLN_OK;
+}
+
+// cuTensorMapEncodeTiled, looked up once through the runtime (no link
+// against the driver library).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+std::once_flag g_encode_once;
+EncodeTiledFn g_encode = nullptr;
+
+// The tensor map of W for the staged y pass: floats, dims {2 (P/2+2), P,
+// (P/2+1) count} (the z planes of all volumes in one dimension), row stride
+// (P/2+2) 8 bytes (a multiple of 16), box {32, BOX, 1}.
+template <int P>
+int w_tensor_map(float2* W, int count, CUtensorMap* map) {
+  std::call_once(g_encode_once, [] {
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void**)&g_encode, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      g_encode = nullptr;
+    cudaGetLastError();
+  });
+  if (!g_encode) return set_error(GTOMRLN_ERR_CUDA, "gridsym: cuTensorMapEncodeTiled is not available");
+  if (reinterpret_cast<uintptr_t>(W) % 16)
+    return set_error(GTOMRLN_ERR_INVALID, "gridsym: work array not 16-byte aligned");
+  constexpr int RW = w_pitch<P>();
+  const cuuint64_t dims[3] = {(cuuint64_t)2 * RW, (cuuint64_t)P, (cuuint64_t)(P / 2 + 1) * (cuuint64_t)count};
+  const cuuint64_t strides[2] = {(cuuint64_t)RW * sizeof(float2), (cuuint64_t)P * RW * sizeof(float2)};
+  const cuuint32_t box[3] = {2 * kCols, (cuuint32_t)YStage<P>::BOX, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, W, dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(GTOMRLN_ERR_CUDA, "gridsym: tensor map encoding failed (%d)", (int)r);
+  return GTOMRLN_OK;
+}
+
+// CTAs of the staged y pass resident on the device (both directions have the
+// same resources), per (device, context, P).
+std::mutex g_ctas_mutex;
+std::map<std::tuple<int, unsigned long long, int>, int> g_ctas;
+
+template <int P>
+int y_stage_ctas(int* out) {
+  int dev = 0;
+  GTOMRLN_CUDA_TRY(cudaGetDevice(&dev));
+  const auto key = std::make_tuple(dev, context_id(), P);
+  std::lock_guard<std::mutex> lock(g_ctas_mutex);
+  auto it = g_ctas.find(key);
+  if (it == g_ctas.end()) {
+    int per_sm = 0, sms = 0;
+    GTOMRLN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gridsym_y_tma_kernel<P, true>,
+                                                                   SymSizes<P>::y_threads, YStage<P>::smem));
+    GTOMRLN_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (per_sm < 1) return set_error(GTOMRLN_ERR_CUDA, "gridsym: staged y pass does not fit an SM");
+    it = g_ctas.emplace(key, per_sm * sms).first;
+  }
+  *out = it->second;
   return GTOMRLN_OK;
 }
 
@@ -809,13 +1067,22 @@ int run_iteration(float2* W, int count, const float* table, const float* Fw, flo
   using Z = SymSizes<P>;
   const float inv_n = 1.0f / ((float)P * (float)P * (float)P);
   const float funcsampling = (float)(0.5 / kBlobSamples);
-  gridsym_y_kernel<P, true><<<dim3(Z::y_tiles, count), Z::y_threads, Z::y_smem, stream>>>(W, tw);
-  GTOMRLN_LAUNCH_CHECK("gridsym_y_kernel (inverse)");
+  CUtensorMap map;
+  int st = w_tensor_map<P>(W, count, &map);
+  if (st) return st;
+  int ctas = 0;
+  st = y_stage_ctas<P>(&ctas);
+  if (st) return st;
+  const int tiles = (P / 2 / kCols) * (P / 2 + 1) * count;
+  const unsigned grid_y = (unsigned)std::min(tiles, ctas);
+  const int nyq = (P / 2 + 1 + kCols - 1) / kCols * count;
+  gridsym_y_tma_kernel<P, true><<<grid_y, Z::y_threads, YStage<P>::smem, stream>>>(map, W, tw, tiles, nyq);
+  GTOMRLN_LAUNCH_CHECK("gridsym_y_tma_kernel (inverse)");
   gridsym_x_kernel<P><<<dim3(Z::x_tiles, count), Z::xz_threads, Z::x_smem, stream>>>(W, tw, table, inv_n,
                                                                                      funcsampling);
   GTOMRLN_LAUNCH_CHECK("gridsym_x_kernel");
-  gridsym_y_kernel<P, false><<<dim3(Z::y_tiles, count), Z::y_threads, Z::y_smem, stream>>>(W, tw);
-  GTOMRLN_LAUNCH_CHECK("gridsym_y_kernel (forward)");
+  gridsym_y_tma_kernel<P, false><<<grid_y, Z::y_threads, YStage<P>::smem, stream>>>(map, W, tw, tiles, nyq);
+  GTOMRLN_LAUNCH_CHECK("gridsym_y_tma_kernel (forward)");
   const dim3 grid(Z::z_tiles, count);
   if (V)
     gridsym_z_kernel<P, kZIter, true><<<grid, Z::xz_threads, Z::z_smem, stream>>>(W, Fw, Fnw, V, tw, beta,
@@ -937,10 +1204,19 @@ int gridsym_final(float2* T, const GridGeom& g, int count, const float2* data, i
 // Forgets the launch attributes set on device dev (a context reset drops
 // them with the context).
 int release_gridsym_caches(int dev, unsigned long long /*ctx*/) {
-  std::lock_guard<std::mutex> lock(g_attr_mutex);
-  for (auto it = g_attr_done.begin(); it != g_attr_done.end();) {
-    if (std::get<0>(it->first) == dev) it = g_attr_done.erase(it);
-    else ++it;
+  {
+    std::lock_guard<std::mutex> lock(g_attr_mutex);
+    for (auto it = g_attr_done.begin(); it != g_attr_done.end();) {
+      if (std::get<0>(it->first) == dev) it = g_attr_done.erase(it);
+      else ++it;
+    }
+  }
+  {
+    std::lock_guard<std::mutex> lock(g_ctas_mutex);
+    for (auto it = g_ctas.begin(); it != g_ctas.end();) {
+      if (std::get<0>(it->first) == dev) it = g_ctas.erase(it);
+      else ++it;
+    }
   }
   return GTOMRLN_OK;
 }
