@@ -77,6 +77,10 @@ def parse_args():
     ap.add_argument("--config5", action="store_true",
                     help="instead of the bench: the large combined configuration (400^3, padding 2, "
                          "2 half-maps x 4 classes) end to end on one GPU")
+    ap.add_argument("--gridding-profile", type=int, default=-1, metavar="ITERATIONS",
+                    help="instead of the bench: one gridding reconstruction of synthetic accumulators "
+                         "(256^3 at padding 2, P = 512) with this many iterations after one warm-up "
+                         "run, for profilers (prints its time)")
     ap.add_argument("--c5-particles", type=int, default=1000000)
     ap.add_argument("--c5-chunk", type=int, default=20000)
     return ap.parse_args()
@@ -1415,6 +1419,42 @@ def run_config5(args):
         "accumulators_gb": round(8 * nvox * 12 / 1e9, 2)}), flush=True)
 
 
+def run_gridding_profile(iterations):
+    """One d_ReconstructGridding of smooth synthetic accumulators (a radial
+    weight profile with 20 % noise, Hermitian on x = 0, and random data
+    under it) at the bench's box, after one warm-up run: the launch sequence
+    a profiler captures for the gridding kernels."""
+    import torch
+    import gtom_b200 as G
+    dev = torch.device("cuda:0")
+    n, D = BOX, BOX * PAD + 1
+    g = torch.Generator(device=dev)
+    g.manual_seed(512)
+    z = torch.arange(D, device=dev, dtype=torch.float32) - D // 2
+    x = torch.arange(D // 2 + 1, device=dev, dtype=torch.float32)
+    r = torch.sqrt(z[:, None, None] ** 2 + z[None, :, None] ** 2 + x[None, None, :] ** 2)
+    w = torch.where(r < n * PAD / 2, 1.0 + 30.0 * torch.exp(-r / (n / 3)), torch.zeros_like(r))
+    w = w * (0.8 + 0.4 * torch.rand(w.shape, device=dev, generator=g))
+    w[:, :, 0] = 0.5 * (w[:, :, 0] + torch.flip(w[:, :, 0], (0, 1)))
+    data = torch.complex(torch.randn(w.shape, device=dev, generator=g),
+                         torch.randn(w.shape, device=dev, generator=g)) * (w * torch.exp(-r / n))
+    data[:, :, 0] = 0.5 * (data[:, :, 0] + torch.flip(data[:, :, 0], (0, 1)).conj())
+    del r
+    acc_w, acc_ft = w.reshape(-1).contiguous(), data.reshape(-1).contiguous()
+    del w, data
+    out = torch.zeros(n ** 3, device=dev)
+    G.d_ReconstructGridding(acc_ft, acc_w, out, (n,) * 3, (D,) * 3, PAD, 0, 0, iterations)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    G.d_ReconstructGridding(acc_ft, acc_w, out, (n,) * 3, (D,) * 3, PAD, 0, 0, iterations)
+    b.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"gridding_profile": {"P": n * PAD, "iterations": iterations,
+                                           "ms": round(a.elapsed_time(b), 3),
+                                           "finite": bool(torch.isfinite(out).all().item())}}))
+
+
 def main():
     args = parse_args()
     if args.sweep:
@@ -1422,6 +1462,9 @@ def main():
         return
     if args.config5:
         run_config5(args)
+        return
+    if args.gridding_profile >= 0:
+        run_gridding_profile(args.gridding_profile)
         return
     if args.impl == "reference":
         run_reference(args)
