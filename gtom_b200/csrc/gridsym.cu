@@ -562,17 +562,44 @@ gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const f
     const int z = (int)(rg / P), y = (int)(rg - (int64_t)z * P);
     const int zp = z < H ? z : z - P, yp = y < H ? y : y - P;
     const float cyz = (float)(yp * yp + zp * zp);
+    auto blob = [&](int x) {
+      const float xp = (float)(x < H ? x : x - P);
+      return __ldg(table + grid_blob_index_sq(xp * xp + cyz, (float)P, funcsampling));
+    };
+    if constexpr (WROW) {
+      // x and P - x have the same radius, bit for bit: the blob values of
+      // elements m <= N1/2 are computed, the others taken from the thread
+      // holding P - x (x = 2n: element N1-1-m of thread N2-t, or element
+      // N1-m of thread 0 for t = 0; x = 2n+1: element N1-1-m of thread
+      // N2-1-t)
+      constexpr int M0 = N1 / 2;
+      const unsigned partner1 = (lane & ~(unsigned)(N2 - 1)) | (unsigned)(N2 - 1 - t);
+      float bl[M0 + 1][2];
 #pragma unroll
-    for (int m = 0; m < N1; m++) {
-      const int n = t + N2 * m;
+      for (int m = 0; m <= M0; m++) {
+        bl[m][0] = blob(2 * (t + N2 * m));
+        bl[m][1] = blob(2 * (t + N2 * m) + 1);
+      }
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int x = 2 * n + h;
-        const float xp = (float)(x < H ? x : x - P);
-        const int ti = grid_blob_index_sq(xp * xp + cyz, (float)P, funcsampling);
-        const float bv = __ldg(table + ti);
-        if (h == 0) v[m].x = v[m].x * inv_n * bv;
-        else v[m].y = v[m].y * inv_n * bv;
+      for (int m = 0; m < N1; m++) {
+        float b0, b1;
+        if (m <= M0) {
+          b0 = bl[m][0];
+          b1 = bl[m][1];
+        } else {
+          const float s0 = __shfl_sync(0xffffffffu, bl[N1 - 1 - m][0], partner);
+          b0 = t != 0 ? s0 : bl[N1 - m][0];
+          b1 = __shfl_sync(0xffffffffu, bl[N1 - 1 - m][1], partner1);
+        }
+        v[m].x = v[m].x * inv_n * b0;
+        v[m].y = v[m].y * inv_n * b1;
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < N1; m++) {
+        const int n = t + N2 * m;
+        v[m].x = v[m].x * inv_n * blob(2 * n);
+        v[m].y = v[m].y * inv_n * blob(2 * n + 1);
       }
     }
   }
