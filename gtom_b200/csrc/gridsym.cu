@@ -978,7 +978,6 @@ struct SymSizes {
   static constexpr int H = P / 2;
   static constexpr int y_threads = kCols * Split<P>::N2;
   static constexpr int xz_threads = kCols * Split<H>::N2;
-  static constexpr int y_tiles = (H / kCols) * (H + 1) + (H + 1 + kCols - 1) / kCols;
   static constexpr int x_tiles = (H + 1) * P / kCols;
   static constexpr int z_tiles = P * (H / kCols) + P / kCols;
   // twiddle table + exchange buffer
