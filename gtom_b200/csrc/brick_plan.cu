@@ -304,28 +304,78 @@ segment_pairs_kernel(const float* __restrict__ mats, BrickGrid g, float pmax, fl
   const float n0 = m[1] * m[5] - m[2] * m[4], n1 = m[2] * m[3] - m[0] * m[5], n2 = m[0] * m[4] - m[1] * m[3];
   const float R2 = R * R * (1.f + 1e-5f) + 1e-3f;
   const float lo_pad = below + widen + kSegMargin, hi_pad = (float)g.B + widen + kSegMargin;
-  for (int base = 0; base < g.nbricks; base += kPairThreads) {
-    const int b = base + tid;
-    bool hit = false;
-    if (b < g.nbricks) {
-      const int3 o = brick_origin(g, b);
-      const float lo0 = o.x - lo_pad, lo1 = o.y - lo_pad, lo2 = o.z - lo_pad;
-      const float hi0 = o.x + hi_pad, hi1 = o.y + hi_pad, hi2 = o.z + hi_pad;
-      const float c0 = 0.5f * (lo0 + hi0), c1 = 0.5f * (lo1 + hi1), c2 = 0.5f * (lo2 + hi2);
-      const float h0 = 0.5f * (hi0 - lo0), h1 = 0.5f * (hi1 - lo1), h2 = 0.5f * (hi2 - lo2);
-      const float dist = fabsf(n0 * c0 + n1 * c1 + n2 * c2);
-      const float reach = fabsf(n0) * h0 + fabsf(n1) * h1 + fabsf(n2) * h2;
-      const float eps = 1e-5f * (fabsf(n0) * (fabsf(c0) + h0) + fabsf(n1) * (fabsf(c1) + h1) +
-                                 fabsf(n2) * (fabsf(c2) + h2));
-      const float d0 = fmaxf(0.f, fmaxf(lo0, -hi0)), d1 = fmaxf(0.f, fmaxf(lo1, -hi1)),
-                  d2 = fmaxf(0.f, fmaxf(lo2, -hi2));
-      hit = dist <= reach + eps && d0 * d0 + d1 * d1 + d2 * d2 <= R2;
+  // The exact test of brick b: its widened box meets the slice's plane and
+  // the sphere of radius R.
+  auto crosses = [&](int b) {
+    const int3 o = brick_origin(g, b);
+    const float lo0 = o.x - lo_pad, lo1 = o.y - lo_pad, lo2 = o.z - lo_pad;
+    const float hi0 = o.x + hi_pad, hi1 = o.y + hi_pad, hi2 = o.z + hi_pad;
+    const float c0 = 0.5f * (lo0 + hi0), c1 = 0.5f * (lo1 + hi1), c2 = 0.5f * (lo2 + hi2);
+    const float h0 = 0.5f * (hi0 - lo0), h1 = 0.5f * (hi1 - lo1), h2 = 0.5f * (hi2 - lo2);
+    const float dist = fabsf(n0 * c0 + n1 * c1 + n2 * c2);
+    const float reach = fabsf(n0) * h0 + fabsf(n1) * h1 + fabsf(n2) * h2;
+    const float eps = 1e-5f * (fabsf(n0) * (fabsf(c0) + h0) + fabsf(n1) * (fabsf(c1) + h1) +
+                               fabsf(n2) * (fabsf(c2) + h2));
+    const float d0 = fmaxf(0.f, fmaxf(lo0, -hi0)), d1 = fmaxf(0.f, fmaxf(lo1, -hi1)),
+                d2 = fmaxf(0.f, fmaxf(lo2, -hi2));
+    return dist <= reach + eps && d0 * d0 + d1 * d1 + d2 * d2 <= R2;
+  };
+  // Candidates: along the axis k where the normal is largest, a column of
+  // bricks (fixed indices on the other two axes) meets the plane only where
+  // the centre's k coordinate is within (reach + eps) / |n_k| of the plane's
+  // over the column; that range, widened well beyond the float error of the
+  // test, is searched with the exact test, so the hits are the ones testing
+  // every brick finds (in another order).  A zero or non-finite normal tests
+  // every brick.
+  const float an0 = fabsf(n0), an1 = fabsf(n1), an2 = fabsf(n2);
+  const int k = an0 >= an1 && an0 >= an2 ? 0 : (an1 >= an2 ? 1 : 2);
+  const float ank = k == 0 ? an0 : (k == 1 ? an1 : an2);
+  const bool columns = ank > 1e-30f && isfinite(n0) && isfinite(n1) && isfinite(n2) && isfinite(R2);
+  if (columns) {
+    const int nb[3] = {g.nbx, g.nby, g.nbz};
+    const float base[3] = {0.f, (float)g.ylo, (float)g.zlo};
+    const float nv[3] = {n0, n1, n2};
+    const int i = k == 0 ? 1 : 0, j = k == 2 ? 1 : 2;  // the other two axes
+    const float d = 0.5f * (hi_pad - lo_pad), h = 0.5f * (hi_pad + lo_pad);
+    const float reach = (an0 + an1 + an2) * h;
+    // |c| <= extent of the grid on every axis: a bound on the test's eps
+    const float cmax = fmaxf(fmaxf((float)(g.nbx * g.B), fabsf(base[1])), fabsf(base[2])) +
+                       (float)(g.nby > g.nbz ? g.nby : g.nbz) * (float)g.B + h;
+    const float slack = reach + 1e-5f * (an0 + an1 + an2) * (cmax + h);
+    const float invB = 1.f / (float)g.B;
+    const int ncol = nb[i] * nb[j];
+    for (int col = tid; col < ncol; col += kPairThreads) {
+      const int a = col % nb[i], bj = col / nb[i];
+      const float ci = base[i] + (float)(a * g.B) + d, cj = base[j] + (float)(bj * g.B) + d;
+      const float sp = nv[i] * ci + nv[j] * cj;
+      // centre k coordinate c with |n_k c + sp| <= slack
+      const float mid = -sp / nv[k], half = slack / ank;
+      const float margin = 1e-3f * (fabsf(mid) + half) + 0.01f * (float)g.B;
+      float flo = (mid - half - margin - base[k] - d) * invB;
+      float fhi = (mid + half + margin - base[k] - d) * invB;
+      if (!(flo <= fhi)) continue;
+      flo = fminf(fmaxf(flo, -1.f), (float)nb[k]);
+      fhi = fminf(fmaxf(fhi, -1.f), (float)nb[k]);
+      const int l0 = max(0, (int)floorf(flo)), l1 = min(nb[k] - 1, (int)ceilf(fhi));
+      for (int l = l0; l <= l1; l++) {
+        int idx[3];
+        idx[k] = l;
+        idx[i] = a;
+        idx[j] = bj;
+        const int b = idx[0] + g.nbx * (idx[1] + g.nby * idx[2]);
+        if (crosses(b)) hits[atomicAdd(&s_n, 1)] = b;
+      }
     }
-    const unsigned mask = __ballot_sync(0xffffffffu, hit);
-    int wbase = 0;
-    if (lane == 0 && mask) wbase = atomicAdd(&s_n, __popc(mask));
-    wbase = __shfl_sync(0xffffffffu, wbase, 0);
-    if (hit) hits[wbase + __popc(mask & ((1u << lane) - 1u))] = b;
+  } else {
+    for (int base = 0; base < g.nbricks; base += kPairThreads) {
+      const int b = base + tid;
+      const bool hit = b < g.nbricks && crosses(b);
+      const unsigned mask = __ballot_sync(0xffffffffu, hit);
+      int wbase = 0;
+      if (lane == 0 && mask) wbase = atomicAdd(&s_n, __popc(mask));
+      wbase = __shfl_sync(0xffffffffu, wbase, 0);
+      if (hit) hits[wbase + __popc(mask & ((1u << lane) - 1u))] = b;
+    }
   }
   __syncthreads();
   const int nh = s_n;
