@@ -78,8 +78,8 @@ GTOMRLN_API int gtomrln_release_caches(void);
 #define GTOMRLN_OP_PROJECT 0
 #define GTOMRLN_OP_BACKPROJECT 1
 /* op GTOMRLN_OP_GRIDDING: GTOMRLN_PATH_AUTO (default) runs the gridding
- * iterations as GTOMRLN_PATH_SYMMETRIC (below) on power-of-two grids
- * P = 64 .. 512 and with cuFFT's 3D transforms elsewhere;
+ * as GTOMRLN_PATH_SYMMETRIC (below) on the grids P = 64, 96, 128, 192, 256,
+ * 512 and 800 and with cuFFT's 3D transforms elsewhere;
  * GTOMRLN_PATH_DIRECT always uses cuFFT; GTOMRLN_PATH_FUSED runs each
  * iteration as two fused passes with the library's own transforms on
  * power-of-two grids P = 64 .. 512 (cuFFT elsewhere). */
@@ -95,8 +95,10 @@ GTOMRLN_API int gtomrln_release_caches(void);
  * fall back to FP32 for an item whose sums could overflow). */
 #define GTOMRLN_PATH_SEGMENT_FP32 5
 /* op GTOMRLN_OP_GRIDDING: each iteration as four streaming passes over the
- * Hermitian half along z of the (real) iterated spectrum, with the library's
- * own transforms, on power-of-two grids P = 64 .. 512 (cuFFT elsewhere). */
+ * Hermitian half along z of the (real) iterated spectrum, and the final map
+ * as three passes that write only the cropped output, all with the library's
+ * own transforms (no cuFFT plan), on the grids P = 64, 96, 128, 192, 256,
+ * 512 and 800 (cuFFT elsewhere). */
 #define GTOMRLN_PATH_SYMMETRIC 6
 GTOMRLN_API int gtomrln_set_path(int op, int path);
 
@@ -318,7 +320,9 @@ GTOMRLN_API int gtomrln_backproject_shifted_angles(float* d_volumeft, float* d_v
  *     double blobalpha = 15)
  * include/Reconstruction.cuh:16, src/Reconstruction/RecFourier.cu:98-241.
  * pre_planforw / pre_planback: 0 lets the library use its own cached plans
- * for the P^3 R2C / C2R transforms; otherwise they must be such plans. */
+ * for the P^3 R2C / C2R transforms; otherwise they must be such plans.  They
+ * are used only where the gridding runs on cuFFT (GTOMRLN_PATH_DIRECT, or a
+ * grid the library's own transforms do not take). */
 GTOMRLN_API int gtomrln_reconstruct_gridding(const float* d_dataft, const float* d_weight,
                                  float* d_reconstructed, int ox, int oy, int oz, int padx,
                                  int pady, int padz, int paddingfactor, int pre_planforw,
