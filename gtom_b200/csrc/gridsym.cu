@@ -258,7 +258,9 @@ __device__ __forceinline__ void four_step(float2* v, float2* xb, const float2* t
 // half-warp's access one 128-byte row).  Round j's N2-point DFTs return
 // X(k1 + N1 k2), k1 = N2 j + t, i.e. outputs t + N2 (j + J k2), written back
 // into the registers the round's inputs left and renamed at the end.
-template <int N, bool INV>
+// SYNC0: begin with a CTA barrier (a caller whose own last barrier already
+// follows its threads' earlier reads of xb passes false).
+template <int N, bool INV, bool SYNC0 = true>
 __device__ __forceinline__ void four_step_rounds(float2* v, float2* xb, const float2* tw, int t, int c) {
   constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2, J = N1 / N2;
   static_assert(J * N2 == N1, "four_step_rounds: N1 must be a multiple of N2");
@@ -267,7 +269,7 @@ __device__ __forceinline__ void four_step_rounds(float2* v, float2* xb, const fl
   for (int k1 = 1; k1 < N1; k1++) v[k1] = cmul(v[k1], twiddle<1, INV>(tw, t * k1));
 #pragma unroll
   for (int j = 0; j < J; j++) {
-    __syncthreads();  // the previous round's (or the caller's) reads of xb are done
+    if (j > 0 || SYNC0) __syncthreads();  // the previous round's (or the caller's) reads of xb are done
 #pragma unroll
     for (int k = 0; k < N2; k++) xb[(t * N2 + k) * kCols + c] = v[N2 * j + k];
     __syncthreads();
@@ -474,7 +476,10 @@ gridsym_y_tma_kernel(const __grid_constant__ CUtensorMap map, float2* __restrict
       __syncthreads();  // every thread has read next_s
       if (threadIdx.x == 0) take_next();
     }
-    four_step_rounds<P, INV>(v, xb, tw, t, c);  // begins with a CTA barrier: next_s is visible after it
+    // no leading barrier: both branches end with one after every thread's
+    // reads of xb for the previous unit; next_s is visible after the rounds'
+    // own barriers
+    four_step_rounds<P, INV, false>(v, xb, tw, t, c);
     if (in) {
 #pragma unroll
       for (int m = 0; m < N1; m++) col[(int64_t)(t + N2 * m) * RW] = v[m];
