@@ -16,8 +16,11 @@
 //   final  : decentre of the data, the weight product (or the division of
 //            the iterations == 0 branch) and the centring shift as a sign;
 //   crop   : centred crop, sinc^2 correction and the 1/(pad^3 ori) scale.
-// The P^3 R2C / C2R transforms are cuFFT library calls; plans are cached
-// per (device, P).
+// On the grids gridsym.cu takes (the default there) the iterations and the
+// final map (final, its inverse transform and crop) run on the library's own
+// transforms, with no P^3 real grid; elsewhere, and on GTOMRLN_PATH_DIRECT,
+// the P^3 R2C / C2R transforms are cuFFT library calls, plans cached per
+// (device, P).
 #include <cufft.h>
 #include <algorithm>
 #include <cmath>
