@@ -270,8 +270,9 @@ segment_pairs_kernel(const float* __restrict__ mats, BrickGrid g, float pmax, fl
                      PixelBin* __restrict__ bins, int64_t bins_cap, unsigned long long* __restrict__ counters,
                      int* __restrict__ brick_pairs, int* __restrict__ fallback, int* __restrict__ nfallback,
                      float2* __restrict__ zero_out, PixelSet zpx, SliceGeom gm) {
-  extern __shared__ int hits[];  // brick ids of this slice
+  extern __shared__ int hits[];  // brick ids of this slice, then a bitmap of the bricks
   __shared__ int s_n;
+  __shared__ int s_wsum[kPairThreads / 32];
   __shared__ long long s_base;
   const int slice = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
   float m0[9], m[9];
@@ -332,6 +333,12 @@ segment_pairs_kernel(const float* __restrict__ mats, BrickGrid g, float pmax, fl
   const float ank = k == 0 ? an0 : (k == 1 ? an1 : an2);
   const bool columns = ank > 1e-30f && isfinite(n0) && isfinite(n1) && isfinite(n2) && isfinite(R2);
   if (columns) {
+    // hits marked in a bitmap, then listed in brick order (pairs_fill_kernel's
+    // per-brick atomics from consecutive bins then fall on neighbouring words)
+    unsigned* bits = reinterpret_cast<unsigned*>(hits + g.nbricks);
+    const int nwords = (g.nbricks + 31) / 32;
+    for (int w = tid; w < nwords; w += kPairThreads) bits[w] = 0u;
+    __syncthreads();
     const int nb[3] = {g.nbx, g.nby, g.nbz};
     const float base[3] = {0.f, (float)g.ylo, (float)g.zlo};
     const float nv[3] = {n0, n1, n2};
@@ -363,9 +370,34 @@ segment_pairs_kernel(const float* __restrict__ mats, BrickGrid g, float pmax, fl
         idx[i] = a;
         idx[j] = bj;
         const int b = idx[0] + g.nbx * (idx[1] + g.nby * idx[2]);
-        if (crosses(b)) hits[atomicAdd(&s_n, 1)] = b;
+        if (crosses(b)) atomicOr(bits + (b >> 5), 1u << (b & 31));
       }
     }
+    __syncthreads();
+    // thread t lists the set bits of words [t W, (t+1) W) at its offset in a
+    // block-wide scan of the words' counts
+    const int W = (nwords + kPairThreads - 1) / kPairThreads;
+    const int w0 = min(tid * W, nwords), w1 = min(w0 + W, nwords);
+    int cnt = 0;
+    for (int w = w0; w < w1; w++) cnt += __popc(bits[w]);
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t2 = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t2;
+    }
+    if (lane == 31) s_wsum[tid >> 5] = incl;
+    __syncthreads();
+    int pos = incl - cnt;
+    for (int k2 = 0; k2 < (tid >> 5); k2++) pos += s_wsum[k2];
+    for (int w = w0; w < w1; w++) {
+      unsigned m = bits[w];
+      while (m) {
+        hits[pos++] = 32 * w + __ffs(m) - 1;
+        m &= m - 1u;
+      }
+    }
+    if (tid == kPairThreads - 1) s_n = pos;
   } else {
     for (int base = 0; base < g.nbricks; base += kPairThreads) {
       const int b = base + tid;
@@ -542,7 +574,8 @@ int build_brick_plan(int op, const float* d_mats, int batch, const BrickGrid& g,
   // pixel id of a slice: 66 KB at n = 256).
   const size_t code_bytes = ((size_t)px.elements * 2 + 3) & ~(size_t)3;
   const int use_codes = g.nbricks < 65535 && hist_bytes + code_bytes <= 200 * 1024 ? 1 : 0;
-  const size_t smem_bytes = segments ? sizeof(int) * (size_t)g.nbricks
+  // segment plan: the hit list and a bitmap of the bricks
+  const size_t smem_bytes = segments ? sizeof(int) * ((size_t)g.nbricks + ((size_t)g.nbricks + 31) / 32)
                                      : hist_bytes + (use_codes ? code_bytes : 0);
   const int* d_order = nullptr;
   int st = brick_order(g, &d_order);
