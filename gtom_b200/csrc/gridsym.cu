@@ -202,10 +202,16 @@ GTOMRLN_SPLIT(512, 32, 16)
 GTOMRLN_SPLIT(800, 40, 20)
 #undef GTOMRLN_SPLIT
 
-// Runtime twiddle e(-m/N) (or e(+m/N), INV) from the table e(-j/P), N = P/S.
-template <int S, bool INV>
+// Padded place of table entry i in the x passes' copy of the twiddle table
+// (one spare entry after every 16): their lanes read entries 2 t k1 for
+// t = 0 .. N2-1, strides that would put up to 16 lanes on one bank.
+__host__ __device__ constexpr int tw_pad(int i) { return i + (i >> 4); }
+
+// Runtime twiddle e(-m/N) (or e(+m/N), INV) from the table e(-j/P), N = P/S
+// (PAD: the padded copy).
+template <int S, bool INV, bool PAD = false>
 __device__ __forceinline__ float2 twiddle(const float2* tw, int m) {
-  float2 w = tw[m * S];
+  float2 w = tw[PAD ? tw_pad(m * S) : m * S];
   if (INV) w.y = -w.y;
   return w;
 }
@@ -235,7 +241,7 @@ __device__ __forceinline__ void four_step(float2* v, float2* xb, const float2* t
   static_assert(J * N2 == N1, "four_step: N1 must be a multiple of N2");
   dftr<N1, INV>(v);
 #pragma unroll
-  for (int k1 = 1; k1 < N1; k1++) v[k1] = cmul(v[k1], twiddle<S, INV>(tw, t * k1));
+  for (int k1 = 1; k1 < N1; k1++) v[k1] = cmul(v[k1], twiddle<S, INV, ROWS>(tw, t * k1));
   if (WSYNC) __syncwarp(); else __syncthreads();
 #pragma unroll
   for (int k1 = 0; k1 < N1; k1++) xb[xplace<N1, N2, ROWS>(k1, t, c)] = v[k1];
@@ -318,6 +324,10 @@ __device__ __forceinline__ float2 r2c_post(float2 zk, float2 zm, float2 w) {
 
 __device__ __forceinline__ void load_twiddles(float2* tw, const float2* __restrict__ twg, int P) {
   for (int m = threadIdx.x; m < P; m += blockDim.x) tw[m] = __ldg(twg + m);
+}
+// The padded copy (tw_pad) for the x passes: P + P/16 entries.
+__device__ __forceinline__ void load_twiddles_padded(float2* tw, const float2* __restrict__ twg, int P) {
+  for (int m = threadIdx.x; m < P; m += blockDim.x) tw[tw_pad(m)] = __ldg(twg + m);
 }
 
 // ------------------------------------------------------- TMA staging --
@@ -516,8 +526,8 @@ gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const f
   constexpr int XS = N2 * (N1 + 1);      // a row's block of the exchange buffer
   extern __shared__ float2 smem[];
   float2* tw = smem;
-  float2* xb = smem + P;
-  load_twiddles(tw, twg, P);
+  float2* xb = smem + P + P / 16;  // after the padded twiddle table
+  load_twiddles_padded(tw, twg, P);
   const int t = threadIdx.x % N2, r = threadIdx.x / N2;
   const unsigned lane = threadIdx.x & 31;
   const unsigned partner = WROW ? (lane & ~(unsigned)(N2 - 1)) | ((unsigned)(N2 - t) & (N2 - 1)) : lane;
@@ -543,7 +553,7 @@ gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const f
         const float2 sh = make_float2(__shfl_sync(0xffffffffu, v[N1 - 1 - m].x, partner),
                                       __shfl_sync(0xffffffffu, v[N1 - 1 - m].y, partner));
         const float2 xm = t != 0 ? sh : (m == 0 ? xH : v[(N1 - m) % N1]);
-        z[m] = c2r_pre<true>(v[m], xm, tw[t + N2 * m]);
+        z[m] = c2r_pre<true>(v[m], xm, tw[tw_pad(t + N2 * m)]);
       }
     } else {
 #pragma unroll
@@ -553,7 +563,7 @@ gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const f
 #pragma unroll
       for (int m = 0; m < N1; m++) {
         const int k = t + N2 * m;
-        z[m] = c2r_pre<true>(v[m], xb[r * XS + H - k], tw[k]);
+        z[m] = c2r_pre<true>(v[m], xb[r * XS + H - k], tw[tw_pad(k)]);
       }
     }
 #pragma unroll
@@ -618,7 +628,7 @@ gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const f
       const float2 sh = make_float2(__shfl_sync(0xffffffffu, v[N1 - 1 - m].x, partner),
                                     __shfl_sync(0xffffffffu, v[N1 - 1 - m].y, partner));
       const float2 zm = t != 0 ? sh : v[(N1 - m) % N1];
-      y[m] = r2c_post<false>(v[m], zm, tw[t + N2 * m]);
+      y[m] = r2c_post<false>(v[m], zm, tw[tw_pad(t + N2 * m)]);
     }
   } else {
     __syncthreads();  // the exchange buffer is free
@@ -628,7 +638,7 @@ gridsym_x_kernel(float2* __restrict__ W, const float2* __restrict__ twg, const f
 #pragma unroll
     for (int m = 0; m < N1; m++) {
       const int k = t + N2 * m;
-      y[m] = r2c_post<false>(v[m], xb[r * XS + (k == 0 ? 0 : H - k)], tw[k]);
+      y[m] = r2c_post<false>(v[m], xb[r * XS + (k == 0 ? 0 : H - k)], tw[tw_pad(k)]);
     }
   }
 #pragma unroll
@@ -918,8 +928,8 @@ gridsym_final_x_kernel(const float2* __restrict__ T, FinalArgs f, const float2* 
   constexpr int XS = N2 * (N1 + 1);
   extern __shared__ float2 smem[];
   float2* tw = smem;
-  float2* xb = smem + P;
-  load_twiddles(tw, twg, P);
+  float2* xb = smem + P + P / 16;  // after the padded twiddle table
+  load_twiddles_padded(tw, twg, P);
   const int t = threadIdx.x % N2, r = threadIdx.x / N2;
   const unsigned lane = threadIdx.x & 31;
   const unsigned partner = WROW ? (lane & ~(unsigned)(N2 - 1)) | ((unsigned)(N2 - t) & (N2 - 1)) : lane;
@@ -943,7 +953,7 @@ gridsym_final_x_kernel(const float2* __restrict__ T, FinalArgs f, const float2* 
         const float2 sh = make_float2(__shfl_sync(0xffffffffu, v[N1 - 1 - m].x, partner),
                                       __shfl_sync(0xffffffffu, v[N1 - 1 - m].y, partner));
         const float2 xm = t != 0 ? sh : (m == 0 ? xH : v[(N1 - m) % N1]);
-        z[m] = c2r_pre<true>(v[m], xm, tw[t + N2 * m]);
+        z[m] = c2r_pre<true>(v[m], xm, tw[tw_pad(t + N2 * m)]);
       }
     } else {
 #pragma unroll
@@ -953,7 +963,7 @@ gridsym_final_x_kernel(const float2* __restrict__ T, FinalArgs f, const float2* 
 #pragma unroll
       for (int m = 0; m < N1; m++) {
         const int k = t + N2 * m;
-        z[m] = c2r_pre<true>(v[m], xb[r * XS + H - k], tw[k]);
+        z[m] = c2r_pre<true>(v[m], xb[r * XS + H - k], tw[tw_pad(k)]);
       }
     }
 #pragma unroll
@@ -987,7 +997,8 @@ struct SymSizes {
   static constexpr int z_tiles = P * (H / kCols) + P / kCols;
   // twiddle table + exchange buffer
   static constexpr size_t y_smem = sizeof(float2) * (P + (size_t)P * kPitch);
-  static constexpr size_t x_smem = sizeof(float2) * (P + (size_t)kCols * Split<H>::N2 * (Split<H>::N1 + 1));
+  static constexpr size_t x_smem =
+      sizeof(float2) * (P + P / 16 + (size_t)kCols * Split<H>::N2 * (Split<H>::N1 + 1));  // padded twiddles
   static constexpr size_t z_smem = sizeof(float2) * (P + (size_t)(H + 1) * kPitch);
 };
 
