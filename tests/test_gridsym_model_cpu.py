@@ -1,6 +1,8 @@
 """CPU model of the symmetric-spectrum gridding iteration (gtom_b200/csrc/
 gridsym.cu), written with the kernels' own index logic, against numpy's full
-C2R -> blob -> R2C of the cuFFT path (RecFourier.cu:158-171).
+C2R -> blob -> R2C of the cuFFT path (RecFourier.cu:158-171), and of its
+final map (three passes keeping only the crop) against irfftn and the crop
+(RecFourier.cu:175-216, Padding.cu:22-42).
 
 It pins what the GPU kernels rely on: that a real half spectrum's transforms
 stay Hermitian in z, so the planes z <= P/2 carry the whole iteration; the
@@ -122,4 +124,33 @@ def test_symmetric_iteration_model_equals_full_transforms(P):
     # z pass: Hermitian-to-real along z with exp(-)
     cols = W.transpose(1, 2, 0).reshape(-1, H + 1)      # (y, x) x z
     got = c2r_rows(cols, plus=False).reshape(P, H + 1, P).transpose(2, 0, 1)
+    assert np.abs(got - want).max() <= 1e-9 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("P,ori", [(32, 16), (64, 32), (64, 20), (96, 48), (96, 30)])
+def test_final_map_model_equals_irfftn_crop(P, ori):
+    """The final map's three passes (gridsym_final_{z,y,x}_kernel) with the
+    kernels' transforms: the inverse transform along z keeping only the
+    crop's planes, along y keeping only its rows, then the C2R along x with
+    the x = 0 and x = P/2 terms taken as real, keeping the crop's x; equal to
+    numpy's irfftn (unnormalised) cropped to the central ori^3 — on a
+    spectrum that is not Hermitian anywhere, which irfftn's last-axis C2R
+    treats the same way."""
+    rng = np.random.default_rng(P + ori)
+    H = P // 2
+    S = rng.standard_normal((P, P, H + 1)) + 1j * rng.standard_normal((P, P, H + 1))  # [kz][ky][kx]
+    off = P // 2 - ori // 2
+    want = np.fft.irfftn(S, s=(P, P, P), axes=(0, 1, 2)) * P ** 3
+    want = want[off:off + ori, off:off + ori, off:off + ori]
+    # z pass: every (y, x) column along z, the crop's planes kept -> T[zc][y][x]
+    cols = S.transpose(1, 2, 0).reshape(-1, P)
+    T = four_step(cols, inverse=True).reshape(P, H + 1, P).transpose(2, 0, 1)[off:off + ori]
+    # y pass: every (zc, x) column along y, the crop's rows kept -> T[zc][yc][x]
+    cols = T.transpose(0, 2, 1).reshape(-1, P)
+    T = four_step(cols, inverse=True).reshape(ori, H + 1, P).transpose(0, 2, 1)[:, off:off + ori]
+    # x pass: C2R of each kept row, the crop's x
+    rows = T.reshape(-1, H + 1).copy()
+    rows[:, 0] = rows[:, 0].real
+    rows[:, H] = rows[:, H].real
+    got = c2r_rows(rows, plus=True).reshape(ori, ori, P)[:, :, off:off + ori]
     assert np.abs(got - want).max() <= 1e-9 * np.abs(want).max()
