@@ -19,8 +19,8 @@
 // are zero up to rounding; the kept real parts are the same sums.
 //
 // Per iteration (W: the (P/2+1) x P x (P/2+1) complex work array, layout
-// [z][y][x] with rows of P/2 + 2, the last element padding, so that rows
-// start on 16-byte boundaries as tensor copies need):
+// [z][y][x] with rows of P/2 + 4, the last three elements padding, so that
+// rows start on 32-byte boundaries):
 //   gridsym_y_tma_kernel<INV>  inverse transform along y of W (columns of 16
 //                          consecutive x at one z, staged in shared memory
 //                          by tensor copies, or of x = P/2 at 16 z);
@@ -388,10 +388,11 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
 }
 
 // ------------------------------------------------------------ y pass --
-// W's rows hold P/2 + 2 complex elements (the last one padding), so that
-// every row starts on a 16-byte boundary, as tensor copies need.
+// W's rows hold P/2 + 4 complex elements (the last three padding), so that
+// every row starts on a 32-byte boundary: tensor copies need 16, and a
+// warp's run of 16 columns then covers whole sectors.
 template <int P>
-constexpr int w_pitch() { return P / 2 + 2; }
+constexpr int w_pitch() { return P / 2 + 4; }
 
 // Sizes of the staged y pass: a tile (16 columns x P rows) arrives as NB
 // tensor boxes of BOX rows (a box has at most 256 rows).
