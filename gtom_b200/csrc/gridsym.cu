@@ -411,7 +411,7 @@ struct YStage {
 // The y pass, persistent, over nyq + tiles work units: first the columns
 // x = P/2 (16 consecutive z of one volume per unit, plain loads), then the
 // tiles of 16 consecutive x < P/2 at one (volume, z), each of which arrives
-// in shared memory by tensor copies (map: W as floats, dims {2 (P/2+2), P,
+// in shared memory by tensor copies (map: W as floats, dims {2 w_pitch, P,
 // (P/2+1) volumes}, box {32, BOX, 1}).  CTA i starts with unit i and takes
 // the next from a counter as soon as it holds its current unit in
 // registers, starting the next tile's copy then, so the copy runs during the
@@ -1037,9 +1037,9 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
 std::once_flag g_encode_once;
 EncodeTiledFn g_encode = nullptr;
 
-// The tensor map of W for the staged y pass: floats, dims {2 (P/2+2), P,
+// The tensor map of W for the staged y pass: floats, dims {2 w_pitch, P,
 // (P/2+1) count} (the z planes of all volumes in one dimension), row stride
-// (P/2+2) 8 bytes (a multiple of 16), box {32, BOX, 1}.
+// w_pitch 8 bytes (a multiple of 32), box {32, BOX, 1}.
 template <int P>
 int w_tensor_map(float2* W, int count, CUtensorMap* map) {
   std::call_once(g_encode_once, [] {
